@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark: ICD voxel-updates/s of the finest multi-resolution stage.
+
+Workload (the 3-D single-GPU configuration): a seeded random-ellipsoid phantom
+(10 ellipsoids, attenuation 0-0.02), volume 256 x 256 x 8, 256 views uniform
+over 180 degrees, 256 detector columns x 8 rows, Poisson counts at I0 = 1e4
+(weights = counts), qGGMRF p = 1.2, q = 2, c_s = 1 (T = 1), sigma_s = 0.002
+(a tenth of the phantom's range), quadratic data term (quad_convex = 1), no
+ring correction.  The stage starts warm, from the 2x-coarser phantom
+up-sampled, as the multi-resolution driver hands it over.  A step is one outer
+ICD iteration (updateVoxelsTimeSlices: HICD sweep, NHICD sweeps from the
+second iteration, zero skipping).  The metric counts executed voxel updates.
+
+Arms:
+  (default)          the GPU engine (libtimbir_b200.so) through its C ABI
+  --impl reference   the reference's own CPU implementation, built from its
+                     sources (oracle/_ref/XT_Main_ref), in restart mode at the
+                     same stage, all host threads; else the CPU restatement.
+
+Under torchrun (N > 1 GPUs) every rank reconstructs its own copy of the
+workload (independent problems, weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from timbir_b200 import synth  # noqa: E402
+
+CFG = dict(n_xy=256, rows=8, views=256, I0=1e4, seed=0)
+PRIOR = dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=0, quad_convex=1,
+             huber_delta=0.5, huber_T=4.0)
+WORKLOAD = "3d-shepp-logan-like 256x256x8, 256 views, I0=1e4, finest stage"
+METRIC = "ICD voxel-updates/s"
+
+
+def make_scan(seed_offset=0):
+    return synth.ellipsoid_scan(CFG["n_xy"], CFG["rows"], CFG["views"], I0=CFG["I0"], seed=CFG["seed"] + seed_offset)
+
+
+def coarse_start(scan):
+    """The 2x-coarser phantom (mean over 2x2x2 cells) and its trilinear x2
+    up-sampling onto the stage grid: the warm start both arms use."""
+    ph = scan.phantom[0]
+    z, y, x = ph.shape
+    coarse = ph.reshape(z // 2, 2, y // 2, 2, x // 2, 2).mean(axis=(1, 3, 5)).astype(np.float32)
+
+    def up(a, axis):
+        n = a.shape[axis]
+        a = np.moveaxis(a, axis, 0)
+        out = np.empty((2 * n,) + a.shape[1:], np.float64)
+        out[0], out[-1] = a[0], a[-1]
+        out[1] = (3.0 * a[0] + a[1]) / 4.0
+        out[-2] = (a[-2] + 3.0 * a[-1]) / 4.0
+        out[2:2 * n - 2:2] = (a[0:n - 2] + 3.0 * a[1:n - 1]) / 4.0
+        out[3:2 * n - 2:2] = (3.0 * a[1:n - 1] + a[2:n]) / 4.0
+        return np.moveaxis(out, 0, axis)
+
+    fine = up(up(up(coarse.astype(np.float64), 2), 1), 0).astype(np.float32)
+    return coarse, fine[None]
+
+
+def mean_amatrix_count(stage, scan):
+    """Mean number of detector bins per (voxel line, view) of the A matrix over
+    the in-mask lines (the c-bar of the algorithmic byte count), from the
+    same index arithmetic as the kernels, in float64 numpy."""
+    hr = stage.hr().astype(np.float64)
+    n, dr = scan.proj_cols, scan.vox_wid
+    R0 = -scan.rot_center * dr
+    off_r = (dr / np.sqrt(2.0) + dr / 2.0) / 64
+    k = np.arange(n)
+    x = R0 + (k + 0.5) * dr
+    y = -n * dr / 2.0 + (k + 0.5) * dr
+    X, Y = np.meshgrid(x, y)
+    m = stage.mask().astype(bool)
+    X, Y = X[m], Y[m]
+    total = 0
+    for v in range(0, scan.proj_num, 4):
+        c, s = np.cos(np.float64(scan.proj_angles[v])), np.sin(np.float64(scan.proj_angles[v]))
+        r = X * c - Y * s
+        imin = np.maximum(np.floor((r - dr - R0) / dr), 0).astype(int)
+        imax = np.minimum(np.floor((r + dr - R0) / dr), n - 1).astype(int)
+        for d in range(0, 4):
+            j = imin + d
+            ok = j <= imax
+            rc = R0 + (j + 0.5) * dr
+            dd = np.abs(r - rc)
+            idx = np.floor(dd / off_r).astype(int)
+            ok &= (idx >= 0) & (idx < 64)
+            idc = np.clip(idx, 0, 63)
+            w1 = dd - idc * off_r
+            f = (off_r - w1) * hr[v, idc] + w1 * hr[v, idc + 1]
+            total += int(np.count_nonzero(ok & (f > 0)))
+    return total / (len(X) * len(range(0, scan.proj_num, 4)))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(self.rows[0][2]) if self.rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons}
+
+
+# --------------------------------------------------------------------- CPU --
+def run_reference_binary(scan, coarse, iters, threads):
+    """Reference driver in restart mode at the finest stage: the files a
+    finished coarser stage leaves behind are written, then XT_Main_ref runs
+    `iters` ICD iterations (ORACLE_MAX_ITERS).  Returns [(seconds, updates)]."""
+    from oracle.bind import REF_BIN
+    wd = tempfile.mkdtemp(prefix="timbir_ref_")
+    scan.write_bin(wd)
+    p = np.transpose(scan.projections, (0, 2, 1)).astype(np.float32)  # [view][col][row]
+    w = np.transpose(scan.weights, (0, 2, 1)).astype(np.float32)
+    p.tofile(os.path.join(wd, "projs_runtime.bin"))
+    w.tofile(os.path.join(wd, "weights_runtime.bin"))
+    np.array([1.0], np.float64).tofile(os.path.join(wd, "variance_estimate.bin"))
+    np.zeros((scan.proj_cols, scan.proj_rows), np.float32).tofile(os.path.join(wd, "proj_offset.bin"))
+    coarse.astype(np.float32).tofile(os.path.join(wd, "object_time_0.bin"))
+    np.zeros(scan.proj_rows * scan.proj_cols * scan.proj_cols, np.float32).tofile(os.path.join(wd, "mag_update.bin"))
+    n_stages = 3  # 256 columns: voxel scales 4, 2, 1 (XT_Engine.c:111-141)
+    np.array([n_stages - 1], np.int32).tofile(os.path.join(wd, "status.bin"))
+    a = PRIOR
+    cmd = [REF_BIN, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
+           str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
+           str(scan.rot_center), "--sig_s", str(a["sig_s"]), "--sig_t", str(a["sig_t"]), "--c_s", str(a["c_s"]),
+           "--c_t", str(a["c_t"]), "--convg_thresh", str(a["convg_thresh"]), "--remove_rings", "0",
+           "--quad_convex", "--restart"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), ORACLE_MAX_ITERS=str(iters))
+    r = subprocess.run(cmd, cwd=wd, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
+                       timeout=1800)
+    shutil.rmtree(wd, ignore_errors=True)
+    out = []
+    for line in r.stderr.splitlines():
+        if line.startswith("ORACLE_ITER"):
+            _, n, dt, upd = line.split()
+            out.append((float(dt), int(upd)))
+    if not out:
+        raise RuntimeError("reference run produced no iterations: " + r.stderr[-500:])
+    return out
+
+
+def run_port(scan, coarse_fine, iters):
+    """CPU restatement (single thread), when the reference build is absent."""
+    from oracle.bind import Oracle
+    o = Oracle(scan, **{k: v for k, v in PRIOR.items()}, blocks=CFG["rows"])
+    o.prepare(coarse_fine)
+    out = []
+    last = 0
+    for it in range(1, iters + 1):
+        t0 = time.perf_counter()
+        o.iterate(it)
+        dt = time.perf_counter() - t0
+        out.append((dt, o.update_count() - last))
+        last = o.update_count()
+    o.close()
+    return out
+
+
+def cpu_measure(scan, coarse, fine, warm, steps, threads):
+    from oracle.bind import Reference
+    if Reference.available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "XT_Main_ref")):
+        its = run_reference_binary(scan, coarse, warm + steps, threads)
+        kind, cores = "reference", threads
+    else:
+        its = run_port(scan, fine, warm + steps)
+        kind, cores = "port", 1
+    timed = its[warm:] if len(its) > warm else its
+    secs = sum(t for t, _ in timed)
+    upd = sum(u for _, u in timed)
+    return upd / secs, kind, cores, len(timed), secs
+
+
+# --------------------------------------------------------------------- GPU --
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import timbir_b200
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    scan = make_scan(rank)
+    coarse, fine = coarse_start(scan)
+    st = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+    st.prepare(fine)
+    for it in range(1, args.warmup + 1):
+        st.iterate(it)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
+    ms0, n_icd0, n_all0 = st.kernel_stats()
+    upd0 = st.update_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = []
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            st.time_begin()
+            st.iterate(args.warmup + 1 + k)
+            step_ms.append(st.time_end())
+    torch.cuda.synchronize()
+    ms1, n_icd1, n_all1 = st.kernel_stats()
+    updates = st.update_count() - upd0
+    total_ms = sum(step_ms)
+    icd_ms = ms1 - ms0
+    if dist:
+        t = torch.tensor([total_ms, float(updates)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        total_ms_max, updates_all = float(mx[0]), float(t[1])
+    else:
+        total_ms_max, updates_all = total_ms, float(updates)
+    cbar = mean_amatrix_count(st, scan) if rank == 0 else 0.0
+    st.close()
+
+    # end to end through the C ABI with host buffers: set-up from host arrays
+    # (H2D), prologue, one ICD iteration, object back to the host (D2H)
+    e2e_ms, e2e_upd = [], 0
+    h2d = sum(a.nbytes for a in (scan.projections, scan.weights, scan.proj_angles, scan.proj_times,
+                                 scan.recon_times, fine))
+    d2h = fine.nbytes
+    for k in range(max(1, min(args.steps, 3))):
+        flush.fill_(0.0)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        s2 = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+        s2.prepare(fine)
+        s2.iterate(1)
+        _ = s2.object()
+        t1.record()
+        torch.cuda.synchronize()
+        e2e_ms.append(t0.elapsed_time(t1))
+        e2e_upd += s2.update_count()
+        s2.close()
+    if dist:
+        t = torch.tensor([sum(e2e_ms), float(e2e_upd)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        e2e_value = float(t[1]) / (float(mx[0]) / 1e3)
+        dist.barrier()
+        dist.destroy_process_group()
+    else:
+        e2e_value = e2e_upd / (sum(e2e_ms) / 1e3)
+    if rank != 0:
+        return
+    value = updates_all / (total_ms_max / 1e3)
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    npf = scan.proj_num
+    b_vu = npf * (cbar * 1 * 12 + 2 * cbar + 2) + 29 * 4 + 4
+    achieved = (updates * b_vu) / (icd_ms / 1e3) / 1e9 if icd_ms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 theta, prior and update)",
+        "data": "synthetic (seeded random-ellipsoid phantom, Poisson counts)",
+        "config": {"workload": WORKLOAD, "volume": [CFG["rows"], CFG["n_xy"], CFG["n_xy"]],
+                   "views": CFG["views"], "schedule": "reference (checkerboard z-blocks)",
+                   "z_blocks": CFG["rows"], "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "bytes_per_update": b_vu, "mean_bins_per_view": cbar,
+                     "kernel": "k_icd_ref", "kernel_ms": icd_ms,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "gpu_launches": int(n_all1 - n_all0),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu:
+        v, kind, cores, n, secs = cpu_measure(scan, coarse, fine, 1, 1, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
+                                "sample": f"{n} ICD iteration(s) of the same stage after 1 warm-up, {secs:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    scan = make_scan(0)
+    coarse, fine = coarse_start(scan)
+    threads = os.cpu_count() or 1
+    v, kind, cores, n, secs = cpu_measure(scan, coarse, fine, args.warmup, args.steps, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "voxel-updates/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(n, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 scalars)",
+            "data": "synthetic (seeded random-ellipsoid phantom, Poisson counts)",
+            "config": {"workload": WORKLOAD, "volume": [CFG["rows"], CFG["n_xy"], CFG["n_xy"]],
+                       "views": CFG["views"], "threads": threads},
+            "cpu_baseline": {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
+                             "sample": f"{n} ICD iterations after {args.warmup} warm-up, {secs:.1f} s"},
+            "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+    else:
+        gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

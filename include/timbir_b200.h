@@ -1,0 +1,124 @@
+/*
+ * timbir_b200 -- C ABI of the B200 (sm_100a) MBIR ICD/NHICD engine.
+ *
+ * Two levels:
+ *
+ *  1. The drop-in library call, declared in mbir4d.h beside this file:
+ *     reconstruct(), with the signature, argument meaning, file outputs and
+ *     ownership rules of the reference's (TIMBIR v0.0.2
+ *     src/include/mbir4d.h:35, src/MBIR_4D/XT_Engine.c:81).
+ *
+ *  2. Stage-level entry points that reconstruct() is built from.  Each one
+ *     replaces the reference function named beside it, operates on one
+ *     resolution stage held in device memory, and returns 0 on success or -1
+ *     with a message available from mbir_last_error().  Plain pointers and
+ *     sizes only; host arrays use the reference's layouts:
+ *       projections / weights  float [proj_num][proj_rows][proj_cols]
+ *       sinogram-shaped output float [proj_num][proj_cols][proj_rows]
+ *                              (the reference's internal [N_p][N_r][N_t])
+ *       object                 float [recon_num][N_z][N_y][N_x]
+ *       ring offsets           float [proj_cols][proj_rows]
+ *       magnitude map          float [recon_num][num_z_blocks][N_y][N_x]
+ */
+#ifndef TIMBIR_B200_H_
+#define TIMBIR_B200_H_
+
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct MbirStage MbirStage;
+
+/* initStatStructures + initDynStructures for one stage whose voxels are
+ * mult_xy detector columns wide and mult_z detector rows high
+ * (src/MBIR_4D/XT_Init.c:449-669 and 211-445).  The object starts at zero,
+ * the ring offsets at zero, the variance estimate at 1.  num_z_blocks plays
+ * the role the OpenMP thread count plays in the reference
+ * (XT_Init.c:389-398): the number of z-blocks of the checkerboard schedule;
+ * it must be even, >= 2 and <= N_z. */
+int mbir_init_stage(MbirStage **out, const float *projections, const float *weights,
+                    const float *proj_angles, const float *proj_times, const float *recon_times,
+                    int32_t proj_rows, int32_t proj_cols, int32_t proj_num, int32_t recon_num,
+                    float vox_wid, float rot_center, float sig_s, float sig_t, float c_s, float c_t,
+                    float convg_thresh, int32_t remove_rings, int32_t quad_convex, float huber_delta,
+                    float huber_T, int32_t mult_xy, int32_t mult_z, int32_t num_z_blocks);
+
+/* freeDynMemory + freeStatMemory (XT_Init.c:672-707). */
+void mbir_free_stage(MbirStage *stage);
+
+/* Message of the last failing call on this thread. */
+const char *mbir_last_error(void);
+
+/* Stage switches set by initDynStructures from the stage index
+ * (updateProjOffset, updateVar; XT_Init.c:236-266) and the variance estimate
+ * read from the previous stage (XT_Init.c:290-291, 327-330). */
+int mbir_set_stage_switches(MbirStage *stage, int32_t update_proj_offset, int32_t update_var,
+                            double var_est);
+
+/* State of the voxel-line order generator (randlib.c srandom2/random2); one
+ * stream runs through a whole reconstruct() call. */
+int mbir_set_rng_state(MbirStage *stage, uint32_t state);
+uint32_t mbir_get_rng_state(MbirStage *stage);
+
+/* Stage prologue of ICD_BackProject (XT_ICD_update.c:1134-1159): mask,
+ * detector response (DetectorResponseProfile, XT_Profile.c:129), initial
+ * object / offsets / magnitude map (any may be NULL for zero), and the error
+ * sinogram e = y - A x - d (initErrorSinogam, XT_ICD_update.c:655). */
+int mbir_icd_prepare(MbirStage *stage, const float *object, const float *offset,
+                     const float *magmap);
+
+/* One outer ICD iteration with the reference schedule
+ * (updateVoxelsTimeSlices, XT_ICD_update.c:936-1105): random line order,
+ * 10 sub-iterations of checkerboard HICD half-sweeps with ring-offset updates,
+ * NHICD selection and (iter > 1) NHICD half-sweeps, variance update, and the
+ * convergence test; *converged is set to its result. */
+int mbir_update_voxels_time_slices(MbirStage *stage, int32_t iter, int32_t *converged);
+
+/* computeCost (XT_ICD_update.c:186-319), FP64 on the GPU. */
+int mbir_compute_cost(MbirStage *stage, double *total, double *forward, double *prior);
+
+/* update_Sinogram_Offset (XT_ICD_update.c:919-927), by remove_rings. */
+int mbir_update_sinogram_offset(MbirStage *stage);
+
+/* update_variance_parameter (XT_ICD_update.c:720-751). */
+int mbir_update_variance_parameter(MbirStage *stage);
+
+/* State read-back.  dims: N_p, N_r, N_t, N_x, N_y, N_z, N_time,
+ * num_z_blocks, z_overlap_num. */
+int mbir_stage_dims(MbirStage *stage, int32_t *dims);
+int mbir_get_object(MbirStage *stage, float *out);
+int mbir_set_object(MbirStage *stage, const float *in);
+int mbir_get_errorsino(MbirStage *stage, float *out);
+int mbir_get_weight(MbirStage *stage, float *out);
+int mbir_get_offset(MbirStage *stage, float *out);
+int mbir_get_magmap(MbirStage *stage, float *out);
+int mbir_get_hr(MbirStage *stage, float *out);
+int mbir_get_mask(MbirStage *stage, uint8_t *out);
+/* kind 0: HICD random order of (frame, block); kind 1: NHICD selection.
+ * Returns the number of lines (or -1). */
+int mbir_get_lines(MbirStage *stage, int32_t kind, int32_t frame, int32_t block, int32_t *xs,
+                   int32_t *ys);
+double mbir_get_var_est(MbirStage *stage);
+double mbir_get_update_percentage(MbirStage *stage);
+long long mbir_get_update_count(MbirStage *stage);
+/* Device time of the ICD update kernels, measured with CUDA events on the
+ * stage's stream, and the number of kernels the stage has launched (no
+ * reference counterpart: instrumentation). */
+int mbir_get_kernel_stats(MbirStage *stage, double *icd_ms, long long *icd_launches, long long *launches);
+/* Device clock around a span of stage calls: CUDA events recorded on the
+ * stage's stream at begin and end (instrumentation; no reference counterpart). */
+int mbir_time_begin(MbirStage *stage);
+int mbir_time_end(MbirStage *stage, double *ms);
+
+/* A x of an object into a sinogram [proj_num][proj_rows][proj_cols], with the
+ * forward projector of initErrorSinogam (XT_ForwardProject.c:8-25).  Meant
+ * for a fresh stage: it overwrites the stage's object and error sinogram. */
+int mbir_forward_project(MbirStage *stage, const float *object, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,99 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Needs the reference library built from its own sources (``make -C oracle ref``,
+which needs the TIMBIR tree).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Outputs (committed):
+  park_miller_seed1.json   the known-answer table of the reference's generator,
+                           read from the comment block of src/MBIR_4D/randlib.c
+  stage_<name>.npz         per scenario of tests/scenarios.py: detector response,
+                           mask, initial error sinogram and cost, and the state
+                           after ICD iterations 1 and 3 of the reference schedule
+  recon_small.npz          a full reconstruct() run of the reference driver
+                           binary (object, cost trace) on a seeded 32x32x4 scan
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from oracle.bind import REF_BIN, Reference  # noqa: E402
+from timbir_b200 import synth  # noqa: E402
+
+import scenarios  # noqa: E402
+
+REF_SRC = "/root/reference/src"
+
+
+def park_miller_table():
+    text = open(os.path.join(REF_SRC, "MBIR_4D", "randlib.c")).read()
+    block = text[text.index("TABLE:"):]
+    nums = [int(v) for v in re.findall(r"^\s*(\d+)\s*$", block, flags=re.M)[:20]]
+    assert len(nums) == 20
+    with open(os.path.join(HERE, "park_miller_seed1.json"), "w") as f:
+        json.dump({"seed": 1, "values": nums, "source": "src/MBIR_4D/randlib.c:69-90"}, f, indent=1)
+
+
+def stage_fixtures():
+    for name in scenarios.SCENARIOS:
+        wd = tempfile.mkdtemp()
+        R = scenarios.make(name, Reference, workdir=wd)
+        R.prepare()
+        out = dict(hr=R.hr(), mask=R.mask()[0], e0=R.errorsino(), cost0=np.float64(R.cost()[0]))
+        for it in (1, 2, 3):
+            conv = R.iterate(it)
+            if it in (1, 3):
+                out[f"obj{it}"] = R.object()
+                out[f"conv{it}"] = np.int32(conv)
+                out[f"var{it}"] = np.float64(R.var_est())
+        out["e3"] = R.errorsino()
+        out["offset3"] = R.offset()
+        out["cost3"] = np.float64(R.cost()[0])
+        xs, ys = R.lines(0, 0, 0)
+        out["hicd_x3"], out["hicd_y3"] = xs, ys
+        xs, ys = R.lines(1, 0, 0)
+        out["nhicd_x3"], out["nhicd_y3"] = xs, ys
+        np.savez_compressed(os.path.join(HERE, f"stage_{name}.npz"), **out)
+        print(name, {k: getattr(v, "shape", v) for k, v in out.items() if k.startswith("obj")})
+
+
+RECON_ARGS = dict(sig_s=0.002, sig_t=1.0, c_s=1e-3, c_t=1e-3, convg_thresh=0.05, remove_rings=0,
+                  quad_convex=1, huber_delta=0.5, huber_T=4.0)
+
+
+def recon_fixture():
+    scan = synth.ellipsoid_scan(32, 4, 48, seed=11)
+    wd = tempfile.mkdtemp()
+    scan.write_bin(wd)
+    a = RECON_ARGS
+    cmd = [REF_BIN, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
+           str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
+           str(scan.rot_center), "--sig_s", str(a["sig_s"]), "--sig_t", str(a["sig_t"]), "--c_s", str(a["c_s"]),
+           "--c_t", str(a["c_t"]), "--convg_thresh", str(a["convg_thresh"]), "--remove_rings", "0", "--quad_convex"]
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    subprocess.run(cmd, cwd=wd, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    obj = np.fromfile(os.path.join(wd, "object_time_0.bin"), np.float32).reshape(4, 32, 32)
+    cost = np.fromfile(os.path.join(wd, "cost.bin"), np.float64)
+    np.savez_compressed(os.path.join(HERE, "recon_small.npz"), object=obj, cost=cost, threads=np.int32(4))
+    print("recon", obj.shape, cost[-3:])
+
+
+if __name__ == "__main__":
+    if not Reference.available():
+        sys.exit("build the reference first: make -C oracle ref")
+    park_miller_table()
+    stage_fixtures()
+    recon_fixture()

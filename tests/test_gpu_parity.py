@@ -1,0 +1,117 @@
+"""GPU parity of the reference-schedule path against the oracle and the
+reference's golden fixtures.
+
+Tolerances.  Integer work is compared exactly: A-matrix bins enter through
+the detector response table and the mask (bit-exact) and through the line
+orders (exact).  Floating-point state is compared with tolerances stated per
+assertion: the GPU forms theta1/theta2 and the prior sums by tree reductions
+and the forward projection in FP64 before one float rounding, where the
+reference adds sequentially in the same precisions, so voxel values may
+differ in the last float bits after an update.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import scenarios
+import timbir_b200
+from oracle.bind import Oracle
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+SCALE = 0.02  # phantom dynamic range
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("name", list(scenarios.SCENARIOS))
+def test_stage_prologue_matches_reference(name):
+    g = np.load(os.path.join(GOLD, f"stage_{name}.npz"))
+    s = scenarios.make(name, timbir_b200.Stage)
+    s.prepare()
+    np.testing.assert_array_equal(s.hr(), g["hr"])           # detector response: bit-exact
+    np.testing.assert_array_equal(s.mask(), g["mask"])       # voxel-line set: exact
+    assert rel(s.errorsino(), g["e0"]) < 2e-6                 # y - Ax - d, float rounding of Ax
+    assert s.cost()[0] == pytest.approx(float(g["cost0"]), rel=1e-6)
+
+
+@pytest.mark.parametrize("name", list(scenarios.SCENARIOS))
+def test_first_iteration_matches_oracle(name):
+    s = scenarios.make(name, timbir_b200.Stage)
+    o = scenarios.make(name, Oracle)
+    s.prepare()
+    o.prepare()
+    assert s.iterate(1) == o.iterate(1)
+    for f in range(s.N_time):
+        for b in range(s.nblk):
+            for kind in (0, 1):
+                xs, ys = s.lines(kind, f, b)
+                oxs, oys = o.lines(kind, f, b)
+                np.testing.assert_array_equal(xs, oxs)
+                np.testing.assert_array_equal(ys, oys)
+    # voxel values: within 1e-5 of the phantom range after a full iteration
+    assert np.abs(s.object() - o.object()).max() < 1e-5 * SCALE
+    assert rel(s.errorsino(), o.errorsino()) < 1e-5
+    assert rel(s.offset(), o.offset()) < 1e-4 if np.abs(o.offset()).max() > 0 else True
+    assert s.var_est() == pytest.approx(o.var_est(), rel=1e-6)
+    assert s.update_count() == o.update_count()
+
+
+def _load_state(stage, oracle, seed):
+    """Give both the same object (so the same error sinogram) after prepare."""
+    rng = np.random.default_rng(seed)
+    x = (0.01 + 0.005 * rng.standard_normal((stage.N_time, stage.N_z, stage.N_y, stage.N_x))).astype(np.float32)
+    off = (0.01 * rng.standard_normal((stage.N_r, stage.N_t))).astype(np.float32)
+    stage.prepare(x, off)
+    oracle.prepare(x, off)
+
+
+@pytest.mark.parametrize("name", ["rings1", "rings2", "rings3", "zinger_var"])
+def test_offset_update_matches_oracle(name):
+    s = scenarios.make(name, timbir_b200.Stage)
+    o = scenarios.make(name, Oracle)
+    _load_state(s, o, 7)
+    for _ in range(2):
+        s.offset_update()
+        o.offset_update()
+    assert rel(s.offset(), o.offset()) < 1e-5
+    assert rel(s.errorsino(), o.errorsino()) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["zinger_var", "frames4"])
+def test_variance_update_matches_oracle(name):
+    s = scenarios.make(name, timbir_b200.Stage)
+    o = scenarios.make(name, Oracle)
+    _load_state(s, o, 8)
+    s.variance_update()
+    o.variance_update()
+    assert s.var_est() == pytest.approx(o.var_est(), rel=1e-6)
+    assert rel(s.weight(), o.weight()) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["plain", "frames4", "zinger_var"])
+def test_cost_matches_oracle_fp64(name):
+    s = scenarios.make(name, timbir_b200.Stage)
+    o = scenarios.make(name, Oracle)
+    _load_state(s, o, 9)
+    t, f, p = s.cost()
+    ot, of, op = o.cost()[:3]
+    assert p == pytest.approx(op, rel=1e-12)   # prior: same float inputs, FP64 sums
+    assert f == pytest.approx(of, rel=1e-6)    # data term rides on e (float rounding of Ax)
+    assert t == pytest.approx(ot, rel=1e-6)
+
+
+def test_forward_projection_matches_error_sinogram():
+    s = scenarios.make("plain", timbir_b200.Stage)
+    o = scenarios.make("plain", Oracle)
+    rng = np.random.default_rng(1)
+    x = rng.random((1, s.N_z, s.N_y, s.N_x)).astype(np.float32) * 0.02
+    o.prepare(x)
+    ax = s.forward_project(x)          # [view][row][col]
+    y = s.scan.projections
+    e = np.transpose(o.errorsino(), (0, 2, 1))  # oracle e = y - Ax, [view][row][col]
+    assert rel(ax, y - e) < 1e-5

@@ -1,0 +1,256 @@
+"""timbir_b200 -- B200-native MBIR ICD/NHICD engine behind TIMBIR's reconstruct() call.
+
+Python host mirror of the native library's C ABI (libtimbir_b200.so, built from
+timbir_b200/csrc by ``python -m timbir_b200.build``):
+
+* :func:`reconstruct` -- the drop-in call, same argument names and meaning as
+  the reference's ``reconstruct()`` (TIMBIR v0.0.2 src/include/mbir4d.h:35);
+  it writes the same files in the working directory.
+* :class:`Stage` -- one resolution stage on the GPU, exposing the stage-level
+  entry points (set-up, ICD iteration, cost, ring offsets, variance) and state
+  read-back in the reference's array layouts.
+
+There is no CPU fallback: importing the package loads the native library and
+raises if it is missing or if no CUDA device is usable when a call needs one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtimbir_b200.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_VP = C.c_void_p
+
+_lib = None
+
+
+def load_library() -> C.CDLL:
+    """Load libtimbir_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"native library missing: {LIB_PATH} (run `python -m timbir_b200.build`)")
+    lib = C.CDLL(LIB_PATH)
+    fl, i32 = C.c_float, C.c_int32
+    lib.mbir_init_stage.argtypes = [C.POINTER(_VP), _VP, _VP, _VP, _VP, _VP, i32, i32, i32, i32, fl, fl, fl, fl,
+                                    fl, fl, fl, i32, i32, fl, fl, i32, i32, i32]
+    lib.mbir_free_stage.argtypes = [_VP]
+    lib.mbir_last_error.restype = C.c_char_p
+    lib.mbir_set_stage_switches.argtypes = [_VP, i32, i32, C.c_double]
+    lib.mbir_set_rng_state.argtypes = [_VP, C.c_uint32]
+    lib.mbir_get_rng_state.argtypes = [_VP]
+    lib.mbir_get_rng_state.restype = C.c_uint32
+    lib.mbir_icd_prepare.argtypes = [_VP, _VP, _VP, _VP]
+    lib.mbir_update_voxels_time_slices.argtypes = [_VP, i32, C.POINTER(i32)]
+    lib.mbir_compute_cost.argtypes = [_VP] + [C.POINTER(C.c_double)] * 3
+    lib.mbir_update_sinogram_offset.argtypes = [_VP]
+    lib.mbir_update_variance_parameter.argtypes = [_VP]
+    lib.mbir_stage_dims.argtypes = [_VP, _i32p]
+    for n in ("mbir_get_object", "mbir_set_object", "mbir_get_errorsino", "mbir_get_weight", "mbir_get_offset",
+              "mbir_get_magmap", "mbir_get_hr"):
+        getattr(lib, n).argtypes = [_VP, _f32p]
+    lib.mbir_get_mask.argtypes = [_VP, _u8p]
+    lib.mbir_get_lines.argtypes = [_VP, i32, i32, i32, _i32p, _i32p]
+    for n in ("mbir_get_var_est", "mbir_get_update_percentage"):
+        getattr(lib, n).argtypes = [_VP]
+        getattr(lib, n).restype = C.c_double
+    lib.mbir_get_update_count.argtypes = [_VP]
+    lib.mbir_get_update_count.restype = C.c_longlong
+    lib.mbir_forward_project.argtypes = [_VP, _f32p, _f32p]
+    lib.mbir_get_kernel_stats.argtypes = [_VP, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                          C.POINTER(C.c_longlong)]
+    lib.mbir_time_begin.argtypes = [_VP]
+    lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
+    lib.reconstruct.argtypes = [C.POINTER(C.POINTER(C.c_float))] + [_VP] * 5 + [i32] * 4 + [fl] * 7 + \
+        [i32, i32, fl, fl, C.c_uint8, _VP]
+    _lib = lib
+    return lib
+
+
+class MbirError(RuntimeError):
+    pass
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise MbirError(load_library().mbir_last_error().decode(errors="replace"))
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Stage:
+    """One resolution stage on the GPU (include/timbir_b200.h).
+
+    Constructed like the reference's initStatStructures + initDynStructures for
+    a stage with voxel scales (mult_xy, mult_z); ``blocks`` is num_z_blocks."""
+
+    def __init__(self, scan, sig_s, sig_t, c_s, c_t, convg_thresh=1.0, remove_rings=0, quad_convex=1,
+                 huber_delta=0.5, huber_T=4.0, mult_xy=1, mult_z=1, blocks=2):
+        lib = load_library()
+        self.lib = lib
+        self.scan = scan
+        keep = [_f32(a) for a in (scan.projections, scan.weights, scan.proj_angles, scan.proj_times,
+                                  scan.recon_times)]
+        h = _VP()
+        _check(lib.mbir_init_stage(C.byref(h), *[a.ctypes.data for a in keep], scan.proj_rows, scan.proj_cols,
+                                   scan.proj_num, scan.recon_num, scan.vox_wid, scan.rot_center, sig_s, sig_t,
+                                   c_s, c_t, convg_thresh, remove_rings, quad_convex, huber_delta, huber_T,
+                                   mult_xy, mult_z, blocks))
+        self.h = h
+        d = np.zeros(9, np.int32)
+        lib.mbir_stage_dims(self.h, d)
+        (self.N_p, self.N_r, self.N_t, self.N_x, self.N_y, self.N_z, self.N_time, self.nblk,
+         self.z_overlap) = [int(v) for v in d]
+
+    def close(self):
+        if self.h:
+            self.lib.mbir_free_stage(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- driving -------------------------------------------------------
+    def set_switches(self, update_proj_offset=0, update_var=0, var_est=0.0):
+        _check(self.lib.mbir_set_stage_switches(self.h, update_proj_offset, update_var, var_est))
+
+    def set_rng_state(self, state: int):
+        self.lib.mbir_set_rng_state(self.h, state)
+
+    def rng_state(self) -> int:
+        return self.lib.mbir_get_rng_state(self.h)
+
+    def prepare(self, obj=None, offset=None, magmap=None):
+        arrs = [None if a is None else _f32(a) for a in (obj, offset, magmap)]
+        _check(self.lib.mbir_icd_prepare(self.h, *[None if a is None else a.ctypes.data for a in arrs]))
+
+    def iterate(self, it: int) -> int:
+        conv = C.c_int32()
+        _check(self.lib.mbir_update_voxels_time_slices(self.h, it, C.byref(conv)))
+        return conv.value
+
+    def cost(self):
+        t, f, p = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.mbir_compute_cost(self.h, C.byref(t), C.byref(f), C.byref(p)))
+        return t.value, f.value, p.value
+
+    def offset_update(self):
+        _check(self.lib.mbir_update_sinogram_offset(self.h))
+
+    def variance_update(self):
+        _check(self.lib.mbir_update_variance_parameter(self.h))
+
+    # --- state ---------------------------------------------------------
+    def _get(self, fn, shape, dt=np.float32):
+        out = np.zeros(shape, dt)
+        _check(getattr(self.lib, fn)(self.h, out.reshape(-1)))
+        return out
+
+    def object(self):
+        return self._get("mbir_get_object", (self.N_time, self.N_z, self.N_y, self.N_x))
+
+    def set_object(self, x):
+        _check(self.lib.mbir_set_object(self.h, _f32(x).reshape(-1)))
+
+    def errorsino(self):
+        return self._get("mbir_get_errorsino", (self.N_p, self.N_r, self.N_t))
+
+    def weight(self):
+        return self._get("mbir_get_weight", (self.N_p, self.N_r, self.N_t))
+
+    def offset(self):
+        return self._get("mbir_get_offset", (self.N_r, self.N_t))
+
+    def magmap(self):
+        return self._get("mbir_get_magmap", (self.N_time, self.nblk, self.N_y, self.N_x))
+
+    def hr(self):
+        return self._get("mbir_get_hr", (self.N_p, 65))
+
+    def mask(self):
+        return self._get("mbir_get_mask", (self.N_y, self.N_x), np.uint8)
+
+    def lines(self, kind, frame, block):
+        xs = np.zeros(self.N_x * self.N_y, np.int32)
+        ys = np.zeros(self.N_x * self.N_y, np.int32)
+        n = self.lib.mbir_get_lines(self.h, kind, frame, block, xs, ys)
+        if n < 0:
+            _check(n)
+        return xs[:n].copy(), ys[:n].copy()
+
+    def var_est(self) -> float:
+        return self.lib.mbir_get_var_est(self.h)
+
+    def update_percentage(self) -> float:
+        return self.lib.mbir_get_update_percentage(self.h)
+
+    def update_count(self) -> int:
+        return self.lib.mbir_get_update_count(self.h)
+
+    def kernel_stats(self):
+        """(ICD kernel device ms, ICD kernel launches, all kernel launches)."""
+        ms, n_icd, n_all = C.c_double(), C.c_longlong(), C.c_longlong()
+        self.lib.mbir_get_kernel_stats(self.h, C.byref(ms), C.byref(n_icd), C.byref(n_all))
+        return ms.value, n_icd.value, n_all.value
+
+    def time_begin(self):
+        _check(self.lib.mbir_time_begin(self.h))
+
+    def time_end(self) -> float:
+        ms = C.c_double()
+        _check(self.lib.mbir_time_end(self.h, C.byref(ms)))
+        return ms.value
+
+    def forward_project(self, obj) -> np.ndarray:
+        out = np.zeros((self.N_p, self.N_t, self.N_r), np.float32)
+        _check(self.lib.mbir_forward_project(self.h, _f32(obj).reshape(-1), out.reshape(-1)))
+        return out
+
+
+def _malloc_copy(a: np.ndarray) -> C.c_void_p:
+    """Copy into a malloc'd block: reconstruct() free()s its inputs."""
+    libc = C.CDLL(None)
+    libc.malloc.restype = C.c_void_p
+    libc.malloc.argtypes = [C.c_size_t]
+    a = _f32(a)
+    p = libc.malloc(max(a.nbytes, 4))
+    if not p:
+        raise MemoryError
+    C.memmove(p, a.ctypes.data, a.nbytes)
+    return C.c_void_p(p)
+
+
+def reconstruct(projections, weights, proj_angles, proj_times, recon_times, proj_rows, proj_cols, proj_num,
+                recon_num, vox_wid, rot_center, sig_s, sig_t, c_s, c_t, convg_thresh, remove_rings,
+                quad_convex, huber_delta, huber_T, restart=0, debug_log: str | None = None) -> int:
+    """The drop-in reconstruct() on numpy arrays; outputs go to the working
+    directory (object_time_<t>.bin, proj_offset.bin, ...).  Returns the C
+    call's status (0 on success, -1 on failure)."""
+    lib = load_library()
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    fp = libc.fopen((debug_log or os.devnull).encode(), b"a")
+    obj = C.POINTER(C.c_float)()
+    try:
+        return lib.reconstruct(C.byref(obj), _malloc_copy(projections), _malloc_copy(weights),
+                               _malloc_copy(proj_angles), _malloc_copy(proj_times), _malloc_copy(recon_times),
+                               proj_rows, proj_cols, proj_num, recon_num, vox_wid, rot_center, sig_s, sig_t, c_s,
+                               c_t, convg_thresh, remove_rings, quad_convex, huber_delta, huber_T, restart,
+                               C.c_void_p(fp))
+    finally:
+        libc.fclose(fp)

@@ -1,0 +1,90 @@
+// Internal declarations shared by the host driver (mbir_stage.cu,
+// mbir_reconstruct.cpp) and the CUDA kernels (mbir_kernels.cu).
+//
+// Device layouts (chosen for the access patterns of the kernels, not copied
+// from the reference's [view][col][row] layout, which is kept only at the file
+// boundary):
+//   sinogram-shaped arrays  e, w, y : float [N_t][N_p][N_r]  (slice-major,
+//                                      detector column fastest; one slice's
+//                                      sinogram is one contiguous plane)
+//   ring offset d                   : float [N_t][N_r]
+//   object x                        : float [N_time][N_z][N_y][N_x]
+//   update-magnitude map            : float [N_time][nblk][N_y][N_x]
+//   detector response H_r           : float [N_p][65]
+//   cos/sin of view angles          : double [N_p]
+//   views of frame i                : int32 view_idx[i*max_views + k]
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MBIR_RESP_BINS 64
+#define MBIR_MAX_STAGES 8
+
+struct MbirGeom {
+    // detector
+    int N_p, N_r, N_t, m_z;
+    double delta_r, R0, RMax, OffsetR;
+    // object
+    int N_x, N_y, N_z, N_time;
+    double x0, y0, delta_xy;
+    // views
+    int max_views;
+    const int *view_idx;   // [N_time][max_views]
+    const int *view_num;   // [N_time]
+    const double *cosv, *sinv;
+    const float *H_r;      // [N_p][65]
+};
+
+struct MbirPrior {
+    double sSQ, sSQP, sTQ, sTQP, c_s, c_t;
+    double SF[27];  // spatial weights, index 9*dz + 3*dy + dx (each 0..2)
+    double TF;      // temporal weight
+    double alpha;   // over-relaxation
+    double hT, hdelta;  // generalized-Huber threshold and slope
+};
+
+struct MbirDev {
+    float *e, *w, *d, *x, *mag;
+    const uint8_t *mask;   // [N_y][N_x]
+};
+
+// One task of a reference-schedule half-sweep: a (frame, z-block) pair and a
+// range of one of its line lists.
+struct MbirTask {
+    int frame, z0, z1, b0, b1;
+    const int *xs, *ys;    // line list (device)
+    float *mag;            // [N_y][N_x] plane of the magnitude map
+};
+
+struct MbirTaskOut {
+    double vox_mag;        // sum of |x'| over updated voxels
+    long long updates;     // voxel updates performed
+    long long zero_skips;  // voxels skipped by zero skipping
+};
+
+// ---- kernel launchers (mbir_kernels.cu) -------------------------------------
+// mode 0: out = y - A x - d; mode 1: out = A x.  frame_of_view[p] = frame of
+// view p, or -1 for a view outside every frame.
+cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
+                                const float *y, const float *d, float *out, int mode,
+                                cudaStream_t s);
+cudaError_t mbir_launch_icd_ref(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                                const MbirTask *tasks, int ntasks, MbirTaskOut *out, int iter,
+                                int threads, size_t acache_bytes, void *acache_global,
+                                cudaStream_t s);
+cudaError_t mbir_launch_cost(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                             double *partials, int nparts, double *result, cudaStream_t s);
+cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
+                               double *num, double *den, double *partials, int nparts,
+                               cudaStream_t s);
+cudaError_t mbir_launch_variance(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                                 double var_est, double *partials, int nparts, double *result,
+                                 cudaStream_t s);
+cudaError_t mbir_launch_variance_apply(const MbirGeom &g, const MbirDev &dv, double var_new,
+                                       cudaStream_t s);
+cudaError_t mbir_launch_vsc_filter(const float *mag, float *filt, int planes, int N_y, int N_x,
+                                   cudaStream_t s);
+cudaError_t mbir_launch_select_stats(const float *mag, const int *xs, const int *ys,
+                                     const int *counts, int planes, int stride, double *out,
+                                     cudaStream_t s);
+int mbir_amax(double delta_xy, double delta_r);

@@ -1,0 +1,629 @@
+// CUDA kernels for the MBIR ICD hot path (sm_100a).
+//
+// Reference algorithm: TIMBIR v0.0.2, src/MBIR_4D.  Every kernel cites the
+// reference function whose arithmetic it reproduces.  Arithmetic that feeds
+// an index decision (detector bin of the A-matrix column) or that the
+// reference performs in float is written with explicit round-to-nearest
+// intrinsics so that no fused multiply-add changes a rounding step.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "mbir_internal.h"
+
+namespace {
+
+constexpr double kP = 1.2;  // qGGMRF p (XT_Constants.h:61)
+constexpr double kQ = 2.0;  // qGGMRF q (XT_Constants.h:62)
+
+// ----------------------------------------------------------------------------
+// A-matrix column (XT_AMatrix.c:50-110): detector bins within delta_xy of the
+// voxel's projected centre r = x cos - y sin, weight = linear interpolation of
+// H_r[view] at |r - R_c| / OffsetR, kept if > 0.  Returns the count.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ double voxel_x(const MbirGeom &g, int col)
+{
+    return __dadd_rn(g.x0, __dmul_rn((double)col + 0.5, g.delta_xy));
+}
+__device__ __forceinline__ double voxel_y(const MbirGeom &g, int row)
+{
+    return __dadd_rn(g.y0, __dmul_rn((double)row + 0.5, g.delta_xy));
+}
+
+// Visits every kept (bin, weight) pair of the column; f(bin, weight).
+template <typename F>
+__device__ __forceinline__ void acol_visit(const MbirGeom &g, double x, double y, int view, F &&f)
+{
+    const double r = __dsub_rn(__dmul_rn(x, g.cosv[view]), __dmul_rn(y, g.sinv[view]));
+    const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
+    if (rmax < g.R0 || rmin > g.RMax) return;
+    int imin = (int)floor(__ddiv_rn(__dsub_rn(rmin, g.R0), g.delta_r));
+    int imax = (int)floor(__ddiv_rn(__dsub_rn(rmax, g.R0), g.delta_r));
+    if (imax >= g.N_r) imax = g.N_r - 1;
+    if (imin < 0) imin = 0;
+    const float *H = g.H_r + (size_t)view * (MBIR_RESP_BINS + 1);
+    for (int j = imin; j <= imax; j++) {
+        const double rc = __dadd_rn(g.R0, __dmul_rn((double)j + 0.5, g.delta_r));
+        const double dr = fabs(__dsub_rn(r, rc));
+        const int id = (int)floor(__ddiv_rn(dr, g.OffsetR));
+        if (id >= 0 && id < MBIR_RESP_BINS) {
+            const double w1 = __dsub_rn(dr, __dmul_rn((double)id, g.OffsetR));
+            const double w2 = __dsub_rn(g.OffsetR, w1);
+            const double f1 = __ddiv_rn(
+                __dadd_rn(__dmul_rn(w2, (double)__ldg(H + id)), __dmul_rn(w1, (double)__ldg(H + id + 1))),
+                g.OffsetR);
+            if (f1 > 0) f(j, f1);
+        }
+    }
+}
+
+__device__ __forceinline__ int acol_exact(const MbirGeom &g, double x, double y, int view, int *idx,
+                                          double *val, int cap)
+{
+    int n = 0;
+    acol_visit(g, x, y, view, [&](int j, double f1) {
+        if (n < cap) {
+            idx[n] = j;
+            val[n] = f1;
+            n++;
+        }
+    });
+    return n;
+}
+
+// qGGMRF derivative rho'(d) (XT_ICD_update.c:93-128).
+__device__ __forceinline__ double qggmrf_deriv(double d, double sQ, double sQP, double c)
+{
+    const double ad = fabs(d);
+    const double t1 = pow(ad, kQ - kP) / sQP;
+    const double t2 = ad;  // |d|^(q-1), q = 2
+    const double t3 = c + t1;
+    const double m = __dsub_rn(kQ, __ddiv_rn(__dmul_rn(kQ - kP, t1), t3));
+    const double v = __dmul_rn(t2 / __dmul_rn(t3, sQ), m);
+    return d < 0 ? -v : v;
+}
+
+// qGGMRF potential rho(d) (XT_ICD_update.c:83-91); pow(|d|, 2) is |d|^2.
+__device__ __forceinline__ double qggmrf_value(double d, double sQ, double sQP, double c)
+{
+    const double ad = fabs(d);
+    return (__dmul_rn(ad, ad) / sQ) / (c + pow(ad, kQ - kP) / sQP);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ----------------------------------------------------------------------------
+// Error sinogram e = y - A x - d (XT_ICD_update.c:655-716 with the forward
+// projector of XT_ForwardProject.c:8-25).  One CTA per (view, slice): the
+// slice's projection at that view is accumulated in FP64 shared memory, then
+// written to the m_z detector rows of the slice.  Views that belong to no
+// frame project nothing (the reference never visits them).
+// mode 0: out = y - Ax - d (float arithmetic as the reference); mode 1: out = Ax.
+// ----------------------------------------------------------------------------
+__global__ void k_forward(MbirGeom g, const float *__restrict__ x, const int *__restrict__ frame_of_view,
+                          const float *__restrict__ y, const float *__restrict__ d,
+                          float *__restrict__ out, int mode)
+{
+    extern __shared__ double acc[];  // [N_r]
+    const int p = blockIdx.x, s = blockIdx.y;
+    for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) acc[r] = 0.0;
+    __syncthreads();
+    const int f = frame_of_view[p];
+    if (f >= 0) {
+        const float *xs = x + ((size_t)f * g.N_z + s) * g.N_y * g.N_x;
+        const int nxy = g.N_y * g.N_x;
+        for (int v = threadIdx.x; v < nxy; v += blockDim.x) {
+            const float pix = xs[v];
+            if (pix == 0.0f) continue;
+            const int j = v / g.N_x, k = v - j * g.N_x;
+            acol_visit(g, voxel_x(g, k), voxel_y(g, j), p,
+                       [&](int bin, double f1) { atomicAdd(&acc[bin], __dmul_rn((double)pix, f1)); });
+        }
+    }
+    __syncthreads();
+    for (int rr = 0; rr < g.m_z; rr++) {
+        const int t = s * g.m_z + rr;
+        for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) {
+            const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+            const float ax = (float)acc[r];
+            if (mode == 0)
+                out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + r]);
+            else
+                out[o] = ax;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Reference-schedule ICD (XT_VoxUpdate.c:43-281 inside the half-sweeps of
+// XT_ICD_update.c:974-1060).  One CTA per (frame, z-block) task; it walks the
+// task's voxel lines in list order and, per line, the slices of the block in
+// order, exactly as updateVoxels_Atten does.  Per voxel:
+//   * every thread forms theta1/theta2 over its views (generalized-Huber
+//     weights; a view is always handled by the same thread, so the error
+//     sinogram entries it updates are private to it);
+//   * warp 0 gathers the 26+2 neighbourhood, applies zero skipping and forms
+//     the surrogate's prior sums;
+//   * thread 0 solves the 1-D surrogate with over-relaxation (FP64), stores the
+//     voxel and broadcasts the float-rounded change;
+//   * every thread subtracts a * change from its error sinogram entries.
+// The A column of each (line, view) is computed once per line into a cache
+// (shared memory when it fits, else a per-task global slab).
+// ----------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(NT) k_icd_ref(MbirGeom g, MbirPrior pr, MbirDev dv,
+                                                 const MbirTask *__restrict__ tasks,
+                                                 MbirTaskOut *__restrict__ out, int iter, int amax,
+                                                 int acache_smem, char *acache_global,
+                                                 size_t acache_bytes)
+{
+    extern __shared__ __align__(16) char smem_raw[];
+    __shared__ double s_t1[NT / 32], s_t2[NT / 32];
+    __shared__ double s_pt1, s_pt2, s_V, s_delta;
+    __shared__ int s_zs, s_skip;
+    constexpr int NW = NT / 32;
+    const MbirTask t = tasks[blockIdx.x];
+    const int i = t.frame;
+    const int nv = g.view_num[i];
+    const int *vl = g.view_idx + (size_t)i * g.max_views;
+    char *base = acache_smem ? smem_raw : acache_global + (size_t)blockIdx.x * acache_bytes;
+    double *aval = reinterpret_cast<double *>(base);
+    int *aidx = reinterpret_cast<int *>(aval + (size_t)nv * amax);
+    int *acnt = aidx + (size_t)nv * amax;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int N_x = g.N_x, N_y = g.N_y, N_z = g.N_z;
+    const size_t plane = (size_t)N_y * N_x;
+
+    double vox_mag = 0.0;
+    long long upd = 0, zskips = 0;
+    for (int li = t.b0; li <= t.b1; li++) {
+        const int k = t.xs[li], j = t.ys[li];
+        if (threadIdx.x == 0) t.mag[(size_t)j * N_x + k] = 0.0f;
+        const double xc = voxel_x(g, k), yc = voxel_y(g, j);
+        for (int v = threadIdx.x; v < nv; v += NT)
+            acnt[v] = acol_exact(g, xc, yc, vl[v], aidx + (size_t)v * amax, aval + (size_t)v * amax, amax);
+        if (dv.mask[(size_t)j * N_x + k] != 1) continue;
+        for (int s = t.z0; s <= t.z1; s++) {
+            // ---- data term: theta1, theta2 ----
+            double th1 = 0.0, th2 = 0.0;
+            for (int v = threadIdx.x; v < nv; v += NT) {
+                const int view = vl[v], cnt = acnt[v];
+                for (int q = 0; q < cnt; q++) {
+                    const int ir = aidx[(size_t)v * amax + q];
+                    const double a = aval[(size_t)v * amax + q];
+                    for (int rr = 0; rr < g.m_z; rr++) {
+                        const size_t o = ((size_t)(s * g.m_z + rr) * g.N_p + view) * g.N_r + ir;
+                        const double ed = dv.e[o], wd = dv.w[o];
+                        const double sw = sqrt(wd);
+                        if (fabs(__dmul_rn(ed, sw)) < pr.hT) {
+                            th2 = __dadd_rn(th2, __dmul_rn(__dmul_rn(a, a), wd));
+                            th1 = __dadd_rn(th1, -__dmul_rn(__dmul_rn(ed, a), wd));
+                        } else {
+                            const double tmp = __ddiv_rn(__dmul_rn(__dmul_rn(pr.hT, pr.hdelta), sw), fabs(ed));
+                            th2 = __dadd_rn(th2, __dmul_rn(__dmul_rn(a, a), tmp));
+                            th1 = __dadd_rn(th1, -__dmul_rn(__dmul_rn(ed, a), tmp));
+                        }
+                    }
+                }
+            }
+            th1 = warp_sum(th1);
+            th2 = warp_sum(th2);
+            if (lane == 0) {
+                s_t1[warp] = th1;
+                s_t2[warp] = th2;
+            }
+            // ---- prior: 26 spatial + 2 temporal neighbours (warp 0) ----
+            if (warp == 0) {
+                const float *xf = dv.x + (size_t)i * N_z * plane;
+                const double V = xf[(size_t)s * plane + (size_t)j * N_x + k];
+                double nb = 0.0, b = 0.0;
+                bool valid = false;
+                if (lane < 27 && lane != 13) {
+                    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
+                    const int zz = s + dz, yy = j + dy, xx = k + dx;
+                    if (zz >= 0 && zz < N_z && yy >= 0 && yy < N_y && xx >= 0 && xx < N_x) {
+                        valid = true;
+                        nb = xf[(size_t)zz * plane + (size_t)yy * N_x + xx];
+                    }
+                    if (valid) {
+                        const double d0 = V - nb;
+                        const double prm = d0 != 0 ? qggmrf_deriv(d0, pr.sSQ, pr.sSQP, pr.c_s) / d0
+                                                   : kQ / (pr.sSQ * pr.c_s);
+                        b = pr.SF[lane] * prm;
+                    }
+                } else if (lane == 27 || lane == 28) {
+                    const int ti = i + (lane == 27 ? -1 : 1);
+                    if (ti >= 0 && ti < g.N_time) {
+                        valid = true;
+                        nb = dv.x[((size_t)ti * N_z + s) * plane + (size_t)j * N_x + k];
+                        const double d0 = V - nb;
+                        const double prm = d0 != 0 ? qggmrf_deriv(d0, pr.sTQ, pr.sTQP, pr.c_t) / d0
+                                                   : kQ / (pr.sTQ * pr.c_t);
+                        b = pr.TF * prm;
+                    }
+                }
+                const unsigned pos = __ballot_sync(0xffffffffu, valid && nb > 0.0);
+                double p1 = warp_sum(__dmul_rn(b, nb));
+                double p2 = warp_sum(b);
+                if (lane == 0) {
+                    s_pt1 = p1;
+                    s_pt2 = p2;
+                    s_V = V;
+                    s_zs = (V == 0.0 && iter > 1 && pos == 0u) ? 1 : 0;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                if (s_zs) {
+                    s_skip = 1;
+                    zskips++;
+                } else {
+                    double T1 = 0.0, T2 = 0.0;
+#pragma unroll
+                    for (int w = 0; w < NW; w++) {
+                        T1 += s_t1[w];
+                        T2 += s_t2[w];
+                    }
+                    const double V = s_V;
+                    const double u = __ddiv_rn(__dsub_rn(__dadd_rn(s_pt1, __dmul_rn(T2, V)), T1),
+                                               __dadd_rn(s_pt2, T2));
+                    const double xn = __dadd_rn(V, __dmul_rn(pr.alpha, __dsub_rn(u, V)));
+                    const float xf = (float)xn;
+                    const size_t o = ((size_t)i * N_z + s) * plane + (size_t)j * N_x + k;
+                    dv.x[o] = xf;
+                    const double dl = (double)xf - V;
+                    s_delta = dl;
+                    s_skip = 0;
+                    float *m = t.mag + (size_t)j * N_x + k;
+                    *m = (float)((double)*m + fabs(dl));
+                    vox_mag += fabs((double)xf);
+                    upd++;
+                }
+            }
+            __syncthreads();
+            if (!s_skip) {
+                const double dl = s_delta;
+                for (int v = threadIdx.x; v < nv; v += NT) {
+                    const int view = vl[v], cnt = acnt[v];
+                    for (int q = 0; q < cnt; q++) {
+                        const int ir = aidx[(size_t)v * amax + q];
+                        const double a = aval[(size_t)v * amax + q];
+                        for (int rr = 0; rr < g.m_z; rr++) {
+                            const size_t o = ((size_t)(s * g.m_z + rr) * g.N_p + view) * g.N_r + ir;
+                            dv.e[o] = (float)__dsub_rn((double)dv.e[o], __dmul_rn(a, dl));
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        out[blockIdx.x].vox_mag = vox_mag;
+        out[blockIdx.x].updates = upd;
+        out[blockIdx.x].zero_skips = zskips;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Deterministic block reduction helpers: each block writes one partial per
+// quantity; a single block sums the partials in index order.
+// ----------------------------------------------------------------------------
+template <int NQ>
+__device__ void block_partials(double (&v)[NQ], double *partials, int nparts)
+{
+    __shared__ double sh[NQ][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        double s = warp_sum(v[q]);
+        if (lane == 0) sh[q][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            double s = 0.0;
+            for (int w = 0; w < nw; w++) s += sh[q][w];
+            partials[(size_t)q * nparts + blockIdx.x] = s;
+        }
+    }
+}
+
+__global__ void k_sum_partials(const double *partials, int nparts, int nq, double *result)
+{
+    __shared__ double sh[32];
+    for (int q = 0; q < nq; q++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nparts; b += blockDim.x) s += partials[(size_t)q * nparts + b];
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += sh[w];
+            result[q] = tot;
+        }
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------------------------
+// MAP cost (XT_ICD_update.c:186-319): generalized-Huber data term and the
+// prior over the 13 causal spatial pairs plus the forward temporal pair, in
+// FP64.  partials[0][b] = data sum, partials[1][b] = prior sum.
+// ----------------------------------------------------------------------------
+__global__ void k_cost(MbirGeom g, MbirPrior pr, MbirDev dv, double *partials, int nparts)
+{
+    double v[2] = {0.0, 0.0};
+    const size_t ns = (size_t)g.N_t * g.N_p * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < ns; o += stride) {
+        double t = __dmul_rn((double)dv.e[o], sqrt((double)dv.w[o]));
+        if (fabs(t) < pr.hT)
+            t = __dmul_rn(t, t);
+        else
+            t = __dadd_rn(__dmul_rn(__dmul_rn(2.0 * pr.hdelta, pr.hT), fabs(t)),
+                          __dmul_rn(__dmul_rn(pr.hT, pr.hT), 1.0 - 2.0 * pr.hdelta));
+        v[0] += t;
+    }
+    const size_t plane = (size_t)g.N_y * g.N_x;
+    const size_t nvox = (size_t)g.N_time * g.N_z * plane;
+    // causal spatial offsets (dz, dy, dx) and their filter index 9*(dz+1)+3*(dy+1)+(dx+1)
+    const int off[13][3] = {{0, 0, 1},  {0, 1, -1}, {0, 1, 0},  {0, 1, 1},  {1, -1, 0},
+                            {1, 0, 0},  {1, 1, 0},  {1, -1, -1}, {1, -1, 1}, {1, 0, -1},
+                            {1, 1, -1}, {1, 1, 1},  {1, 0, 1}};
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < nvox; o += stride) {
+        const int k = (int)(o % g.N_x);
+        const int j = (int)((o / g.N_x) % g.N_y);
+        const int s = (int)((o / plane) % g.N_z);
+        const int i = (int)(o / ((size_t)g.N_z * plane));
+        const float xv = dv.x[o];
+        for (int n = 0; n < 13; n++) {
+            const int zz = s + off[n][0], yy = j + off[n][1], xx = k + off[n][2];
+            if (zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x) {
+                const float nbv = dv.x[((size_t)i * g.N_z + zz) * plane + (size_t)yy * g.N_x + xx];
+                const double dl = (double)__fsub_rn(xv, nbv);
+                const int fi = 9 * (off[n][0] + 1) + 3 * (off[n][1] + 1) + (off[n][2] + 1);
+                v[1] += pr.SF[fi] * qggmrf_value(dl, pr.sSQ, pr.sSQP, pr.c_s);
+            }
+        }
+        if (i + 1 < g.N_time) {
+            const double dl = (double)__fsub_rn(xv, dv.x[o + (size_t)g.N_z * plane]);
+            v[1] += pr.TF * qggmrf_value(dl, pr.sTQ, pr.sTQP, pr.c_t);
+        }
+    }
+    block_partials<2>(v, partials, nparts);
+}
+
+// ----------------------------------------------------------------------------
+// Ring offsets (XT_ICD_update.c:753-927).  Pass 1: per detector element
+// (t, r), num and den summed over all views in view order (FP64, with the
+// reference's float products), plus block partials of sum(d + num/den) and
+// sum(1/den) for the zero-mean gamma.  Pass 2: shift = (num - gamma)/den,
+// d += shift, e -= shift over all views (types 1, 2); type 3 (rectangular
+// patches with no constraint windows, as on the reference's reconstruct path)
+// sets d = b/Lambda and e += d_old - d.
+// ----------------------------------------------------------------------------
+__global__ void k_offset_terms(MbirGeom g, MbirPrior pr, MbirDev dv, int type, double *num, double *den,
+                               double *partials, int nparts)
+{
+    double v[2] = {0.0, 0.0};
+    const size_t nel = (size_t)g.N_t * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nel; q += stride) {
+        const int t = (int)(q / g.N_r), r = (int)(q % g.N_r);
+        const float dq = dv.d[q];
+        double nm = 0.0, dn = 0.0;
+        for (int p = 0; p < g.N_p; p++) {
+            const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+            const float ef = dv.e[o], wf = dv.w[o];
+            const double sw = sqrt((double)wf);
+            const double tmp = __dmul_rn(__dmul_rn(pr.hT, pr.hdelta), sw);
+            const bool sel = fabs(__dmul_rn((double)ef, sw)) < pr.hT;
+            if (type == 3) {
+                if (sel) {
+                    dn += (double)wf;
+                    nm += (double)__fmul_rn(__fadd_rn(ef, dq), wf);
+                } else {
+                    const double om = __ddiv_rn(tmp, fabs((double)ef));
+                    dn += om;
+                    nm += __ddiv_rn(__dmul_rn((double)__fadd_rn(ef, dq), tmp), fabs((double)ef));
+                }
+            } else {
+                if (sel) {
+                    nm += (double)__fmul_rn(ef, wf);
+                    dn += (double)wf;
+                } else {
+                    const double sg = (double)((ef > 0) - (ef < 0));
+                    nm += __dmul_rn(tmp, sg);
+                    dn += __ddiv_rn(tmp, fabs((double)ef));
+                }
+            }
+        }
+        num[q] = nm;
+        den[q] = dn;
+        v[0] += (double)dq + nm / dn;
+        v[1] += 1.0 / dn;
+    }
+    block_partials<2>(v, partials, nparts);
+}
+
+__global__ void k_offset_apply(MbirGeom g, MbirDev dv, int type, const double *num, const double *den,
+                               const double *sums)
+{
+    const size_t nel = (size_t)g.N_t * g.N_r;
+    const double gamma = type == 2 ? sums[0] / sums[1] : 0.0;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nel) return;
+    const int t = (int)(q / g.N_r), r = (int)(q % g.N_r);
+    if (type == 3) {
+        const float xn = (float)((num[q] - 0.0) / den[q]);
+        const float dd = __fsub_rn(dv.d[q], xn);
+        for (int p = 0; p < g.N_p; p++) {
+            const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+            dv.e[o] = __fadd_rn(dv.e[o], dd);
+        }
+        dv.d[q] = xn;
+    } else {
+        const double sh = __ddiv_rn(num[q] - gamma, den[q]);
+        dv.d[q] = (float)__dadd_rn((double)dv.d[q], sh);
+        for (int p = 0; p < g.N_p; p++) {
+            const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+            dv.e[o] = (float)__dsub_rn((double)dv.e[o], sh);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Variance (XT_ICD_update.c:720-751).  Pass 1 restores w_orig = w * sigma^2
+// (float) and sums e^2 w_orig (selected, float products) or
+// |e| delta T sqrt(w_orig sigma^2) (zingers); pass 2 divides by the new sigma^2.
+// ----------------------------------------------------------------------------
+__global__ void k_variance(MbirGeom g, MbirPrior pr, MbirDev dv, double var_est, double *partials,
+                           int nparts)
+{
+    double v[1] = {0.0};
+    const size_t ns = (size_t)g.N_t * g.N_p * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < ns; o += stride) {
+        const float ef = dv.e[o], wold = dv.w[o];
+        const bool sel = fabs(__dmul_rn((double)ef, sqrt((double)wold))) < pr.hT;
+        const float wn = (float)__dmul_rn((double)wold, var_est);
+        dv.w[o] = wn;
+        if (sel)
+            v[0] += (double)__fmul_rn(__fmul_rn(ef, ef), wn);
+        else
+            v[0] += __dmul_rn(__dmul_rn(__dmul_rn(fabs((double)ef), pr.hdelta), pr.hT),
+                              sqrt(__dmul_rn((double)wn, var_est)));
+    }
+    block_partials<1>(v, partials, nparts);
+}
+
+__global__ void k_variance_apply(MbirGeom g, MbirDev dv, double var_new)
+{
+    const size_t ns = (size_t)g.N_t * g.N_p * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < ns; o += stride)
+        dv.w[o] = (float)__ddiv_rn((double)dv.w[o], var_new);
+}
+
+// ----------------------------------------------------------------------------
+// NHICD voxel-selection criterion (XT_NHICD.c:128-162): 5x5 Hamming-weighted
+// sum of the update-magnitude map, zero outside the image.
+// ----------------------------------------------------------------------------
+__constant__ double c_hamming[25] = {0.0064, 0.0432, 0.0800, 0.0432, 0.0064, 0.0432, 0.2916,
+                                     0.5400, 0.2916, 0.0432, 0.0800, 0.5400, 1.0000, 0.5400,
+                                     0.0800, 0.0432, 0.2916, 0.5400, 0.2916, 0.0432, 0.0064,
+                                     0.0432, 0.0800, 0.0432, 0.0064};
+
+__global__ void k_vsc_filter(const float *mag, float *filt, int planes, int N_y, int N_x)
+{
+    const size_t n = (size_t)planes * N_y * N_x;
+    const size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int k = (int)(o % N_x), j = (int)((o / N_x) % N_y);
+    const float *m = mag + (o - (size_t)j * N_x - k);
+    double acc = 0.0;
+    for (int p = -2; p <= 2; p++)
+        for (int q = -2; q <= 2; q++)
+            if (j + p >= 0 && j + p < N_y && k + q >= 0 && k + q < N_x)
+                acc = __dadd_rn(acc, __dmul_rn(c_hamming[(p + 2) * 5 + q + 2], (double)m[(size_t)(j + p) * N_x + k + q]));
+    filt[o] = (float)acc;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers --
+int mbir_amax(double delta_xy, double delta_r) { return (int)ceil(3 * delta_xy / delta_r) + 2; }
+
+cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
+                                     const float *y, const float *d, float *out, int mode,
+                                     cudaStream_t s)
+{
+    dim3 grid(g.N_p, g.N_z);
+    size_t sm = sizeof(double) * g.N_r;
+    if (sm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+    }
+    k_forward<<<grid, 256, sm, s>>>(g, x, frame_of_view, y, d, out, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_icd_ref(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                                const MbirTask *tasks, int ntasks, MbirTaskOut *out, int iter,
+                                int threads, size_t acache_bytes, void *acache_global,
+                                cudaStream_t s)
+{
+    if (ntasks <= 0) return cudaSuccess;
+    const int amax = mbir_amax(g.delta_xy, g.delta_r);
+    const int smem_ok = acache_bytes <= 160 * 1024;
+    const size_t sm = smem_ok ? acache_bytes : 0;
+    cudaError_t e = cudaSuccess;
+#define MBIR_LAUNCH_REF(NT)                                                                        \
+    do {                                                                                           \
+        e = cudaFuncSetAttribute(k_icd_ref<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                 (int)(sm > 0 ? sm : 1));                                          \
+        if (e != cudaSuccess) return e;                                                            \
+        k_icd_ref<NT><<<ntasks, NT, sm, s>>>(g, pr, dv, tasks, out, iter, amax, smem_ok,           \
+                                             (char *)acache_global, acache_bytes);                 \
+    } while (0)
+    if (threads <= 64)
+        MBIR_LAUNCH_REF(64);
+    else if (threads <= 128)
+        MBIR_LAUNCH_REF(128);
+    else
+        MBIR_LAUNCH_REF(256);
+#undef MBIR_LAUNCH_REF
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_cost(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                             double *partials, int nparts, double *result, cudaStream_t s)
+{
+    k_cost<<<nparts, 256, 0, s>>>(g, pr, dv, partials, nparts);
+    k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, result);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
+                               double *num, double *den, double *partials, int nparts,
+                               cudaStream_t s)
+{
+    k_offset_terms<<<nparts, 128, 0, s>>>(g, pr, dv, type, num, den, partials, nparts);
+    double *sums = partials + 2 * (size_t)nparts;
+    k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, sums);
+    const size_t nel = (size_t)g.N_t * g.N_r;
+    k_offset_apply<<<(unsigned)((nel + 127) / 128), 128, 0, s>>>(g, dv, type, num, den, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_variance(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
+                                 double var_est, double *partials, int nparts, double *result,
+                                 cudaStream_t s)
+{
+    k_variance<<<nparts, 256, 0, s>>>(g, pr, dv, var_est, partials, nparts);
+    k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 1, result);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_variance_apply(const MbirGeom &g, const MbirDev &dv, double var_new,
+                                       cudaStream_t s)
+{
+    k_variance_apply<<<1184, 256, 0, s>>>(g, dv, var_new);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_vsc_filter(const float *mag, float *filt, int planes, int N_y, int N_x,
+                                   cudaStream_t s)
+{
+    const size_t n = (size_t)planes * N_y * N_x;
+    k_vsc_filter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(mag, filt, planes, N_y, N_x);
+    return cudaGetLastError();
+}

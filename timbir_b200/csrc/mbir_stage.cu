@@ -1,0 +1,619 @@
+// One resolution stage of the reconstruction on the GPU: device state, the
+// reference ICD schedule, cost, ring offsets and variance, behind the C ABI
+// declared in include/timbir_b200.h.
+//
+// Reference: TIMBIR v0.0.2, src/MBIR_4D/XT_ICD_update.c (ICD_BackProject,
+// updateVoxelsTimeSlices) and XT_Init.c (stage set-up).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/timbir_b200.h"
+#include "mbir_host.h"
+#include "mbir_internal.h"
+
+using namespace mbir;
+
+static thread_local char g_err[512];
+
+static int fail(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return -1;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return fail("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));    \
+    } while (0)
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t n)
+{
+    return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+struct MbirStage {
+    ScanGeom sg;
+    StageGeom st;
+    ParkMiller rng;
+    int nblk = 2, K = 10, offset_type = 0, upd_offset = 0, upd_var = 0, prepared = 0;
+    double var_est = 1.0, stop_thresh = 1.0, hT = 0, hdelta = 0, last_pct = 0;
+    long long updates = 0, zero_skips = 0;
+    std::vector<float> H_r;
+    std::vector<uint8_t> mask;
+    std::vector<int> nr, nn;  // line counts [N_time][nblk]
+    MbirGeom g{};
+    MbirPrior pr{};
+    MbirDev dv{};
+    cudaStream_t stream = nullptr;
+    // device buffers
+    float *d_e = nullptr, *d_w = nullptr, *d_y = nullptr, *d_d = nullptr, *d_x = nullptr,
+          *d_mag = nullptr, *d_filt = nullptr, *d_H = nullptr;
+    double *d_cos = nullptr, *d_sin = nullptr, *d_num = nullptr, *d_den = nullptr,
+           *d_partials = nullptr, *d_result = nullptr;
+    int *d_vidx = nullptr, *d_vnum = nullptr, *d_fov = nullptr, *d_xr = nullptr, *d_yr = nullptr,
+        *d_xn = nullptr, *d_yn = nullptr;
+    uint8_t *d_mask = nullptr;
+    MbirTask *d_tasks = nullptr;
+    MbirTaskOut *d_tout = nullptr;
+    char *d_acache = nullptr;
+    size_t acache_bytes = 0;
+    int nparts = 592;
+    int threads = 256;
+    // CUDA events around the ICD kernel launches, on the stage's stream
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
+    double icd_ms = 0;
+    long long launches = 0, icd_launches = 0;
+
+    size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
+    size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
+    size_t nxy() const { return (size_t)st.N_y * st.N_x; }
+    size_t nmag() const { return (size_t)sg.N_time * nblk * nxy(); }
+    int max_views() const
+    {
+        int m = 1;
+        for (auto &v : sg.views) m = std::max<int>(m, (int)v.size());
+        return m;
+    }
+    ~MbirStage()
+    {
+        void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
+                        d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
+                        d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (tev0) cudaEventDestroy(tev0);
+        if (tev1) cudaEventDestroy(tev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Set-up (initStatStructures + initDynStructures, XT_Init.c:211-669)
+// ---------------------------------------------------------------------------
+extern "C" int mbir_init_stage(MbirStage **out, const float *projections, const float *weights,
+                               const float *proj_angles, const float *proj_times,
+                               const float *recon_times, int32_t proj_rows, int32_t proj_cols,
+                               int32_t proj_num, int32_t recon_num, float vox_wid, float rot_center,
+                               float sig_s, float sig_t, float c_s, float c_t, float convg_thresh,
+                               int32_t remove_rings, int32_t quad_convex, float huber_delta,
+                               float huber_T, int32_t mult_xy, int32_t mult_z, int32_t num_z_blocks)
+{
+    *out = nullptr;
+    if (proj_rows <= 0 || proj_cols <= 0 || proj_num <= 0 || recon_num <= 0)
+        return fail("non-positive dimensions");
+    if (mult_xy <= 0 || mult_z <= 0 || proj_cols % mult_xy != 0 || proj_rows % mult_z != 0)
+        return fail("voxel scales (%d, %d) do not divide the detector (%d, %d)", mult_xy, mult_z,
+                    proj_cols, proj_rows);
+    if (remove_rings < 0 || remove_rings > 3) return fail("remove_rings must be 0..3");
+    if (quad_convex < 0 || quad_convex > 1) return fail("quad_convex must be 0 or 1");
+    MbirStage *S = new MbirStage();
+    char err[256];
+    if (scan_geom(S->sg, proj_angles, proj_times, recon_times, proj_rows, proj_cols, proj_num,
+                  recon_num, vox_wid, rot_center, err, sizeof(err))) {
+        delete S;
+        return fail("%s", err);
+    }
+    stage_geom(S->sg, S->st, mult_xy, mult_z, sig_s, sig_t);
+    if (num_z_blocks < 2 || num_z_blocks % 2 || num_z_blocks > std::max(2, S->st.N_z)) {
+        const int nz = S->st.N_z;
+        delete S;
+        return fail("num_z_blocks %d must be even, >= 2 and <= N_z = %d", num_z_blocks, nz);
+    }
+    S->nblk = num_z_blocks;
+    S->offset_type = remove_rings;
+    S->stop_thresh = convg_thresh;
+    S->hT = quad_convex == 0 ? (double)huber_T : 100000.0;
+    S->hdelta = quad_convex == 0 ? (double)huber_delta : 1.0;
+    S->nr.assign((size_t)recon_num * S->nblk, 0);
+    S->nn.assign((size_t)recon_num * S->nblk, 0);
+
+    const ScanGeom &sg = S->sg;
+    const StageGeom &st = S->st;
+    int rc = 0;
+#define CKS(call)                                                                               \
+    do {                                                                                        \
+        cudaError_t _e = (call);                                                                \
+        if (_e != cudaSuccess) {                                                                \
+            rc = fail("%s: %s", #call, cudaGetErrorString(_e));                                 \
+            delete S;                                                                           \
+            return rc;                                                                          \
+        }                                                                                       \
+    } while (0)
+    CKS(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    CKS(cudaEventCreate(&S->ev0));
+    CKS(cudaEventCreate(&S->ev1));
+    CKS(cudaEventCreate(&S->tev0));
+    CKS(cudaEventCreate(&S->tev1));
+    const size_t ns = S->nsino();
+    CKS(dalloc(&S->d_e, ns));
+    CKS(dalloc(&S->d_w, ns));
+    CKS(dalloc(&S->d_y, ns));
+    CKS(dalloc(&S->d_d, (size_t)sg.N_t * sg.N_r));
+    CKS(dalloc(&S->d_x, S->nvox()));
+    CKS(dalloc(&S->d_mag, S->nmag()));
+    CKS(dalloc(&S->d_filt, S->nmag()));
+    CKS(dalloc(&S->d_H, (size_t)sg.N_p * (MBIR_RESP_BINS + 1)));
+    CKS(dalloc(&S->d_cos, sg.N_p));
+    CKS(dalloc(&S->d_sin, sg.N_p));
+    CKS(dalloc(&S->d_num, (size_t)sg.N_t * sg.N_r));
+    CKS(dalloc(&S->d_den, (size_t)sg.N_t * sg.N_r));
+    CKS(dalloc(&S->d_partials, (size_t)4 * S->nparts));
+    CKS(dalloc(&S->d_result, 8));
+    const int mv = S->max_views();
+    CKS(dalloc(&S->d_vidx, (size_t)recon_num * mv));
+    CKS(dalloc(&S->d_vnum, recon_num));
+    CKS(dalloc(&S->d_fov, sg.N_p));
+    CKS(dalloc(&S->d_xr, S->nmag()));
+    CKS(dalloc(&S->d_yr, S->nmag()));
+    CKS(dalloc(&S->d_xn, S->nmag()));
+    CKS(dalloc(&S->d_yn, S->nmag()));
+    CKS(dalloc(&S->d_mask, S->nxy()));
+    CKS(dalloc(&S->d_tasks, (size_t)recon_num * S->nblk));
+    CKS(dalloc(&S->d_tout, (size_t)recon_num * S->nblk));
+    // per-task A-column cache: views x entries x (double value + int bin) + counts
+    const int amax = mbir_amax(st.delta_xy, sg.delta_r);
+    S->acache_bytes = (size_t)mv * amax * (sizeof(double) + sizeof(int)) + (size_t)mv * sizeof(int);
+    S->acache_bytes = (S->acache_bytes + 255) & ~(size_t)255;
+    if (S->acache_bytes > 160 * 1024)
+        CKS(cudaMalloc((void **)&S->d_acache, S->acache_bytes * (size_t)recon_num * (S->nblk / 2)));
+    S->threads = mv <= 64 ? 64 : (mv <= 128 ? 128 : 256);
+
+    // upload inputs: reference layout [view][row][col] -> device [row][view][col]
+    {
+        std::vector<float> ty(ns), tw(ns);
+        for (int p = 0; p < sg.N_p; p++)
+            for (int t = 0; t < sg.N_t; t++)
+                for (int r = 0; r < sg.N_r; r++) {
+                    const size_t src = ((size_t)p * sg.N_t + t) * sg.N_r + r;
+                    const size_t dst = ((size_t)t * sg.N_p + p) * sg.N_r + r;
+                    ty[dst] = projections[src];
+                    tw[dst] = weights[src] / S->var_est;
+                }
+        CKS(cudaMemcpy(S->d_y, ty.data(), ns * sizeof(float), cudaMemcpyHostToDevice));
+        CKS(cudaMemcpy(S->d_w, tw.data(), ns * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    CKS(cudaMemset(S->d_d, 0, (size_t)sg.N_t * sg.N_r * sizeof(float)));
+    CKS(cudaMemset(S->d_x, 0, S->nvox() * sizeof(float)));
+    CKS(cudaMemset(S->d_mag, 0, S->nmag() * sizeof(float)));
+    CKS(cudaMemcpy(S->d_cos, sg.cosv.data(), sg.N_p * sizeof(double), cudaMemcpyHostToDevice));
+    CKS(cudaMemcpy(S->d_sin, sg.sinv.data(), sg.N_p * sizeof(double), cudaMemcpyHostToDevice));
+    {
+        std::vector<int> vidx((size_t)recon_num * mv, 0), vnum(recon_num);
+        for (int i = 0; i < recon_num; i++) {
+            vnum[i] = (int)sg.views[i].size();
+            std::copy(sg.views[i].begin(), sg.views[i].end(), vidx.begin() + (size_t)i * mv);
+        }
+        CKS(cudaMemcpy(S->d_vidx, vidx.data(), vidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CKS(cudaMemcpy(S->d_vnum, vnum.data(), vnum.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CKS(cudaMemcpy(S->d_fov, sg.frame_of_view.data(), sg.N_p * sizeof(int), cudaMemcpyHostToDevice));
+    }
+#undef CKS
+    // device-side views of the geometry and prior
+    MbirGeom &g = S->g;
+    g.N_p = sg.N_p; g.N_r = sg.N_r; g.N_t = sg.N_t; g.m_z = st.m_z;
+    g.delta_r = sg.delta_r; g.R0 = sg.R0; g.RMax = sg.RMax; g.OffsetR = st.OffsetR;
+    g.N_x = st.N_x; g.N_y = st.N_y; g.N_z = st.N_z; g.N_time = sg.N_time;
+    g.x0 = st.x0; g.y0 = sg.y0; g.delta_xy = st.delta_xy;
+    g.max_views = mv; g.view_idx = S->d_vidx; g.view_num = S->d_vnum;
+    g.cosv = S->d_cos; g.sinv = S->d_sin; g.H_r = S->d_H;
+    MbirPrior &pr = S->pr;
+    pr.sSQ = st.sSQ; pr.sSQP = st.sSQP; pr.sTQ = st.sTQ; pr.sTQP = st.sTQP;
+    pr.c_s = c_s; pr.c_t = c_t;
+    std::copy(st.SF, st.SF + 27, pr.SF);
+    pr.TF = st.TF; pr.alpha = 1.5; pr.hT = S->hT; pr.hdelta = S->hdelta;
+    S->dv.e = S->d_e; S->dv.w = S->d_w; S->dv.d = S->d_d; S->dv.x = S->d_x; S->dv.mag = S->d_mag;
+    S->dv.mask = S->d_mask;
+    *out = S;
+    return 0;
+}
+
+extern "C" void mbir_free_stage(MbirStage *S) { delete S; }
+
+extern "C" const char *mbir_last_error(void) { return g_err; }
+
+// Per-stage switches (XT_Init.c:236-266) and the variance estimate carried
+// from the previous stage; weights are rescaled as at XT_Init.c:327-330.
+extern "C" int mbir_set_stage_switches(MbirStage *S, int32_t update_proj_offset, int32_t update_var,
+                                       double var_est)
+{
+    S->upd_offset = update_proj_offset;
+    S->upd_var = update_var;
+    if (var_est > 0 && var_est != S->var_est) {
+        std::vector<float> w(S->nsino());
+        CK(cudaMemcpy(w.data(), S->d_w, w.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (auto &v : w) v = (float)(v * S->var_est);
+        for (auto &v : w) v /= var_est;
+        S->var_est = var_est;
+        CK(cudaMemcpy(S->d_w, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+extern "C" int mbir_set_rng_state(MbirStage *S, uint32_t state)
+{
+    S->rng.state = state;
+    return 0;
+}
+
+extern "C" uint32_t mbir_get_rng_state(MbirStage *S) { return S->rng.state; }
+
+// Stage prologue of ICD_BackProject (XT_ICD_update.c:1134-1159): mask,
+// detector response, initial object (zero unless given, [N_time][N_z][N_y][N_x]),
+// ring offsets (zero unless given, [N_r][N_t] as the reference stores them),
+// update-magnitude map (zero unless given) and the error sinogram.
+extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *offset,
+                                const float *magmap)
+{
+    const ScanGeom &sg = S->sg;
+    detector_response(sg, S->st, S->H_r);
+    object_mask(sg, S->st, S->mask);
+    CK(cudaMemcpy(S->d_H, S->H_r.data(), S->H_r.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice));
+    if (object)
+        CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
+    if (offset) {
+        std::vector<float> d((size_t)sg.N_t * sg.N_r);
+        for (int r = 0; r < sg.N_r; r++)
+            for (int t = 0; t < sg.N_t; t++) d[(size_t)t * sg.N_r + r] = offset[(size_t)r * sg.N_t + t];
+        CK(cudaMemcpy(S->d_d, d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (magmap)
+        CK(cudaMemcpy(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(mbir_launch_forward(S->g, S->d_x, S->d_fov, S->d_y, S->d_d, S->d_e, 0, S->stream));
+    S->launches++;
+    CK(cudaStreamSynchronize(S->stream));
+    S->prepared = 1;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Reference schedule (updateVoxelsTimeSlices, XT_ICD_update.c:936-1105)
+// ---------------------------------------------------------------------------
+static int run_half(MbirStage *S, int j, int second, int nhicd, int iter, double *vox_mag)
+{
+    const int per = S->st.N_z / S->nblk;
+    std::vector<MbirTask> tasks;
+    for (int i = 0; i < S->sg.N_time; i++)
+        for (int b = 0; b < S->nblk; b += 2) {
+            const int idx = second ? ((i % 2 == 0) ? b + 1 : b) : ((i % 2 == 0) ? b : b + 1);
+            MbirTask t{};
+            t.frame = i;
+            t.z0 = idx * per;
+            t.z1 = (idx >= S->nblk - 1) ? S->st.N_z - 1 : (idx + 1) * per - 1;
+            const size_t plane = ((size_t)i * S->nblk + idx);
+            t.mag = S->d_mag + plane * S->nxy();
+            if (!nhicd) {
+                const int num = S->nr[plane];
+                t.b0 = j * (num / S->K);
+                t.b1 = (j == S->K - 1) ? num - 1 : (j + 1) * (num / S->K) - 1;
+                t.xs = S->d_xr + plane * S->nxy();
+                t.ys = S->d_yr + plane * S->nxy();
+            } else {
+                t.b0 = 0;
+                t.b1 = S->nn[plane] - 1;
+                t.xs = S->d_xn + plane * S->nxy();
+                t.ys = S->d_yn + plane * S->nxy();
+            }
+            if (t.b1 >= t.b0) tasks.push_back(t);
+        }
+    if (tasks.empty()) return 0;
+    CK(cudaMemcpyAsync(S->d_tasks, tasks.data(), tasks.size() * sizeof(MbirTask), cudaMemcpyHostToDevice,
+                       S->stream));
+    CK(cudaEventRecord(S->ev0, S->stream));
+    CK(mbir_launch_icd_ref(S->g, S->pr, S->dv, S->d_tasks, (int)tasks.size(), S->d_tout, iter,
+                           S->threads, S->acache_bytes, S->d_acache, S->stream));
+    CK(cudaEventRecord(S->ev1, S->stream));
+    S->launches++;
+    S->icd_launches++;
+    std::vector<MbirTaskOut> out(tasks.size());
+    CK(cudaMemcpyAsync(out.data(), S->d_tout, out.size() * sizeof(MbirTaskOut), cudaMemcpyDeviceToHost,
+                       S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+    S->icd_ms += ms;
+    for (auto &o : out) {
+        *vox_mag += o.vox_mag;
+        S->updates += o.updates;
+        S->zero_skips += o.zero_skips;
+    }
+    return 0;
+}
+
+extern "C" int mbir_update_sinogram_offset(MbirStage *S)
+{
+    CK(mbir_launch_offset(S->g, S->pr, S->dv, S->offset_type, S->d_num, S->d_den, S->d_partials,
+                          S->nparts, S->stream));
+    S->launches += 3;
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
+extern "C" int mbir_update_variance_parameter(MbirStage *S)
+{
+    CK(mbir_launch_variance(S->g, S->pr, S->dv, S->var_est, S->d_partials, S->nparts, S->d_result,
+                            S->stream));
+    S->launches += 3;
+    double sum = 0;
+    CK(cudaMemcpyAsync(&sum, S->d_result, sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    S->var_est = sum / ((double)1 * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t);
+    CK(mbir_launch_variance_apply(S->g, S->dv, S->var_est, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
+// NHICD line selection (VSC_based_Voxel_Line_Select, XT_NHICD.c:164-216):
+// filter on the GPU, order statistic and raster-order selection on the host
+// so that the generator's draws follow the reference's.
+static int vsc_select(MbirStage *S)
+{
+    const int planes = S->sg.N_time * S->nblk;
+    const size_t nxy = S->nxy();
+    CK(mbir_launch_vsc_filter(S->d_mag, S->d_filt, planes, S->st.N_y, S->st.N_x, S->stream));
+    S->launches++;
+    std::vector<float> f((size_t)planes * nxy), work(nxy);
+    CK(cudaMemcpyAsync(f.data(), S->d_filt, f.size() * sizeof(float), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    std::vector<int> xs((size_t)planes * nxy), ys((size_t)planes * nxy);
+    for (int pl = 0; pl < planes; pl++) {
+        const float *fc = &f[(size_t)pl * nxy];
+        std::copy(fc, fc + nxy, work.begin());
+        const int n = S->nr[pl] / S->K;
+        const double th = order_statistic(S->rng, work.data(), (uint32_t)nxy, (uint32_t)(nxy - n));
+        int cnt = 0;
+        for (size_t q = 0; q < nxy; q++)
+            if (fc[q] > th) {
+                xs[(size_t)pl * nxy + cnt] = (int)(q % S->st.N_x);
+                ys[(size_t)pl * nxy + cnt] = (int)(q / S->st.N_x);
+                cnt++;
+            }
+        S->nn[pl] = cnt;
+    }
+    CK(cudaMemcpyAsync(S->d_xn, xs.data(), xs.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->d_yn, ys.data(), ys.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
+static int random_select(MbirStage *S)
+{
+    const int planes = S->sg.N_time * S->nblk;
+    const size_t nxy = S->nxy();
+    std::vector<int> xs((size_t)planes * nxy), ys((size_t)planes * nxy);
+    const int per = S->st.N_z / S->nblk;
+    for (int pl = 0; pl < planes; pl++)
+        S->nr[pl] = random_lines(S->rng, S->mask.data(), S->st.N_y, S->st.N_x, per, &xs[(size_t)pl * nxy],
+                                 &ys[(size_t)pl * nxy]);
+    CK(cudaMemcpyAsync(S->d_xr, xs.data(), xs.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->d_yr, ys.data(), ys.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
+extern "C" int mbir_update_voxels_time_slices(MbirStage *S, int32_t iter, int32_t *converged)
+{
+    if (!S->prepared) return fail("mbir_icd_prepare has not run");
+    if (random_select(S)) return -1;
+    double vox = 0;
+    for (int j = 0; j < S->K; j++) {
+        vox = 0;
+        if (run_half(S, j, 0, 0, iter, &vox)) return -1;
+        if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+        if (run_half(S, j, 1, 0, iter, &vox)) return -1;
+        if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+        if (vsc_select(S)) return -1;
+        if (iter > 1) {
+            double unused = 0;
+            if (run_half(S, j, 0, 1, iter, &unused)) return -1;
+            if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+            if (run_half(S, j, 1, 1, iter, &unused)) return -1;
+            if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+        }
+    }
+    if (S->upd_var == 1 && mbir_update_variance_parameter(S)) return -1;
+    // convergence (XT_ICD_update.c:1066-1103): summed last-visit magnitudes of
+    // the HICD lines over the summed |x'| of the last sub-iteration's HICD updates
+    std::vector<float> mag(S->nmag());
+    std::vector<int> xs(S->nmag()), ys(S->nmag());
+    CK(cudaMemcpy(mag.data(), S->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(xs.data(), S->d_xr, xs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ys.data(), S->d_yr, ys.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    double avg = 0;
+    const size_t nxy = S->nxy();
+    for (int pl = 0; pl < S->sg.N_time * S->nblk; pl++)
+        for (int q = 0; q < S->nr[pl]; q++)
+            avg += mag[(size_t)pl * nxy + (size_t)ys[(size_t)pl * nxy + q] * S->st.N_x + xs[(size_t)pl * nxy + q]];
+    S->last_pct = 100 * avg / vox;
+    *converged = S->last_pct < S->stop_thresh ? 1 : 0;
+    return 0;
+}
+
+// MAP cost (computeCost, XT_ICD_update.c:186-319) in FP64.
+extern "C" int mbir_compute_cost(MbirStage *S, double *total, double *forward, double *prior)
+{
+    CK(mbir_launch_cost(S->g, S->pr, S->dv, S->d_partials, S->nparts, S->d_result, S->stream));
+    S->launches += 2;
+    double r[2];
+    CK(cudaMemcpyAsync(r, S->d_result, sizeof(r), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    const double data = r[0] / 2.0;
+    const double fw = data + (double)1 * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t *
+                                 log(S->var_est) / 2;
+    if (forward) *forward = fw;
+    if (prior) *prior = r[1];
+    if (total) *total = fw + r[1];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// State access
+// ---------------------------------------------------------------------------
+extern "C" int mbir_stage_dims(MbirStage *S, int32_t *d)
+{
+    d[0] = S->sg.N_p; d[1] = S->sg.N_r; d[2] = S->sg.N_t; d[3] = S->st.N_x; d[4] = S->st.N_y;
+    d[5] = S->st.N_z; d[6] = S->sg.N_time; d[7] = S->nblk; d[8] = S->st.m_z;
+    return 0;
+}
+
+extern "C" int mbir_get_object(MbirStage *S, float *out)
+{
+    CK(cudaMemcpy(out, S->d_x, S->nvox() * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int mbir_set_object(MbirStage *S, const float *in)
+{
+    CK(cudaMemcpy(S->d_x, in, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// Sinogram-shaped arrays come back in the reference's [view][col][row] layout.
+static int get_sino(MbirStage *S, const float *dev, float *out)
+{
+    const ScanGeom &sg = S->sg;
+    std::vector<float> tmp(S->nsino());
+    CK(cudaMemcpy(tmp.data(), dev, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < sg.N_t; t++)
+        for (int p = 0; p < sg.N_p; p++)
+            for (int r = 0; r < sg.N_r; r++)
+                out[((size_t)p * sg.N_r + r) * sg.N_t + t] = tmp[((size_t)t * sg.N_p + p) * sg.N_r + r];
+    return 0;
+}
+
+extern "C" int mbir_get_errorsino(MbirStage *S, float *out) { return get_sino(S, S->d_e, out); }
+extern "C" int mbir_get_weight(MbirStage *S, float *out) { return get_sino(S, S->d_w, out); }
+
+extern "C" int mbir_get_offset(MbirStage *S, float *out)
+{
+    const ScanGeom &sg = S->sg;
+    std::vector<float> d((size_t)sg.N_t * sg.N_r);
+    CK(cudaMemcpy(d.data(), S->d_d, d.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < sg.N_r; r++)
+        for (int t = 0; t < sg.N_t; t++) out[(size_t)r * sg.N_t + t] = d[(size_t)t * sg.N_r + r];
+    return 0;
+}
+
+extern "C" int mbir_get_magmap(MbirStage *S, float *out)
+{
+    CK(cudaMemcpy(out, S->d_mag, S->nmag() * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int mbir_get_hr(MbirStage *S, float *out)
+{
+    std::copy(S->H_r.begin(), S->H_r.end(), out);
+    return 0;
+}
+
+extern "C" int mbir_get_mask(MbirStage *S, uint8_t *out)
+{
+    std::copy(S->mask.begin(), S->mask.end(), out);
+    return 0;
+}
+
+extern "C" int mbir_get_lines(MbirStage *S, int32_t kind, int32_t frame, int32_t block, int32_t *xs,
+                              int32_t *ys)
+{
+    const size_t plane = (size_t)frame * S->nblk + block;
+    const int n = kind == 0 ? S->nr[plane] : S->nn[plane];
+    const int *dx = (kind == 0 ? S->d_xr : S->d_xn) + plane * S->nxy();
+    const int *dy = (kind == 0 ? S->d_yr : S->d_yn) + plane * S->nxy();
+    if (n > 0) {
+        CK(cudaMemcpy(xs, dx, n * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(ys, dy, n * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    return n;
+}
+
+extern "C" double mbir_get_var_est(MbirStage *S) { return S->var_est; }
+extern "C" double mbir_get_update_percentage(MbirStage *S) { return S->last_pct; }
+extern "C" long long mbir_get_update_count(MbirStage *S) { return S->updates; }
+
+// Device-side clock around a span of stage calls: events recorded on the
+// stage's stream (all stage calls are synchronous, so the span covers them).
+extern "C" int mbir_time_begin(MbirStage *S)
+{
+    CK(cudaStreamSynchronize(S->stream));
+    CK(cudaEventRecord(S->tev0, S->stream));
+    return 0;
+}
+
+extern "C" int mbir_time_end(MbirStage *S, double *ms)
+{
+    CK(cudaEventRecord(S->tev1, S->stream));
+    CK(cudaEventSynchronize(S->tev1));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, S->tev0, S->tev1));
+    *ms = f;
+    return 0;
+}
+
+// Device time of the ICD update kernels (CUDA events on the stage's stream)
+// and the number of kernels this stage has launched.
+extern "C" int mbir_get_kernel_stats(MbirStage *S, double *icd_ms, long long *icd_launches,
+                                     long long *launches)
+{
+    if (icd_ms) *icd_ms = S->icd_ms;
+    if (icd_launches) *icd_launches = S->icd_launches;
+    if (launches) *launches = S->launches;
+    return 0;
+}
+
+// Forward projection A x of an object [N_time][N_z][N_y][N_x] into a
+// sinogram [view][row][col] (the layout reconstruct() takes), with this
+// stage's geometry.  Used to synthesise scans of voxelised phantoms.
+extern "C" int mbir_forward_project(MbirStage *S, const float *object, float *out)
+{
+    if (S->H_r.empty()) {
+        detector_response(S->sg, S->st, S->H_r);
+        CK(cudaMemcpy(S->d_H, S->H_r.data(), S->H_r.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(mbir_launch_forward(S->g, S->d_x, S->d_fov, nullptr, nullptr, S->d_e, 1, S->stream));
+    S->launches++;
+    CK(cudaStreamSynchronize(S->stream));
+    const ScanGeom &sg = S->sg;
+    std::vector<float> tmp(S->nsino());
+    CK(cudaMemcpy(tmp.data(), S->d_e, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < sg.N_t; t++)
+        for (int p = 0; p < sg.N_p; p++)
+            for (int r = 0; r < sg.N_r; r++)
+                out[((size_t)p * sg.N_t + t) * sg.N_r + r] = tmp[((size_t)t * sg.N_p + p) * sg.N_r + r];
+    return 0;
+}
