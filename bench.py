@@ -228,7 +228,10 @@ def gpu_arm(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     scan = make_scan(rank)
     coarse, fine = coarse_start(scan)
+    sched = 1 if args.schedule == "sv" else 0
     st = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+    st.set_schedule(sched, args.sv_side)
+    sched_info = st.schedule_info()
     st.prepare(fine)
     for it in range(1, args.warmup + 1):
         st.iterate(it)
@@ -275,6 +278,7 @@ def gpu_arm(args, rank, world, local_rank):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
         s2 = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+        s2.set_schedule(sched, args.sv_side)
         s2.prepare(fine)
         s2.iterate(1)
         _ = s2.object()
@@ -310,15 +314,16 @@ def gpu_arm(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 theta, prior and update)",
         "data": "synthetic (seeded random-ellipsoid phantom, Poisson counts)",
         "config": {"workload": WORKLOAD, "volume": [CFG["rows"], CFG["n_xy"], CFG["n_xy"]],
-                   "views": CFG["views"], "schedule": "reference (checkerboard z-blocks)",
-                   "z_blocks": CFG["rows"], "parallelism": f"replicas x{world}",
+                   "views": CFG["views"],
+                   "schedule": ("super-voxel" if sched else "reference (checkerboard z-blocks)"),
+                   "schedule_info": sched_info, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None,
                      "bytes_per_update": b_vu, "mean_bins_per_view": cbar,
-                     "kernel": "k_icd_ref", "kernel_ms": icd_ms,
+                     "kernel": "k_icd_sv" if sched else "k_icd_ref", "kernel_ms": icd_ms,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "gpu_launches": int(n_all1 - n_all0),
         "clocks": clk.summary(),
@@ -356,6 +361,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
+    ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -70,6 +70,20 @@ uint32_t mbir_get_rng_state(MbirStage *stage);
 int mbir_icd_prepare(MbirStage *stage, const float *object, const float *offset,
                      const float *magmap);
 
+/* Voxel-update schedule of mbir_update_voxels_time_slices:
+ *   0  the reference's (default): checkerboard (frame, z-block) tasks, random
+ *      line order, 10 HICD/NHICD sub-iterations, exactly as
+ *      updateVoxelsTimeSlices (XT_ICD_update.c:936-1105);
+ *   1  super-voxel schedule (no reference counterpart): sv_side x sv_side
+ *      blocks of voxel lines updated by one CTA each from a shared-memory copy
+ *      of the error-sinogram band they touch, blocks of one colour of a
+ *      (x, y, z-group, frame) checkerboard in parallel.  sv_side 0 picks the
+ *      largest side (<= 16) whose band fits shared memory.
+ * The magnitude map of schedule 1 has one plane per (frame, z-group). */
+int mbir_set_schedule(MbirStage *stage, int32_t schedule, int32_t sv_side);
+int mbir_get_schedule(MbirStage *stage, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
+                      int32_t *band_width, int32_t *phases);
+
 /* One outer ICD iteration with the reference schedule
  * (updateVoxelsTimeSlices, XT_ICD_update.c:936-1105): random line order,
  * 10 sub-iterations of checkerboard HICD half-sweeps with ring-offset updates,

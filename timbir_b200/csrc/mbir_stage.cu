@@ -17,6 +17,7 @@
 #include "../../include/timbir_b200.h"
 #include "mbir_host.h"
 #include "mbir_internal.h"
+#include "mbir_sv.h"
 
 using namespace mbir;
 
@@ -76,6 +77,18 @@ struct MbirStage {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
     double icd_ms = 0;
     long long launches = 0, icd_launches = 0;
+    // super-voxel schedule
+    int schedule = 0;  // 0: reference schedule, 1: super-voxel schedule
+    SvParams sp{};
+    int nzg = 1, gz = 1;
+    std::vector<std::vector<SvTask>> sv_phase;  // tasks of each colour phase
+    std::vector<SvTask> sv_all;                 // every task, with its phase
+    std::vector<int> sv_all_phase;
+    SvTask *d_sv_tasks = nullptr;
+    SvTaskOut *d_sv_out = nullptr;
+    float *d_scratch = nullptr;
+    int *d_err = nullptr;
+    double nh_fraction = 0.2;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
     size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
@@ -91,7 +104,8 @@ struct MbirStage {
     {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
-                        d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache};
+                        d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
+                        d_sv_tasks, d_sv_out, d_scratch, d_err};
         for (void *b : bufs)
             if (b) cudaFree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -426,9 +440,229 @@ static int random_select(MbirStage *S)
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Super-voxel schedule
+// ---------------------------------------------------------------------------
+static SvParams sv_params(const MbirStage *S, int side, int nz)
+{
+    SvParams sp{};
+    const double m = S->st.delta_xy / S->sg.delta_r;
+    sp.S = side;
+    // band width: projected extent of the block plus each voxel's footprint
+    // (+-delta_xy) plus floor effects at both ends
+    sp.W = (int)floor((side - 1) * sqrt(2.0) * m + 2 * m + 1e-9) + 3;
+    sp.amax = 2 * (int)ceil(m) + 1;
+    sp.max_views = S->max_views();
+    sp.max_nz = nz;
+    sp.max_rows = nz * S->st.m_z;
+    sp.band_floats = (size_t)sp.max_rows * sp.W * sp.max_views;
+    return sp;
+}
+
+static const size_t kSmemLimit = 227 * 1024;
+
+// Super-voxel side 0 = choose the largest side (<= 16) whose band for a
+// z-group of min(N_z, 32) slices fits shared memory, shrinking the group if
+// even side 4 does not fit.
+extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side)
+{
+    if (schedule == 0) {
+        S->schedule = 0;
+        return 0;
+    }
+    if (schedule != 1) return fail("unknown schedule %d", schedule);
+    const int Nz = S->st.N_z;
+    int gz = std::min(Nz, 32), side = sv_side;
+    SvParams sp{};
+    for (;;) {
+        if (side > 0) {
+            sp = sv_params(S, side, gz);
+            if (mbir_sv_smem_bytes(sp) <= kSmemLimit) break;
+        } else {
+            int best = 0;
+            for (int s = 16; s >= 4; s--) {
+                sp = sv_params(S, s, gz);
+                if (mbir_sv_smem_bytes(sp) <= kSmemLimit) {
+                    best = s;
+                    break;
+                }
+            }
+            if (best) {
+                sp = sv_params(S, best, gz);
+                break;
+            }
+        }
+        if (gz == 1) return fail("no super-voxel configuration fits shared memory");
+        gz = std::max(1, gz / 2);
+    }
+    S->sp = sp;
+    S->gz = gz;
+    S->nzg = (Nz + gz - 1) / gz;
+    // the magnitude map holds one plane per (frame, z-group)
+    if (S->nzg != S->nblk) {
+        cudaFree(S->d_mag);
+        cudaFree(S->d_filt);
+        S->d_mag = S->d_filt = nullptr;
+        S->nblk = S->nzg;
+        CK(dalloc(&S->d_mag, S->nmag()));
+        CK(dalloc(&S->d_filt, S->nmag()));
+        CK(cudaMemset(S->d_mag, 0, S->nmag() * sizeof(float)));
+        S->dv.mag = S->d_mag;
+        S->nr.assign((size_t)S->sg.N_time * S->nblk, 0);
+        S->nn.assign((size_t)S->sg.N_time * S->nblk, 0);
+    }
+    // tasks by colour: SV x / y parity, z-group parity, frame parity
+    if (S->mask.empty()) object_mask(S->sg, S->st, S->mask);
+    const int side_ = sp.S, N_x = S->st.N_x, N_y = S->st.N_y;
+    const int ntx = (N_x + side_ - 1) / side_, nty = (N_y + side_ - 1) / side_;
+    std::vector<int> phase_of(16, -1);
+    int nphase = 0;
+    S->sv_all.clear();
+    S->sv_all_phase.clear();
+    for (int i = 0; i < S->sg.N_time; i++)
+        for (int zg = 0; zg < S->nzg; zg++)
+            for (int ty = 0; ty < nty; ty++)
+                for (int tx = 0; tx < ntx; tx++) {
+                    const int k0 = tx * side_, j0 = ty * side_;
+                    bool any = false;
+                    for (int y = j0; y < std::min(N_y, j0 + side_) && !any; y++)
+                        for (int x = k0; x < std::min(N_x, k0 + side_); x++)
+                            if (S->mask[(size_t)y * N_x + x]) {
+                                any = true;
+                                break;
+                            }
+                    if (!any) continue;
+                    const int colour = (tx & 1) | ((ty & 1) << 1) | ((S->nzg > 1 ? (zg & 1) : 0) << 2) |
+                                       ((S->sg.N_time > 1 ? (i & 1) : 0) << 3);
+                    if (phase_of[colour] < 0) phase_of[colour] = nphase++;
+                    SvTask t{};
+                    t.frame = i;
+                    t.k0 = k0;
+                    t.j0 = j0;
+                    t.z0 = zg * gz;
+                    t.nz = std::min(gz, Nz - t.z0);
+                    t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
+                    S->sv_all.push_back(t);
+                    S->sv_all_phase.push_back(phase_of[colour]);
+                }
+    S->sv_phase.assign(nphase, {});
+    for (size_t q = 0; q < S->sv_all.size(); q++) S->sv_phase[S->sv_all_phase[q]].push_back(S->sv_all[q]);
+    size_t maxt = 1;
+    for (auto &ph : S->sv_phase) maxt = std::max(maxt, ph.size());
+    cudaFree(S->d_sv_tasks);
+    cudaFree(S->d_sv_out);
+    cudaFree(S->d_scratch);
+    S->d_sv_tasks = nullptr;
+    S->d_sv_out = nullptr;
+    S->d_scratch = nullptr;
+    CK(dalloc(&S->d_sv_tasks, maxt));
+    CK(dalloc(&S->d_sv_out, maxt));
+    CK(dalloc(&S->d_scratch, maxt * sp.band_floats));
+    if (!S->d_err) CK(dalloc(&S->d_err, 1));
+    CK(cudaMemset(S->d_err, 0, sizeof(int)));
+    S->schedule = 1;
+    return 0;
+}
+
+extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
+                                 int32_t *band_width, int32_t *phases)
+{
+    if (schedule) *schedule = S->schedule;
+    if (sv_side) *sv_side = S->sp.S;
+    if (z_group) *z_group = S->gz;
+    if (band_width) *band_width = S->sp.W;
+    if (phases) *phases = (int)S->sv_phase.size();
+    return 0;
+}
+
+static int sv_launch(MbirStage *S, const std::vector<SvTask> &tasks, int iter, uint32_t seed, double *dx,
+                     double *ax)
+{
+    if (tasks.empty()) return 0;
+    CK(cudaMemcpyAsync(S->d_sv_tasks, tasks.data(), tasks.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
+                       S->stream));
+    CK(cudaEventRecord(S->ev0, S->stream));
+    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, S->d_sv_tasks, (int)tasks.size(), S->d_scratch,
+                          S->d_sv_out, iter, seed, S->d_err, S->stream));
+    CK(cudaEventRecord(S->ev1, S->stream));
+    S->launches++;
+    S->icd_launches++;
+    std::vector<SvTaskOut> out(tasks.size());
+    CK(cudaMemcpyAsync(out.data(), S->d_sv_out, out.size() * sizeof(SvTaskOut), cudaMemcpyDeviceToHost,
+                       S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+    S->icd_ms += ms;
+    for (auto &o : out) {
+        *dx += o.sum_abs_dx;
+        *ax += o.sum_abs_x;
+        S->updates += o.updates;
+        S->zero_skips += o.zero_skips;
+    }
+    return 0;
+}
+
+// One outer iteration of the super-voxel schedule: a sweep over every SV,
+// colour phase by colour phase (phase order rotates with the iteration), a
+// ring-offset update, then (from the second iteration) a non-homogeneous pass
+// over the SVs whose lines changed most in the sweep, another ring-offset
+// update, and the variance update.  Convergence uses the reference's
+// criterion, with the ratio of summed |dx| to summed |x'| over the sweep
+// scaled by its 10 sub-iterations (XT_ICD_update.c:1066-1103).
+static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
+{
+    const int P = (int)S->sv_phase.size();
+    double dx = 0, ax = 0;
+    for (int q = 0; q < P; q++) {
+        const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
+        if (sv_launch(S, S->sv_phase[(q + iter) % P], iter, seed, &dx, &ax)) return -1;
+    }
+    if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+    const double hicd_dx = dx, hicd_ax = ax;
+    if (iter > 1 && S->nh_fraction > 0) {
+        // score = summed last-visit magnitude over the SV's lines
+        std::vector<float> mag(S->nmag());
+        CK(cudaMemcpy(mag.data(), S->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        const int side = S->sp.S, N_x = S->st.N_x, N_y = S->st.N_y;
+        std::vector<std::pair<float, int>> score(S->sv_all.size());
+        for (size_t q = 0; q < S->sv_all.size(); q++) {
+            const SvTask &t = S->sv_all[q];
+            const float *pl = mag.data() + ((size_t)t.frame * S->nzg + t.z0 / S->gz) * S->nxy();
+            double s = 0;
+            for (int y = t.j0; y < std::min(N_y, t.j0 + side); y++)
+                for (int x = t.k0; x < std::min(N_x, t.k0 + side); x++) s += pl[(size_t)y * N_x + x];
+            score[q] = {(float)s, (int)q};
+        }
+        const size_t nsel = (size_t)std::ceil(S->nh_fraction * score.size());
+        std::partial_sort(score.begin(), score.begin() + nsel, score.end(),
+                          [](const std::pair<float, int> &a, const std::pair<float, int> &b) { return a.first > b.first; });
+        std::vector<std::vector<SvTask>> sel(P);
+        for (size_t q = 0; q < nsel; q++) {
+            if (score[q].first <= 0) break;
+            const int id = score[q].second;
+            sel[S->sv_all_phase[id]].push_back(S->sv_all[id]);
+        }
+        double ndx = 0, nax = 0;
+        for (int q = 0; q < P; q++) {
+            const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
+            if (sv_launch(S, sel[(q + iter) % P], iter, seed, &ndx, &nax)) return -1;
+        }
+        if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+    }
+    if (S->upd_var == 1 && mbir_update_variance_parameter(S)) return -1;
+    int err = 0;
+    CK(cudaMemcpy(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
+    S->last_pct = hicd_ax > 0 ? 100.0 * S->K * hicd_dx / hicd_ax : 0.0;
+    *converged = S->last_pct < S->stop_thresh ? 1 : 0;
+    return 0;
+}
+
 extern "C" int mbir_update_voxels_time_slices(MbirStage *S, int32_t iter, int32_t *converged)
 {
     if (!S->prepared) return fail("mbir_icd_prepare has not run");
+    if (S->schedule == 1) return sv_iterate(S, iter, converged);
     if (random_select(S)) return -1;
     double vox = 0;
     for (int j = 0; j < S->K; j++) {
