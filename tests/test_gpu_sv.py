@@ -58,7 +58,7 @@ def test_sv_side_does_not_change_the_map(side):
     s = sv_stage("plain", side)
     assert s.schedule_info()["sv_side"] == side
     s.prepare()
-    for it in range(1, 201):
+    for it in range(1, 301):
         s.iterate(it)
     c = fresh_cost_fp64("plain", s.object())
     assert abs(c - float(g["ref_fresh_cost"])) / float(g["ref_fresh_cost"]) < 1e-5
@@ -89,3 +89,22 @@ def test_sv_decreases_cost(name):
     c5 = s.cost()[0]
     assert np.isfinite(c5) and c5 < c0
     assert s.update_count() > 0
+
+
+def test_sv_one_warp_per_slice_for_tall_groups():
+    # 16 slices in one z-group: one warp per slice (two only up to 15)
+    from timbir_b200 import synth
+    scan = synth.ellipsoid_scan(32, 16, 48, seed=21)
+    kw = dict(scenarios.BASE)
+    s = timbir_b200.Stage(scan, blocks=2, **kw)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0)
+    assert s.schedule_info()["z_group"] == 16
+    s.prepare()
+    c0 = s.cost()[0]
+    for it in range(1, 11):
+        s.iterate(it)
+    assert s.cost()[0] < c0
+    f = timbir_b200.Stage(scan, blocks=2, **kw)
+    f.prepare(s.object(), s.offset())
+    scale = np.abs(f.errorsino()).max()
+    assert np.abs(s.errorsino() - f.errorsino()).max() < 2e-5 * scale

@@ -87,7 +87,8 @@ struct MbirStage {
     SvTask *d_sv_tasks = nullptr;
     SvTaskOut *d_sv_out = nullptr;
     float *d_scratch = nullptr;
-    int *d_err = nullptr;
+    int *d_err = nullptr, *d_queue = nullptr;
+    int sm_count = 148;
     double nh_fraction = 0.2;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
@@ -105,7 +106,7 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_tasks, d_sv_out, d_scratch, d_err};
+                        d_sv_tasks, d_sv_out, d_scratch, d_err, d_queue};
         for (void *b : bufs)
             if (b) cudaFree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -455,6 +456,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz)
     sp.max_views = S->max_views();
     sp.max_nz = nz;
     sp.max_rows = nz * S->st.m_z;
+    sp.vsplit = nz <= 15 ? 2 : 1;
     sp.band_floats = (size_t)sp.max_rows * sp.W * sp.max_views;
     return sp;
 }
@@ -524,14 +526,11 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
             for (int ty = 0; ty < nty; ty++)
                 for (int tx = 0; tx < ntx; tx++) {
                     const int k0 = tx * side_, j0 = ty * side_;
-                    bool any = false;
-                    for (int y = j0; y < std::min(N_y, j0 + side_) && !any; y++)
+                    int lines = 0;
+                    for (int y = j0; y < std::min(N_y, j0 + side_); y++)
                         for (int x = k0; x < std::min(N_x, k0 + side_); x++)
-                            if (S->mask[(size_t)y * N_x + x]) {
-                                any = true;
-                                break;
-                            }
-                    if (!any) continue;
+                            if (S->mask[(size_t)y * N_x + x]) lines++;
+                    if (!lines) continue;
                     const int colour = (tx & 1) | ((ty & 1) << 1) | ((S->nzg > 1 ? (zg & 1) : 0) << 2) |
                                        ((S->sg.N_time > 1 ? (i & 1) : 0) << 3);
                     if (phase_of[colour] < 0) phase_of[colour] = nphase++;
@@ -541,12 +540,19 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
                     t.j0 = j0;
                     t.z0 = zg * gz;
                     t.nz = std::min(gz, Nz - t.z0);
+                    t.nlines = lines;
                     t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
                     S->sv_all.push_back(t);
                     S->sv_all_phase.push_back(phase_of[colour]);
                 }
     S->sv_phase.assign(nphase, {});
     for (size_t q = 0; q < S->sv_all.size(); q++) S->sv_phase[S->sv_all_phase[q]].push_back(S->sv_all[q]);
+    // the work queue hands out the largest SVs first
+    for (auto &ph : S->sv_phase)
+        std::stable_sort(ph.begin(), ph.end(), [](const SvTask &a, const SvTask &b) { return a.nlines > b.nlines; });
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev));
     size_t maxt = 1;
     for (auto &ph : S->sv_phase) maxt = std::max(maxt, ph.size());
     cudaFree(S->d_sv_tasks);
@@ -556,8 +562,10 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     S->d_sv_out = nullptr;
     S->d_scratch = nullptr;
     CK(dalloc(&S->d_sv_tasks, maxt));
-    CK(dalloc(&S->d_sv_out, maxt));
-    CK(dalloc(&S->d_scratch, maxt * sp.band_floats));
+    const size_t ctas = std::min<size_t>(maxt, (size_t)S->sm_count);
+    CK(dalloc(&S->d_sv_out, ctas));
+    CK(dalloc(&S->d_scratch, ctas * sp.band_floats));
+    if (!S->d_queue) CK(dalloc(&S->d_queue, 1));
     if (!S->d_err) CK(dalloc(&S->d_err, 1));
     CK(cudaMemset(S->d_err, 0, sizeof(int)));
     S->schedule = 1;
@@ -582,12 +590,13 @@ static int sv_launch(MbirStage *S, const std::vector<SvTask> &tasks, int iter, u
     CK(cudaMemcpyAsync(S->d_sv_tasks, tasks.data(), tasks.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
                        S->stream));
     CK(cudaEventRecord(S->ev0, S->stream));
-    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, S->d_sv_tasks, (int)tasks.size(), S->d_scratch,
+    const int ctas = std::min((int)tasks.size(), S->sm_count);
+    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, S->d_sv_tasks, (int)tasks.size(), ctas, S->d_queue, S->d_scratch,
                           S->d_sv_out, iter, seed, S->d_err, S->stream));
     CK(cudaEventRecord(S->ev1, S->stream));
     S->launches++;
     S->icd_launches++;
-    std::vector<SvTaskOut> out(tasks.size());
+    std::vector<SvTaskOut> out(ctas);
     CK(cudaMemcpyAsync(out.data(), S->d_sv_out, out.size() * sizeof(SvTaskOut), cudaMemcpyDeviceToHost,
                        S->stream));
     CK(cudaStreamSynchronize(S->stream));

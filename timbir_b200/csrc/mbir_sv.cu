@@ -12,20 +12,26 @@
 // and finally adds the band's change back to the global error sinogram with
 // atomics, so that SVs running concurrently on other CTAs compose.
 //
-// Inside the CTA, warp w owns slice w of the group: it walks the SV's lines
-// one step at a time, and the slices of odd parity lag one line behind the
-// even ones, so a voxel's z-neighbours are never being updated while it is;
-// lines are ordered by their 2x2 (x, y) parity class, so consecutive lines
-// are never x-y neighbours.  Only warp w touches slice w's band rows, so the
-// error-sinogram updates need no synchronisation; one CTA barrier per line
-// step hands the next line's A-matrix column (computed cooperatively into a
-// three-slot ring) and the updated voxels to all warps.
+// Inside the CTA, `vsplit` warps own slice z of the group (each a share of
+// the frame's views): they walk the SV's lines one step at a time, and the
+// slices of odd parity lag one line behind the even ones, so a voxel's
+// z-neighbours are never being updated while it is; lines are ordered by
+// their 2x2 (x, y) parity class, so consecutive lines are never x-y
+// neighbours.  Only slice z's warps touch slice z's band rows, and each view
+// is always handled by the same lane, so error-sinogram updates need no
+// synchronisation; the warps of one slice combine theta through shared
+// memory and a named barrier; one CTA barrier per line step hands the next
+// line's A-matrix column (computed cooperatively into a three-slot ring) and
+// the updated voxels to all warps.
+//
+// CTAs are persistent: each takes SVs from a device work queue (host-sorted
+// by decreasing work) until the queue of the launch is empty.
 //
 // Concurrent SVs are chosen by the host so that no two share a prior
 // neighbourhood (2x2 SV checkerboard, z-group and frame parity); they may
-// share error-sinogram entries, whose concurrent changes they see at the next
-// visit (the super-voxel ICD scheme of Wang et al., "High performance model
-// based image reconstruction", PPoPP 2016).
+// share error-sinogram entries, whose concurrent changes they see at their
+// next visit (the super-voxel ICD scheme of Wang et al., "High performance
+// model based image reconstruction", PPoPP 2016).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -44,14 +50,16 @@ __device__ __forceinline__ double vy(const MbirGeom &g, int row)
     return __dadd_rn(g.y0, __dmul_rn((double)row + 0.5, g.delta_xy));
 }
 
-// First / last detector bin of a voxel's footprint at a view, before
-// clamping (XT_AMatrix.c:61-82), exact FP64.
-__device__ __forceinline__ void bin_range(const MbirGeom &g, double x, double y, double c, double s,
-                                          int &imin, int &imax)
+// floor(a / b) for b > 0, bit-exact with the IEEE quotient: the product with
+// the reciprocal is exact enough away from integers; near one the true
+// quotient decides.
+__device__ __forceinline__ int floor_div(double a, double b, double inv_b)
 {
-    const double r = __dsub_rn(__dmul_rn(x, c), __dmul_rn(y, s));
-    imin = (int)floor(__ddiv_rn(__dsub_rn(__dsub_rn(r, g.delta_xy), g.R0), g.delta_r));
-    imax = (int)floor(__ddiv_rn(__dsub_rn(__dadd_rn(r, g.delta_xy), g.R0), g.delta_r));
+    const double q = __dmul_rn(a, inv_b);
+    const double f = floor(q);
+    const double fr = q - f;
+    if (fr < 1e-9 || fr > 1.0 - 1e-9) return (int)floor(__ddiv_rn(a, b));
+    return (int)f;
 }
 
 __device__ __forceinline__ float warp_allsum(float v)
@@ -71,194 +79,49 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x)
     return x;
 }
 
-struct SvSmem {
-    float *eb, *wb;          // [rows][W][Np]
-    float *xb;               // [nz+2][S+2][S+2]
-    float *tb;               // [2][nz][S][S]
-    double *cs, *sn;         // [Np]
-    int *vidx, *rlo;         // [Np]
-    float *aval;             // [3][amax][Np]
-    uint8_t *aoff;           // [3][amax][Np]
-    uint8_t *acnt;           // [3][Np]
-    int *order;              // [S*S] line (local index ly*S+lx) per step
-    float *magl;             // [S*S]
-};
+__device__ __forceinline__ void named_barrier(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 
 __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp,
-                                                  const SvTask *__restrict__ tasks, float *scratch,
-                                                  SvTaskOut *__restrict__ out, int iter, uint32_t seed,
-                                                  int *err)
+                                                  const SvTask *__restrict__ tasks, int ntasks,
+                                                  int *queue, float *scratch, SvTaskOut *__restrict__ out,
+                                                  int iter, uint32_t seed, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const SvTask task = tasks[blockIdx.x];
-    const int S = sp.S, W = sp.W, amax = sp.amax, mz = g.m_z;
-    const int nz = task.nz, rows = nz * mz;
-    const int i = task.frame;
-    const int Np = g.view_num[i];
+    const int S = sp.S, W = sp.W, amax = sp.amax, mz = g.m_z, vsplit = sp.vsplit;
     const int NpS = sp.max_views;  // smem stride (views)
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const int S2 = S + 2;
 
     // ---- carve shared memory (sizes fixed by the host in sp) ----
-    SvSmem m;
     unsigned char *p = smraw;
-    m.cs = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
-    m.sn = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
-    m.eb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
-    m.wb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
-    m.aval = reinterpret_cast<float *>(p); p += sizeof(float) * 3 * amax * NpS;
-    m.xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
-    m.tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
-    m.magl = reinterpret_cast<float *>(p); p += sizeof(float) * S * S;
-    m.vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
-    m.rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
-    m.order = reinterpret_cast<int *>(p); p += sizeof(int) * S * S;
-    m.aoff = p; p += 3 * amax * NpS;
-    m.acnt = p; p += 3 * NpS;
-    __shared__ int s_nlines;
+    double *cs = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
+    double *sn = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
+    float *eb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
+    float *wb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
+    float *aval = reinterpret_cast<float *>(p); p += sizeof(float) * 3 * amax * NpS;
+    int *aso = reinterpret_cast<int *>(p); p += sizeof(int) * 3 * amax * NpS;  // smem offset off*NpS+v
+    float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
+    float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
+    float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * S * S;
+    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * 2 * 2 * sp.max_nz * 2;
+    int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
+    int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
+    int *order = reinterpret_cast<int *>(p); p += sizeof(int) * S * S;
+    uint8_t *acnt = p; p += 3 * NpS;
+    __shared__ int s_nlines, s_task;
     __shared__ float s_red[32][4];
 
-    const int k0 = task.k0, j0 = task.j0, z0 = task.z0;
-    const int kx = min(S, g.N_x - k0), ky = min(S, g.N_y - j0);
-    const int *vl = g.view_idx + (size_t)i * g.max_views;
-
-    // ---- views, trig, band origin per view ----
-    for (int v = tid; v < Np; v += nthr) {
-        const int view = vl[v];
-        m.vidx[v] = view;
-        const double c = g.cosv[view], s = g.sinv[view];
-        m.cs[v] = c;
-        m.sn[v] = s;
-        int lo = 1 << 30, a, b;
-        const double xs[2] = {vx(g, k0), vx(g, k0 + kx - 1)};
-        const double ys[2] = {vy(g, j0), vy(g, j0 + ky - 1)};
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            bin_range(g, xs[u & 1], ys[u >> 1], c, s, a, b);
-            lo = min(lo, a);
-        }
-        m.rlo[v] = max(lo, 0);
-    }
-    // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
-    if (tid == 0) {
-        int n = 0;
-        for (int cls = 0; cls < 4; cls++) {
-            const int base = n;
-            for (int ly = 0; ly < ky; ly++)
-                for (int lx = 0; lx < kx; lx++)
-                    if ((((k0 + lx) & 1) | (((j0 + ly) & 1) << 1)) == cls &&
-                        dv.mask[(size_t)(j0 + ly) * g.N_x + k0 + lx] == 1)
-                        m.order[n++] = ly * S + lx;
-            // shuffle the class with hash keys (Fisher-Yates)
-            for (int q = n - 1; q > base; q--) {
-                const uint32_t h = hash32(seed ^ hash32(blockIdx.x * 1315423911u + q));
-                const int r = base + (int)(h % (uint32_t)(q - base + 1));
-                const int t = m.order[q];
-                m.order[q] = m.order[r];
-                m.order[r] = t;
-            }
-        }
-        s_nlines = n;
-    }
-    for (int q = tid; q < S * S; q += nthr) m.magl[q] = 0.0f;
-    __syncthreads();
-    const int nl = s_nlines;
-
-    // ---- stage bands (e also to this CTA's scratch slot for the commit) ----
-    float *scr = scratch + (size_t)blockIdx.x * sp.band_floats;
-    const size_t bandn = (size_t)rows * W * Np;
-    for (size_t q = tid; q < bandn; q += nthr) {
-        const int v = (int)(q % Np);
-        const int off = (int)((q / Np) % W);
-        const int row = (int)(q / ((size_t)Np * W));
-        const int r = m.rlo[v] + off;
-        const int t = z0 * mz + row;
-        float ev = 0.0f, wv = 0.0f;
-        if (r < g.N_r) {
-            const size_t o = ((size_t)t * g.N_p + m.vidx[v]) * g.N_r + r;
-            ev = dv.e[o];
-            wv = dv.w[o];
-        }
-        const size_t so = ((size_t)row * W + off) * NpS + v;
-        m.eb[so] = ev;
-        m.wb[so] = wv;
-        scr[q] = ev;
-    }
-    // ---- voxel block with halo, temporal neighbours ----
-    const size_t plane = (size_t)g.N_y * g.N_x;
-    const float *xf = dv.x + (size_t)i * g.N_z * plane;
-    const int nb = (nz + 2) * S2 * S2;
-    for (int q = tid; q < nb; q += nthr) {
-        const int lx = q % S2, ly = (q / S2) % S2, lz = q / (S2 * S2);
-        const int xx = k0 + lx - 1, yy = j0 + ly - 1, zz = z0 + lz - 1;
-        float v = 0.0f;
-        if (xx >= 0 && xx < g.N_x && yy >= 0 && yy < g.N_y && zz >= 0 && zz < g.N_z)
-            v = xf[(size_t)zz * plane + (size_t)yy * g.N_x + xx];
-        m.xb[q] = v;
-    }
-    const int nt = 2 * nz * S * S;
-    for (int q = tid; q < nt; q += nthr) {
-        const int lx = q % S, ly = (q / S) % S, lz = (q / (S * S)) % nz, side = q / (nz * S * S);
-        const int ti = i + (side == 0 ? -1 : 1);
-        float v = 0.0f;
-        if (ti >= 0 && ti < g.N_time && lx < kx && ly < ky)
-            v = dv.x[((size_t)ti * g.N_z + z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx];
-        m.tb[q] = v;
-    }
-
-    // ---- A-matrix column of line `li` into ring slot `slot` (exact bins) ----
-    auto acol = [&](int li, int slot) {
-        const int loc = m.order[li];
-        const int col = k0 + loc % S, row = j0 + loc / S;
-        const double x = vx(g, col), y = vy(g, row);
-        float *av = m.aval + (size_t)slot * amax * NpS;
-        uint8_t *ao = m.aoff + (size_t)slot * amax * NpS;
-        uint8_t *ac = m.acnt + (size_t)slot * NpS;
-        for (int v = tid; v < Np; v += nthr) {
-            const double r = __dsub_rn(__dmul_rn(x, m.cs[v]), __dmul_rn(y, m.sn[v]));
-            const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
-            int n = 0;
-            if (!(rmax < g.R0 || rmin > g.RMax)) {
-                int imin = (int)floor(__ddiv_rn(__dsub_rn(rmin, g.R0), g.delta_r));
-                int imax = (int)floor(__ddiv_rn(__dsub_rn(rmax, g.R0), g.delta_r));
-                if (imax >= g.N_r) imax = g.N_r - 1;
-                if (imin < 0) imin = 0;
-                const float *H = g.H_r + (size_t)m.vidx[v] * (MBIR_RESP_BINS + 1);
-                for (int j = imin; j <= imax; j++) {
-                    const double rc = __dadd_rn(g.R0, __dmul_rn((double)j + 0.5, g.delta_r));
-                    const double dr = fabs(__dsub_rn(r, rc));
-                    const int id = (int)floor(__ddiv_rn(dr, g.OffsetR));
-                    if (id >= 0 && id < MBIR_RESP_BINS) {
-                        const double w1 = __dsub_rn(dr, __dmul_rn((double)id, g.OffsetR));
-                        const double w2 = __dsub_rn(g.OffsetR, w1);
-                        const double f1 = __ddiv_rn(__dadd_rn(__dmul_rn(w2, (double)__ldg(H + id)),
-                                                              __dmul_rn(w1, (double)__ldg(H + id + 1))),
-                                                    g.OffsetR);
-                        const int off = j - m.rlo[v];
-                        if (f1 > 0) {
-                            if (off < 0 || off >= W || n >= amax) {
-                                atomicOr(err, 1);
-                            } else {
-                                av[(size_t)n * NpS + v] = (float)f1;
-                                ao[(size_t)n * NpS + v] = (uint8_t)off;
-                                n++;
-                            }
-                        }
-                    }
-                }
-            }
-            ac[v] = (uint8_t)n;
-        }
-    };
-
-    __syncthreads();
-    if (nl > 0) acol(0, 0);
-    __syncthreads();
-
+    const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
+    const float inv_off_f = (float)inv_off;
     const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
     const float sSQ = (float)pr.sSQ, sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
     const float sTQ = (float)pr.sTQ, sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
+    // this warp's slice and view share
+    const int zl = warp / vsplit, vh = warp - zl * vsplit;
     // neighbour of lane: spatial (dz, dy, dx) for lanes 0..25, temporal 26, 27
     int ndz = 0, ndy = 0, ndx = 0;
     float bw = 0.0f;
@@ -274,137 +137,301 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         bw = (float)pr.TF;
         temporal = true;
     }
-    const int zl = warp;  // this warp's slice in the group
-    const bool active_warp = zl < nz;
-    const int zg = z0 + zl;
     float sum_abs_dx = 0.0f, sum_abs_x = 0.0f;
     int n_upd = 0, n_skip = 0;
 
-    for (int step = 0; step <= nl; step++) {
-        const int li = (zl & 1) ? step - 1 : step;
-        if (active_warp && li >= 0 && li < nl) {
-            const int slot = li % 3;
-            const int loc = m.order[li];
-            const int lx = loc % S, ly = loc / S;
-            const int col = k0 + lx, row = j0 + ly;
-            float *xc = m.xb + ((size_t)(zl + 1) * S2 + ly + 1) * S2 + lx + 1;
-            const float V = *xc;
-            // ---- prior neighbourhood ----
-            float nbv = 0.0f;
-            bool valid = false;
-            if (spatial) {
-                const int zz = zg + ndz, yy = row + ndy, xx = col + ndx;
-                valid = zz >= 0 && zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x;
-                if (valid) nbv = xc[(ndz * S2 + ndy) * S2 + ndx];
-            } else if (temporal) {
-                const int ti = i + (lane == 26 ? -1 : 1);
-                valid = ti >= 0 && ti < g.N_time;
-                if (valid) nbv = m.tb[(((size_t)(lane - 26) * nz + zl) * S + ly) * S + lx];
-            }
-            const unsigned pos = __ballot_sync(0xffffffffu, valid && nbv > 0.0f);
-            if (V == 0.0f && iter > 1 && pos == 0u) {
-                n_skip++;
-            } else {
-                float b = 0.0f;
-                if (valid) {
-                    // f * rho'(D)/D for q = 2, p = 1.2: (2 - 0.8 t1/t3) / (t3 s^q)
-                    const float d = V - nbv;
-                    const float ad = fabsf(d);
-                    const float t1 = (ad > 0.0f ? exp2f(0.8f * log2f(ad)) : 0.0f) * (spatial ? sSQP_inv : sTQP_inv);
-                    const float t3 = (spatial ? cS : cT) + t1;
-                    b = bw * (2.0f - 0.8f * t1 / t3) / (t3 * (spatial ? sSQ : sTQ));
-                }
-                float p1 = warp_allsum(b * nbv);
-                float p2 = warp_allsum(b);
-                // ---- data term over this slice's band rows ----
-                float th1 = 0.0f, th2 = 0.0f;
-                const float *av = m.aval + (size_t)slot * amax * NpS;
-                const uint8_t *ao = m.aoff + (size_t)slot * amax * NpS;
-                const uint8_t *ac = m.acnt + (size_t)slot * NpS;
-                for (int v = lane; v < Np; v += 32) {
-                    const int cnt = ac[v];
-                    for (int q = 0; q < cnt; q++) {
-                        const float a = av[(size_t)q * NpS + v];
-                        const int off = ao[(size_t)q * NpS + v];
-                        for (int rr = 0; rr < mz; rr++) {
-                            const size_t so = ((size_t)(zl * mz + rr) * W + off) * NpS + v;
-                            const float e = m.eb[so], w = m.wb[so];
-                            const float sw = sqrtf(w);
-                            float om = w;
-                            if (!(fabsf(e * sw) < hT)) om = hTd * sw / fabsf(e);
-                            th2 = fmaf(a * a, om, th2);
-                            th1 = fmaf(-e * a, om, th1);
-                        }
-                    }
-                }
-                th1 = warp_allsum(th1);
-                th2 = warp_allsum(th2);
-                const float u = (p1 + th2 * V - th1) / (p2 + th2);
-                const float xn = V + alpha * (u - V);
-                const float dx = xn - V;
-                __syncwarp();
-                if (lane == 0) {
-                    *xc = xn;
-                    atomicAdd(&m.magl[loc], fabsf(dx));
-                }
-                sum_abs_dx += fabsf(dx);
-                sum_abs_x += fabsf(xn);
-                n_upd++;
-                // ---- error sinogram: e -= a dx over this slice's rows ----
-                for (int v = lane; v < Np; v += 32) {
-                    const int cnt = ac[v];
-                    for (int q = 0; q < cnt; q++) {
-                        const float a = av[(size_t)q * NpS + v];
-                        const int off = ao[(size_t)q * NpS + v];
-                        for (int rr = 0; rr < mz; rr++) {
-                            const size_t so = ((size_t)(zl * mz + rr) * W + off) * NpS + v;
-                            m.eb[so] = fmaf(-a, dx, m.eb[so]);
-                        }
-                    }
-                }
-            }
-        }
-        if (step + 1 < nl) acol(step + 1, (step + 1) % 3);
+    for (;;) {
         __syncthreads();
-    }
+        if (tid == 0) s_task = atomicAdd(queue, 1);
+        __syncthreads();
+        const int tix = s_task;
+        if (tix >= ntasks) break;
+        const SvTask task = tasks[tix];
+        const int nz = task.nz, rows = nz * mz;
+        const int i = task.frame;
+        const int Np = g.view_num[i];
+        const int k0 = task.k0, j0 = task.j0, z0 = task.z0;
+        const int kx = min(S, g.N_x - k0), ky = min(S, g.N_y - j0);
+        const int *vl = g.view_idx + (size_t)i * g.max_views;
+        const bool active = zl < nz;
+        const int zg = z0 + zl;
 
-    // ---- write back voxels, magnitude map, band change ----
-    float *xo = dv.x + (size_t)i * g.N_z * plane;
-    for (int q = tid; q < nz * S * S; q += nthr) {
-        const int lx = q % S, ly = (q / S) % S, lz = q / (S * S);
-        if (lx < kx && ly < ky)
-            xo[(size_t)(z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx] =
-                m.xb[((size_t)(lz + 1) * S2 + ly + 1) * S2 + lx + 1];
-    }
-    for (int q = tid; q < nl; q += nthr) {
-        const int loc = m.order[q];
-        task.mag[(size_t)(j0 + loc / S) * g.N_x + k0 + loc % S] = m.magl[loc];
-    }
-    for (size_t q = tid; q < bandn; q += nthr) {
-        const int v = (int)(q % Np);
-        const int off = (int)((q / Np) % W);
-        const int row = (int)(q / ((size_t)Np * W));
-        const int r = m.rlo[v] + off;
-        if (r >= g.N_r) continue;
-        const float dnew = m.eb[((size_t)row * W + off) * NpS + v] - scr[q];
-        if (dnew != 0.0f) {
+        // ---- views, trig, band origin per view ----
+        for (int v = tid; v < Np; v += nthr) {
+            const int view = vl[v];
+            vidx[v] = view;
+            const double c = g.cosv[view], s = g.sinv[view];
+            cs[v] = c;
+            sn[v] = s;
+            int lo = 1 << 30;
+            const double xs[2] = {vx(g, k0), vx(g, k0 + kx - 1)};
+            const double ys[2] = {vy(g, j0), vy(g, j0 + ky - 1)};
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const double r = __dsub_rn(__dmul_rn(xs[u & 1], c), __dmul_rn(ys[u >> 1], s));
+                lo = min(lo, floor_div(__dsub_rn(__dsub_rn(r, g.delta_xy), g.R0), g.delta_r, inv_dr));
+            }
+            rlo[v] = max(lo, 0);
+        }
+        // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
+        if (warp == 0) {
+            // lane-parallel compaction per class, then a serial shuffle by lane 0
+            int n = 0;
+            for (int cls = 0; cls < 4; cls++) {
+                const int base = n;
+                for (int q0 = 0; q0 < S * S; q0 += 32) {
+                    const int q = q0 + lane;
+                    const int lx = q % S, ly = q / S;
+                    bool take = false;
+                    if (q < S * S && lx < kx && ly < ky)
+                        take = ((((k0 + lx) & 1) | (((j0 + ly) & 1) << 1)) == cls) &&
+                               dv.mask[(size_t)(j0 + ly) * g.N_x + k0 + lx] == 1;
+                    const unsigned bal = __ballot_sync(0xffffffffu, take);
+                    if (take) order[n + __popc(bal & ((1u << lane) - 1))] = q;
+                    n += __popc(bal);
+                }
+                __syncwarp();
+                if (lane == 0)
+                    for (int q = n - 1; q > base; q--) {
+                        const uint32_t h = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)q));
+                        const int r = base + (int)(h % (uint32_t)(q - base + 1));
+                        const int t = order[q];
+                        order[q] = order[r];
+                        order[r] = t;
+                    }
+                __syncwarp();
+            }
+            if (lane == 0) s_nlines = n;
+        }
+        for (int q = tid; q < S * S; q += nthr) magl[q] = 0.0f;
+        __syncthreads();
+        const int nl = s_nlines;
+
+        // ---- stage bands (e also to this CTA's scratch slot for the commit) ----
+        float *scr = scratch + (size_t)blockIdx.x * sp.band_floats;
+        for (int ro = warp; ro < rows * W; ro += nwarps) {
+            const int row = ro / W, off = ro - row * W;
             const int t = z0 * mz + row;
-            atomicAdd(&dv.e[((size_t)t * g.N_p + m.vidx[v]) * g.N_r + r], dnew);
+            const float *erow = dv.e + (size_t)t * g.N_p * g.N_r;
+            const float *wrow = dv.w + (size_t)t * g.N_p * g.N_r;
+            for (int v = lane; v < Np; v += 32) {
+                const int r = rlo[v] + off;
+                float ev = 0.0f, wv = 0.0f;
+                if (r < g.N_r) {
+                    const size_t o = (size_t)vidx[v] * g.N_r + r;
+                    ev = erow[o];
+                    wv = __ldg(wrow + o);
+                }
+                eb[ro * NpS + v] = ev;
+                wb[ro * NpS + v] = wv;
+                scr[ro * NpS + v] = ev;
+            }
+        }
+        // ---- voxel block with halo, temporal neighbours ----
+        const size_t plane = (size_t)g.N_y * g.N_x;
+        const float *xf = dv.x + (size_t)i * g.N_z * plane;
+        for (int lz = warp; lz < nz + 2; lz += nwarps)
+            for (int q = lane; q < S2 * S2; q += 32) {
+                const int lx = q % S2, ly = q / S2;
+                const int xx = k0 + lx - 1, yy = j0 + ly - 1, zz = z0 + lz - 1;
+                float v = 0.0f;
+                if (xx >= 0 && xx < g.N_x && yy >= 0 && yy < g.N_y && zz >= 0 && zz < g.N_z)
+                    v = xf[(size_t)zz * plane + (size_t)yy * g.N_x + xx];
+                xb[lz * S2 * S2 + q] = v;
+            }
+        for (int sz = warp; sz < 2 * nz; sz += nwarps) {
+            const int side = sz / nz, lz = sz - side * nz;
+            const int ti = i + (side == 0 ? -1 : 1);
+            for (int q = lane; q < S * S; q += 32) {
+                const int lx = q % S, ly = q / S;
+                float v = 0.0f;
+                if (ti >= 0 && ti < g.N_time && lx < kx && ly < ky)
+                    v = dv.x[((size_t)ti * g.N_z + z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx];
+                tb[sz * S * S + q] = v;
+            }
+        }
+
+        // ---- A-matrix column of line `li` into ring slot `slot` (exact bins) ----
+        auto acol = [&](int li, int slot) {
+            const int loc = order[li];
+            const int col = k0 + loc % S, row = j0 + loc / S;
+            const double x = vx(g, col), y = vy(g, row);
+            float *av = aval + slot * amax * NpS;
+            int *ao = aso + slot * amax * NpS;
+            uint8_t *ac = acnt + slot * NpS;
+            for (int v = tid; v < Np; v += nthr) {
+                const double r = __dsub_rn(__dmul_rn(x, cs[v]), __dmul_rn(y, sn[v]));
+                const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
+                int n = 0;
+                if (!(rmax < g.R0 || rmin > g.RMax)) {
+                    int imin = floor_div(__dsub_rn(rmin, g.R0), g.delta_r, inv_dr);
+                    int imax = floor_div(__dsub_rn(rmax, g.R0), g.delta_r, inv_dr);
+                    if (imax >= g.N_r) imax = g.N_r - 1;
+                    if (imin < 0) imin = 0;
+                    const float *H = g.H_r + (size_t)vidx[v] * (MBIR_RESP_BINS + 1);
+                    const int base = rlo[v];
+                    for (int j = imin; j <= imax; j++) {
+                        const double rc = __dadd_rn(g.R0, __dmul_rn((double)j + 0.5, g.delta_r));
+                        const double dr = fabs(__dsub_rn(r, rc));
+                        const int id = floor_div(dr, g.OffsetR, inv_off);
+                        if (id >= 0 && id < MBIR_RESP_BINS) {
+                            const double w1 = __dsub_rn(dr, __dmul_rn((double)id, g.OffsetR));
+                            const double w2 = __dsub_rn(g.OffsetR, w1);
+                            const double num = __dadd_rn(__dmul_rn(w2, (double)__ldg(H + id)),
+                                                         __dmul_rn(w1, (double)__ldg(H + id + 1)));
+                            const int off = j - base;
+                            if (num > 0) {
+                                if (off < 0 || off >= W || n >= amax) {
+                                    atomicOr(err, 1);
+                                } else {
+                                    av[n * NpS + v] = (float)num * inv_off_f;
+                                    ao[n * NpS + v] = off * NpS + v;
+                                    n++;
+                                }
+                            }
+                        }
+                    }
+                }
+                ac[v] = (uint8_t)n;
+            }
+        };
+
+        __syncthreads();
+        if (nl > 0) acol(0, 0);
+        __syncthreads();
+
+        for (int step = 0; step <= nl; step++) {
+            const int li = (zl & 1) ? step - 1 : step;
+            if (active && li >= 0 && li < nl) {
+                const int slot = li % 3;
+                const int loc = order[li];
+                const int lx = loc % S, ly = loc / S;
+                const int col = k0 + lx, row = j0 + ly;
+                float *xc = xb + ((zl + 1) * S2 + ly + 1) * S2 + lx + 1;
+                const float V = *xc;
+                // ---- prior neighbourhood ----
+                float nbv = 0.0f;
+                bool valid = false;
+                if (spatial) {
+                    const int zz = zg + ndz, yy = row + ndy, xx = col + ndx;
+                    valid = zz >= 0 && zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x;
+                    if (valid) nbv = xc[(ndz * S2 + ndy) * S2 + ndx];
+                } else if (temporal) {
+                    const int ti = i + (lane == 26 ? -1 : 1);
+                    valid = ti >= 0 && ti < g.N_time;
+                    if (valid) nbv = tb[((lane - 26) * nz + zl) * S * S + ly * S + lx];
+                }
+                const unsigned pos = __ballot_sync(0xffffffffu, valid && nbv > 0.0f);
+                if (V == 0.0f && iter > 1 && pos == 0u) {
+                    if (vh == 0 && lane == 0) n_skip++;
+                } else {
+                    // ---- data term over this slice's band rows, this warp's views ----
+                    float th1 = 0.0f, th2 = 0.0f;
+                    const float *av = aval + slot * amax * NpS;
+                    const int *ao = aso + slot * amax * NpS;
+                    const uint8_t *ac = acnt + slot * NpS;
+                    const int rowbase = zl * mz * W * NpS;
+                    for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+                        const int cnt = ac[v];
+                        for (int q = 0; q < cnt; q++) {
+                            const float a = av[q * NpS + v];
+                            int so = rowbase + ao[q * NpS + v];
+                            for (int rr = 0; rr < mz; rr++, so += W * NpS) {
+                                const float e = eb[so], w = wb[so];
+                                const float sw = sqrtf(w);
+                                float om = w;
+                                if (!(fabsf(e * sw) < hT)) om = hTd * sw / fabsf(e);
+                                th2 = fmaf(a * a, om, th2);
+                                th1 = fmaf(-e * a, om, th1);
+                            }
+                        }
+                    }
+                    th1 = warp_allsum(th1);
+                    th2 = warp_allsum(th2);
+                    // prior sums: f * rho'(D)/D for q = 2, p = 1.2 is (2 - 0.8 t1/t3) / (t3 s^q)
+                    float b = 0.0f;
+                    if (valid) {
+                        const float d = V - nbv;
+                        const float ad = fabsf(d);
+                        const float t1 = (ad > 0.0f ? exp2f(0.8f * log2f(ad)) : 0.0f) * (spatial ? sSQP_inv : sTQP_inv);
+                        const float t3 = (spatial ? cS : cT) + t1;
+                        b = bw * (2.0f - 0.8f * t1 / t3) / (t3 * (spatial ? sSQ : sTQ));
+                    }
+                    const float p1 = warp_allsum(b * nbv);
+                    const float p2 = warp_allsum(b);
+                    if (vsplit > 1) {
+                        float *pp = part + (((step & 1) * sp.max_nz + zl) * 2) * 2;
+                        if (lane == 0) {
+                            pp[vh * 2 + 0] = th1;
+                            pp[vh * 2 + 1] = th2;
+                        }
+                        named_barrier(1 + zl, 32 * vsplit);
+                        th1 = pp[0] + pp[2];
+                        th2 = pp[1] + pp[3];
+                    }
+                    const float u = (p1 + th2 * V - th1) / (p2 + th2);
+                    const float xn = V + alpha * (u - V);
+                    const float dx = xn - V;
+                    if (vh == 0) {
+                        __syncwarp();
+                        if (lane == 0) {
+                            *xc = xn;
+                            magl[loc] += fabsf(dx);
+                            sum_abs_dx += fabsf(dx);
+                            sum_abs_x += fabsf(xn);
+                            n_upd++;
+                        }
+                    }
+                    // ---- error sinogram: e -= a dx over this slice's rows ----
+                    for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+                        const int cnt = ac[v];
+                        for (int q = 0; q < cnt; q++) {
+                            const float a = av[q * NpS + v];
+                            int so = rowbase + ao[q * NpS + v];
+                            for (int rr = 0; rr < mz; rr++, so += W * NpS) eb[so] = fmaf(-a, dx, eb[so]);
+                        }
+                    }
+                }
+            }
+            if (step + 1 < nl) acol(step + 1, (step + 1) % 3);
+            __syncthreads();
+        }
+
+        // ---- write back voxels, magnitude map, band change ----
+        float *xo = dv.x + (size_t)i * g.N_z * plane;
+        for (int lz = warp; lz < nz; lz += nwarps)
+            for (int q = lane; q < S * S; q += 32) {
+                const int lx = q % S, ly = q / S;
+                if (lx < kx && ly < ky)
+                    xo[(size_t)(z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx] =
+                        xb[((lz + 1) * S2 + ly + 1) * S2 + lx + 1];
+            }
+        for (int q = tid; q < nl; q += nthr) {
+            const int loc = order[q];
+            task.mag[(size_t)(j0 + loc / S) * g.N_x + k0 + loc % S] = magl[loc];
+        }
+        for (int ro = warp; ro < rows * W; ro += nwarps) {
+            const int row = ro / W, off = ro - row * W;
+            float *erow = dv.e + (size_t)(z0 * mz + row) * g.N_p * g.N_r;
+            for (int v = lane; v < Np; v += 32) {
+                const int r = rlo[v] + off;
+                if (r >= g.N_r) continue;
+                const float dnew = eb[ro * NpS + v] - scr[ro * NpS + v];
+                if (dnew != 0.0f) atomicAdd(erow + (size_t)vidx[v] * g.N_r + r, dnew);
+            }
         }
     }
-    // ---- per-task statistics ----
-    float a0 = warp_allsum(sum_abs_dx), a1 = warp_allsum(sum_abs_x);
-    float a2 = warp_allsum((float)n_upd), a3 = warp_allsum((float)n_skip);
+    // ---- per-CTA statistics (only lane 0 of each slice's first warp counts) ----
     if (lane == 0) {
-        s_red[warp][0] = a0;
-        s_red[warp][1] = a1;
-        s_red[warp][2] = a2;
-        s_red[warp][3] = a3;
+        s_red[warp][0] = sum_abs_dx;
+        s_red[warp][1] = sum_abs_x;
+        s_red[warp][2] = (float)n_upd;
+        s_red[warp][3] = (float)n_skip;
     }
     __syncthreads();
     if (tid == 0) {
         double d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-        for (int w = 0; w < (nthr >> 5); w++) {
+        for (int w = 0; w < nwarps; w++) {
             d0 += s_red[w][0];
             d1 += s_red[w][1];
             d2 += s_red[w][2];
@@ -425,24 +452,33 @@ size_t mbir_sv_smem_bytes(const SvParams &sp)
     size_t b = 0;
     b += 2 * sizeof(double) * NpS;
     b += 2 * sizeof(float) * (size_t)sp.max_rows * sp.W * NpS;
-    b += sizeof(float) * 3 * sp.amax * NpS;
+    b += (sizeof(float) + sizeof(int)) * 3 * sp.amax * NpS;
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     b += sizeof(float) * 2 * sp.max_nz * S * S;
     b += sizeof(float) * S * S;
+    b += sizeof(float) * 2 * 2 * 2 * sp.max_nz * 2;
     b += sizeof(int) * NpS * 2;
     b += sizeof(int) * S * S;
-    b += 3 * sp.amax * NpS + 3 * NpS;
+    b += 3 * NpS;
     return (b + 15) & ~(size_t)15;
 }
 
+int mbir_sv_ctas(int ntasks, int sm_count)
+{
+    return ntasks < sm_count ? ntasks : sm_count;
+}
+
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               const SvTask *tasks, int ntasks, float *scratch, SvTaskOut *out, int iter,
-                               uint32_t seed, int *err, cudaStream_t s)
+                               const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
+                               SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
 {
     if (ntasks <= 0) return cudaSuccess;
     const size_t sm = mbir_sv_smem_bytes(sp);
     cudaError_t e = cudaFuncSetAttribute(k_icd_sv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_icd_sv<<<ntasks, 32 * sp.max_nz, sm, s>>>(g, pr, dv, sp, tasks, scratch, out, iter, seed, err);
+    e = cudaMemsetAsync(queue, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_icd_sv<<<ctas, 32 * sp.max_nz * sp.vsplit, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter,
+                                                          seed, err);
     return cudaGetLastError();
 }

@@ -11,13 +11,15 @@ struct SvParams {
     int W;          // band width (detector columns per view)
     int amax;       // max A-matrix entries per (line, view): 2 mult_xy + 1
     int max_views;  // max views of any frame (shared-memory stride)
-    int max_nz;     // slices per CTA (one warp each)
+    int max_nz;     // slices per CTA
     int max_rows;   // detector rows per CTA: max_nz * m_z
+    int vsplit;     // warps per slice (1 or 2; 2 needs max_nz <= 15)
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
 };
 
 struct SvTask {
     int frame, k0, j0, z0, nz;
+    int nlines;  // in-mask voxel lines (host-side ordering of the work queue)
     float *mag;  // [N_y][N_x] plane of the magnitude map for (frame, z-group)
 };
 
@@ -27,6 +29,9 @@ struct SvTaskOut {
 };
 
 size_t mbir_sv_smem_bytes(const SvParams &sp);
+// ctas persistent CTAs take the ntasks tasks from the queue counter (reset by
+// the launcher); scratch holds ctas * sp.band_floats floats; out holds ctas
+// entries.
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               const SvTask *tasks, int ntasks, float *scratch, SvTaskOut *out, int iter,
-                               uint32_t seed, int *err, cudaStream_t s);
+                               const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
+                               SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s);
