@@ -84,47 +84,57 @@ __device__ __forceinline__ void named_barrier(int id, int count)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+struct AEnt {
+    float a;  // A-matrix value
+    int so;   // shared-memory offset of the entry in a band row: off * NpS + v
+};
+
+// AMAXC: entries per (line, view) known at compile time (3 at full
+// resolution), 0 = runtime sp.amax.  MZC: detector rows per slice known at
+// compile time (1 at full resolution), 0 = runtime m_z.
+template <int AMAXC, int MZC>
 __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp,
                                                   const SvTask *__restrict__ tasks, int ntasks,
                                                   int *queue, float *scratch, SvTaskOut *__restrict__ out,
                                                   int iter, uint32_t seed, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const int S = sp.S, W = sp.W, amax = sp.amax, mz = g.m_z, vsplit = sp.vsplit;
+    const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
+    const int amax = AMAXC > 0 ? AMAXC : sp.amax;
+    const int mz = MZC > 0 ? MZC : g.m_z;
     const int NpS = sp.max_views;  // smem stride (views)
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const int S2 = S + 2;
+    const int rowstride = W * NpS;
 
     // ---- carve shared memory (sizes fixed by the host in sp) ----
     unsigned char *p = smraw;
     double *cs = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
     double *sn = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
-    float *eb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
-    float *wb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * W * NpS;
-    float *aval = reinterpret_cast<float *>(p); p += sizeof(float) * 3 * amax * NpS;
-    int *aso = reinterpret_cast<int *>(p); p += sizeof(int) * 3 * amax * NpS;  // smem offset off*NpS+v
+    AEnt *aring = reinterpret_cast<AEnt *>(p); p += sizeof(AEnt) * 3 * amax * NpS;
+    float *eb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * rowstride;
+    float *sb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * rowstride;
     float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
     float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * S * S;
-    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * 2 * 2 * sp.max_nz * 2;
+    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 4 * sp.max_nz;
     int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
     int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
     int *order = reinterpret_cast<int *>(p); p += sizeof(int) * S * S;
-    uint8_t *acnt = p; p += 3 * NpS;
     __shared__ int s_nlines, s_task;
     __shared__ float s_red[32][4];
 
     const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
     const float inv_off_f = (float)inv_off;
     const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
-    const float sSQ = (float)pr.sSQ, sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
-    const float sTQ = (float)pr.sTQ, sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
+    const float sSQ_inv = (float)(1.0 / pr.sSQ), sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
+    const float sTQ_inv = (float)(1.0 / pr.sTQ), sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
     // this warp's slice and view share
     const int zl = warp / vsplit, vh = warp - zl * vsplit;
     // neighbour of lane: spatial (dz, dy, dx) for lanes 0..25, temporal 26, 27
     int ndz = 0, ndy = 0, ndx = 0;
-    float bw = 0.0f;
+    float bw = 0.0f, qinv = 0.0f, qpinv = 0.0f, cc = 1.0f;
     bool spatial = false, temporal = false;
     if (lane < 26) {
         const int n = lane < 13 ? lane : lane + 1;  // skip the centre (13)
@@ -132,11 +142,19 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         ndy = (n / 3) % 3 - 1;
         ndx = n % 3 - 1;
         bw = (float)pr.SF[n];
+        qinv = sSQ_inv;
+        qpinv = sSQP_inv;
+        cc = cS;
         spatial = true;
     } else if (lane < 28) {
         bw = (float)pr.TF;
+        qinv = sTQ_inv;
+        qpinv = sTQP_inv;
+        cc = cT;
         temporal = true;
     }
+    // views of the A-column computation: spread over all warps
+    const int av_lanes = (NpS + nwarps - 1) / nwarps;
     float sum_abs_dx = 0.0f, sum_abs_x = 0.0f;
     int n_upd = 0, n_skip = 0;
 
@@ -175,7 +193,6 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         }
         // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
         if (warp == 0) {
-            // lane-parallel compaction per class, then a serial shuffle by lane 0
             int n = 0;
             for (int cls = 0; cls < 4; cls++) {
                 const int base = n;
@@ -207,7 +224,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         __syncthreads();
         const int nl = s_nlines;
 
-        // ---- stage bands (e also to this CTA's scratch slot for the commit) ----
+        // ---- stage bands: e (also to this CTA's scratch slot) and sqrt(w) ----
         float *scr = scratch + (size_t)blockIdx.x * sp.band_floats;
         for (int ro = warp; ro < rows * W; ro += nwarps) {
             const int row = ro / W, off = ro - row * W;
@@ -223,7 +240,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     wv = __ldg(wrow + o);
                 }
                 eb[ro * NpS + v] = ev;
-                wb[ro * NpS + v] = wv;
+                sb[ro * NpS + v] = sqrtf(wv);
                 scr[ro * NpS + v] = ev;
             }
         }
@@ -251,15 +268,16 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             }
         }
 
-        // ---- A-matrix column of line `li` into ring slot `slot` (exact bins) ----
+        // ---- A-matrix column of line `li` into ring slot `slot` (exact bins);
+        //      unused entries carry a = 0 ----
         auto acol = [&](int li, int slot) {
             const int loc = order[li];
             const int col = k0 + loc % S, row = j0 + loc / S;
             const double x = vx(g, col), y = vy(g, row);
-            float *av = aval + slot * amax * NpS;
-            int *ao = aso + slot * amax * NpS;
-            uint8_t *ac = acnt + slot * NpS;
-            for (int v = tid; v < Np; v += nthr) {
+            AEnt *ar = aring + slot * amax * NpS;
+            for (int l = lane; l < av_lanes; l += 32) {
+                const int v = l * nwarps + warp;
+                if (v >= Np) break;
                 const double r = __dsub_rn(__dmul_rn(x, cs[v]), __dmul_rn(y, sn[v]));
                 const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
                 int n = 0;
@@ -284,15 +302,22 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                                 if (off < 0 || off >= W || n >= amax) {
                                     atomicOr(err, 1);
                                 } else {
-                                    av[n * NpS + v] = (float)num * inv_off_f;
-                                    ao[n * NpS + v] = off * NpS + v;
+                                    AEnt en;
+                                    en.a = (float)num * inv_off_f;
+                                    en.so = off * NpS + v;
+                                    ar[n * NpS + v] = en;
                                     n++;
                                 }
                             }
                         }
                     }
                 }
-                ac[v] = (uint8_t)n;
+                for (; n < amax; n++) {
+                    AEnt en;
+                    en.a = 0.0f;
+                    en.so = v;
+                    ar[n * NpS + v] = en;
+                }
             }
         };
 
@@ -327,40 +352,51 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 } else {
                     // ---- data term over this slice's band rows, this warp's views ----
                     float th1 = 0.0f, th2 = 0.0f;
-                    const float *av = aval + slot * amax * NpS;
-                    const int *ao = aso + slot * amax * NpS;
-                    const uint8_t *ac = acnt + slot * NpS;
-                    const int rowbase = zl * mz * W * NpS;
-                    for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
-                        const int cnt = ac[v];
-                        for (int q = 0; q < cnt; q++) {
-                            const float a = av[q * NpS + v];
-                            int so = rowbase + ao[q * NpS + v];
-                            for (int rr = 0; rr < mz; rr++, so += W * NpS) {
-                                const float e = eb[so], w = wb[so];
-                                const float sw = sqrtf(w);
-                                float om = w;
-                                if (!(fabsf(e * sw) < hT)) om = hTd * sw / fabsf(e);
-                                th2 = fmaf(a * a, om, th2);
-                                th1 = fmaf(-e * a, om, th1);
+                    const AEnt *ar = aring + slot * amax * NpS;
+                    const float *erow = eb + zl * mz * rowstride;
+                    const float *srow = sb + zl * mz * rowstride;
+                    auto theta_entry = [&](const AEnt &en, int rr) {
+                        const float e = erow[rr * rowstride + en.so];
+                        const float sw = srow[rr * rowstride + en.so];
+                        float om = sw * sw;
+                        if (!(fabsf(e * sw) < hT)) om = __fdividef(hTd * sw, fabsf(e));
+                        if (en.a != 0.0f) {
+                            th2 = fmaf(en.a * en.a, om, th2);
+                            th1 = fmaf(-e * en.a, om, th1);
+                        }
+                    };
+                    if constexpr (AMAXC > 0 && MZC > 0) {
+#pragma unroll 2
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+#pragma unroll
+                            for (int q = 0; q < AMAXC; q++) {
+                                const AEnt en = ar[q * NpS + v];
+#pragma unroll
+                                for (int rr = 0; rr < MZC; rr++) theta_entry(en, rr);
                             }
                         }
+                    } else {
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit)
+                            for (int q = 0; q < amax; q++) {
+                                const AEnt en = ar[q * NpS + v];
+                                if (en.a == 0.0f) break;
+                                for (int rr = 0; rr < mz; rr++) theta_entry(en, rr);
+                            }
                     }
                     th1 = warp_allsum(th1);
                     th2 = warp_allsum(th2);
-                    // prior sums: f * rho'(D)/D for q = 2, p = 1.2 is (2 - 0.8 t1/t3) / (t3 s^q)
+                    // prior: f * rho'(D)/D for q = 2, p = 1.2 is (2 - 0.8 t1/t3) / (t3 s^q)
                     float b = 0.0f;
                     if (valid) {
-                        const float d = V - nbv;
-                        const float ad = fabsf(d);
-                        const float t1 = (ad > 0.0f ? exp2f(0.8f * log2f(ad)) : 0.0f) * (spatial ? sSQP_inv : sTQP_inv);
-                        const float t3 = (spatial ? cS : cT) + t1;
-                        b = bw * (2.0f - 0.8f * t1 / t3) / (t3 * (spatial ? sSQ : sTQ));
+                        const float ad = fabsf(V - nbv);
+                        const float t1 = (ad > 0.0f ? exp2f(0.8f * __log2f(ad)) : 0.0f) * qpinv;
+                        const float rt3 = __frcp_rn(cc + t1);
+                        b = bw * (2.0f - 0.8f * t1 * rt3) * rt3 * qinv;
                     }
                     const float p1 = warp_allsum(b * nbv);
                     const float p2 = warp_allsum(b);
                     if (vsplit > 1) {
-                        float *pp = part + (((step & 1) * sp.max_nz + zl) * 2) * 2;
+                        float *pp = part + 4 * zl;
                         if (lane == 0) {
                             pp[vh * 2 + 0] = th1;
                             pp[vh * 2 + 1] = th2;
@@ -383,13 +419,32 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         }
                     }
                     // ---- error sinogram: e -= a dx over this slice's rows ----
-                    for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
-                        const int cnt = ac[v];
-                        for (int q = 0; q < cnt; q++) {
-                            const float a = av[q * NpS + v];
-                            int so = rowbase + ao[q * NpS + v];
-                            for (int rr = 0; rr < mz; rr++, so += W * NpS) eb[so] = fmaf(-a, dx, eb[so]);
+                    float *erw = eb + zl * mz * rowstride;
+                    if constexpr (AMAXC > 0 && MZC > 0) {
+#pragma unroll 2
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+#pragma unroll
+                            for (int q = 0; q < AMAXC; q++) {
+                                const AEnt en = ar[q * NpS + v];
+                                if (en.a != 0.0f) {
+#pragma unroll
+                                    for (int rr = 0; rr < MZC; rr++) {
+                                        float *pe = erw + rr * rowstride + en.so;
+                                        *pe = fmaf(-en.a, dx, *pe);
+                                    }
+                                }
+                            }
                         }
+                    } else {
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit)
+                            for (int q = 0; q < amax; q++) {
+                                const AEnt en = ar[q * NpS + v];
+                                if (en.a == 0.0f) break;
+                                for (int rr = 0; rr < mz; rr++) {
+                                    float *pe = erw + rr * rowstride + en.so;
+                                    *pe = fmaf(-en.a, dx, *pe);
+                                }
+                            }
                     }
                 }
             }
@@ -421,7 +476,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             }
         }
     }
-    // ---- per-CTA statistics (only lane 0 of each slice's first warp counts) ----
+    // ---- per-CTA statistics (lane 0 of each slice's first warp counts) ----
     if (lane == 0) {
         s_red[warp][0] = sum_abs_dx;
         s_red[warp][1] = sum_abs_x;
@@ -451,21 +506,15 @@ size_t mbir_sv_smem_bytes(const SvParams &sp)
     const size_t NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
     size_t b = 0;
     b += 2 * sizeof(double) * NpS;
+    b += 8 * 3 * (size_t)sp.amax * NpS;  // A ring of (value, offset) pairs
     b += 2 * sizeof(float) * (size_t)sp.max_rows * sp.W * NpS;
-    b += (sizeof(float) + sizeof(int)) * 3 * sp.amax * NpS;
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     b += sizeof(float) * 2 * sp.max_nz * S * S;
     b += sizeof(float) * S * S;
-    b += sizeof(float) * 2 * 2 * 2 * sp.max_nz * 2;
+    b += sizeof(float) * 4 * sp.max_nz;
     b += sizeof(int) * NpS * 2;
     b += sizeof(int) * S * S;
-    b += 3 * NpS;
     return (b + 15) & ~(size_t)15;
-}
-
-int mbir_sv_ctas(int ntasks, int sm_count)
-{
-    return ntasks < sm_count ? ntasks : sm_count;
 }
 
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
@@ -474,11 +523,19 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
 {
     if (ntasks <= 0) return cudaSuccess;
     const size_t sm = mbir_sv_smem_bytes(sp);
-    cudaError_t e = cudaFuncSetAttribute(k_icd_sv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(queue, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
-    k_icd_sv<<<ctas, 32 * sp.max_nz * sp.vsplit, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter,
-                                                          seed, err);
+    const int threads = 32 * sp.max_nz * sp.vsplit;
+    // full resolution (3 bins per column, one detector row per slice) has its
+    // own instantiation with fixed trip counts
+    if (sp.amax == 3 && g.m_z == 1) {
+        e = cudaFuncSetAttribute(k_icd_sv<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_icd_sv<3, 1><<<ctas, threads, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter, seed, err);
+    } else {
+        e = cudaFuncSetAttribute(k_icd_sv<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_icd_sv<0, 0><<<ctas, threads, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter, seed, err);
+    }
     return cudaGetLastError();
 }
