@@ -230,7 +230,7 @@ def gpu_arm(args, rank, world, local_rank):
     coarse, fine = coarse_start(scan)
     sched = 1 if args.schedule == "sv" else 0
     st = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
-    st.set_schedule(sched, args.sv_side)
+    st.set_schedule(sched, args.sv_side, args.warps_per_slice)
     sched_info = st.schedule_info()
     st.prepare(fine)
     for it in range(1, args.warmup + 1):
@@ -278,7 +278,7 @@ def gpu_arm(args, rank, world, local_rank):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
         s2 = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
-        s2.set_schedule(sched, args.sv_side)
+        s2.set_schedule(sched, args.sv_side, args.warps_per_slice)
         s2.prepare(fine)
         s2.iterate(1)
         _ = s2.object()
@@ -363,6 +363,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
+    ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

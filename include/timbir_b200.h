@@ -78,11 +78,13 @@ int mbir_icd_prepare(MbirStage *stage, const float *object, const float *offset,
  *      blocks of voxel lines updated by one CTA each from a shared-memory copy
  *      of the error-sinogram band they touch, blocks of one colour of a
  *      (x, y, z-group, frame) checkerboard in parallel.  sv_side 0 picks the
- *      largest side (<= 16) whose band fits shared memory.
+ *      largest side (<= 16) whose band fits shared memory; warps_per_slice
+ *      (1, 2 or 4; 0 = 2 when a z-group has at most 15 slices) splits each
+ *      slice's views over that many warps.
  * The magnitude map of schedule 1 has one plane per (frame, z-group). */
-int mbir_set_schedule(MbirStage *stage, int32_t schedule, int32_t sv_side);
+int mbir_set_schedule(MbirStage *stage, int32_t schedule, int32_t sv_side, int32_t warps_per_slice);
 int mbir_get_schedule(MbirStage *stage, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
-                      int32_t *band_width, int32_t *phases);
+                      int32_t *band_width, int32_t *phases, int32_t *warps_per_slice);
 
 /* One outer ICD iteration with the reference schedule
  * (updateVoxelsTimeSlices, XT_ICD_update.c:936-1105): random line order,

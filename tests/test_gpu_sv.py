@@ -108,3 +108,16 @@ def test_sv_one_warp_per_slice_for_tall_groups():
     f.prepare(s.object(), s.offset())
     scale = np.abs(f.errorsino()).max()
     assert np.abs(s.errorsino() - f.errorsino()).max() < 2e-5 * scale
+
+
+@pytest.mark.parametrize("wps", [1, 2, 4])
+def test_sv_warps_per_slice_reach_the_same_map(wps):
+    g = np.load(os.path.join(GOLD, "converged_plain.npz"))
+    s = scenarios.make("plain", timbir_b200.Stage)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0, wps)
+    assert s.schedule_info()["warps_per_slice"] == wps
+    s.prepare()
+    for it in range(1, 301):
+        s.iterate(it)
+    c = fresh_cost_fp64("plain", s.object())
+    assert abs(c - float(g["ref_fresh_cost"])) / float(g["ref_fresh_cost"]) < 1e-5

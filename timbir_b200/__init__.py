@@ -67,8 +67,8 @@ def load_library() -> C.CDLL:
     lib.mbir_forward_project.argtypes = [_VP, _f32p, _f32p]
     lib.mbir_get_kernel_stats.argtypes = [_VP, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                           C.POINTER(C.c_longlong)]
-    lib.mbir_set_schedule.argtypes = [_VP, i32, i32]
-    lib.mbir_get_schedule.argtypes = [_VP] + [C.POINTER(i32)] * 5
+    lib.mbir_set_schedule.argtypes = [_VP, i32, i32, i32]
+    lib.mbir_get_schedule.argtypes = [_VP] + [C.POINTER(i32)] * 6
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     lib.reconstruct.argtypes = [C.POINTER(C.POINTER(C.c_float))] + [_VP] * 5 + [i32] * 4 + [fl] * 7 + \
@@ -138,18 +138,20 @@ class Stage:
     SCHEDULE_REFERENCE = 0
     SCHEDULE_SUPERVOXEL = 1
 
-    def set_schedule(self, schedule: int, sv_side: int = 0):
+    def set_schedule(self, schedule: int, sv_side: int = 0, warps_per_slice: int = 0):
         """0: the reference's checkerboard z-block schedule; 1: super-voxel
-        schedule (sv_side 0 = largest side whose band fits shared memory)."""
-        _check(self.lib.mbir_set_schedule(self.h, schedule, sv_side))
+        schedule (sv_side 0 = largest side whose band fits shared memory;
+        warps_per_slice 0 = automatic)."""
+        _check(self.lib.mbir_set_schedule(self.h, schedule, sv_side, warps_per_slice))
         d = np.zeros(9, np.int32)
         self.lib.mbir_stage_dims(self.h, d)
         self.nblk = int(d[7])
 
     def schedule_info(self) -> dict:
-        v = [C.c_int32() for _ in range(5)]
+        v = [C.c_int32() for _ in range(6)]
         self.lib.mbir_get_schedule(self.h, *[C.byref(x) for x in v])
-        return dict(zip(("schedule", "sv_side", "z_group", "band_width", "phases"), [x.value for x in v]))
+        return dict(zip(("schedule", "sv_side", "z_group", "band_width", "phases", "warps_per_slice"),
+                        [x.value for x in v]))
 
     def prepare(self, obj=None, offset=None, magmap=None):
         arrs = [None if a is None else _f32(a) for a in (obj, offset, magmap)]

@@ -444,7 +444,7 @@ static int random_select(MbirStage *S)
 // ---------------------------------------------------------------------------
 // Super-voxel schedule
 // ---------------------------------------------------------------------------
-static SvParams sv_params(const MbirStage *S, int side, int nz)
+static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
 {
     SvParams sp{};
     const double m = S->st.delta_xy / S->sg.delta_r;
@@ -456,7 +456,10 @@ static SvParams sv_params(const MbirStage *S, int side, int nz)
     sp.max_views = S->max_views();
     sp.max_nz = nz;
     sp.max_rows = nz * S->st.m_z;
-    sp.vsplit = nz <= 15 ? 2 : 1;
+    // warps per slice: up to 4 (named barriers 1..15 serve one slice each)
+    if (vsplit <= 0) vsplit = nz <= 15 ? 2 : 1;
+    while (vsplit > 1 && (nz > 15 || 32 * nz * vsplit > 1024)) vsplit /= 2;
+    sp.vsplit = std::min(vsplit, 4);
     sp.band_floats = (size_t)sp.max_rows * sp.W * sp.max_views;
     return sp;
 }
@@ -466,7 +469,7 @@ static const size_t kSmemLimit = 227 * 1024;
 // Super-voxel side 0 = choose the largest side (<= 16) whose band for a
 // z-group of min(N_z, 32) slices fits shared memory, shrinking the group if
 // even side 4 does not fit.
-extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side)
+extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side, int32_t warps_per_slice)
 {
     if (schedule == 0) {
         S->schedule = 0;
@@ -478,19 +481,19 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     SvParams sp{};
     for (;;) {
         if (side > 0) {
-            sp = sv_params(S, side, gz);
+            sp = sv_params(S, side, gz, warps_per_slice);
             if (mbir_sv_smem_bytes(sp) <= kSmemLimit) break;
         } else {
             int best = 0;
             for (int s = 16; s >= 4; s--) {
-                sp = sv_params(S, s, gz);
+                sp = sv_params(S, s, gz, warps_per_slice);
                 if (mbir_sv_smem_bytes(sp) <= kSmemLimit) {
                     best = s;
                     break;
                 }
             }
             if (best) {
-                sp = sv_params(S, best, gz);
+                sp = sv_params(S, best, gz, warps_per_slice);
                 break;
             }
         }
@@ -573,8 +576,9 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
 }
 
 extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
-                                 int32_t *band_width, int32_t *phases)
+                                 int32_t *band_width, int32_t *phases, int32_t *warps_per_slice)
 {
+    if (warps_per_slice) *warps_per_slice = S->sp.vsplit;
     if (schedule) *schedule = S->schedule;
     if (sv_side) *sv_side = S->sp.S;
     if (z_group) *z_group = S->gz;

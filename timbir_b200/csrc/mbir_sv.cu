@@ -69,6 +69,23 @@ __device__ __forceinline__ float warp_allsum(float v)
     return v;
 }
 
+// Four independent butterfly all-reductions, interleaved so their shuffle
+// latencies overlap.
+__device__ __forceinline__ void warp_allsum4(float &a, float &b, float &c, float &d)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ta = __shfl_xor_sync(0xffffffffu, a, o);
+        const float tb = __shfl_xor_sync(0xffffffffu, b, o);
+        const float tc = __shfl_xor_sync(0xffffffffu, c, o);
+        const float td = __shfl_xor_sync(0xffffffffu, d, o);
+        a += ta;
+        b += tb;
+        c += tc;
+        d += td;
+    }
+}
+
 __device__ __forceinline__ uint32_t hash32(uint32_t x)
 {
     x ^= x >> 16;
@@ -118,7 +135,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
     float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * S * S;
-    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 4 * sp.max_nz;
+    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 4 * 4 * sp.max_nz;
     int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
     int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
     int *order = reinterpret_cast<int *>(p); p += sizeof(int) * S * S;
@@ -276,7 +293,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             const double x = vx(g, col), y = vy(g, row);
             AEnt *ar = aring + slot * amax * NpS;
             for (int l = lane; l < av_lanes; l += 32) {
-                const int v = l * nwarps + warp;
+                const int v = warp * av_lanes + l;
                 if (v >= Np) break;
                 const double r = __dsub_rn(__dmul_rn(x, cs[v]), __dmul_rn(y, sn[v]));
                 const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
@@ -351,28 +368,44 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     if (vh == 0 && lane == 0) n_skip++;
                 } else {
                     // ---- data term over this slice's band rows, this warp's views ----
-                    float th1 = 0.0f, th2 = 0.0f;
+                    float th1 = 0.0f, th2 = 0.0f, th1b = 0.0f, th2b = 0.0f;
                     const AEnt *ar = aring + slot * amax * NpS;
                     const float *erow = eb + zl * mz * rowstride;
                     const float *srow = sb + zl * mz * rowstride;
-                    auto theta_entry = [&](const AEnt &en, int rr) {
+                    auto theta_entry = [&](const AEnt &en, int rr, float &t1, float &t2) {
                         const float e = erow[rr * rowstride + en.so];
                         const float sw = srow[rr * rowstride + en.so];
                         float om = sw * sw;
                         if (!(fabsf(e * sw) < hT)) om = __fdividef(hTd * sw, fabsf(e));
                         if (en.a != 0.0f) {
-                            th2 = fmaf(en.a * en.a, om, th2);
-                            th1 = fmaf(-e * en.a, om, th1);
+                            t2 = fmaf(en.a * en.a, om, t2);
+                            t1 = fmaf(-e * en.a, om, t1);
                         }
                     };
                     if constexpr (AMAXC > 0 && MZC > 0) {
-#pragma unroll 2
-                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+                        int v = vh * 32 + lane;
+                        const int vstep = 32 * vsplit;
+                        for (; v + vstep < Np; v += 2 * vstep) {
+                            AEnt ea[AMAXC], eb2[AMAXC];
+#pragma unroll
+                            for (int q = 0; q < AMAXC; q++) {
+                                ea[q] = ar[q * NpS + v];
+                                eb2[q] = ar[q * NpS + v + vstep];
+                            }
+#pragma unroll
+                            for (int q = 0; q < AMAXC; q++)
+#pragma unroll
+                                for (int rr = 0; rr < MZC; rr++) {
+                                    theta_entry(ea[q], rr, th1, th2);
+                                    theta_entry(eb2[q], rr, th1b, th2b);
+                                }
+                        }
+                        if (v < Np) {
 #pragma unroll
                             for (int q = 0; q < AMAXC; q++) {
                                 const AEnt en = ar[q * NpS + v];
 #pragma unroll
-                                for (int rr = 0; rr < MZC; rr++) theta_entry(en, rr);
+                                for (int rr = 0; rr < MZC; rr++) theta_entry(en, rr, th1, th2);
                             }
                         }
                     } else {
@@ -380,30 +413,39 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                             for (int q = 0; q < amax; q++) {
                                 const AEnt en = ar[q * NpS + v];
                                 if (en.a == 0.0f) break;
-                                for (int rr = 0; rr < mz; rr++) theta_entry(en, rr);
+                                for (int rr = 0; rr < mz; rr++) theta_entry(en, rr, th1, th2);
                             }
                     }
-                    th1 = warp_allsum(th1);
-                    th2 = warp_allsum(th2);
-                    // prior: f * rho'(D)/D for q = 2, p = 1.2 is (2 - 0.8 t1/t3) / (t3 s^q)
-                    float b = 0.0f;
-                    if (valid) {
+                    th1 += th1b;
+                    th2 += th2b;
+                    // prior (first warp of the slice): f rho'(D)/D for q = 2, p = 1.2
+                    // is (2 - 0.8 t1/t3) / (t3 s^q)
+                    float p1 = 0.0f, p2 = 0.0f;
+                    if (vh == 0 && valid) {
                         const float ad = fabsf(V - nbv);
                         const float t1 = (ad > 0.0f ? exp2f(0.8f * __log2f(ad)) : 0.0f) * qpinv;
                         const float rt3 = __frcp_rn(cc + t1);
-                        b = bw * (2.0f - 0.8f * t1 * rt3) * rt3 * qinv;
+                        const float b = bw * (2.0f - 0.8f * t1 * rt3) * rt3 * qinv;
+                        p1 = b * nbv;
+                        p2 = b;
                     }
-                    const float p1 = warp_allsum(b * nbv);
-                    const float p2 = warp_allsum(b);
+                    warp_allsum4(th1, th2, p1, p2);
                     if (vsplit > 1) {
-                        float *pp = part + 4 * zl;
+                        float *pp = part + 4 * vsplit * zl;
                         if (lane == 0) {
-                            pp[vh * 2 + 0] = th1;
-                            pp[vh * 2 + 1] = th2;
+                            pp[vh * 4 + 0] = th1;
+                            pp[vh * 4 + 1] = th2;
+                            pp[vh * 4 + 2] = p1;
+                            pp[vh * 4 + 3] = p2;
                         }
                         named_barrier(1 + zl, 32 * vsplit);
-                        th1 = pp[0] + pp[2];
-                        th2 = pp[1] + pp[3];
+                        th1 = th2 = 0.0f;
+                        for (int h = 0; h < vsplit; h++) {
+                            th1 += pp[h * 4 + 0];
+                            th2 += pp[h * 4 + 1];
+                        }
+                        p1 = pp[2];
+                        p2 = pp[3];
                     }
                     const float u = (p1 + th2 * V - th1) / (p2 + th2);
                     const float xn = V + alpha * (u - V);
@@ -511,7 +553,7 @@ size_t mbir_sv_smem_bytes(const SvParams &sp)
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     b += sizeof(float) * 2 * sp.max_nz * S * S;
     b += sizeof(float) * S * S;
-    b += sizeof(float) * 4 * sp.max_nz;
+    b += sizeof(float) * 4 * 4 * sp.max_nz;
     b += sizeof(int) * NpS * 2;
     b += sizeof(int) * S * S;
     return (b + 15) & ~(size_t)15;
