@@ -84,7 +84,9 @@ struct MbirStage {
     std::vector<std::vector<SvTask>> sv_phase;  // tasks of each colour phase
     std::vector<SvTask> sv_all;                 // every task, with its phase
     std::vector<int> sv_all_phase;
-    SvTask *d_sv_tasks = nullptr;
+    SvTask *d_sv_tasks = nullptr, *d_sv_sel = nullptr;
+    std::vector<int> sv_phase_off;  // phase q's tasks: [off[q], off[q+1]) of d_sv_tasks
+    cudaEvent_t sv_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     SvTaskOut *d_sv_out = nullptr;
     float *d_scratch = nullptr;
     int *d_err = nullptr, *d_queue = nullptr;
@@ -106,13 +108,15 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_tasks, d_sv_out, d_scratch, d_err, d_queue};
+                        d_sv_tasks, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue};
         for (void *b : bufs)
             if (b) cudaFree(b);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (tev0) cudaEventDestroy(tev0);
         if (tev1) cudaEventDestroy(tev1);
+        for (auto e : sv_ev)
+            if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -460,11 +464,16 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     if (vsplit <= 0) vsplit = nz <= 15 ? 2 : 1;
     while (vsplit > 1 && (nz > 15 || 32 * nz * vsplit > 1024)) vsplit /= 2;
     sp.vsplit = std::min(vsplit, 4);
+    // producer warps for the A-matrix columns: one view per lane, within the
+    // 1024-thread limit
+    const int want = (sp.max_views + 31) / 32;
+    sp.prod_warps = std::max(0, std::min(std::min(want, 8), (1024 - 32 * nz * sp.vsplit) / 32));
     sp.band_floats = (size_t)sp.max_rows * sp.W * sp.max_views;
     return sp;
 }
 
 static const size_t kSmemLimit = 227 * 1024;
+static const int kMaxLaunchesPerIter = 64;
 
 // Super-voxel side 0 = choose the largest side (<= 16) whose band for a
 // z-group of min(N_z, 32) slices fits shared memory, shrinking the group if
@@ -556,21 +565,37 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    // every phase's task list lives on the device; the non-homogeneous
+    // selection gets a second list of the same capacity
+    std::vector<SvTask> flat;
+    S->sv_phase_off.assign(nphase + 1, 0);
+    for (int q = 0; q < nphase; q++) {
+        S->sv_phase_off[q] = (int)flat.size();
+        flat.insert(flat.end(), S->sv_phase[q].begin(), S->sv_phase[q].end());
+    }
+    S->sv_phase_off[nphase] = (int)flat.size();
     size_t maxt = 1;
     for (auto &ph : S->sv_phase) maxt = std::max(maxt, ph.size());
     cudaFree(S->d_sv_tasks);
+    cudaFree(S->d_sv_sel);
     cudaFree(S->d_sv_out);
     cudaFree(S->d_scratch);
-    S->d_sv_tasks = nullptr;
+    cudaFree(S->d_queue);
+    S->d_sv_tasks = S->d_sv_sel = nullptr;
     S->d_sv_out = nullptr;
     S->d_scratch = nullptr;
-    CK(dalloc(&S->d_sv_tasks, maxt));
+    S->d_queue = nullptr;
+    CK(dalloc(&S->d_sv_tasks, flat.size()));
+    CK(dalloc(&S->d_sv_sel, flat.size()));
+    CK(cudaMemcpy(S->d_sv_tasks, flat.data(), flat.size() * sizeof(SvTask), cudaMemcpyHostToDevice));
     const size_t ctas = std::min<size_t>(maxt, (size_t)S->sm_count);
-    CK(dalloc(&S->d_sv_out, ctas));
+    CK(dalloc(&S->d_sv_out, 2));
     CK(dalloc(&S->d_scratch, ctas * sp.band_floats));
-    if (!S->d_queue) CK(dalloc(&S->d_queue, 1));
+    CK(dalloc(&S->d_queue, kMaxLaunchesPerIter));
     if (!S->d_err) CK(dalloc(&S->d_err, 1));
     CK(cudaMemset(S->d_err, 0, sizeof(int)));
+    if (!S->sv_ev[0])
+        for (auto &e : S->sv_ev) CK(cudaEventCreate(&e));
     S->schedule = 1;
     return 0;
 }
@@ -587,32 +612,16 @@ extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_si
     return 0;
 }
 
-static int sv_launch(MbirStage *S, const std::vector<SvTask> &tasks, int iter, uint32_t seed, double *dx,
-                     double *ax)
+// One launch of the SV kernel over `n` device-resident tasks; no host sync.
+static int sv_launch(MbirStage *S, const SvTask *d_tasks, int n, int iter, uint32_t seed, int qslot,
+                     SvTaskOut *acc)
 {
-    if (tasks.empty()) return 0;
-    CK(cudaMemcpyAsync(S->d_sv_tasks, tasks.data(), tasks.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
-                       S->stream));
-    CK(cudaEventRecord(S->ev0, S->stream));
-    const int ctas = std::min((int)tasks.size(), S->sm_count);
-    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, S->d_sv_tasks, (int)tasks.size(), ctas, S->d_queue, S->d_scratch,
-                          S->d_sv_out, iter, seed, S->d_err, S->stream));
-    CK(cudaEventRecord(S->ev1, S->stream));
+    if (n <= 0) return 0;
+    const int ctas = std::min(n, S->sm_count);
+    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, d_tasks, n, ctas, S->d_queue + qslot, S->d_scratch, acc,
+                          iter, seed, S->d_err, S->stream));
     S->launches++;
     S->icd_launches++;
-    std::vector<SvTaskOut> out(ctas);
-    CK(cudaMemcpyAsync(out.data(), S->d_sv_out, out.size() * sizeof(SvTaskOut), cudaMemcpyDeviceToHost,
-                       S->stream));
-    CK(cudaStreamSynchronize(S->stream));
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
-    S->icd_ms += ms;
-    for (auto &o : out) {
-        *dx += o.sum_abs_dx;
-        *ax += o.sum_abs_x;
-        S->updates += o.updates;
-        S->zero_skips += o.zero_skips;
-    }
     return 0;
 }
 
@@ -626,26 +635,34 @@ static int sv_launch(MbirStage *S, const std::vector<SvTask> &tasks, int iter, u
 static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
     const int P = (int)S->sv_phase.size();
-    double dx = 0, ax = 0;
+    int qslot = 0;
+    CK(cudaMemsetAsync(S->d_queue, 0, kMaxLaunchesPerIter * sizeof(int), S->stream));
+    CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
+    CK(cudaEventRecord(S->sv_ev[0], S->stream));
     for (int q = 0; q < P; q++) {
+        const int ph = (q + iter) % P;
         const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
-        if (sv_launch(S, S->sv_phase[(q + iter) % P], iter, seed, &dx, &ax)) return -1;
+        if (sv_launch(S, S->d_sv_tasks + S->sv_phase_off[ph], S->sv_phase_off[ph + 1] - S->sv_phase_off[ph], iter,
+                      seed, qslot++, S->d_sv_out))
+            return -1;
     }
+    CK(cudaEventRecord(S->sv_ev[1], S->stream));
     if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
-    const double hicd_dx = dx, hicd_ax = ax;
+    bool nh = false;
     if (iter > 1 && S->nh_fraction > 0) {
         // score = summed last-visit magnitude over the SV's lines
         std::vector<float> mag(S->nmag());
-        CK(cudaMemcpy(mag.data(), S->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(mag.data(), S->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost, S->stream));
+        CK(cudaStreamSynchronize(S->stream));
         const int side = S->sp.S, N_x = S->st.N_x, N_y = S->st.N_y;
         std::vector<std::pair<float, int>> score(S->sv_all.size());
         for (size_t q = 0; q < S->sv_all.size(); q++) {
             const SvTask &t = S->sv_all[q];
             const float *pl = mag.data() + ((size_t)t.frame * S->nzg + t.z0 / S->gz) * S->nxy();
-            double s = 0;
+            double sc = 0;
             for (int y = t.j0; y < std::min(N_y, t.j0 + side); y++)
-                for (int x = t.k0; x < std::min(N_x, t.k0 + side); x++) s += pl[(size_t)y * N_x + x];
-            score[q] = {(float)s, (int)q};
+                for (int x = t.k0; x < std::min(N_x, t.k0 + side); x++) sc += pl[(size_t)y * N_x + x];
+            score[q] = {(float)sc, (int)q};
         }
         const size_t nsel = (size_t)std::ceil(S->nh_fraction * score.size());
         std::partial_sort(score.begin(), score.begin() + nsel, score.end(),
@@ -656,18 +673,50 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
             const int id = score[q].second;
             sel[S->sv_all_phase[id]].push_back(S->sv_all[id]);
         }
-        double ndx = 0, nax = 0;
+        std::vector<SvTask> flat;
+        std::vector<int> off(P + 1, 0);
         for (int q = 0; q < P; q++) {
-            const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
-            if (sv_launch(S, sel[(q + iter) % P], iter, seed, &ndx, &nax)) return -1;
+            off[q] = (int)flat.size();
+            std::stable_sort(sel[q].begin(), sel[q].end(),
+                             [](const SvTask &a, const SvTask &b) { return a.nlines > b.nlines; });
+            flat.insert(flat.end(), sel[q].begin(), sel[q].end());
+        }
+        off[P] = (int)flat.size();
+        if (!flat.empty()) {
+            nh = true;
+            CK(cudaMemcpyAsync(S->d_sv_sel, flat.data(), flat.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
+                               S->stream));
+            CK(cudaEventRecord(S->sv_ev[2], S->stream));
+            for (int q = 0; q < P; q++) {
+                const int ph = (q + iter) % P;
+                const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
+                if (sv_launch(S, S->d_sv_sel + off[ph], off[ph + 1] - off[ph], iter, seed, qslot++, S->d_sv_out + 1))
+                    return -1;
+            }
+            CK(cudaEventRecord(S->sv_ev[3], S->stream));
+            CK(cudaStreamSynchronize(S->stream));  // keep `flat` alive until the copy ran
         }
         if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
     }
     if (S->upd_var == 1 && mbir_update_variance_parameter(S)) return -1;
+    SvTaskOut acc[2];
     int err = 0;
-    CK(cudaMemcpy(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(acc, S->d_sv_out, sizeof(acc), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaMemcpyAsync(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, S->sv_ev[0], S->sv_ev[1]));
+    S->icd_ms += ms;
+    if (nh) {
+        CK(cudaEventElapsedTime(&ms, S->sv_ev[2], S->sv_ev[3]));
+        S->icd_ms += ms;
+    }
     if (err) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
-    S->last_pct = hicd_ax > 0 ? 100.0 * S->K * hicd_dx / hicd_ax : 0.0;
+    for (int q = 0; q < (nh ? 2 : 1); q++) {
+        S->updates += acc[q].updates;
+        S->zero_skips += acc[q].zero_skips;
+    }
+    S->last_pct = acc[0].sum_abs_x > 0 ? 100.0 * S->K * acc[0].sum_abs_dx / acc[0].sum_abs_x : 0.0;
     *converged = S->last_pct < S->stop_thresh ? 1 : 0;
     return 0;
 }

@@ -62,13 +62,6 @@ __device__ __forceinline__ int floor_div(double a, double b, double inv_b)
     return (int)f;
 }
 
-__device__ __forceinline__ float warp_allsum(float v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 // Four independent butterfly all-reductions, interleaved so their shuffle
 // latencies overlap.
 __device__ __forceinline__ void warp_allsum4(float &a, float &b, float &c, float &d)
@@ -112,8 +105,8 @@ struct AEnt {
 template <int AMAXC, int MZC>
 __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp,
                                                   const SvTask *__restrict__ tasks, int ntasks,
-                                                  int *queue, float *scratch, SvTaskOut *__restrict__ out,
-                                                  int iter, uint32_t seed, int *err)
+                                                  int *queue, float *__restrict__ scratch,
+                                                  SvTaskOut *__restrict__ out, int iter, uint32_t seed, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
@@ -147,8 +140,11 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
     const float sSQ_inv = (float)(1.0 / pr.sSQ), sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
     const float sTQ_inv = (float)(1.0 / pr.sTQ), sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
-    // this warp's slice and view share
-    const int zl = warp / vsplit, vh = warp - zl * vsplit;
+    // warps [0, ncons) update voxels (vsplit per slice); warps [ncons, nwarps)
+    // produce the next line's A-matrix column while they do
+    const int ncons = sp.max_nz * vsplit, nprod = nwarps - ncons;
+    const bool consumer = warp < ncons;
+    const int zl = consumer ? warp / vsplit : 0, vh = consumer ? warp - zl * vsplit : 0;
     // neighbour of lane: spatial (dz, dy, dx) for lanes 0..25, temporal 26, 27
     int ndz = 0, ndy = 0, ndx = 0;
     float bw = 0.0f, qinv = 0.0f, qpinv = 0.0f, cc = 1.0f;
@@ -170,8 +166,10 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         cc = cT;
         temporal = true;
     }
-    // views of the A-column computation: spread over all warps
-    const int av_lanes = (NpS + nwarps - 1) / nwarps;
+    // views of the A-column computation: the producer warps' (all warps
+    // for the first line of a task, or when there are no producers)
+    const int av_all = (NpS + nwarps - 1) / nwarps;
+    const int av_prod = nprod > 0 ? (NpS + nprod - 1) / nprod : 0;
     float sum_abs_dx = 0.0f, sum_abs_x = 0.0f;
     int n_upd = 0, n_skip = 0;
 
@@ -188,7 +186,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         const int k0 = task.k0, j0 = task.j0, z0 = task.z0;
         const int kx = min(S, g.N_x - k0), ky = min(S, g.N_y - j0);
         const int *vl = g.view_idx + (size_t)i * g.max_views;
-        const bool active = zl < nz;
+        const bool active = consumer && zl < nz;
         const int zg = z0 + zl;
 
         // ---- views, trig, band origin per view ----
@@ -241,24 +239,39 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         __syncthreads();
         const int nl = s_nlines;
 
-        // ---- stage bands: e (also to this CTA's scratch slot) and sqrt(w) ----
-        float *scr = scratch + (size_t)blockIdx.x * sp.band_floats;
+        // ---- stage bands: e (also to this CTA's scratch slot) and sqrt(w);
+        //      four loads in flight per thread before the stores ----
+        float *__restrict__ scr = scratch + (size_t)blockIdx.x * sp.band_floats;
         for (int ro = warp; ro < rows * W; ro += nwarps) {
             const int row = ro / W, off = ro - row * W;
             const int t = z0 * mz + row;
-            const float *erow = dv.e + (size_t)t * g.N_p * g.N_r;
-            const float *wrow = dv.w + (size_t)t * g.N_p * g.N_r;
-            for (int v = lane; v < Np; v += 32) {
-                const int r = rlo[v] + off;
-                float ev = 0.0f, wv = 0.0f;
-                if (r < g.N_r) {
-                    const size_t o = (size_t)vidx[v] * g.N_r + r;
-                    ev = erow[o];
-                    wv = __ldg(wrow + o);
+            const float *__restrict__ erow = dv.e + (size_t)t * g.N_p * g.N_r;
+            const float *__restrict__ wrow = dv.w + (size_t)t * g.N_p * g.N_r;
+            for (int v0 = lane; v0 < Np; v0 += 128) {
+                float ev[4], wv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int v = v0 + 32 * u;
+                    ev[u] = 0.0f;
+                    wv[u] = 0.0f;
+                    if (v < Np) {
+                        const int r = rlo[v] + off;
+                        if (r < g.N_r) {
+                            const size_t o = (size_t)vidx[v] * g.N_r + r;
+                            ev[u] = __ldcg(erow + o);
+                            wv[u] = __ldg(wrow + o);
+                        }
+                    }
                 }
-                eb[ro * NpS + v] = ev;
-                sb[ro * NpS + v] = sqrtf(wv);
-                scr[ro * NpS + v] = ev;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int v = v0 + 32 * u;
+                    if (v < Np) {
+                        eb[ro * NpS + v] = ev[u];
+                        sb[ro * NpS + v] = sqrtf(wv[u]);
+                        scr[ro * NpS + v] = ev[u];
+                    }
+                }
             }
         }
         // ---- voxel block with halo, temporal neighbours ----
@@ -287,13 +300,15 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
 
         // ---- A-matrix column of line `li` into ring slot `slot` (exact bins);
         //      unused entries carry a = 0 ----
-        auto acol = [&](int li, int slot) {
+        auto acol = [&](int li, int slot, int w0, int av_lanes) {
+            const int wr = warp - w0;
+            if (wr < 0) return;
             const int loc = order[li];
             const int col = k0 + loc % S, row = j0 + loc / S;
             const double x = vx(g, col), y = vy(g, row);
             AEnt *ar = aring + slot * amax * NpS;
             for (int l = lane; l < av_lanes; l += 32) {
-                const int v = warp * av_lanes + l;
+                const int v = wr * av_lanes + l;
                 if (v >= Np) break;
                 const double r = __dsub_rn(__dmul_rn(x, cs[v]), __dmul_rn(y, sn[v]));
                 const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
@@ -339,7 +354,7 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         };
 
         __syncthreads();
-        if (nl > 0) acol(0, 0);
+        if (nl > 0) acol(0, 0, 0, av_all);
         __syncthreads();
 
         for (int step = 0; step <= nl; step++) {
@@ -490,7 +505,13 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     }
                 }
             }
-            if (step + 1 < nl) acol(step + 1, (step + 1) % 3);
+            if (step + 1 < nl) {
+                if (nprod > 0) {
+                    if (!consumer) acol(step + 1, (step + 1) % 3, ncons, av_prod);
+                } else {
+                    acol(step + 1, (step + 1) % 3, 0, av_all);
+                }
+            }
             __syncthreads();
         }
 
@@ -510,11 +531,22 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         for (int ro = warp; ro < rows * W; ro += nwarps) {
             const int row = ro / W, off = ro - row * W;
             float *erow = dv.e + (size_t)(z0 * mz + row) * g.N_p * g.N_r;
-            for (int v = lane; v < Np; v += 32) {
-                const int r = rlo[v] + off;
-                if (r >= g.N_r) continue;
-                const float dnew = eb[ro * NpS + v] - scr[ro * NpS + v];
-                if (dnew != 0.0f) atomicAdd(erow + (size_t)vidx[v] * g.N_r + r, dnew);
+            for (int v0 = lane; v0 < Np; v0 += 128) {
+                float old[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int v = v0 + 32 * u;
+                    old[u] = v < Np ? scr[ro * NpS + v] : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int v = v0 + 32 * u;
+                    if (v >= Np) continue;
+                    const int r = rlo[v] + off;
+                    if (r >= g.N_r) continue;
+                    const float dnew = eb[ro * NpS + v] - old[u];
+                    if (dnew != 0.0f) atomicAdd(erow + (size_t)vidx[v] * g.N_r + r, dnew);
+                }
             }
         }
     }
@@ -534,10 +566,10 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             d2 += s_red[w][2];
             d3 += s_red[w][3];
         }
-        out[blockIdx.x].sum_abs_dx = d0;
-        out[blockIdx.x].sum_abs_x = d1;
-        out[blockIdx.x].updates = (long long)d2;
-        out[blockIdx.x].zero_skips = (long long)d3;
+        atomicAdd(&out->sum_abs_dx, d0);
+        atomicAdd(&out->sum_abs_x, d1);
+        atomicAdd((unsigned long long *)&out->updates, (unsigned long long)d2);
+        atomicAdd((unsigned long long *)&out->zero_skips, (unsigned long long)d3);
     }
 }
 
@@ -565,9 +597,8 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
 {
     if (ntasks <= 0) return cudaSuccess;
     const size_t sm = mbir_sv_smem_bytes(sp);
-    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
-    const int threads = 32 * sp.max_nz * sp.vsplit;
+    cudaError_t e = cudaSuccess;
+    const int threads = 32 * (sp.max_nz * sp.vsplit + sp.prod_warps);
     // full resolution (3 bins per column, one detector row per slice) has its
     // own instantiation with fixed trip counts
     if (sp.amax == 3 && g.m_z == 1) {

@@ -13,7 +13,8 @@ struct SvParams {
     int max_views;  // max views of any frame (shared-memory stride)
     int max_nz;     // slices per CTA
     int max_rows;   // detector rows per CTA: max_nz * m_z
-    int vsplit;     // warps per slice (1 or 2; 2 needs max_nz <= 15)
+    int vsplit;     // warps per slice (1, 2 or 4; > 1 needs max_nz <= 15)
+    int prod_warps; // warps computing the next line's A-matrix column
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
 };
 
@@ -29,9 +30,9 @@ struct SvTaskOut {
 };
 
 size_t mbir_sv_smem_bytes(const SvParams &sp);
-// ctas persistent CTAs take the ntasks tasks from the queue counter (reset by
-// the launcher); scratch holds ctas * sp.band_floats floats; out holds ctas
-// entries.
+// ctas persistent CTAs take the ntasks tasks from the queue counter (zero
+// before the launch); scratch holds ctas * sp.band_floats floats; the CTAs
+// add their statistics to *out.
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
                                const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
                                SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s);
