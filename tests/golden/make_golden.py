@@ -70,7 +70,7 @@ def stage_fixtures():
         print(name, {k: getattr(v, "shape", v) for k, v in out.items() if k.startswith("obj")})
 
 
-RECON_ARGS = dict(sig_s=0.002, sig_t=1.0, c_s=1e-3, c_t=1e-3, convg_thresh=0.05, remove_rings=0,
+RECON_ARGS = dict(sig_s=0.002, sig_t=1.0, c_s=1e-3, c_t=1e-3, convg_thresh=0.005, remove_rings=0,
                   quad_convex=1, huber_delta=0.5, huber_T=4.0)
 
 

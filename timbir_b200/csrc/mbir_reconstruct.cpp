@@ -14,7 +14,13 @@
 //                             MAX_NUM_ITERATIONS of XT_Constants.h:86).
 //   TIMBIR_Z_BLOCK_THREADS=n  thread count fed to the reference's z-block rule
 //                             (XT_Init.c:389-398); default: as many z-blocks as
-//                             the stage allows.
+//                             the stage allows (reference schedule only).
+//   TIMBIR_SCHEDULE=reference the reference's voxel-update schedule on the GPU
+//                             (checkerboard z-block tasks, random line order,
+//                             exactly updateVoxelsTimeSlices); default: the
+//                             super-voxel schedule, which reaches the same MAP
+//                             estimate far faster.
+//   TIMBIR_SV_SIDE=n          super-voxel side (default: largest that fits).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -162,6 +168,10 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
     const int max_iters = env_int("TIMBIR_MAX_ITERS", 1000);
     const int want_cost = env_int("TIMBIR_COMPUTE_COST", 0);
     const int zthreads = env_int("TIMBIR_Z_BLOCK_THREADS", 1 << 20);
+    const char *sched_env = getenv("TIMBIR_SCHEDULE");
+    const int use_sv = !(sched_env && strcmp(sched_env, "reference") == 0);
+    const int sv_side = env_int("TIMBIR_SV_SIDE", 0);
+    int prev_sv_blocks = -1;  // magnitude-map planes per frame of the previous stage (this call)
     uint32_t rng_state = 761521u;
     std::vector<float> carried_offset;  // ring offsets kept in memory between stages
     const size_t nsino = (size_t)proj_num * proj_rows * proj_cols;
@@ -246,6 +256,20 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
         }
         if (i == last) in.release();
         mbir_set_rng_state(S, rng_state);
+        int nblk_stage = nblk;
+        if (use_sv) {
+            if (mbir_set_schedule(S, 1, sv_side, 0)) {
+                LOG_ERR(log, "Super-voxel schedule set-up failed: %s\n", mbir_last_error());
+                mbir_free_stage(S);
+                in.release_all();
+                return -1;
+            }
+            int32_t d[9];
+            mbir_stage_dims(S, d);
+            nblk_stage = d[7];
+            // the previous stage's map planes are known only within this call
+            prev = prev_sv_blocks > 0 ? prev_sv_blocks : -1;
+        }
         mbir_set_stage_switches(S, upd_offset, upd_var, var_est);
         // ring offsets: read back at stages that re-read them (XT_Init.c:343-351)
         std::vector<float> off((size_t)proj_cols * proj_rows, 0.0f);
@@ -260,7 +284,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
         // initial object and magnitude map (initObject, XT_ICD_update.c:540-651)
         const int N_y = N_x;
         const size_t nvox = (size_t)recon_num * N_z * N_y * N_x, nxy = (size_t)N_y * N_x;
-        std::vector<float> obj(nvox, 0.0f), mag((size_t)recon_num * nblk * nxy, 0.0f);
+        std::vector<float> obj(nvox, 0.0f), mag((size_t)recon_num * nblk_stage * nxy, 0.0f);
         bool have_mag = false;
         if (initICD == 2 || initICD == 3) {
             const int cz = initICD == 3 ? N_z / 2 : N_z;
@@ -281,14 +305,14 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
                     upsample_xy(coarse.data(), dst, cz, N_y / 2, N_x / 2);
             }
             if (init_mag) {
-                if (prev == nblk || prev == nblk / 2) {
+                if (prev > 0 && (prev == nblk_stage || prev == nblk_stage / 2)) {
                     const int pb = prev;
                     std::vector<float> cm((size_t)recon_num * pb * (nxy / 4));
                     if (read_bin("mag_update", cm.data(), sizeof(float), cm.size()) == 0) {
                         for (int f = 0; f < recon_num; f++) {
                             const float *src = cm.data() + (size_t)f * pb * (nxy / 4);
-                            float *dst = mag.data() + (size_t)f * nblk * nxy;
-                            if (pb == nblk)
+                            float *dst = mag.data() + (size_t)f * nblk_stage * nxy;
+                            if (pb == nblk_stage)
                                 upsample_xy(src, dst, pb, N_y / 2, N_x / 2);
                             else
                                 upsample_xyz(src, dst, pb, N_y / 2, N_x / 2);
@@ -361,6 +385,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
             write_bin("proj_offset", carried_offset.data(), sizeof(float), carried_offset.size());
             int32_t st = i;
             write_bin("status", &st, sizeof(int32_t), 1);
+            prev_sv_blocks = nblk_stage;
             rng_state = mbir_get_rng_state(S);
         }
         LOG_INFO(log, "Time elapsed is %f minutes.\n", difftime(time(nullptr), start) / 60.0);
