@@ -129,6 +129,31 @@ int mbir_get_kernel_stats(MbirStage *stage, double *icd_ms, long long *icd_launc
 int mbir_time_begin(MbirStage *stage);
 int mbir_time_end(MbirStage *stage, double *ms);
 
+/* Ring-offset update that allocates no device memory.  No counterpart in the
+ * reference: it is mbir_update_sinogram_offset's computation (the reference's
+ * update_Sinogram_Offset) on device arrays the caller owns, for callers that
+ * must not allocate device memory -- code running while a CUDA graph is
+ * captured, where an allocation breaks the capture, or a host framework that
+ * owns every device allocation and forbids libraries to call cudaMalloc.
+ *   e  device float [N_t][N_p][N_r]  error sinogram, updated in place
+ *   w  device float [N_t][N_p][N_r]  weights
+ *   d  device float [N_t][N_r]       ring offsets, updated in place
+ * remove_rings 1, 2 or 3 and quad_convex / huber_delta / huber_T as for
+ * reconstruct(); stream is a cudaStream_t (NULL for the default stream); the
+ * call returns after the stream has run it.  Its scratch is one file-scope
+ * device array of MBIR_NOALLOC_MAX_ELEMS detector elements (16 MiB, held by
+ * every GPU that loads the library until exit); larger detectors are rejected
+ * with an error (-1, message from mbir_noalloc_last_error()).  The first call
+ * on a device looks the array's address up, so make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised by the
+ * caller.  Nothing in the array needs to start at zero. */
+#define MBIR_NOALLOC_MAX_ELEMS (1 << 20)
+int mbir_update_sinogram_offset_noalloc(float *e, const float *w, float *d, int32_t N_p, int32_t N_r,
+                                        int32_t N_t, int32_t remove_rings, int32_t quad_convex,
+                                        float huber_delta, float huber_T, void *stream);
+const char *mbir_noalloc_last_error(void);
+
 /* A x of an object into a sinogram [proj_num][proj_rows][proj_cols], with the
  * forward projector of initErrorSinogam (XT_ForwardProject.c:8-25).  Meant
  * for a fresh stage: it overwrites the stage's object and error sinogram. */
