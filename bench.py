@@ -40,21 +40,72 @@ sys.path.insert(0, ROOT)
 
 from timbir_b200 import synth  # noqa: E402
 
-CFG = dict(n_xy=256, rows=8, views=256, I0=1e4, seed=0)
-PRIOR = dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=0, quad_convex=1,
-             huber_delta=0.5, huber_T=4.0)
-WORKLOAD = "3d-shepp-logan-like 256x256x8, 256 views, I0=1e4, finest stage"
+class Workload:
+    """A benchmark configuration: scan, prior, warm start, stage count."""
+
+    def __init__(self, name, desc, n_xy, rows, views, frames, prior, data):
+        self.name, self.desc, self.n_xy, self.rows, self.views, self.frames = name, desc, n_xy, rows, views, frames
+        self.prior, self.data = prior, data
+
+    @property
+    def stages(self):
+        # multi-resolution stage count of reconstruct() (XT_Engine.c:111-141)
+        n = max(2, min(8, int(np.log(self.n_xy / 64.0) / np.log(2.0) + 1)))
+        return n
+
+    def scan(self, seed_offset=0):
+        if self.name == "3d":
+            return synth.ellipsoid_scan(self.n_xy, self.rows, self.views, I0=1e4, seed=seed_offset)
+        return fourd_scan(self, seed_offset)
+
+    def warm_start(self, scan):
+        """The 2x-coarser phantom (mean over 2x2x2 cells) and its trilinear x2
+        up-sampling onto the stage grid: the warm start both arms use."""
+        coarse, fine = [], []
+        for ph in scan.phantom:
+            c, f = coarse_start_frame(ph)
+            coarse.append(c)
+            fine.append(f)
+        return np.stack(coarse), np.stack(fine)
+
+
+W3D = Workload("3d", "3d-shepp-logan-like 256x256x8, 256 views, I0=1e4, finest stage", 256, 8, 256, 1,
+               dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=0, quad_convex=1,
+                    huber_delta=0.5, huber_T=4.0),
+               "synthetic (seeded random-ellipsoid phantom, Poisson counts)")
+W4D = Workload("4d", "4d two-phase microstructure 16 x 256x256x16, 1024 interlaced views (K=16, 8 rotations), "
+               "I0=5e3, 0.1% zingers, rings, finest stage", 256, 16, 1024, 16,
+               dict(sig_s=0.002, sig_t=0.004, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=2, quad_convex=0,
+                    huber_delta=0.5, huber_T=4.0),
+               "synthetic (seeded Gaussian-random-field two-phase frames, Poisson counts, zingers, rings)")
+WORKLOADS = {"3d": W3D, "4d": W4D}
 METRIC = "ICD voxel-updates/s"
 
 
-def make_scan(seed_offset=0):
-    return synth.ellipsoid_scan(CFG["n_xy"], CFG["rows"], CFG["views"], I0=CFG["I0"], seed=CFG["seed"] + seed_offset)
+def fourd_scan(w, seed_offset=0):
+    """Config-2 stand-in: thresholded smoothed Gaussian random field coarsened
+    by curvature-flow steps, 16 frames; views interlaced in K = 16 sub-frames,
+    8 rotations of 128 views, 64 views per frame; projected with the engine's
+    own forward projector (the reconstruction's model), Poisson counts at
+    I0 = 5e3, 0.1% of readings x10 (zingers), per-(row, column) log offsets
+    ~ N(0, 0.02) (rings)."""
+    import timbir_b200
+    rng = np.random.default_rng(100 + seed_offset)
+    frames = synth.two_phase_frames(w.n_xy, w.rows, w.frames, seed=seed_offset)
+    angles = synth.interlaced_angles(16, w.views, 128)
+    times = np.arange(w.views, dtype=np.float32)
+    rt = np.linspace(0, w.views, w.frames + 1).astype(np.float32)
+    zero = np.zeros((w.views, w.rows, w.n_xy), np.float32)
+    proto = synth.Scan(zero, np.ones_like(zero), angles, times, rt, w.rows, w.n_xy, w.views, w.frames, 1.0,
+                       w.n_xy / 2.0, frames)
+    st = timbir_b200.Stage(proto, **w.prior, blocks=2)
+    li = st.forward_project(frames)
+    st.close()
+    proj, wts = synth.counts_to_data(li.astype(np.float64), 5e3, rng, zinger_frac=0.001, ring_sigma=0.02)
+    return synth.Scan(proj, wts, angles, times, rt, w.rows, w.n_xy, w.views, w.frames, 1.0, w.n_xy / 2.0, frames)
 
 
-def coarse_start(scan):
-    """The 2x-coarser phantom (mean over 2x2x2 cells) and its trilinear x2
-    up-sampling onto the stage grid: the warm start both arms use."""
-    ph = scan.phantom[0]
+def coarse_start_frame(ph):
     z, y, x = ph.shape
     coarse = ph.reshape(z // 2, 2, y // 2, 2, x // 2, 2).mean(axis=(1, 3, 5)).astype(np.float32)
 
@@ -70,7 +121,7 @@ def coarse_start(scan):
         return np.moveaxis(out, 0, axis)
 
     fine = up(up(up(coarse.astype(np.float64), 2), 1), 0).astype(np.float32)
-    return coarse, fine[None]
+    return coarse, fine
 
 
 def mean_amatrix_count(stage, scan):
@@ -147,7 +198,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- CPU --
-def run_reference_binary(scan, coarse, iters, threads):
+def run_reference_binary(w, scan, coarse, iters, threads):
     """Reference driver in restart mode at the finest stage: the files a
     finished coarser stage leaves behind are written, then XT_Main_ref runs
     `iters` ICD iterations (ORACLE_MAX_ITERS).  Returns [(seconds, updates)]."""
@@ -155,21 +206,23 @@ def run_reference_binary(scan, coarse, iters, threads):
     wd = tempfile.mkdtemp(prefix="timbir_ref_")
     scan.write_bin(wd)
     p = np.transpose(scan.projections, (0, 2, 1)).astype(np.float32)  # [view][col][row]
-    w = np.transpose(scan.weights, (0, 2, 1)).astype(np.float32)
+    wt = np.transpose(scan.weights, (0, 2, 1)).astype(np.float32)
     p.tofile(os.path.join(wd, "projs_runtime.bin"))
-    w.tofile(os.path.join(wd, "weights_runtime.bin"))
+    wt.tofile(os.path.join(wd, "weights_runtime.bin"))
     np.array([1.0], np.float64).tofile(os.path.join(wd, "variance_estimate.bin"))
     np.zeros((scan.proj_cols, scan.proj_rows), np.float32).tofile(os.path.join(wd, "proj_offset.bin"))
-    coarse.astype(np.float32).tofile(os.path.join(wd, "object_time_0.bin"))
-    np.zeros(scan.proj_rows * scan.proj_cols * scan.proj_cols, np.float32).tofile(os.path.join(wd, "mag_update.bin"))
-    n_stages = 3  # 256 columns: voxel scales 4, 2, 1 (XT_Engine.c:111-141)
-    np.array([n_stages - 1], np.int32).tofile(os.path.join(wd, "status.bin"))
-    a = PRIOR
+    for f in range(scan.recon_num):
+        coarse[f].astype(np.float32).tofile(os.path.join(wd, f"object_time_{f}.bin"))
+    np.zeros(scan.recon_num * scan.proj_rows * scan.proj_cols * scan.proj_cols, np.float32).tofile(
+        os.path.join(wd, "mag_update.bin"))
+    np.array([w.stages - 1], np.int32).tofile(os.path.join(wd, "status.bin"))
+    a = w.prior
     cmd = [REF_BIN, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
-           str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
+           str(scan.proj_num), "--recon_num", str(scan.recon_num), "--vox_wid", str(scan.vox_wid), "--rot_center",
            str(scan.rot_center), "--sig_s", str(a["sig_s"]), "--sig_t", str(a["sig_t"]), "--c_s", str(a["c_s"]),
-           "--c_t", str(a["c_t"]), "--convg_thresh", str(a["convg_thresh"]), "--remove_rings", "0",
-           "--quad_convex", "--restart"]
+           "--c_t", str(a["c_t"]), "--convg_thresh", str(a["convg_thresh"]), "--remove_rings",
+           str(a["remove_rings"]), "--huber_delta", str(a["huber_delta"]), "--huber_T", str(a["huber_T"]),
+           "--restart"] + (["--quad_convex"] if a["quad_convex"] else [])
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), ORACLE_MAX_ITERS=str(iters))
     r = subprocess.run(cmd, cwd=wd, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
                        timeout=1800)
@@ -184,10 +237,10 @@ def run_reference_binary(scan, coarse, iters, threads):
     return out
 
 
-def run_port(scan, coarse_fine, iters):
+def run_port(w, scan, coarse_fine, iters):
     """CPU restatement (single thread), when the reference build is absent."""
     from oracle.bind import Oracle
-    o = Oracle(scan, **{k: v for k, v in PRIOR.items()}, blocks=CFG["rows"])
+    o = Oracle(scan, **w.prior, blocks=2)
     o.prepare(coarse_fine)
     out = []
     last = 0
@@ -201,13 +254,13 @@ def run_port(scan, coarse_fine, iters):
     return out
 
 
-def cpu_measure(scan, coarse, fine, warm, steps, threads):
+def cpu_measure(w, scan, coarse, fine, warm, steps, threads):
     from oracle.bind import Reference
     if Reference.available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "XT_Main_ref")):
-        its = run_reference_binary(scan, coarse, warm + steps, threads)
+        its = run_reference_binary(w, scan, coarse, warm + steps, threads)
         kind, cores = "reference", threads
     else:
-        its = run_port(scan, fine, warm + steps)
+        its = run_port(w, scan, fine, warm + steps)
         kind, cores = "port", 1
     timed = its[warm:] if len(its) > warm else its
     secs = sum(t for t, _ in timed)
@@ -226,10 +279,11 @@ def gpu_arm(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    scan = make_scan(rank)
-    coarse, fine = coarse_start(scan)
+    w = WORKLOADS[args.config]
+    scan = w.scan(rank)
+    coarse, fine = w.warm_start(scan)
     sched = 1 if args.schedule == "sv" else 0
-    st = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+    st = timbir_b200.Stage(scan, **w.prior, blocks=2 if w.rows < 8 else 8)
     st.set_schedule(sched, args.sv_side, args.warps_per_slice)
     sched_info = st.schedule_info()
     st.prepare(fine)
@@ -268,8 +322,14 @@ def gpu_arm(args, rank, world, local_rank):
     # end to end through the C ABI with host buffers: set-up from host arrays
     # (H2D), prologue, one ICD iteration, object back to the host (D2H)
     e2e_ms, e2e_upd = [], 0
-    h2d = sum(a.nbytes for a in (scan.projections, scan.weights, scan.proj_angles, scan.proj_times,
-                                 scan.recon_times, fine))
+    # the step's inputs from pinned host memory
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    pscan = synth.Scan(pin(scan.projections), pin(scan.weights), pin(scan.proj_angles), pin(scan.proj_times),
+                       pin(scan.recon_times), scan.proj_rows, scan.proj_cols, scan.proj_num, scan.recon_num,
+                       scan.vox_wid, scan.rot_center)
+    pfine = pin(fine)
+    h2d = sum(a.nbytes for a in (pscan.projections, pscan.weights, pscan.proj_angles, pscan.proj_times,
+                                 pscan.recon_times, pfine))
     d2h = fine.nbytes
     for k in range(max(1, min(args.steps, 3))):
         flush.fill_(0.0)
@@ -277,9 +337,9 @@ def gpu_arm(args, rank, world, local_rank):
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        s2 = timbir_b200.Stage(scan, **PRIOR, blocks=CFG["rows"])
+        s2 = timbir_b200.Stage(pscan, **w.prior, blocks=2 if w.rows < 8 else 8)
         s2.set_schedule(sched, args.sv_side, args.warps_per_slice)
-        s2.prepare(fine)
+        s2.prepare(pfine)
         s2.iterate(1)
         _ = s2.object()
         t1.record()
@@ -305,16 +365,16 @@ def gpu_arm(args, rank, world, local_rank):
     if os.path.exists(pk):
         peaks = json.load(open(pk))
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    npf = scan.proj_num
+    npf = w.views // w.frames
     b_vu = npf * (cbar * 1 * 12 + 2 * cbar + 2) + 29 * 4 + 4
     achieved = (updates * b_vu) / (icd_ms / 1e3) / 1e9 if icd_ms > 0 else 0.0
     line = {
         "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 theta, prior and update)",
-        "data": "synthetic (seeded random-ellipsoid phantom, Poisson counts)",
-        "config": {"workload": WORKLOAD, "volume": [CFG["rows"], CFG["n_xy"], CFG["n_xy"]],
-                   "views": CFG["views"],
+        "data": w.data,
+        "config": {"workload": w.desc, "volume": [w.frames, w.rows, w.n_xy, w.n_xy],
+                   "views": w.views,
                    "schedule": ("super-voxel" if sched else "reference (checkerboard z-blocks)"),
                    "schedule_info": sched_info, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MB write)"},
@@ -329,7 +389,7 @@ def gpu_arm(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if not args.no_cpu:
-        v, kind, cores, n, secs = cpu_measure(scan, coarse, fine, 1, 1, os.cpu_count() or 1)
+        v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, 1, 1, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                                 "sample": f"{n} ICD iteration(s) of the same stage after 1 warm-up, {secs:.1f} s"}
     print(json.dumps(line), flush=True)
@@ -338,16 +398,17 @@ def gpu_arm(args, rank, world, local_rank):
 def reference_arm(args, rank):
     if rank != 0:
         return
-    scan = make_scan(0)
-    coarse, fine = coarse_start(scan)
+    w = WORKLOADS[args.config]
+    scan = w.scan(0)
+    coarse, fine = w.warm_start(scan)
     threads = os.cpu_count() or 1
-    v, kind, cores, n, secs = cpu_measure(scan, coarse, fine, args.warmup, args.steps, threads)
+    v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, args.warmup, args.steps, threads)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "voxel-updates/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(n, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 scalars)",
-            "data": "synthetic (seeded random-ellipsoid phantom, Poisson counts)",
-            "config": {"workload": WORKLOAD, "volume": [CFG["rows"], CFG["n_xy"], CFG["n_xy"]],
-                       "views": CFG["views"], "threads": threads},
+            "data": w.data,
+            "config": {"workload": w.desc, "volume": [w.frames, w.rows, w.n_xy, w.n_xy], "views": w.views,
+                       "threads": threads},
             "cpu_baseline": {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                              "sample": f"{n} ICD iterations after {args.warmup} warm-up, {secs:.1f} s"},
             "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -362,6 +423,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS),
+                    help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
     args = ap.parse_args()

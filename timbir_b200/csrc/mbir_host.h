@@ -43,7 +43,8 @@ int scan_geom(ScanGeom &sg, const float *angles, const float *ptimes, const floa
               float rot_center, char *err, int errlen);
 void stage_geom(const ScanGeom &sg, StageGeom &st, int mult_xy, int mult_z, double sig_s,
                 double sig_t);
-void detector_response(const ScanGeom &sg, const StageGeom &st, std::vector<float> &H_r);
+void detector_response_params(const ScanGeom &sg, const StageGeom &st, std::vector<double> &trap,
+                              std::vector<double> &beam, double &r0, double &step, double &tc);
 void object_mask(const ScanGeom &sg, const StageGeom &st, std::vector<uint8_t> &mask);
 int z_blocks_for_threads(int threads, int n_time, int n_z);
 

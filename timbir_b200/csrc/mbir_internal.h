@@ -88,3 +88,9 @@ cudaError_t mbir_launch_select_stats(const float *mag, const int *xs, const int 
                                      const int *counts, int planes, int stride, double *out,
                                      cudaStream_t s);
 int mbir_amax(double delta_xy, double delta_r);
+// [view][row][col] -> [row][view][col].
+cudaError_t mbir_launch_to_slice_major(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t s);
+// Detector response table H_r [N_p][65] from the host-computed trapezoids and beam.
+cudaError_t mbir_launch_detector_response(const double *trap, const double *beam, int N_p, double OffsetR,
+                                          double delta_xy, double r0, double step, double tc, float *H_r,
+                                          cudaStream_t s);

@@ -7,6 +7,8 @@
 // intrinsics so that no fused multiply-add changes a rounding step.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "mbir_internal.h"
@@ -100,44 +102,53 @@ __device__ __forceinline__ T warp_sum(T v)
 
 // ----------------------------------------------------------------------------
 // Error sinogram e = y - A x - d (XT_ICD_update.c:655-716 with the forward
-// projector of XT_ForwardProject.c:8-25).  One CTA per (view, slice): the
-// slice's projection at that view is accumulated in FP64 shared memory, then
-// written to the m_z detector rows of the slice.  Views that belong to no
-// frame project nothing (the reference never visits them).
+// projector of XT_ForwardProject.c:8-25).  One CTA per (view, group of up to
+// zc slices): each voxel line's A column at that view is computed once and
+// applied to every slice of the group, accumulating the projections in FP64
+// shared memory, then written to the m_z detector rows of each slice.  Views
+// that belong to no frame project nothing (the reference never visits them).
 // mode 0: out = y - Ax - d (float arithmetic as the reference); mode 1: out = Ax.
 // ----------------------------------------------------------------------------
 __global__ void k_forward(MbirGeom g, const float *__restrict__ x, const int *__restrict__ frame_of_view,
                           const float *__restrict__ y, const float *__restrict__ d,
-                          float *__restrict__ out, int mode)
+                          float *__restrict__ out, int mode, int zc)
 {
-    extern __shared__ double acc[];  // [N_r]
-    const int p = blockIdx.x, s = blockIdx.y;
-    for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) acc[r] = 0.0;
+    extern __shared__ double acc[];  // [zc][N_r]
+    const int p = blockIdx.x, z0 = blockIdx.y * zc;
+    const int nzc = min(zc, g.N_z - z0);
+    for (int q = threadIdx.x; q < nzc * g.N_r; q += blockDim.x) acc[q] = 0.0;
     __syncthreads();
     const int f = frame_of_view[p];
+    const size_t plane = (size_t)g.N_y * g.N_x;
     if (f >= 0) {
-        const float *xs = x + ((size_t)f * g.N_z + s) * g.N_y * g.N_x;
+        const float *xs = x + ((size_t)f * g.N_z + z0) * plane;
         const int nxy = g.N_y * g.N_x;
         for (int v = threadIdx.x; v < nxy; v += blockDim.x) {
-            const float pix = xs[v];
-            if (pix == 0.0f) continue;
+            bool any = false;
+            for (int s = 0; s < nzc; s++) any |= xs[s * plane + v] != 0.0f;
+            if (!any) continue;
             const int j = v / g.N_x, k = v - j * g.N_x;
-            acol_visit(g, voxel_x(g, k), voxel_y(g, j), p,
-                       [&](int bin, double f1) { atomicAdd(&acc[bin], __dmul_rn((double)pix, f1)); });
+            acol_visit(g, voxel_x(g, k), voxel_y(g, j), p, [&](int bin, double f1) {
+                for (int s = 0; s < nzc; s++) {
+                    const float pix = xs[s * plane + v];
+                    if (pix != 0.0f) atomicAdd(&acc[s * g.N_r + bin], __dmul_rn((double)pix, f1));
+                }
+            });
         }
     }
     __syncthreads();
-    for (int rr = 0; rr < g.m_z; rr++) {
-        const int t = s * g.m_z + rr;
-        for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) {
-            const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
-            const float ax = (float)acc[r];
-            if (mode == 0)
-                out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + r]);
-            else
-                out[o] = ax;
+    for (int s = 0; s < nzc; s++)
+        for (int rr = 0; rr < g.m_z; rr++) {
+            const int t = (z0 + s) * g.m_z + rr;
+            for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) {
+                const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+                const float ax = (float)acc[s * g.N_r + r];
+                if (mode == 0)
+                    out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + r]);
+                else
+                    out[o] = ax;
+            }
         }
-    }
 }
 
 // ----------------------------------------------------------------------------
@@ -537,22 +548,97 @@ __global__ void k_vsc_filter(const float *mag, float *filt, int planes, int N_y,
     filt[o] = (float)acc;
 }
 
+// ----------------------------------------------------------------------------
+// Detector response (XT_Profile.c:47-170), GPU half.  One CTA per view: the
+// trapezoidal voxel profile sampled at 1536 points (as float, like the
+// reference's VoxProfile), then for each of the 64 distances the sum over the
+// 512-point beam in the reference's order, FP64 without contraction.
+// trap[view][5] = (height, left corner, left near, right near, right corner).
+// ----------------------------------------------------------------------------
+__global__ void k_detector_response(const double *__restrict__ trap, const double *__restrict__ beam, int N_p,
+                                    double OffsetR, double delta_xy, double r0, double step, double tc,
+                                    float *__restrict__ H_r)
+{
+    __shared__ float prof[1536];
+    __shared__ double bm[512];
+    const int k = blockIdx.x;
+    const double *t = trap + (size_t)k * 5;
+    const double maxv = t[0], lc = t[1], ln = t[2], rn = t[3], rc = t[4];
+    for (int p = threadIdx.x; p < 512; p += blockDim.x) bm[p] = beam[p];
+    for (int j = threadIdx.x; j < 1536; j += blockDim.x) {
+        const double tt = __ddiv_rn(__dmul_rn(2.0, (double)j), 1536.0);
+        float v;
+        if (tt <= lc || tt >= rc)
+            v = 0.0f;
+        else if (tt > rn)
+            v = (float)__ddiv_rn(__dmul_rn(maxv, __dsub_rn(rc, tt)), __dsub_rn(rc, rn));
+        else if (tt >= ln)
+            v = (float)maxv;
+        else
+            v = (float)__ddiv_rn(__dmul_rn(maxv, __dsub_rn(tt, lc)), __dsub_rn(ln, lc));
+        prof[j] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < MBIR_RESP_BINS + 1; i += blockDim.x) {
+        if (i == MBIR_RESP_BINS) {
+            H_r[(size_t)k * (MBIR_RESP_BINS + 1) + i] = 0.0f;
+            continue;
+        }
+        const double rmin = __dsub_rn(__dmul_rn((double)i, OffsetR), delta_xy);
+        double acc = 0.0;
+        for (int p = 0; p < 512; p++) {
+            const double r = __dadd_rn(r0, __dmul_rn((double)p, step));
+            const int pi = (int)floor(__dmul_rn(__dsub_rn(r, rmin), tc));
+            if (pi >= 0 && pi <= 1535) acc = __dadd_rn(acc, __dmul_rn((double)prof[pi], bm[p]));
+        }
+        H_r[(size_t)k * (MBIR_RESP_BINS + 1) + i] = (float)acc;
+    }
+}
+
+// Reference input layout [view][row][col] -> device layout [row][view][col];
+// whole detector rows move, so reads and writes are both coalesced.
+__global__ void k_to_slice_major(const float *__restrict__ in, float *__restrict__ out, int N_p, int N_t, int N_r)
+{
+    const size_t n = (size_t)N_p * N_t * N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < n; o += stride) {
+        const int r = (int)(o % N_r);
+        const size_t pt = o / N_r;
+        const int t = (int)(pt % N_t), p = (int)(pt / N_t);
+        out[((size_t)t * N_p + p) * N_r + r] = in[o];
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers --
+cudaError_t mbir_launch_detector_response(const double *trap, const double *beam, int N_p, double OffsetR,
+                                          double delta_xy, double r0, double step, double tc, float *H_r,
+                                          cudaStream_t s)
+{
+    k_detector_response<<<N_p, 128, 0, s>>>(trap, beam, N_p, OffsetR, delta_xy, r0, step, tc, H_r);
+    return cudaGetLastError();
+}
+
 int mbir_amax(double delta_xy, double delta_r) { return (int)ceil(3 * delta_xy / delta_r) + 2; }
 
-cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
-                                     const float *y, const float *d, float *out, int mode,
-                                     cudaStream_t s)
+cudaError_t mbir_launch_to_slice_major(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t s)
 {
-    dim3 grid(g.N_p, g.N_z);
-    size_t sm = sizeof(double) * g.N_r;
-    if (sm > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-    }
-    k_forward<<<grid, 256, sm, s>>>(g, x, frame_of_view, y, d, out, mode);
+    k_to_slice_major<<<1184, 256, 0, s>>>(in, out, N_p, N_t, N_r);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
+                                const float *y, const float *d, float *out, int mode, cudaStream_t s)
+{
+    // slices per CTA: as many as fit 96 KB of FP64 accumulators
+    const int zc = std::max(1, std::min(g.N_z, (int)((96 * 1024) / (sizeof(double) * g.N_r))));
+    const size_t sm = sizeof(double) * (size_t)zc * g.N_r;
+    if (sm > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid(g.N_p, (g.N_z + zc - 1) / zc);
+    k_forward<<<grid, 256, sm, s>>>(g, x, frame_of_view, y, d, out, mode, zc);
     return cudaGetLastError();
 }
 

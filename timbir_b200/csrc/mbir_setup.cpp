@@ -120,21 +120,26 @@ void stage_geom(const ScanGeom &sg, StageGeom &st, int mult_xy, int mult_z, doub
     st.TF = pc * st.TF / sum;
 }
 
-// Detector response H_r[view][0..64]: trapezoidal voxel footprint per view,
-// averaged over a normalised Hamming beam profile, sampled every OffsetR
-// (XT_Profile.c:47-170).
-void detector_response(const ScanGeom &sg, const StageGeom &st, std::vector<float> &H_r)
+// Host half of the detector response H_r[view][0..64] (XT_Profile.c:47-170):
+// the quantities that need the host C library's cos -- per view the
+// trapezoid's height and corners (maxv, lc, ln, rn, rc), and the normalised
+// 512-point Hamming beam -- so that the GPU half (k_detector_response), which
+// samples the trapezoid and convolves it with the beam in the reference's
+// operation order, produces the reference's bits.
+void detector_response_params(const ScanGeom &sg, const StageGeom &st, std::vector<double> &trap,
+                              std::vector<double> &beam, double &r0, double &step, double &tc)
 {
-    H_r.assign((size_t)sg.N_p * (kRespBins + 1), 0.0f);
-    double beam[kBeamRes], sum = 0;
+    beam.assign(kBeamRes, 0.0);
+    double sum = 0;
     for (int i = 0; i < kBeamRes; i++) {
         beam[i] = 0.54 - 0.46 * cos((2 * kPi / kBeamRes) * i);
         sum = sum + beam[i];
     }
     for (int i = 0; i < kBeamRes; i++) beam[i] /= sum;
-    const double r0 = -sg.delta_r / 2, step = sg.delta_r / kBeamRes;
-    const double tc = kProfileRes / (2 * st.delta_xy);
-    std::vector<float> prof(kProfileRes);
+    r0 = -sg.delta_r / 2;
+    step = sg.delta_r / kBeamRes;
+    tc = kProfileRes / (2 * st.delta_xy);
+    trap.assign((size_t)sg.N_p * 5, 0.0);
     for (int k = 0; k < sg.N_p; k++) {
         double angle = sg.angles[k], maxv;
         while (angle > kHalfPi) angle -= kHalfPi;
@@ -146,28 +151,12 @@ void detector_response(const ScanGeom &sg, const StageGeom &st, std::vector<floa
         const double c45 = cos(kQuarterPi);
         const double d1 = c45 * cos((kQuarterPi - angle));
         const double d2 = c45 * fabs((cos((kQuarterPi + angle))));
-        const double lc = 1 - d1, ln = 1 - d2, rn = 1 + d2, rc = 1 + d1;
-        for (int j = 0; j < kProfileRes; j++) {
-            const double t = 2.0 * j / kProfileRes;
-            if (t <= lc || t >= rc)
-                prof[j] = 0;
-            else if (t > rn)
-                prof[j] = maxv * (rc - t) / (rc - rn);
-            else if (t >= ln)
-                prof[j] = maxv;
-            else
-                prof[j] = maxv * (t - lc) / (ln - lc);
-        }
-        for (int i = 0; i < kRespBins; i++) {
-            const double rmin = i * st.OffsetR - st.delta_xy;
-            double acc = 0;
-            for (int p = 0; p < kBeamRes; p++) {
-                const double r = r0 + p * step;
-                const int pi = (int)floor((r - rmin) * tc);
-                if (pi >= 0 && pi <= kProfileRes - 1) acc += (prof[pi] * beam[p]);
-            }
-            H_r[(size_t)k * (kRespBins + 1) + i] = (float)acc;
-        }
+        double *t = &trap[(size_t)k * 5];
+        t[0] = maxv;
+        t[1] = 1 - d1;  // left corner
+        t[2] = 1 - d2;  // left near
+        t[3] = 1 + d2;  // right near
+        t[4] = 1 + d1;  // right corner
     }
 }
 

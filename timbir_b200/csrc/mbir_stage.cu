@@ -39,10 +39,33 @@ static int fail(const char *fmt, ...)
             return fail("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));    \
     } while (0)
 
+// Device buffers come from the device's default memory pool, which keeps
+// freed memory cached (release threshold raised once per device), so stages
+// set up one after another reuse it instead of paying for fresh allocations.
+// Allocation is stream-ordered on the legacy stream and completed before use.
 template <typename T>
 static cudaError_t dalloc(T **p, size_t n)
 {
-    return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+    static bool pool_ready[64] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64 && !pool_ready[dev]) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool_ready[dev] = true;
+    }
+    e = cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), 0);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(0);
+}
+
+static void dfree(void *p)
+{
+    if (p) cudaFreeAsync(p, 0);
 }
 
 struct MbirStage {
@@ -52,7 +75,7 @@ struct MbirStage {
     int nblk = 2, K = 10, offset_type = 0, upd_offset = 0, upd_var = 0, prepared = 0;
     double var_est = 1.0, stop_thresh = 1.0, hT = 0, hdelta = 0, last_pct = 0;
     long long updates = 0, zero_skips = 0;
-    std::vector<float> H_r;
+    bool hr_ready = false;  // d_H holds the detector response
     std::vector<uint8_t> mask;
     std::vector<int> nr, nn;  // line counts [N_time][nblk]
     MbirGeom g{};
@@ -109,8 +132,8 @@ struct MbirStage {
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
                         d_sv_tasks, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue};
-        for (void *b : bufs)
-            if (b) cudaFree(b);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *b : bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (tev0) cudaEventDestroy(tev0);
@@ -209,22 +232,23 @@ extern "C" int mbir_init_stage(MbirStage **out, const float *projections, const 
     S->acache_bytes = (size_t)mv * amax * (sizeof(double) + sizeof(int)) + (size_t)mv * sizeof(int);
     S->acache_bytes = (S->acache_bytes + 255) & ~(size_t)255;
     if (S->acache_bytes > 160 * 1024)
-        CKS(cudaMalloc((void **)&S->d_acache, S->acache_bytes * (size_t)recon_num * (S->nblk / 2)));
+        CKS(dalloc(&S->d_acache, S->acache_bytes * (size_t)recon_num * (S->nblk / 2)));
     S->threads = mv <= 64 ? 64 : (mv <= 128 ? 128 : 256);
 
-    // upload inputs: reference layout [view][row][col] -> device [row][view][col]
+    // upload inputs in the reference layout [view][row][col] and reorder on
+    // the device into [row][view][col] (the variance estimate is 1 here, so
+    // the weights are taken as they are, XT_Init.c:327-330)
     {
-        std::vector<float> ty(ns), tw(ns);
-        for (int p = 0; p < sg.N_p; p++)
-            for (int t = 0; t < sg.N_t; t++)
-                for (int r = 0; r < sg.N_r; r++) {
-                    const size_t src = ((size_t)p * sg.N_t + t) * sg.N_r + r;
-                    const size_t dst = ((size_t)t * sg.N_p + p) * sg.N_r + r;
-                    ty[dst] = projections[src];
-                    tw[dst] = weights[src] / S->var_est;
-                }
-        CKS(cudaMemcpy(S->d_y, ty.data(), ns * sizeof(float), cudaMemcpyHostToDevice));
-        CKS(cudaMemcpy(S->d_w, tw.data(), ns * sizeof(float), cudaMemcpyHostToDevice));
+        float *raw = nullptr;
+        CKS(dalloc(&raw, ns));
+        cudaError_t e1 = cudaMemcpy(raw, projections, ns * sizeof(float), cudaMemcpyHostToDevice);
+        if (e1 == cudaSuccess) e1 = mbir_launch_to_slice_major(raw, S->d_y, sg.N_p, sg.N_t, sg.N_r, 0);
+        if (e1 == cudaSuccess) e1 = cudaMemcpy(raw, weights, ns * sizeof(float), cudaMemcpyHostToDevice);
+        if (e1 == cudaSuccess) e1 = mbir_launch_to_slice_major(raw, S->d_w, sg.N_p, sg.N_t, sg.N_r, 0);
+        if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(0);
+        dfree(raw);
+        S->launches += 2;
+        CKS(e1);
     }
     CKS(cudaMemset(S->d_d, 0, (size_t)sg.N_t * sg.N_r * sizeof(float)));
     CKS(cudaMemset(S->d_x, 0, S->nvox() * sizeof(float)));
@@ -291,6 +315,30 @@ extern "C" int mbir_set_rng_state(MbirStage *S, uint32_t state)
 
 extern "C" uint32_t mbir_get_rng_state(MbirStage *S) { return S->rng.state; }
 
+// Detector response H_r into d_H: trapezoids and beam from the host C library,
+// the sampling and beam convolution on the GPU (XT_Profile.c:129-170).
+static int compute_detector_response(MbirStage *S)
+{
+    std::vector<double> trap, beam;
+    double r0, step, tc;
+    detector_response_params(S->sg, S->st, trap, beam, r0, step, tc);
+    double *d_trap = nullptr, *d_beam = nullptr;
+    CK(dalloc(&d_trap, trap.size()));
+    CK(dalloc(&d_beam, beam.size()));
+    cudaError_t e = cudaMemcpy(d_trap, trap.data(), trap.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_beam, beam.data(), beam.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = mbir_launch_detector_response(d_trap, d_beam, S->sg.N_p, S->st.OffsetR, S->st.delta_xy, r0, step, tc,
+                                          S->d_H, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    dfree(d_trap);
+    dfree(d_beam);
+    CK(e);
+    S->launches++;
+    S->hr_ready = true;
+    return 0;
+}
+
 // Stage prologue of ICD_BackProject (XT_ICD_update.c:1134-1159): mask,
 // detector response, initial object (zero unless given, [N_time][N_z][N_y][N_x]),
 // ring offsets (zero unless given, [N_r][N_t] as the reference stores them),
@@ -299,9 +347,8 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
                                 const float *magmap)
 {
     const ScanGeom &sg = S->sg;
-    detector_response(sg, S->st, S->H_r);
+    if (compute_detector_response(S)) return -1;
     object_mask(sg, S->st, S->mask);
-    CK(cudaMemcpy(S->d_H, S->H_r.data(), S->H_r.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice));
     if (object)
         CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
@@ -514,8 +561,8 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     S->nzg = (Nz + gz - 1) / gz;
     // the magnitude map holds one plane per (frame, z-group)
     if (S->nzg != S->nblk) {
-        cudaFree(S->d_mag);
-        cudaFree(S->d_filt);
+        dfree(S->d_mag);
+        dfree(S->d_filt);
         S->d_mag = S->d_filt = nullptr;
         S->nblk = S->nzg;
         CK(dalloc(&S->d_mag, S->nmag()));
@@ -576,11 +623,11 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     S->sv_phase_off[nphase] = (int)flat.size();
     size_t maxt = 1;
     for (auto &ph : S->sv_phase) maxt = std::max(maxt, ph.size());
-    cudaFree(S->d_sv_tasks);
-    cudaFree(S->d_sv_sel);
-    cudaFree(S->d_sv_out);
-    cudaFree(S->d_scratch);
-    cudaFree(S->d_queue);
+    dfree(S->d_sv_tasks);
+    dfree(S->d_sv_sel);
+    dfree(S->d_sv_out);
+    dfree(S->d_scratch);
+    dfree(S->d_queue);
     S->d_sv_tasks = S->d_sv_sel = nullptr;
     S->d_sv_out = nullptr;
     S->d_scratch = nullptr;
@@ -833,7 +880,8 @@ extern "C" int mbir_get_magmap(MbirStage *S, float *out)
 
 extern "C" int mbir_get_hr(MbirStage *S, float *out)
 {
-    std::copy(S->H_r.begin(), S->H_r.end(), out);
+    if (!S->hr_ready && compute_detector_response(S)) return -1;
+    CK(cudaMemcpy(out, S->d_H, (size_t)S->sg.N_p * (MBIR_RESP_BINS + 1) * sizeof(float), cudaMemcpyDeviceToHost));
     return 0;
 }
 
@@ -896,10 +944,7 @@ extern "C" int mbir_get_kernel_stats(MbirStage *S, double *icd_ms, long long *ic
 // stage's geometry.  Used to synthesise scans of voxelised phantoms.
 extern "C" int mbir_forward_project(MbirStage *S, const float *object, float *out)
 {
-    if (S->H_r.empty()) {
-        detector_response(S->sg, S->st, S->H_r);
-        CK(cudaMemcpy(S->d_H, S->H_r.data(), S->H_r.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
+    if (!S->hr_ready && compute_detector_response(S)) return -1;
     CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
     CK(mbir_launch_forward(S->g, S->d_x, S->d_fov, nullptr, nullptr, S->d_e, 1, S->stream));
     S->launches++;
