@@ -103,35 +103,48 @@ __device__ __forceinline__ T warp_sum(T v)
 // ----------------------------------------------------------------------------
 // Error sinogram e = y - A x - d (XT_ICD_update.c:655-716 with the forward
 // projector of XT_ForwardProject.c:8-25).  One CTA per (view, group of up to
-// zc slices): each voxel line's A column at that view is computed once and
-// applied to every slice of the group, accumulating the projections in FP64
-// shared memory, then written to the m_z detector rows of each slice.  Views
-// that belong to no frame project nothing (the reference never visits them).
+// zc slices): each voxel line's A column at that view is computed once
+// (exact FP64 bins) and applied to every slice of the group, accumulating the
+// projections with float shared-memory atomics (the reference accumulates in
+// float too), then written to the m_z detector rows of each slice.  Voxels
+// are visited along the image axis closer to the detector direction, so the
+// lanes of a warp land on different bins.  Views that belong to no frame
+// project nothing (the reference never visits them).
 // mode 0: out = y - Ax - d (float arithmetic as the reference); mode 1: out = Ax.
 // ----------------------------------------------------------------------------
 __global__ void k_forward(MbirGeom g, const float *__restrict__ x, const int *__restrict__ frame_of_view,
                           const float *__restrict__ y, const float *__restrict__ d,
                           float *__restrict__ out, int mode, int zc)
 {
-    extern __shared__ double acc[];  // [zc][N_r]
+    extern __shared__ float facc[];  // [zc][N_r]
     const int p = blockIdx.x, z0 = blockIdx.y * zc;
     const int nzc = min(zc, g.N_z - z0);
-    for (int q = threadIdx.x; q < nzc * g.N_r; q += blockDim.x) acc[q] = 0.0;
+    for (int q = threadIdx.x; q < nzc * g.N_r; q += blockDim.x) facc[q] = 0.0f;
     __syncthreads();
     const int f = frame_of_view[p];
     const size_t plane = (size_t)g.N_y * g.N_x;
     if (f >= 0) {
         const float *xs = x + ((size_t)f * g.N_z + z0) * plane;
         const int nxy = g.N_y * g.N_x;
-        for (int v = threadIdx.x; v < nxy; v += blockDim.x) {
+        const bool along_x = fabs(g.cosv[p]) >= fabs(g.sinv[p]);
+        for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+            int j, k;
+            if (along_x) {
+                j = q / g.N_x;
+                k = q - j * g.N_x;
+            } else {
+                k = q / g.N_y;
+                j = q - k * g.N_y;
+            }
+            const int v = j * g.N_x + k;
             bool any = false;
             for (int s = 0; s < nzc; s++) any |= xs[s * plane + v] != 0.0f;
             if (!any) continue;
-            const int j = v / g.N_x, k = v - j * g.N_x;
             acol_visit(g, voxel_x(g, k), voxel_y(g, j), p, [&](int bin, double f1) {
+                const float a = (float)f1;
                 for (int s = 0; s < nzc; s++) {
                     const float pix = xs[s * plane + v];
-                    if (pix != 0.0f) atomicAdd(&acc[s * g.N_r + bin], __dmul_rn((double)pix, f1));
+                    if (pix != 0.0f) atomicAdd(&facc[s * g.N_r + bin], pix * a);
                 }
             });
         }
@@ -142,7 +155,7 @@ __global__ void k_forward(MbirGeom g, const float *__restrict__ x, const int *__
             const int t = (z0 + s) * g.m_z + rr;
             for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) {
                 const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
-                const float ax = (float)acc[s * g.N_r + r];
+                const float ax = facc[s * g.N_r + r];
                 if (mode == 0)
                     out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + r]);
                 else
@@ -631,9 +644,9 @@ cudaError_t mbir_launch_to_slice_major(const float *in, float *out, int N_p, int
 cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
                                 const float *y, const float *d, float *out, int mode, cudaStream_t s)
 {
-    // slices per CTA: as many as fit 96 KB of FP64 accumulators
-    const int zc = std::max(1, std::min(g.N_z, (int)((96 * 1024) / (sizeof(double) * g.N_r))));
-    const size_t sm = sizeof(double) * (size_t)zc * g.N_r;
+    // two slices per CTA (each A column serves both), within 96 KB of accumulators
+    const int zc = std::max(1, std::min(std::min(g.N_z, 2), (int)((96 * 1024) / (sizeof(float) * g.N_r))));
+    const size_t sm = sizeof(float) * (size_t)zc * g.N_r;
     if (sm > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
