@@ -86,6 +86,26 @@ int mbir_set_schedule(MbirStage *stage, int32_t schedule, int32_t sv_side, int32
 int mbir_get_schedule(MbirStage *stage, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
                       int32_t *band_width, int32_t *phases, int32_t *warps_per_slice);
 
+/* A-matrix column cache of schedule 1 (no reference counterpart; the
+ * reference recomputes every column at every visit, calcAMatrixColumnforAngle,
+ * XT_AMatrix.c:50-110): the exact columns of every in-mask voxel line for
+ * every view, 16 bytes per (line, view) at full resolution, built once per
+ * stage at its first iteration.  mode -1 (default): used when it takes at
+ * most a third of free device memory; 0: never (columns computed in the
+ * kernel); 1: always (mbir_set_schedule fails if it cannot be allocated).
+ * Takes effect at the next mbir_set_schedule. */
+int mbir_set_acache(MbirStage *stage, int32_t mode);
+int mbir_get_acache(MbirStage *stage, int32_t *used, int64_t *bytes);
+/* Persistent CTAs per launch of schedule 1 (0, the default: one per SM).
+ * With 1 the super-voxels of a launch run one after another, which makes
+ * the schedule deterministic (a debugging and testing aid). */
+int mbir_set_sv_ctas(MbirStage *stage, int32_t ctas);
+/* The cached columns of in-mask voxel line (row, col) for every view:
+ * N_p x 4 ceil((2 + 2 mult_xy) / 4) words; per view, word 0 = j0 | n << 16
+ * (first detector column with a positive entry, number of columns from it),
+ * then the n values (float bits), zero-padded. */
+int mbir_get_acache_line(MbirStage *stage, int32_t row, int32_t col, int32_t *words);
+
 /* One outer ICD iteration with the reference schedule
  * (updateVoxelsTimeSlices, XT_ICD_update.c:936-1105): random line order,
  * 10 sub-iterations of checkerboard HICD half-sweeps with ring-offset updates,

@@ -11,7 +11,10 @@ judged on the result:
   * bookkeeping: the error sinogram it maintains by atomics stays equal to
     y - A x - d recomputed from scratch (float tolerance);
   * no A-matrix column ever leaves the staged band (the kernel flags it and
-    the iteration call fails).
+    the iteration call fails);
+  * the A-matrix column cache holds the reference's columns (bin indices
+    bit-exact, values to float rounding) and gives the same iterates as
+    columns computed in the kernel.
 """
 import os
 
@@ -33,15 +36,17 @@ def fresh_cost_fp64(name, x, offset=None):
     return o.cost()[0]
 
 
-def sv_stage(name, side=0):
+def sv_stage(name, side=0, acache=-1):
     s = scenarios.make(name, timbir_b200.Stage)
-    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, side)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, side, 0, acache)
     return s
 
 
-def test_sv_converges_to_reference_map():
+@pytest.mark.parametrize("acache", [1, 0])
+def test_sv_converges_to_reference_map(acache):
     g = np.load(os.path.join(GOLD, "converged_plain.npz"))
-    s = sv_stage("plain")
+    s = sv_stage("plain", acache=acache)
+    assert (s.schedule_info()["column_cache_bytes"] > 0) == (acache == 1)
     s.prepare()
     for it in range(1, 301):
         s.iterate(it)
@@ -64,9 +69,10 @@ def test_sv_side_does_not_change_the_map(side):
     assert abs(c - float(g["ref_fresh_cost"])) / float(g["ref_fresh_cost"]) < 1e-5
 
 
+@pytest.mark.parametrize("acache", [1, 0])
 @pytest.mark.parametrize("name", ["plain", "rings2", "frames4", "coarse4", "blocks4"])
-def test_sv_error_sinogram_stays_consistent(name):
-    s = sv_stage(name)
+def test_sv_error_sinogram_stays_consistent(name, acache):
+    s = sv_stage(name, acache=acache)
     s.prepare()
     for it in range(1, 11):
         s.iterate(it)
@@ -121,3 +127,42 @@ def test_sv_warps_per_slice_reach_the_same_map(wps):
         s.iterate(it)
     c = fresh_cost_fp64("plain", s.object())
     assert abs(c - float(g["ref_fresh_cost"])) / float(g["ref_fresh_cost"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["plain", "coarse2", "coarse4", "frames4"])
+def test_sv_column_cache_holds_the_reference_columns(name):
+    # bin indices bit-exact, values within float rounding of the reference's
+    # double quotient (calcAMatrixColumnforAngle), over a sample of lines
+    s = sv_stage(name, acache=1)
+    s.prepare()
+    o = scenarios.make(name, Oracle)
+    o.prepare()  # detector response
+    ys, xs = np.nonzero(s.mask())
+    pick = np.random.default_rng(3).choice(len(ys), size=min(24, len(ys)), replace=False)
+    for q in pick:
+        row, col = int(ys[q]), int(xs[q])
+        j0, n, vals = s.acache_line(row, col)
+        for view in range(s.N_p):
+            idx, val = o.amatrix(row, col, view)
+            assert n[view] == len(idx), (row, col, view)
+            if len(idx):
+                assert np.array_equal(idx, j0[view] + np.arange(n[view])), (row, col, view)
+                np.testing.assert_allclose(vals[view, :n[view]], val, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("name", ["plain", "coarse2", "frames4", "rings2"])
+def test_sv_cached_and_computed_columns_give_the_same_iterates(name):
+    # one CTA per launch: super-voxels run one after another, so the run is
+    # deterministic and the two column sources must give identical iterates
+    side = sv_stage(name, acache=0).schedule_info()["sv_side"]
+    out = []
+    for acache in (1, 0):
+        s = sv_stage(name, side, acache)
+        s.set_sv_ctas(1)
+        s.prepare()
+        for it in range(1, 4):
+            s.iterate(it)
+        out.append((s.object(), s.errorsino()))
+    (x1, e1), (x0, e0) = out
+    assert np.array_equal(x1, x0), float(np.abs(x1 - x0).max())
+    assert np.array_equal(e1, e0), float(np.abs(e1 - e0).max())

@@ -69,6 +69,10 @@ def load_library() -> C.CDLL:
                                           C.POINTER(C.c_longlong)]
     lib.mbir_set_schedule.argtypes = [_VP, i32, i32, i32]
     lib.mbir_get_schedule.argtypes = [_VP] + [C.POINTER(i32)] * 6
+    lib.mbir_set_acache.argtypes = [_VP, i32]
+    lib.mbir_get_acache.argtypes = [_VP, C.POINTER(i32), C.POINTER(C.c_int64)]
+    lib.mbir_get_acache_line.argtypes = [_VP, i32, i32, _i32p]
+    lib.mbir_set_sv_ctas.argtypes = [_VP, i32]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     lib.reconstruct.argtypes = [C.POINTER(C.POINTER(C.c_float))] + [_VP] * 5 + [i32] * 4 + [fl] * 7 + \
@@ -138,10 +142,12 @@ class Stage:
     SCHEDULE_REFERENCE = 0
     SCHEDULE_SUPERVOXEL = 1
 
-    def set_schedule(self, schedule: int, sv_side: int = 0, warps_per_slice: int = 0):
+    def set_schedule(self, schedule: int, sv_side: int = 0, warps_per_slice: int = 0, acache: int = -1):
         """0: the reference's checkerboard z-block schedule; 1: super-voxel
         schedule (sv_side 0 = largest side whose band fits shared memory;
-        warps_per_slice 0 = automatic)."""
+        warps_per_slice 0 = automatic; acache: A-matrix column cache, -1 when
+        it fits, 0 never, 1 always)."""
+        _check(self.lib.mbir_set_acache(self.h, acache))
         _check(self.lib.mbir_set_schedule(self.h, schedule, sv_side, warps_per_slice))
         d = np.zeros(9, np.int32)
         self.lib.mbir_stage_dims(self.h, d)
@@ -150,8 +156,29 @@ class Stage:
     def schedule_info(self) -> dict:
         v = [C.c_int32() for _ in range(6)]
         self.lib.mbir_get_schedule(self.h, *[C.byref(x) for x in v])
-        return dict(zip(("schedule", "sv_side", "z_group", "band_width", "phases", "warps_per_slice"),
-                        [x.value for x in v]))
+        used, nbytes = C.c_int32(), C.c_int64()
+        self.lib.mbir_get_acache(self.h, C.byref(used), C.byref(nbytes))
+        d = dict(zip(("schedule", "sv_side", "z_group", "band_width", "phases", "warps_per_slice"),
+                     [x.value for x in v]))
+        d["column_cache_bytes"] = int(nbytes.value) if used.value else 0
+        return d
+
+    def set_sv_ctas(self, ctas: int):
+        """Persistent CTAs per super-voxel launch (0 = one per SM; 1 runs the
+        super-voxels one after another, deterministically)."""
+        _check(self.lib.mbir_set_sv_ctas(self.h, ctas))
+
+    def acache_line(self, row: int, col: int):
+        """Cached A-matrix columns of voxel line (row, col): per view the first
+        detector column j0, the column count n and the values (n of them
+        meaningful)."""
+        mult = self.N_r // self.N_x  # mult_xy: columns per voxel
+        eq = (2 * mult + 2 + 3) // 4  # 16-byte words per entry: ceil((1 + amax) / 4), amax = 2 mult + 1
+        words = np.zeros((self.N_p, 4 * eq), np.int32)
+        _check(self.lib.mbir_get_acache_line(self.h, row, col, words))
+        j0 = words[:, 0] & 0xFFFF
+        n = words[:, 0] >> 16
+        return j0, n, words[:, 1:].view(np.float32)
 
     def prepare(self, obj=None, offset=None, magmap=None):
         arrs = [None if a is None else _f32(a) for a in (obj, offset, magmap)]

@@ -21,6 +21,9 @@
 //                             super-voxel schedule, which reaches the same MAP
 //                             estimate far faster.
 //   TIMBIR_SV_SIDE=n          super-voxel side (default: largest that fits).
+//   TIMBIR_SV_ACACHE=m        A-matrix column cache of the super-voxel
+//                             schedule: -1 when it fits (default), 0 never,
+//                             1 always.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -171,6 +174,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
     const char *sched_env = getenv("TIMBIR_SCHEDULE");
     const int use_sv = !(sched_env && strcmp(sched_env, "reference") == 0);
     const int sv_side = env_int("TIMBIR_SV_SIDE", 0);
+    const int sv_acache = env_int("TIMBIR_SV_ACACHE", -1);
     int prev_sv_blocks = -1;  // magnitude-map planes per frame of the previous stage (this call)
     uint32_t rng_state = 761521u;
     std::vector<float> carried_offset;  // ring offsets kept in memory between stages
@@ -258,7 +262,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
         mbir_set_rng_state(S, rng_state);
         int nblk_stage = nblk;
         if (use_sv) {
-            if (mbir_set_schedule(S, 1, sv_side, 0)) {
+            if (mbir_set_acache(S, sv_acache) || mbir_set_schedule(S, 1, sv_side, 0)) {
                 LOG_ERR(log, "Super-voxel schedule set-up failed: %s\n", mbir_last_error());
                 mbir_free_stage(S);
                 in.release_all();

@@ -112,8 +112,15 @@ struct MbirStage {
     cudaEvent_t sv_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     SvTaskOut *d_sv_out = nullptr;
     float *d_scratch = nullptr;
+    // A-matrix column cache of the super-voxel kernel ([N_y N_x][N_p][eq] int4),
+    // filled at the first iteration after the prologue
+    int4 *d_acol = nullptr;
+    size_t acol_bytes = 0;
+    int acol_mode = -1;  // -1: when it fits in a third of free memory, 0: never, 1: always
+    bool acol_built = false;
     int *d_err = nullptr, *d_queue = nullptr;
     int sm_count = 148;
+    int sv_ctas = 0;  // persistent CTAs per launch; 0 = one per SM
     double nh_fraction = 0.2;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
@@ -131,7 +138,7 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_tasks, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue};
+                        d_sv_tasks, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -504,6 +511,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     // (+-delta_xy) plus floor effects at both ends
     sp.W = (int)floor((side - 1) * sqrt(2.0) * m + 2 * m + 1e-9) + 3;
     sp.amax = 2 * (int)ceil(m) + 1;
+    sp.eq = (1 + sp.amax + 3) / 4;
     sp.max_views = S->max_views();
     sp.max_nz = nz;
     sp.max_rows = nz * S->st.m_z;
@@ -533,17 +541,40 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     }
     if (schedule != 1) return fail("unknown schedule %d", schedule);
     const int Nz = S->st.N_z;
+    // the column cache: used when it fits (or always / never, as set)
+    {
+        const SvParams probe = sv_params(S, 4, 1, 1);
+        const size_t bytes = mbir_acache_bytes(S->g, probe.eq);
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const bool want = S->acol_mode == 1 || (S->acol_mode == -1 && bytes <= fr / 3);
+        if (want && bytes != S->acol_bytes) {
+            dfree(S->d_acol);
+            S->d_acol = nullptr;
+            S->acol_bytes = 0;
+            if (S->acol_mode == 1 && bytes > fr)
+                return fail("A-matrix column cache of %zu bytes does not fit (%zu free)", bytes, fr);
+            CK(dalloc(&S->d_acol, bytes / sizeof(int4)));
+            S->acol_bytes = bytes;
+        } else if (!want) {
+            dfree(S->d_acol);
+            S->d_acol = nullptr;
+            S->acol_bytes = 0;
+        }
+        S->acol_built = false;
+    }
+    const bool cached = S->d_acol != nullptr;
     int gz = std::min(Nz, 32), side = sv_side;
     SvParams sp{};
     for (;;) {
         if (side > 0) {
             sp = sv_params(S, side, gz, warps_per_slice);
-            if (mbir_sv_smem_bytes(sp) <= kSmemLimit) break;
+            if (mbir_sv_smem_bytes(sp, cached) <= kSmemLimit) break;
         } else {
             int best = 0;
             for (int s = 16; s >= 4; s--) {
                 sp = sv_params(S, s, gz, warps_per_slice);
-                if (mbir_sv_smem_bytes(sp) <= kSmemLimit) {
+                if (mbir_sv_smem_bytes(sp, cached) <= kSmemLimit) {
                     best = s;
                     break;
                 }
@@ -647,6 +678,46 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     return 0;
 }
 
+extern "C" int mbir_set_acache(MbirStage *S, int32_t mode)
+{
+    if (mode < -1 || mode > 1) return fail("column cache mode must be -1, 0 or 1");
+    S->acol_mode = mode;
+    return 0;
+}
+
+extern "C" int mbir_set_sv_ctas(MbirStage *S, int32_t ctas)
+{
+    if (ctas < 0) return fail("negative CTA count");
+    S->sv_ctas = ctas;
+    return 0;
+}
+
+extern "C" int mbir_get_acache(MbirStage *S, int32_t *used, int64_t *bytes)
+{
+    if (used) *used = S->d_acol != nullptr;
+    if (bytes) *bytes = (int64_t)S->acol_bytes;
+    return 0;
+}
+
+// Cached A-matrix columns of one voxel line, [N_p][4 eq] words in the
+// stored format (word 0 = j0 | n << 16, then the values' bits).
+extern "C" int mbir_get_acache_line(MbirStage *S, int32_t row, int32_t col, int32_t *words)
+{
+    if (!S->d_acol) return fail("no A-matrix column cache (super-voxel schedule with the cache enabled)");
+    if (!S->prepared) return fail("mbir_icd_prepare has not run");
+    if (row < 0 || row >= S->st.N_y || col < 0 || col >= S->st.N_x) return fail("line (%d, %d) outside the grid", row, col);
+    if (!S->mask[(size_t)row * S->st.N_x + col]) return fail("line (%d, %d) outside the reconstruction mask", row, col);
+    if (!S->acol_built) {
+        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
+        S->acol_built = true;
+    }
+    const size_t n = (size_t)S->g.N_p * S->sp.eq;
+    CK(cudaMemcpyAsync(words, S->d_acol + ((size_t)row * S->st.N_x + col) * n, n * sizeof(int4),
+                       cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
 extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_side, int32_t *z_group,
                                  int32_t *band_width, int32_t *phases, int32_t *warps_per_slice)
 {
@@ -664,9 +735,10 @@ static int sv_launch(MbirStage *S, const SvTask *d_tasks, int n, int iter, uint3
                      SvTaskOut *acc)
 {
     if (n <= 0) return 0;
-    const int ctas = std::min(n, S->sm_count);
-    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, d_tasks, n, ctas, S->d_queue + qslot, S->d_scratch, acc,
-                          iter, seed, S->d_err, S->stream));
+    const int ctas = std::min(n, S->sv_ctas > 0 ? S->sv_ctas : S->sm_count);
+    SvACache ac{S->d_acol};
+    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, ac, d_tasks, n, ctas, S->d_queue + qslot, S->d_scratch,
+                          acc, iter, seed, S->d_err, S->stream));
     S->launches++;
     S->icd_launches++;
     return 0;
@@ -683,6 +755,10 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
     const int P = (int)S->sv_phase.size();
     int qslot = 0;
+    if (S->d_acol && !S->acol_built) {
+        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
+        S->acol_built = true;
+    }
     CK(cudaMemsetAsync(S->d_queue, 0, kMaxLaunchesPerIter * sizeof(int), S->stream));
     CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
     CK(cudaEventRecord(S->sv_ev[0], S->stream));
@@ -758,7 +834,8 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
         CK(cudaEventElapsedTime(&ms, S->sv_ev[2], S->sv_ev[3]));
         S->icd_ms += ms;
     }
-    if (err) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
+    if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
+    if (err) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
     for (int q = 0; q < (nh ? 2 : 1); q++) {
         S->updates += acc[q].updates;
         S->zero_skips += acc[q].zero_skips;

@@ -4,7 +4,8 @@
 // frame and a group of nz consecutive slices.  It stages into shared memory
 //   * the error-sinogram and weight band the SV touches: for each view of the
 //     frame, the W consecutive detector columns [rlo_p, rlo_p + W) that cover
-//     every voxel of the block, for each detector row of the slices;
+//     every voxel of the block, for each detector row of the slices, as
+//     (e, sqrt(w)) pairs;
 //   * the block's voxels with a one-voxel halo, and the temporal neighbours;
 // then performs exact ICD steps on its voxels -- theta1/theta2 with the
 // generalized-Huber weights over the band (XT_VoxUpdate.c:43-115), the
@@ -17,12 +18,19 @@
 // slices of odd parity lag one line behind the even ones, so a voxel's
 // z-neighbours are never being updated while it is; lines are ordered by
 // their 2x2 (x, y) parity class, so consecutive lines are never x-y
-// neighbours.  Only slice z's warps touch slice z's band rows, and each view
-// is always handled by the same lane, so error-sinogram updates need no
-// synchronisation; the warps of one slice combine theta through shared
-// memory and a named barrier; one CTA barrier per line step hands the next
-// line's A-matrix column (computed cooperatively into a three-slot ring) and
-// the updated voxels to all warps.
+// neighbours (where the last line of one class and the first of the next
+// would be, a later line of the class is moved to the front, or failing that
+// an idle step separates them).  Only slice z's warps touch slice z's band
+// rows, and each view is always handled by the same lane, so error-sinogram
+// updates need no synchronisation; the warps of one slice combine theta through shared
+// memory and a named barrier; one CTA barrier per line step hands the
+// updated voxels and the next line's A-matrix column to all warps.
+//
+// A-matrix columns reach a four-slot shared-memory ring either from the
+// stage's column cache in HBM (cp.async, two lines ahead, every thread
+// copying a share) or, when the cache does not fit, from producer warps that
+// compute the next line's column (exact FP64 bin arithmetic) while the
+// consumer warps update voxels.
 //
 // CTAs are persistent: each takes SVs from a device work queue (host-sorted
 // by decreasing work) until the queue of the launch is empty.
@@ -94,45 +102,157 @@ __device__ __forceinline__ void named_barrier(int id, int count)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-struct AEnt {
-    float a;  // A-matrix value
-    int so;   // shared-memory offset of the entry in a band row: off * NpS + v
-};
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Exact A-matrix column of the voxel line centred at (x, y) for one view
+// (calcAMatrixColumnforAngle, XT_AMatrix.c:50-110): detector columns
+// floor((r -+ delta_xy - R0) / delta_r) clipped to the detector, value = the
+// view's detector response interpolated at |r - r_j| / OffsetR, kept where
+// positive.  Kept columns are consecutive (the response decreases with
+// distance); the entry records the first, j0, the span n and n values
+// (stored format of SvACache).  Returns false if the span exceeds amax.
+template <int AMAXC>
+__device__ __forceinline__ bool acol_entry(const MbirGeom &g, double x, double y, double c, double s,
+                                           const float *__restrict__ H, double inv_dr, double inv_off,
+                                           float inv_off_f, int amax, int nwd, int *__restrict__ dst)
+{
+    const double r = __dsub_rn(__dmul_rn(x, c), __dmul_rn(y, s));
+    const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
+    int j0 = 0, n = 0;
+    bool ok = true;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    if (!(rmax < g.R0 || rmin > g.RMax)) {
+        int imin = floor_div(__dsub_rn(rmin, g.R0), g.delta_r, inv_dr);
+        int imax = floor_div(__dsub_rn(rmax, g.R0), g.delta_r, inv_dr);
+        if (imax >= g.N_r) imax = g.N_r - 1;
+        if (imin < 0) imin = 0;
+        for (int j = imin; j <= imax; j++) {
+            const double rc = __dadd_rn(g.R0, __dmul_rn((double)j + 0.5, g.delta_r));
+            const double dr = fabs(__dsub_rn(r, rc));
+            const int id = floor_div(dr, g.OffsetR, inv_off);
+            if (id >= 0 && id < MBIR_RESP_BINS) {
+                const double w1 = __dsub_rn(dr, __dmul_rn((double)id, g.OffsetR));
+                const double w2 = __dsub_rn(g.OffsetR, w1);
+                const double num =
+                    __dadd_rn(__dmul_rn(w2, (double)__ldg(H + id)), __dmul_rn(w1, (double)__ldg(H + id + 1)));
+                if (num > 0) {
+                    if (n == 0) j0 = j;
+                    const int k = j - j0;
+                    if (k >= amax) {
+                        ok = false;
+                        break;
+                    }
+                    const float a = (float)num * inv_off_f;
+                    if constexpr (AMAXC == 3) {
+                        if (k == 0) a0 = a;
+                        else if (k == 1) a1 = a;
+                        else a2 = a;
+                    } else {
+                        for (; n < k; n++) dst[1 + n] = 0;  // a gap (not produced by a decreasing response)
+                        dst[1 + k] = __float_as_int(a);
+                    }
+                    n = k + 1;
+                }
+            }
+        }
+    }
+    if constexpr (AMAXC == 3) {
+        *reinterpret_cast<int4 *>(dst) =
+            make_int4(j0 | (n << 16), __float_as_int(a0), __float_as_int(a1), __float_as_int(a2));
+    } else {
+        for (int k = n; k < nwd - 1; k++) dst[1 + k] = 0;
+        dst[0] = j0 | (n << 16);
+    }
+    return ok;
+}
+
+// theta1/theta2 contribution of one band entry (e, sqrt(w)) with A value a:
+// weight w where |e sqrt(w)| < T (ProjSelect), else T delta sqrt(w) / |e|
+// (XT_VoxUpdate.c:62-84).
+__device__ __forceinline__ void theta_acc(float2 es, float a, float hT, float hTd, float &t1, float &t2)
+{
+    const float e = es.x, sw = es.y;
+    float om = sw * sw;
+    if (!(fabsf(e * sw) < hT)) om = __fdividef(hTd * sw, fabsf(e));
+    const float ao = a * om;
+    t2 = fmaf(a, ao, t2);
+    t1 = fmaf(-e, ao, t1);
+}
+
+// Fills the column cache: one warp per in-mask line, lanes over views.
+template <int AMAXC>
+__global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__restrict__ mask, int amax, int eq,
+                                                 int4 *__restrict__ cache, int *err)
+{
+    const int lane = threadIdx.x & 31;
+    const long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (line >= (long long)g.N_y * g.N_x || mask[line] != 1) return;
+    const int row = (int)(line / g.N_x), col = (int)(line - (long long)row * g.N_x);
+    const double x = vx(g, col), y = vy(g, row);
+    const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
+    const float inv_off_f = (float)inv_off;
+    int4 *dst = cache + (size_t)line * g.N_p * eq;
+    bool ok = true;
+    for (int p = lane; p < g.N_p; p += 32)
+        ok &= acol_entry<AMAXC>(g, x, y, g.cosv[p], g.sinv[p], g.H_r + (size_t)p * (MBIR_RESP_BINS + 1), inv_dr,
+                                inv_off, inv_off_f, amax, 4 * eq, reinterpret_cast<int *>(dst + (size_t)p * eq));
+    if (!ok) atomicOr(err, 2);
+}
 
 // AMAXC: entries per (line, view) known at compile time (3 at full
 // resolution), 0 = runtime sp.amax.  MZC: detector rows per slice known at
-// compile time (1 at full resolution), 0 = runtime m_z.
-template <int AMAXC, int MZC>
-__global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp,
-                                                  const SvTask *__restrict__ tasks, int ntasks,
-                                                  int *queue, float *__restrict__ scratch,
-                                                  SvTaskOut *__restrict__ out, int iter, uint32_t seed, int *err)
+// compile time (1 at full resolution), 0 = runtime m_z.  AC: columns come
+// from the column cache (else from producer warps).  MAXT: most threads per
+// CTA (512 leaves 128 registers per thread).
+template <int AMAXC, int MZC, bool AC, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp, SvACache ac,
+                                                  const SvTask *__restrict__ tasks, int ntasks, int *queue,
+                                                  float *__restrict__ scratch, SvTaskOut *__restrict__ out, int iter,
+                                                  uint32_t seed, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
     const int amax = AMAXC > 0 ? AMAXC : sp.amax;
+    const int eq = AMAXC > 0 ? (AMAXC + 4) / 4 : sp.eq;
+    const int nwd = 4 * eq;  // words per ring entry
     const int mz = MZC > 0 ? MZC : g.m_z;
     const int NpS = sp.max_views;  // smem stride (views)
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const int S2 = S + 2;
-    const int rowstride = W * NpS;
+    const size_t rowstride = (size_t)W * NpS;  // band entries per detector row
 
     // ---- carve shared memory (sizes fixed by the host in sp) ----
     unsigned char *p = smraw;
-    double *cs = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
-    double *sn = reinterpret_cast<double *>(p); p += sizeof(double) * NpS;
-    AEnt *aring = reinterpret_cast<AEnt *>(p); p += sizeof(AEnt) * 3 * amax * NpS;
-    float *eb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * rowstride;
-    float *sb = reinterpret_cast<float *>(p); p += sizeof(float) * (size_t)sp.max_rows * rowstride;
+    int4 *ring = reinterpret_cast<int4 *>(p); p += sizeof(int4) * 4 * (size_t)eq * NpS;
+    float2 *band = reinterpret_cast<float2 *>(p); p += sizeof(float2) * (size_t)sp.max_rows * rowstride;
+    double *cs = reinterpret_cast<double *>(p);
+    double *sn = cs + NpS;
+    if (!AC) p += 2 * sizeof(double) * NpS;
     float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
-    float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * S * S;
+    // |dx| of each (slice, line) at this visit; summed over the slices in
+    // slice order at write-back (the line's magnitude-map entry)
+    float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * sp.max_nz * S * S;
     float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 4 * 4 * sp.max_nz;
     int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
     int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
-    int *order = reinterpret_cast<int *>(p); p += sizeof(int) * S * S;
-    __shared__ int s_nlines, s_task;
+    // step sequence: lx | ly << 8 of the line, or -1 for an idle step
+    int *order = reinterpret_cast<int *>(p); p += sizeof(int) * (S * S + 4);
+    __shared__ int s_nlines, s_task, s_bad;
     __shared__ float s_red[32][4];
 
     const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
@@ -175,7 +295,10 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_task = atomicAdd(queue, 1);
+        if (tid == 0) {
+            s_task = atomicAdd(queue, 1);
+            s_bad = 0;
+        }
         __syncthreads();
         const int tix = s_task;
         if (tix >= ntasks) break;
@@ -189,41 +312,57 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         const bool active = consumer && zl < nz;
         const int zg = z0 + zl;
 
-        // ---- views, trig, band origin per view ----
+        // ---- views, trig, band origin per view; the band must hold every
+        //      column of every line (the corners bound r) ----
         for (int v = tid; v < Np; v += nthr) {
             const int view = vl[v];
             vidx[v] = view;
             const double c = g.cosv[view], s = g.sinv[view];
-            cs[v] = c;
-            sn[v] = s;
-            int lo = 1 << 30;
+            if (!AC) {
+                cs[v] = c;
+                sn[v] = s;
+            }
+            int lo = 1 << 30, hi = -(1 << 30);
             const double xs[2] = {vx(g, k0), vx(g, k0 + kx - 1)};
             const double ys[2] = {vy(g, j0), vy(g, j0 + ky - 1)};
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const double r = __dsub_rn(__dmul_rn(xs[u & 1], c), __dmul_rn(ys[u >> 1], s));
                 lo = min(lo, floor_div(__dsub_rn(__dsub_rn(r, g.delta_xy), g.R0), g.delta_r, inv_dr));
+                hi = max(hi, floor_div(__dsub_rn(__dadd_rn(r, g.delta_xy), g.R0), g.delta_r, inv_dr));
             }
-            rlo[v] = max(lo, 0);
+            lo = max(lo, 0);
+            hi = min(hi, g.N_r - 1);
+            rlo[v] = lo;
+            if (hi - lo >= W) {
+                atomicOr(err, 1);
+                s_bad = 1;
+            }
         }
         // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
         if (warp == 0) {
+            // in-mask bit of line q = 32 k + lane in bit k (all loads in flight at once)
+            unsigned mbits = 0;
+            for (int k = 0; 32 * k < S * S; k++) {
+                const int q = 32 * k + lane;
+                const int lx = q % S, ly = q / S;
+                if (q < S * S && lx < kx && ly < ky && dv.mask[(size_t)(j0 + ly) * g.N_x + k0 + lx] == 1)
+                    mbits |= 1u << k;
+            }
             int n = 0;
             for (int cls = 0; cls < 4; cls++) {
                 const int base = n;
                 for (int q0 = 0; q0 < S * S; q0 += 32) {
                     const int q = q0 + lane;
                     const int lx = q % S, ly = q / S;
-                    bool take = false;
-                    if (q < S * S && lx < kx && ly < ky)
-                        take = ((((k0 + lx) & 1) | (((j0 + ly) & 1) << 1)) == cls) &&
-                               dv.mask[(size_t)(j0 + ly) * g.N_x + k0 + lx] == 1;
+                    const bool take = ((mbits >> (q0 >> 5)) & 1u) &&
+                                      ((((k0 + lx) & 1) | (((j0 + ly) & 1) << 1)) == cls);
                     const unsigned bal = __ballot_sync(0xffffffffu, take);
-                    if (take) order[n + __popc(bal & ((1u << lane) - 1))] = q;
+                    if (take) order[n + __popc(bal & ((1u << lane) - 1))] = lx | (ly << 8);
                     n += __popc(bal);
                 }
                 __syncwarp();
-                if (lane == 0)
+                if (lane == 0 && n > base) {
                     for (int q = n - 1; q > base; q--) {
                         const uint32_t h = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)q));
                         const int r = base + (int)(h % (uint32_t)(q - base + 1));
@@ -231,46 +370,85 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         order[q] = order[r];
                         order[r] = t;
                     }
+                    // the odd slices lag one step: keep the previous class's last
+                    // line and this class's first line apart
+                    auto adjacent = [](int a, int b) {
+                        return abs((a & 0xff) - (b & 0xff)) <= 1 && abs((a >> 8) - (b >> 8)) <= 1;
+                    };
+                    if (base > 0 && adjacent(order[base - 1], order[base])) {
+                        int q = base + 1;
+                        while (q < n && adjacent(order[base - 1], order[q])) q++;
+                        if (q < n) {
+                            const int t = order[q];
+                            order[q] = order[base];
+                            order[base] = t;
+                        } else {
+                            for (int k = n; k > base; k--) order[k] = order[k - 1];
+                            order[base] = -1;
+                            n++;
+                        }
+                    }
+                }
+                n = __shfl_sync(0xffffffffu, n, 0);
                 __syncwarp();
             }
             if (lane == 0) s_nlines = n;
         }
-        for (int q = tid; q < S * S; q += nthr) magl[q] = 0.0f;
+        for (int q = tid; q < sp.max_nz * S * S; q += nthr) magl[q] = 0.0f;
         __syncthreads();
-        const int nl = s_nlines;
+        const int nl = s_bad ? 0 : s_nlines;
 
-        // ---- stage bands: e (also to this CTA's scratch slot) and sqrt(w);
-        //      four loads in flight per thread before the stores ----
+        // ---- stage the band: (e, sqrt(w)) pairs, e also to this CTA's
+        //      scratch slot.  A lane owns a (detector row, view) and loads the
+        //      16-byte-aligned words covering its W columns that start inside
+        //      the row (rows of N_r % 4 == 0 are 16-byte aligned) ----
         float *__restrict__ scr = scratch + (size_t)blockIdx.x * sp.band_floats;
-        for (int ro = warp; ro < rows * W; ro += nwarps) {
-            const int row = ro / W, off = ro - row * W;
+        const int nvb = (Np + 31) >> 5;
+        const bool vec = (g.N_r & 3) == 0;
+        for (int job = warp; job < rows * nvb; job += nwarps) {
+            const int row = job / nvb, v = (job - row * nvb) * 32 + lane;
+            if (v >= Np) continue;
             const int t = z0 * mz + row;
-            const float *__restrict__ erow = dv.e + (size_t)t * g.N_p * g.N_r;
-            const float *__restrict__ wrow = dv.w + (size_t)t * g.N_p * g.N_r;
-            for (int v0 = lane; v0 < Np; v0 += 128) {
-                float ev[4], wv[4];
+            const int lo = rlo[v];
+            float2 *bd = band + (size_t)row * rowstride + v;
+            float *sc = scr + (size_t)row * rowstride + v;
+            const size_t rbase = ((size_t)t * g.N_p + vidx[v]) * g.N_r;
+            if (vec) {
+                const int a0 = lo & ~3, sh = lo - a0;
+                const float4 *eg = reinterpret_cast<const float4 *>(dv.e + rbase + a0);
+                const float4 *wg = reinterpret_cast<const float4 *>(dv.w + rbase + a0);
+                const int nvec = min((sh + W + 3) >> 2, (g.N_r - a0) >> 2);
+                for (int q0 = 0; q0 < nvec; q0 += 4) {
+                    float4 ev[4], wv[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int v = v0 + 32 * u;
-                    ev[u] = 0.0f;
-                    wv[u] = 0.0f;
-                    if (v < Np) {
-                        const int r = rlo[v] + off;
-                        if (r < g.N_r) {
-                            const size_t o = (size_t)vidx[v] * g.N_r + r;
-                            ev[u] = __ldcg(erow + o);
-                            wv[u] = __ldg(wrow + o);
+                    for (int u = 0; u < 4; u++) {
+                        ev[u] = wv[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        if (q0 + u < nvec) {
+                            ev[u] = __ldcg(eg + q0 + u);
+                            wv[u] = __ldg(wg + q0 + u);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const float ee[4] = {ev[u].x, ev[u].y, ev[u].z, ev[u].w};
+                        const float ww[4] = {wv[u].x, wv[u].y, wv[u].z, wv[u].w};
+#pragma unroll
+                        for (int c = 0; c < 4; c++) {
+                            const int off = 4 * (q0 + u) + c - sh;
+                            if (off >= 0 && off < W) {
+                                bd[(size_t)off * NpS] = make_float2(ee[c], sqrtf(ww[c]));
+                                sc[(size_t)off * NpS] = ee[c];
+                            }
                         }
                     }
                 }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int v = v0 + 32 * u;
-                    if (v < Np) {
-                        eb[ro * NpS + v] = ev[u];
-                        sb[ro * NpS + v] = sqrtf(wv[u]);
-                        scr[ro * NpS + v] = ev[u];
-                    }
+            } else {
+                for (int off = 0; off < W; off++) {
+                    const int r = lo + off;
+                    const float e = r < g.N_r ? __ldcg(dv.e + rbase + r) : 0.0f;
+                    const float w = r < g.N_r ? __ldg(dv.w + rbase + r) : 0.0f;
+                    bd[(size_t)off * NpS] = make_float2(e, sqrtf(w));
+                    sc[(size_t)off * NpS] = e;
                 }
             }
         }
@@ -298,71 +476,52 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             }
         }
 
-        // ---- A-matrix column of line `li` into ring slot `slot` (exact bins);
-        //      unused entries carry a = 0 ----
-        auto acol = [&](int li, int slot, int w0, int av_lanes) {
+        // ---- A-matrix column of line `li` into ring slot li & 3 ----
+        // from the cache: every thread copies a share (one commit group per call)
+        auto fetch = [&](int li) {
+            if (li < nl && order[li] >= 0) {
+                const int o = order[li];
+                const size_t line = (size_t)(j0 + (o >> 8)) * g.N_x + k0 + (o & 0xff);
+                int4 *dst = ring + (size_t)(li & 3) * eq * NpS;
+                for (int q = tid; q < Np * eq; q += nthr) {
+                    const int v = q / eq, w = q - v * eq;
+                    cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
+                }
+            }
+            cp_async_commit();
+        };
+        // computed: warps [w0, nwarps), av_lanes views per warp
+        auto acol = [&](int li, int w0, int av_lanes) {
             const int wr = warp - w0;
-            if (wr < 0) return;
-            const int loc = order[li];
-            const int col = k0 + loc % S, row = j0 + loc / S;
-            const double x = vx(g, col), y = vy(g, row);
-            AEnt *ar = aring + slot * amax * NpS;
+            const int o = order[li];
+            if (wr < 0 || o < 0) return;
+            const double x = vx(g, k0 + (o & 0xff)), y = vy(g, j0 + (o >> 8));
+            int *rw = reinterpret_cast<int *>(ring + (size_t)(li & 3) * eq * NpS);
             for (int l = lane; l < av_lanes; l += 32) {
                 const int v = wr * av_lanes + l;
                 if (v >= Np) break;
-                const double r = __dsub_rn(__dmul_rn(x, cs[v]), __dmul_rn(y, sn[v]));
-                const double rmin = __dsub_rn(r, g.delta_xy), rmax = __dadd_rn(r, g.delta_xy);
-                int n = 0;
-                if (!(rmax < g.R0 || rmin > g.RMax)) {
-                    int imin = floor_div(__dsub_rn(rmin, g.R0), g.delta_r, inv_dr);
-                    int imax = floor_div(__dsub_rn(rmax, g.R0), g.delta_r, inv_dr);
-                    if (imax >= g.N_r) imax = g.N_r - 1;
-                    if (imin < 0) imin = 0;
-                    const float *H = g.H_r + (size_t)vidx[v] * (MBIR_RESP_BINS + 1);
-                    const int base = rlo[v];
-                    for (int j = imin; j <= imax; j++) {
-                        const double rc = __dadd_rn(g.R0, __dmul_rn((double)j + 0.5, g.delta_r));
-                        const double dr = fabs(__dsub_rn(r, rc));
-                        const int id = floor_div(dr, g.OffsetR, inv_off);
-                        if (id >= 0 && id < MBIR_RESP_BINS) {
-                            const double w1 = __dsub_rn(dr, __dmul_rn((double)id, g.OffsetR));
-                            const double w2 = __dsub_rn(g.OffsetR, w1);
-                            const double num = __dadd_rn(__dmul_rn(w2, (double)__ldg(H + id)),
-                                                         __dmul_rn(w1, (double)__ldg(H + id + 1)));
-                            const int off = j - base;
-                            if (num > 0) {
-                                if (off < 0 || off >= W || n >= amax) {
-                                    atomicOr(err, 1);
-                                } else {
-                                    AEnt en;
-                                    en.a = (float)num * inv_off_f;
-                                    en.so = off * NpS + v;
-                                    ar[n * NpS + v] = en;
-                                    n++;
-                                }
-                            }
-                        }
-                    }
-                }
-                for (; n < amax; n++) {
-                    AEnt en;
-                    en.a = 0.0f;
-                    en.so = v;
-                    ar[n * NpS + v] = en;
+                if (!acol_entry<AMAXC>(g, x, y, cs[v], sn[v], g.H_r + (size_t)vidx[v] * (MBIR_RESP_BINS + 1),
+                                       inv_dr, inv_off, inv_off_f, amax, nwd, rw + (size_t)v * nwd)) {
+                    atomicOr(err, 2);
+                    rw[(size_t)v * nwd] = 0;  // drop the column
                 }
             }
         };
 
-        __syncthreads();
-        if (nl > 0) acol(0, 0, 0, av_all);
+        if (AC) {
+            fetch(0);
+            fetch(1);
+            cp_async_wait1();
+        } else if (nl > 0) {
+            acol(0, 0, av_all);
+        }
         __syncthreads();
 
         for (int step = 0; step <= nl; step++) {
             const int li = (zl & 1) ? step - 1 : step;
-            if (active && li >= 0 && li < nl) {
-                const int slot = li % 3;
-                const int loc = order[li];
-                const int lx = loc % S, ly = loc / S;
+            const int o = li >= 0 && li < nl ? order[li] : -1;
+            if (active && o >= 0) {
+                const int lx = o & 0xff, ly = o >> 8;
                 const int col = k0 + lx, row = j0 + ly;
                 float *xc = xb + ((zl + 1) * S2 + ly + 1) * S2 + lx + 1;
                 const float V = *xc;
@@ -384,52 +543,36 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 } else {
                     // ---- data term over this slice's band rows, this warp's views ----
                     float th1 = 0.0f, th2 = 0.0f, th1b = 0.0f, th2b = 0.0f;
-                    const AEnt *ar = aring + slot * amax * NpS;
-                    const float *erow = eb + zl * mz * rowstride;
-                    const float *srow = sb + zl * mz * rowstride;
-                    auto theta_entry = [&](const AEnt &en, int rr, float &t1, float &t2) {
-                        const float e = erow[rr * rowstride + en.so];
-                        const float sw = srow[rr * rowstride + en.so];
-                        float om = sw * sw;
-                        if (!(fabsf(e * sw) < hT)) om = __fdividef(hTd * sw, fabsf(e));
-                        if (en.a != 0.0f) {
-                            t2 = fmaf(en.a * en.a, om, t2);
-                            t1 = fmaf(-e * en.a, om, t1);
-                        }
-                    };
-                    if constexpr (AMAXC > 0 && MZC > 0) {
+                    const int4 *rq = ring + (size_t)(li & 3) * eq * NpS;
+                    const float2 *bz = band + (size_t)zl * mz * rowstride;
+                    if constexpr (AMAXC == 3 && MZC == 1) {
+                        auto theta_view = [&](int v, float &t1, float &t2) {
+                            const int4 A = rq[v];
+                            const int n = A.x >> 16;
+                            const float2 *pp = bz + ((A.x & 0xffff) - rlo[v]) * NpS + v;
+                            if (n > 0) theta_acc(pp[0], __int_as_float(A.y), hT, hTd, t1, t2);
+                            if (n > 1) theta_acc(pp[NpS], __int_as_float(A.z), hT, hTd, t1, t2);
+                            if (n > 2) theta_acc(pp[2 * NpS], __int_as_float(A.w), hT, hTd, t1, t2);
+                        };
                         int v = vh * 32 + lane;
                         const int vstep = 32 * vsplit;
                         for (; v + vstep < Np; v += 2 * vstep) {
-                            AEnt ea[AMAXC], eb2[AMAXC];
-#pragma unroll
-                            for (int q = 0; q < AMAXC; q++) {
-                                ea[q] = ar[q * NpS + v];
-                                eb2[q] = ar[q * NpS + v + vstep];
-                            }
-#pragma unroll
-                            for (int q = 0; q < AMAXC; q++)
-#pragma unroll
-                                for (int rr = 0; rr < MZC; rr++) {
-                                    theta_entry(ea[q], rr, th1, th2);
-                                    theta_entry(eb2[q], rr, th1b, th2b);
-                                }
+                            theta_view(v, th1, th2);
+                            theta_view(v + vstep, th1b, th2b);
                         }
-                        if (v < Np) {
-#pragma unroll
-                            for (int q = 0; q < AMAXC; q++) {
-                                const AEnt en = ar[q * NpS + v];
-#pragma unroll
-                                for (int rr = 0; rr < MZC; rr++) theta_entry(en, rr, th1, th2);
-                            }
-                        }
+                        if (v < Np) theta_view(v, th1, th2);
                     } else {
-                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit)
-                            for (int q = 0; q < amax; q++) {
-                                const AEnt en = ar[q * NpS + v];
-                                if (en.a == 0.0f) break;
-                                for (int rr = 0; rr < mz; rr++) theta_entry(en, rr, th1, th2);
+                        const int *rw = reinterpret_cast<const int *>(rq);
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+                            const int h = rw[(size_t)v * nwd];
+                            const int n = h >> 16;
+                            const float2 *pp = bz + ((h & 0xffff) - rlo[v]) * NpS + v;
+                            for (int k = 0; k < n; k++) {
+                                const float a = __int_as_float(rw[(size_t)v * nwd + 1 + k]);
+                                for (int rr = 0; rr < mz; rr++)
+                                    theta_acc(pp[rr * rowstride + k * NpS], a, hT, hTd, th1, th2);
                             }
+                        }
                     }
                     th1 += th1b;
                     th2 += th2b;
@@ -469,51 +612,54 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         __syncwarp();
                         if (lane == 0) {
                             *xc = xn;
-                            magl[loc] += fabsf(dx);
+                            magl[(zl * S + ly) * S + lx] = fabsf(dx);
                             sum_abs_dx += fabsf(dx);
                             sum_abs_x += fabsf(xn);
                             n_upd++;
                         }
                     }
                     // ---- error sinogram: e -= a dx over this slice's rows ----
-                    float *erw = eb + zl * mz * rowstride;
-                    if constexpr (AMAXC > 0 && MZC > 0) {
+                    float *bzf = reinterpret_cast<float *>(band + (size_t)zl * mz * rowstride);
+                    if constexpr (AMAXC == 3 && MZC == 1) {
 #pragma unroll 2
                         for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
-#pragma unroll
-                            for (int q = 0; q < AMAXC; q++) {
-                                const AEnt en = ar[q * NpS + v];
-                                if (en.a != 0.0f) {
-#pragma unroll
-                                    for (int rr = 0; rr < MZC; rr++) {
-                                        float *pe = erw + rr * rowstride + en.so;
-                                        *pe = fmaf(-en.a, dx, *pe);
-                                    }
+                            const int4 A = rq[v];
+                            const int n = A.x >> 16;
+                            float *pe = bzf + 2 * (((A.x & 0xffff) - rlo[v]) * NpS + v);
+                            if (n > 0) pe[0] = fmaf(-__int_as_float(A.y), dx, pe[0]);
+                            if (n > 1) pe[2 * NpS] = fmaf(-__int_as_float(A.z), dx, pe[2 * NpS]);
+                            if (n > 2) pe[4 * NpS] = fmaf(-__int_as_float(A.w), dx, pe[4 * NpS]);
+                        }
+                    } else {
+                        const int *rw = reinterpret_cast<const int *>(rq);
+                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
+                            const int h = rw[(size_t)v * nwd];
+                            const int n = h >> 16;
+                            float *pe = bzf + 2 * (((h & 0xffff) - rlo[v]) * NpS + v);
+                            for (int k = 0; k < n; k++) {
+                                const float a = __int_as_float(rw[(size_t)v * nwd + 1 + k]);
+                                for (int rr = 0; rr < mz; rr++) {
+                                    float *q = pe + 2 * (rr * rowstride + k * NpS);
+                                    *q = fmaf(-a, dx, *q);
                                 }
                             }
                         }
-                    } else {
-                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit)
-                            for (int q = 0; q < amax; q++) {
-                                const AEnt en = ar[q * NpS + v];
-                                if (en.a == 0.0f) break;
-                                for (int rr = 0; rr < mz; rr++) {
-                                    float *pe = erw + rr * rowstride + en.so;
-                                    *pe = fmaf(-en.a, dx, *pe);
-                                }
-                            }
                     }
                 }
             }
-            if (step + 1 < nl) {
+            if (AC) {
+                fetch(step + 2);
+                cp_async_wait1();
+            } else if (step + 1 < nl) {
                 if (nprod > 0) {
-                    if (!consumer) acol(step + 1, (step + 1) % 3, ncons, av_prod);
+                    if (!consumer) acol(step + 1, ncons, av_prod);
                 } else {
-                    acol(step + 1, (step + 1) % 3, 0, av_all);
+                    acol(step + 1, 0, av_all);
                 }
             }
             __syncthreads();
         }
+        if (AC) cp_async_wait0();
 
         // ---- write back voxels, magnitude map, band change ----
         float *xo = dv.x + (size_t)i * g.N_z * plane;
@@ -525,27 +671,43 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         xb[((lz + 1) * S2 + ly + 1) * S2 + lx + 1];
             }
         for (int q = tid; q < nl; q += nthr) {
-            const int loc = order[q];
-            task.mag[(size_t)(j0 + loc / S) * g.N_x + k0 + loc % S] = magl[loc];
+            const int o = order[q];
+            if (o < 0) continue;
+            const int lx = o & 0xff, ly = o >> 8;
+            float m = 0.0f;
+            for (int z = 0; z < nz; z++) m += magl[(z * S + ly) * S + lx];
+            task.mag[(size_t)(j0 + ly) * g.N_x + k0 + lx] = m;
         }
-        for (int ro = warp; ro < rows * W; ro += nwarps) {
-            const int row = ro / W, off = ro - row * W;
-            float *erow = dv.e + (size_t)(z0 * mz + row) * g.N_p * g.N_r;
-            for (int v0 = lane; v0 < Np; v0 += 128) {
-                float old[4];
+        // band change back to e: per (row, view) lane, vector atomics over the
+        // same aligned words (zeros outside the band)
+        for (int job = warp; job < rows * nvb; job += nwarps) {
+            const int row = job / nvb, v = (job - row * nvb) * 32 + lane;
+            if (v >= Np) continue;
+            const int t = z0 * mz + row;
+            const int lo = rlo[v];
+            const float2 *bd = band + (size_t)row * rowstride + v;
+            const float *sc = scr + (size_t)row * rowstride + v;
+            float *erow = dv.e + ((size_t)t * g.N_p + vidx[v]) * g.N_r;
+            if (vec) {
+                const int a0 = lo & ~3, sh = lo - a0;
+                const int nvec = min((sh + W + 3) >> 2, (g.N_r - a0) >> 2);
+                for (int q = 0; q < nvec; q++) {
+                    float d[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int v = v0 + 32 * u;
-                    old[u] = v < Np ? scr[ro * NpS + v] : 0.0f;
+                    for (int c = 0; c < 4; c++) {
+                        const int off = 4 * q + c - sh;
+                        d[c] = 0.0f;
+                        if (off >= 0 && off < W) d[c] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
+                    }
+                    if (d[0] != 0.0f || d[1] != 0.0f || d[2] != 0.0f || d[3] != 0.0f)
+                        red_add_v4(erow + a0 + 4 * q, d[0], d[1], d[2], d[3]);
                 }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int v = v0 + 32 * u;
-                    if (v >= Np) continue;
-                    const int r = rlo[v] + off;
-                    if (r >= g.N_r) continue;
-                    const float dnew = eb[ro * NpS + v] - old[u];
-                    if (dnew != 0.0f) atomicAdd(erow + (size_t)vidx[v] * g.N_r + r, dnew);
+            } else {
+                for (int off = 0; off < W; off++) {
+                    const int r = lo + off;
+                    if (r >= g.N_r) break;
+                    const float dnew = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
+                    if (dnew != 0.0f) atomicAdd(erow + r, dnew);
                 }
             }
         }
@@ -573,42 +735,71 @@ __global__ void __launch_bounds__(1024) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     }
 }
 
+template <int AMAXC, int MZC, bool AC, int MAXT>
+cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
+                      const SvTask *tasks, int ntasks, int ctas, int threads, size_t sm, int *queue, float *scratch,
+                      SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_icd_sv<AMAXC, MZC, AC, MAXT>
+        <<<ctas, threads, sm, s>>>(g, pr, dv, sp, ac, tasks, ntasks, queue, scratch, out, iter, seed, err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-size_t mbir_sv_smem_bytes(const SvParams &sp)
+size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached)
 {
     const size_t NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
     size_t b = 0;
-    b += 2 * sizeof(double) * NpS;
-    b += 8 * 3 * (size_t)sp.amax * NpS;  // A ring of (value, offset) pairs
-    b += 2 * sizeof(float) * (size_t)sp.max_rows * sp.W * NpS;
+    b += 16 * 4 * (size_t)sp.eq * NpS;  // A-column ring, four slots
+    b += 8 * (size_t)sp.max_rows * sp.W * NpS;  // (e, sqrt(w)) band
+    if (!cached) b += 2 * sizeof(double) * NpS;
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
     b += sizeof(float) * 2 * sp.max_nz * S * S;
-    b += sizeof(float) * S * S;
+    b += sizeof(float) * sp.max_nz * S * S;
     b += sizeof(float) * 4 * 4 * sp.max_nz;
     b += sizeof(int) * NpS * 2;
-    b += sizeof(int) * S * S;
+    b += sizeof(int) * (S * S + 4);
     return (b + 15) & ~(size_t)15;
 }
 
+size_t mbir_acache_bytes(const MbirGeom &g, int eq)
+{
+    return (size_t)g.N_y * g.N_x * g.N_p * eq * 16;
+}
+
+cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
+                              cudaStream_t s)
+{
+    const long long lines = (long long)g.N_y * g.N_x;
+    const int blocks = (int)((lines + 7) / 8);
+    if (amax == 3)
+        k_acache<3><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
+    else
+        k_acache<0><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
+    return cudaGetLastError();
+}
+
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
+                               SvACache ac, const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
                                SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
 {
     if (ntasks <= 0) return cudaSuccess;
-    const size_t sm = mbir_sv_smem_bytes(sp);
-    cudaError_t e = cudaSuccess;
-    const int threads = 32 * (sp.max_nz * sp.vsplit + sp.prod_warps);
-    // full resolution (3 bins per column, one detector row per slice) has its
-    // own instantiation with fixed trip counts
-    if (sp.amax == 3 && g.m_z == 1) {
-        e = cudaFuncSetAttribute(k_icd_sv<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        k_icd_sv<3, 1><<<ctas, threads, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter, seed, err);
-    } else {
-        e = cudaFuncSetAttribute(k_icd_sv<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        k_icd_sv<0, 0><<<ctas, threads, sm, s>>>(g, pr, dv, sp, tasks, ntasks, queue, scratch, out, iter, seed, err);
+    const bool cached = ac.a != nullptr;
+    const size_t sm = mbir_sv_smem_bytes(sp, cached);
+    const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
+    // full resolution (3 columns per entry, one detector row per slice) has
+    // its own instantiations with fixed trip counts
+    const bool full = sp.amax == 3 && g.m_z == 1;
+#define MBIR_SV_ARGS g, pr, dv, sp, ac, tasks, ntasks, ctas, threads, sm, queue, scratch, out, iter, seed, err, s
+    if (threads <= 512) {
+        if (full) return cached ? launch_sv<3, 1, true, 512>(MBIR_SV_ARGS) : launch_sv<3, 1, false, 512>(MBIR_SV_ARGS);
+        return cached ? launch_sv<0, 0, true, 512>(MBIR_SV_ARGS) : launch_sv<0, 0, false, 512>(MBIR_SV_ARGS);
     }
-    return cudaGetLastError();
+    if (full) return cached ? launch_sv<3, 1, true, 1024>(MBIR_SV_ARGS) : launch_sv<3, 1, false, 1024>(MBIR_SV_ARGS);
+    return cached ? launch_sv<0, 0, true, 1024>(MBIR_SV_ARGS) : launch_sv<0, 0, false, 1024>(MBIR_SV_ARGS);
+#undef MBIR_SV_ARGS
 }

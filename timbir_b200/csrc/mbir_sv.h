@@ -10,12 +10,24 @@ struct SvParams {
     int S;          // super-voxel side (voxel lines)
     int W;          // band width (detector columns per view)
     int amax;       // max A-matrix entries per (line, view): 2 mult_xy + 1
+    int eq;         // 16-byte words per A-matrix column entry: ceil((1 + amax) / 4)
     int max_views;  // max views of any frame (shared-memory stride)
     int max_nz;     // slices per CTA
     int max_rows;   // detector rows per CTA: max_nz * m_z
     int vsplit;     // warps per slice (1, 2 or 4; > 1 needs max_nz <= 15)
-    int prod_warps; // warps computing the next line's A-matrix column
+    int prod_warps; // warps computing the next line's A-matrix column (0 with a column cache)
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
+};
+
+// A-matrix column of one (voxel line, view), as the kernels store it:
+// word 0 = j0 | n << 16 (first kept detector column j0, n kept columns, which
+// are consecutive), words 1..amax = the values of columns j0 .. j0 + amax - 1
+// (0 past n); eq 16-byte words in all.
+//
+// Column cache: the columns of every in-mask line for every view, laid out
+// [N_y * N_x][N_p][eq] (line-major, view next), computed once per stage.
+struct SvACache {
+    const int4 *a;  // nullptr: the kernel computes columns itself
 };
 
 struct SvTask {
@@ -29,10 +41,15 @@ struct SvTaskOut {
     long long updates, zero_skips;
 };
 
-size_t mbir_sv_smem_bytes(const SvParams &sp);
+size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached);
+size_t mbir_acache_bytes(const MbirGeom &g, int eq);
+// Fills the column cache (exact bin indices, FP32 values) for the in-mask
+// lines.  err |= 2 if a column has more than amax entries.
+cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
+                              cudaStream_t s);
 // ctas persistent CTAs take the ntasks tasks from the queue counter (zero
 // before the launch); scratch holds ctas * sp.band_floats floats; the CTAs
 // add their statistics to *out.
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
+                               SvACache ac, const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
                                SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s);
