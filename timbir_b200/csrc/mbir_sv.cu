@@ -70,21 +70,21 @@ __device__ __forceinline__ int floor_div(double a, double b, double inv_b)
     return (int)f;
 }
 
-// Four independent butterfly all-reductions, interleaved so their shuffle
-// latencies overlap.
-__device__ __forceinline__ void warp_allsum4(float &a, float &b, float &c, float &d)
+// Sums four values over the warp by reduce-scatter (six shuffles): the
+// total of value j ends in lanes 8j .. 8j + 7.
+__device__ __forceinline__ float warp_reduce_scatter4(float v0, float v1, float v2, float v3, int lane)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ta = __shfl_xor_sync(0xffffffffu, a, o);
-        const float tb = __shfl_xor_sync(0xffffffffu, b, o);
-        const float tc = __shfl_xor_sync(0xffffffffu, c, o);
-        const float td = __shfl_xor_sync(0xffffffffu, d, o);
-        a += ta;
-        b += tb;
-        c += tc;
-        d += td;
-    }
+    const bool h16 = lane & 16, h8 = lane & 8;
+    float k0 = h16 ? v2 : v0, k1 = h16 ? v3 : v1;
+    const float s0 = h16 ? v0 : v2, s1 = h16 ? v1 : v3;
+    k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+    k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+    float k = h8 ? k1 : k0;
+    k += __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
+    k += __shfl_xor_sync(0xffffffffu, k, 4);
+    k += __shfl_xor_sync(0xffffffffu, k, 2);
+    k += __shfl_xor_sync(0xffffffffu, k, 1);
+    return k;
 }
 
 __device__ __forceinline__ uint32_t hash32(uint32_t x)
@@ -216,8 +216,10 @@ __global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__res
 // resolution), 0 = runtime sp.amax.  MZC: detector rows per slice known at
 // compile time (1 at full resolution), 0 = runtime m_z.  AC: columns come
 // from the column cache (else from producer warps).  MAXT: most threads per
-// CTA (512 leaves 128 registers per thread).
-template <int AMAXC, int MZC, bool AC, int MAXT>
+// CTA (512 leaves 128 registers per thread).  VU (full-resolution path): a
+// lane's views per slice, at most VU, are held in registers from theta to
+// the error-sinogram update.
+template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
 __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp, SvACache ac,
                                                   const SvTask *__restrict__ tasks, int ntasks, int *queue,
                                                   float *__restrict__ scratch, SvTaskOut *__restrict__ out, int iter,
@@ -269,11 +271,13 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     int ndz = 0, ndy = 0, ndx = 0;
     float bw = 0.0f, qinv = 0.0f, qpinv = 0.0f, cc = 1.0f;
     bool spatial = false, temporal = false;
+    int nboff = 0;  // offset of the spatial neighbour in the staged block
     if (lane < 26) {
         const int n = lane < 13 ? lane : lane + 1;  // skip the centre (13)
         ndz = n / 9 - 1;
         ndy = (n / 3) % 3 - 1;
         ndx = n % 3 - 1;
+        nboff = (ndz * S2 + ndy) * S2 + ndx;
         bw = (float)pr.SF[n];
         qinv = sSQ_inv;
         qpinv = sSQP_inv;
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 if (spatial) {
                     const int zz = zg + ndz, yy = row + ndy, xx = col + ndx;
                     valid = zz >= 0 && zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x;
-                    if (valid) nbv = xc[(ndz * S2 + ndy) * S2 + ndx];
+                    if (valid) nbv = xc[nboff];
                 } else if (temporal) {
                     const int ti = i + (lane == 26 ? -1 : 1);
                     valid = ti >= 0 && ti < g.N_time;
@@ -545,22 +549,63 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     float th1 = 0.0f, th2 = 0.0f, th1b = 0.0f, th2b = 0.0f;
                     const int4 *rq = ring + (size_t)(li & 3) * eq * NpS;
                     const float2 *bz = band + (size_t)zl * mz * rowstride;
+                    // full resolution: per view three consecutive columns from
+                    // j0 (clamped into the band; absent ones carry a = 0),
+                    // e kept in registers for the update; the weight is w for
+                    // every entry unless some lane of the warp holds an entry
+                    // with |e sqrt(w)| >= T, which then gets T delta sqrt(w)/|e|
+                    constexpr int VR = VU > 0 ? VU : 1;
+                    float ev[VR][3], av[VR][3];
+                    int cx[VR][3];
                     if constexpr (AMAXC == 3 && MZC == 1) {
-                        auto theta_view = [&](int v, float &t1, float &t2) {
-                            const int4 A = rq[v];
-                            const int n = A.x >> 16;
-                            const float2 *pp = bz + ((A.x & 0xffff) - rlo[v]) * NpS + v;
-                            if (n > 0) theta_acc(pp[0], __int_as_float(A.y), hT, hTd, t1, t2);
-                            if (n > 1) theta_acc(pp[NpS], __int_as_float(A.z), hT, hTd, t1, t2);
-                            if (n > 2) theta_acc(pp[2 * NpS], __int_as_float(A.w), hT, hTd, t1, t2);
-                        };
-                        int v = vh * 32 + lane;
                         const int vstep = 32 * vsplit;
-                        for (; v + vstep < Np; v += 2 * vstep) {
-                            theta_view(v, th1, th2);
-                            theta_view(v + vstep, th1b, th2b);
+                        unsigned big = 0;
+#pragma unroll
+                        for (int u = 0; u < VR; u++) {
+                            const int v = vh * 32 + lane + u * vstep;
+                            const bool ok = v < Np;
+                            const int vv = ok ? v : 0;
+                            int4 A = make_int4(0, 0, 0, 0);
+                            if (ok) A = rq[vv];
+                            const int off0 = max((A.x & 0xffff) - rlo[vv], 0);
+                            cx[u][0] = off0 * NpS + vv;
+                            cx[u][1] = min(off0 + 1, W - 1) * NpS + vv;
+                            cx[u][2] = min(off0 + 2, W - 1) * NpS + vv;
+                            av[u][0] = __int_as_float(A.y);
+                            av[u][1] = __int_as_float(A.z);
+                            av[u][2] = __int_as_float(A.w);
                         }
-                        if (v < Np) theta_view(v, th1, th2);
+#pragma unroll
+                        for (int u = 0; u < VR; u++)
+#pragma unroll
+                            for (int k = 0; k < 3; k++) {
+                                const float2 es = bz[cx[u][k]];
+                                ev[u][k] = es.x;
+                                const float pe = es.x * es.y;
+                                const bool sel = fabsf(pe) < hT;
+                                const float q = sel ? av[u][k] * es.y : 0.0f;
+                                big |= sel ? 0u : 1u << (3 * u + k);
+                                if (u & 1) {
+                                    th2b = fmaf(q, q, th2b);
+                                    th1b = fmaf(-q, pe, th1b);
+                                } else {
+                                    th2 = fmaf(q, q, th2);
+                                    th1 = fmaf(-q, pe, th1);
+                                }
+                            }
+                        if (__any_sync(0xffffffffu, big != 0u)) {
+#pragma unroll
+                            for (int u = 0; u < VR; u++)
+#pragma unroll
+                                for (int k = 0; k < 3; k++)
+                                    if (big & (1u << (3 * u + k))) {
+                                        const float e = ev[u][k], a = av[u][k];
+                                        const float om = __fdividef(hTd * bz[cx[u][k]].y, fabsf(e));
+                                        const float ao = a * om;
+                                        th2 = fmaf(a, ao, th2);
+                                        th1 = fmaf(-e, ao, th1);
+                                    }
+                        }
                     } else {
                         const int *rw = reinterpret_cast<const int *>(rq);
                         for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
@@ -587,15 +632,10 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         p1 = b * nbv;
                         p2 = b;
                     }
-                    warp_allsum4(th1, th2, p1, p2);
+                    const float red = warp_reduce_scatter4(th1, th2, p1, p2, lane);
                     if (vsplit > 1) {
                         float *pp = part + 4 * vsplit * zl;
-                        if (lane == 0) {
-                            pp[vh * 4 + 0] = th1;
-                            pp[vh * 4 + 1] = th2;
-                            pp[vh * 4 + 2] = p1;
-                            pp[vh * 4 + 3] = p2;
-                        }
+                        if ((lane & 7) == 0) pp[vh * 4 + (lane >> 3)] = red;
                         named_barrier(1 + zl, 32 * vsplit);
                         th1 = th2 = 0.0f;
                         for (int h = 0; h < vsplit; h++) {
@@ -604,6 +644,11 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         }
                         p1 = pp[2];
                         p2 = pp[3];
+                    } else {
+                        th1 = __shfl_sync(0xffffffffu, red, 0);
+                        th2 = __shfl_sync(0xffffffffu, red, 8);
+                        p1 = __shfl_sync(0xffffffffu, red, 16);
+                        p2 = __shfl_sync(0xffffffffu, red, 24);
                     }
                     const float u = (p1 + th2 * V - th1) / (p2 + th2);
                     const float xn = V + alpha * (u - V);
@@ -621,15 +666,11 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     // ---- error sinogram: e -= a dx over this slice's rows ----
                     float *bzf = reinterpret_cast<float *>(band + (size_t)zl * mz * rowstride);
                     if constexpr (AMAXC == 3 && MZC == 1) {
-#pragma unroll 2
-                        for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
-                            const int4 A = rq[v];
-                            const int n = A.x >> 16;
-                            float *pe = bzf + 2 * (((A.x & 0xffff) - rlo[v]) * NpS + v);
-                            if (n > 0) pe[0] = fmaf(-__int_as_float(A.y), dx, pe[0]);
-                            if (n > 1) pe[2 * NpS] = fmaf(-__int_as_float(A.z), dx, pe[2 * NpS]);
-                            if (n > 2) pe[4 * NpS] = fmaf(-__int_as_float(A.w), dx, pe[4 * NpS]);
-                        }
+#pragma unroll
+                        for (int u = 0; u < VR; u++)
+#pragma unroll
+                            for (int k = 0; k < 3; k++)
+                                if (av[u][k] != 0.0f) bzf[2 * cx[u][k]] = fmaf(-av[u][k], dx, ev[u][k]);
                     } else {
                         const int *rw = reinterpret_cast<const int *>(rq);
                         for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
@@ -735,15 +776,15 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     }
 }
 
-template <int AMAXC, int MZC, bool AC, int MAXT>
+template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
 cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
                       const SvTask *tasks, int ntasks, int ctas, int threads, size_t sm, int *queue, float *scratch,
                       SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT>,
+    cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_icd_sv<AMAXC, MZC, AC, MAXT>
+    k_icd_sv<AMAXC, MZC, AC, MAXT, VU>
         <<<ctas, threads, sm, s>>>(g, pr, dv, sp, ac, tasks, ntasks, queue, scratch, out, iter, seed, err);
     return cudaGetLastError();
 }
@@ -791,15 +832,22 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
     const bool cached = ac.a != nullptr;
     const size_t sm = mbir_sv_smem_bytes(sp, cached);
     const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
-    // full resolution (3 columns per entry, one detector row per slice) has
-    // its own instantiations with fixed trip counts
-    const bool full = sp.amax == 3 && g.m_z == 1;
+    // full resolution (3 columns per entry, one detector row per slice) with
+    // at most 4 views per lane and slice has its own instantiations with
+    // fixed trip counts
+    const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
+    const bool full = sp.amax == 3 && g.m_z == 1 && vpl <= 4;
 #define MBIR_SV_ARGS g, pr, dv, sp, ac, tasks, ntasks, ctas, threads, sm, queue, scratch, out, iter, seed, err, s
+#define MBIR_SV_PICK(MAXT)                                                                                    \
+    if (full && vpl <= 2)                                                                                     \
+        return cached ? launch_sv<3, 1, true, MAXT, 2>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 2>(MBIR_SV_ARGS); \
+    if (full)                                                                                                 \
+        return cached ? launch_sv<3, 1, true, MAXT, 4>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 4>(MBIR_SV_ARGS); \
+    return cached ? launch_sv<0, 0, true, MAXT, 0>(MBIR_SV_ARGS) : launch_sv<0, 0, false, MAXT, 0>(MBIR_SV_ARGS);
     if (threads <= 512) {
-        if (full) return cached ? launch_sv<3, 1, true, 512>(MBIR_SV_ARGS) : launch_sv<3, 1, false, 512>(MBIR_SV_ARGS);
-        return cached ? launch_sv<0, 0, true, 512>(MBIR_SV_ARGS) : launch_sv<0, 0, false, 512>(MBIR_SV_ARGS);
+        MBIR_SV_PICK(512)
     }
-    if (full) return cached ? launch_sv<3, 1, true, 1024>(MBIR_SV_ARGS) : launch_sv<3, 1, false, 1024>(MBIR_SV_ARGS);
-    return cached ? launch_sv<0, 0, true, 1024>(MBIR_SV_ARGS) : launch_sv<0, 0, false, 1024>(MBIR_SV_ARGS);
+    MBIR_SV_PICK(1024)
+#undef MBIR_SV_PICK
 #undef MBIR_SV_ARGS
 }
