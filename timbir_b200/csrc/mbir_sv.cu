@@ -403,50 +403,46 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         const int nl = s_bad ? 0 : s_nlines;
 
         // ---- stage the band: (e, sqrt(w)) pairs, e also to this CTA's
-        //      scratch slot.  A lane owns a (detector row, view) and loads the
-        //      16-byte-aligned words covering its W columns that start inside
-        //      the row (rows of N_r % 4 == 0 are 16-byte aligned) ----
+        //      scratch slot.  Four lanes serve a (detector row, view), each
+        //      every fourth 16-byte-aligned word of the W columns (rows of
+        //      N_r % 4 == 0 are 16-byte aligned; words starting past the row
+        //      end stage zeros) ----
         float *__restrict__ scr = scratch + (size_t)blockIdx.x * sp.band_floats;
-        const int nvb = (Np + 31) >> 5;
         const bool vec = (g.N_r & 3) == 0;
-        for (int job = warp; job < rows * nvb; job += nwarps) {
-            const int row = job / nvb, v = (job - row * nvb) * 32 + lane;
-            if (v >= Np) continue;
-            const int t = z0 * mz + row;
-            const int lo = rlo[v];
-            float2 *bd = band + (size_t)row * rowstride + v;
-            float *sc = scr + (size_t)row * rowstride + v;
-            const size_t rbase = ((size_t)t * g.N_p + vidx[v]) * g.N_r;
-            if (vec) {
-                const int a0 = lo & ~3, sh = lo - a0;
-                const float4 *eg = reinterpret_cast<const float4 *>(dv.e + rbase + a0);
-                const float4 *wg = reinterpret_cast<const float4 *>(dv.w + rbase + a0);
-                const int nvec = min((sh + W + 3) >> 2, (g.N_r - a0) >> 2);
-                for (int q0 = 0; q0 < nvec; q0 += 4) {
-                    float4 ev[4], wv[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        ev[u] = wv[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        if (q0 + u < nvec) {
-                            ev[u] = __ldcg(eg + q0 + u);
-                            wv[u] = __ldg(wg + q0 + u);
-                        }
+        const int npairs = rows * Np;
+        if (vec) {
+            for (int pqc = warp * 32 + lane; pqc < 4 * npairs; pqc += nwarps * 32) {
+                const int pq = pqc >> 2, row = pq / Np, v = pq - row * Np;
+                const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
+                for (int c = pqc & 3; 4 * c < sh + W; c += 4) {
+                    const int col0 = a0 + 4 * c;
+                    const size_t rbase = ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
+                    float4 ev = make_float4(0.0f, 0.0f, 0.0f, 0.0f), wv = ev;
+                    if (col0 < g.N_r) {
+                        ev = __ldcg(reinterpret_cast<const float4 *>(dv.e + rbase + col0));
+                        wv = __ldg(reinterpret_cast<const float4 *>(dv.w + rbase + col0));
                     }
+                    const float ee[4] = {ev.x, ev.y, ev.z, ev.w};
+                    const float ww[4] = {wv.x, wv.y, wv.z, wv.w};
+                    float2 *bd = band + (size_t)row * rowstride + v;
+                    float *sc = scr + (size_t)row * rowstride + v;
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const float ee[4] = {ev[u].x, ev[u].y, ev[u].z, ev[u].w};
-                        const float ww[4] = {wv[u].x, wv[u].y, wv[u].z, wv[u].w};
-#pragma unroll
-                        for (int c = 0; c < 4; c++) {
-                            const int off = 4 * (q0 + u) + c - sh;
-                            if (off >= 0 && off < W) {
-                                bd[(size_t)off * NpS] = make_float2(ee[c], sqrtf(ww[c]));
-                                sc[(size_t)off * NpS] = ee[c];
-                            }
+                    for (int j = 0; j < 4; j++) {
+                        const int off = 4 * c + j - sh;
+                        if (off >= 0 && off < W) {
+                            bd[(size_t)off * NpS] = make_float2(ee[j], sqrtf(ww[j]));
+                            sc[(size_t)off * NpS] = ee[j];
                         }
                     }
                 }
-            } else {
+            }
+        } else {
+            for (int pq = tid; pq < npairs; pq += nthr) {
+                const int row = pq / Np, v = pq - row * Np;
+                const int lo = rlo[v];
+                const size_t rbase = ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
+                float2 *bd = band + (size_t)row * rowstride + v;
+                float *sc = scr + (size_t)row * rowstride + v;
                 for (int off = 0; off < W; off++) {
                     const int r = lo + off;
                     const float e = r < g.N_r ? __ldcg(dv.e + rbase + r) : 0.0f;
@@ -719,31 +715,35 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             for (int z = 0; z < nz; z++) m += magl[(z * S + ly) * S + lx];
             task.mag[(size_t)(j0 + ly) * g.N_x + k0 + lx] = m;
         }
-        // band change back to e: per (row, view) lane, vector atomics over the
-        // same aligned words (zeros outside the band)
-        for (int job = warp; job < rows * nvb; job += nwarps) {
-            const int row = job / nvb, v = (job - row * nvb) * 32 + lane;
-            if (v >= Np) continue;
-            const int t = z0 * mz + row;
-            const int lo = rlo[v];
-            const float2 *bd = band + (size_t)row * rowstride + v;
-            const float *sc = scr + (size_t)row * rowstride + v;
-            float *erow = dv.e + ((size_t)t * g.N_p + vidx[v]) * g.N_r;
-            if (vec) {
-                const int a0 = lo & ~3, sh = lo - a0;
-                const int nvec = min((sh + W + 3) >> 2, (g.N_r - a0) >> 2);
-                for (int q = 0; q < nvec; q++) {
+        // band change back to e: vector atomics over the same words (zeros
+        // outside the band), one lane per (row, view), so that the atomics of
+        // one instruction go to different rows
+        if (vec) {
+            for (int pq = tid; pq < npairs; pq += nthr) {
+                const int row = pq / Np, v = pq - row * Np;
+                const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
+                const float2 *bd = band + (size_t)row * rowstride + v;
+                const float *sc = scr + (size_t)row * rowstride + v;
+                float *erow = dv.e + ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
+                for (int c = 0; 4 * c < sh + W && a0 + 4 * c < g.N_r; c++) {
                     float d[4];
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int off = 4 * q + c - sh;
-                        d[c] = 0.0f;
-                        if (off >= 0 && off < W) d[c] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
+                    for (int j = 0; j < 4; j++) {
+                        const int off = 4 * c + j - sh;
+                        d[j] = 0.0f;
+                        if (off >= 0 && off < W) d[j] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
                     }
                     if (d[0] != 0.0f || d[1] != 0.0f || d[2] != 0.0f || d[3] != 0.0f)
-                        red_add_v4(erow + a0 + 4 * q, d[0], d[1], d[2], d[3]);
+                        red_add_v4(erow + a0 + 4 * c, d[0], d[1], d[2], d[3]);
                 }
-            } else {
+            }
+        } else {
+            for (int pq = tid; pq < npairs; pq += nthr) {
+                const int row = pq / Np, v = pq - row * Np;
+                const int lo = rlo[v];
+                const float2 *bd = band + (size_t)row * rowstride + v;
+                const float *sc = scr + (size_t)row * rowstride + v;
+                float *erow = dv.e + ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
                 for (int off = 0; off < W; off++) {
                     const int r = lo + off;
                     if (r >= g.N_r) break;
