@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -104,11 +105,18 @@ struct MbirStage {
     int schedule = 0;  // 0: reference schedule, 1: super-voxel schedule
     SvParams sp{};
     int nzg = 1, gz = 1;
-    std::vector<std::vector<SvTask>> sv_phase;  // tasks of each colour phase
-    std::vector<SvTask> sv_all;                 // every task, with its phase
-    std::vector<int> sv_all_phase;
-    SvTask *d_sv_tasks = nullptr, *d_sv_sel = nullptr;
-    std::vector<int> sv_phase_off;  // phase q's tasks: [off[q], off[q+1]) of d_sv_tasks
+    int sv_nphase = 1;
+    std::vector<SvTask> sv_all;            // every super-voxel; its id is its index
+    std::vector<int> sv_all_phase;         // its colour phase
+    std::vector<std::vector<int>> sv_nbr;  // ids of the super-voxels it conflicts with
+    SvTask *d_sv_all = nullptr;
+    int *d_sv_done = nullptr;  // per id: epoch of its last finished visit
+    int sv_epoch = 0;
+    // launch lists [order | dep_off | deps] of the full sweep for each phase
+    // rotation (d_sv_lists), and of the non-homogeneous pass (d_sv_sel)
+    std::vector<std::array<size_t, 4>> sv_rot;  // {n, order, dep_off, deps offsets}
+    int *d_sv_lists = nullptr, *d_sv_sel = nullptr;
+    std::vector<int> sv_sel_host;
     cudaEvent_t sv_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     SvTaskOut *d_sv_out = nullptr;
     float *d_scratch = nullptr;
@@ -138,7 +146,7 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_tasks, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol};
+                        d_sv_all, d_sv_done, d_sv_lists, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -527,6 +535,43 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     return sp;
 }
 
+// Orders super-voxel ids for a sweep: colour phases starting from phase r,
+// the largest super-voxels of a phase first.
+static void sv_sort(const MbirStage *S, std::vector<int> &ids, int r)
+{
+    const int P = S->sv_nphase;
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+        const int pa = (S->sv_all_phase[a] - r + P) % P, pb = (S->sv_all_phase[b] - r + P) % P;
+        if (pa != pb) return pa < pb;
+        return S->sv_all[a].nlines > S->sv_all[b].nlines;
+    });
+}
+
+// Launch list of super-voxels `ids` in that order, appended to buf as
+// [order | dep_off | deps]: for each, the conflicting super-voxels earlier in
+// the list (they finish first; so no two conflicting ones run at once, and
+// every wait is for a super-voxel that an earlier CTA already holds).
+// meta = {n, order offset, dep_off offset, deps offset}.
+static void sv_build_list(const MbirStage *S, const std::vector<int> &ids, std::vector<int> &buf,
+                          std::array<size_t, 4> &meta)
+{
+    std::vector<int> pos(S->sv_all.size(), -1), deps;
+    for (size_t k = 0; k < ids.size(); k++) pos[ids[k]] = (int)k;
+    meta[0] = ids.size();
+    meta[1] = buf.size();
+    buf.insert(buf.end(), ids.begin(), ids.end());
+    meta[2] = buf.size();
+    buf.resize(buf.size() + ids.size() + 1);
+    for (size_t k = 0; k < ids.size(); k++) {
+        buf[meta[2] + k] = (int)deps.size();
+        for (int nb : S->sv_nbr[ids[k]])
+            if (pos[nb] >= 0 && pos[nb] < (int)k) deps.push_back(nb);
+    }
+    buf[meta[2] + ids.size()] = (int)deps.size();
+    meta[3] = buf.size();
+    buf.insert(buf.end(), deps.begin(), deps.end());
+}
+
 static const size_t kSmemLimit = 227 * 1024;
 static const int kMaxLaunchesPerIter = 64;
 
@@ -603,15 +648,16 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         S->nr.assign((size_t)S->sg.N_time * S->nblk, 0);
         S->nn.assign((size_t)S->sg.N_time * S->nblk, 0);
     }
-    // tasks by colour: SV x / y parity, z-group parity, frame parity
+    // super-voxels, coloured by SV x / y parity, z-group parity, frame parity
     if (S->mask.empty()) object_mask(S->sg, S->st, S->mask);
-    const int side_ = sp.S, N_x = S->st.N_x, N_y = S->st.N_y;
+    const int side_ = sp.S, N_x = S->st.N_x, N_y = S->st.N_y, N_time = S->sg.N_time;
     const int ntx = (N_x + side_ - 1) / side_, nty = (N_y + side_ - 1) / side_;
-    std::vector<int> phase_of(16, -1);
+    std::vector<int> phase_of(16, -1), cell((size_t)N_time * S->nzg * nty * ntx, -1);
+    auto cell_of = [&](int i, int zg, int ty, int tx) { return (((size_t)i * S->nzg + zg) * nty + ty) * ntx + tx; };
     int nphase = 0;
     S->sv_all.clear();
     S->sv_all_phase.clear();
-    for (int i = 0; i < S->sg.N_time; i++)
+    for (int i = 0; i < N_time; i++)
         for (int zg = 0; zg < S->nzg; zg++)
             for (int ty = 0; ty < nty; ty++)
                 for (int tx = 0; tx < ntx; tx++) {
@@ -622,7 +668,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
                             if (S->mask[(size_t)y * N_x + x]) lines++;
                     if (!lines) continue;
                     const int colour = (tx & 1) | ((ty & 1) << 1) | ((S->nzg > 1 ? (zg & 1) : 0) << 2) |
-                                       ((S->sg.N_time > 1 ? (i & 1) : 0) << 3);
+                                       ((N_time > 1 ? (i & 1) : 0) << 3);
                     if (phase_of[colour] < 0) phase_of[colour] = nphase++;
                     SvTask t{};
                     t.frame = i;
@@ -632,41 +678,73 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
                     t.nz = std::min(gz, Nz - t.z0);
                     t.nlines = lines;
                     t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
+                    cell[cell_of(i, zg, ty, tx)] = (int)S->sv_all.size();
                     S->sv_all.push_back(t);
                     S->sv_all_phase.push_back(phase_of[colour]);
                 }
-    S->sv_phase.assign(nphase, {});
-    for (size_t q = 0; q < S->sv_all.size(); q++) S->sv_phase[S->sv_all_phase[q]].push_back(S->sv_all[q]);
-    // the work queue hands out the largest SVs first
-    for (auto &ph : S->sv_phase)
-        std::stable_sort(ph.begin(), ph.end(), [](const SvTask &a, const SvTask &b) { return a.nlines > b.nlines; });
+    S->sv_nphase = nphase;
+    // conflicts: super-voxels sharing a prior neighbourhood -- x-y-z neighbours
+    // in the same frame, the same block in adjacent frames
+    S->sv_nbr.assign(S->sv_all.size(), {});
+    for (int i = 0; i < N_time; i++)
+        for (int zg = 0; zg < S->nzg; zg++)
+            for (int ty = 0; ty < nty; ty++)
+                for (int tx = 0; tx < ntx; tx++) {
+                    const int id = cell[cell_of(i, zg, ty, tx)];
+                    if (id < 0) continue;
+                    for (int dz = -1; dz <= 1; dz++)
+                        for (int dy = -1; dy <= 1; dy++)
+                            for (int dx = -1; dx <= 1; dx++) {
+                                const int z2 = zg + dz, y2 = ty + dy, x2 = tx + dx;
+                                if ((dz | dy | dx) == 0 || z2 < 0 || z2 >= S->nzg || y2 < 0 || y2 >= nty || x2 < 0 ||
+                                    x2 >= ntx)
+                                    continue;
+                                const int nb = cell[cell_of(i, z2, y2, x2)];
+                                if (nb >= 0) S->sv_nbr[id].push_back(nb);
+                            }
+                    for (int di = -1; di <= 1; di += 2)
+                        if (i + di >= 0 && i + di < N_time) {
+                            const int nb = cell[cell_of(i + di, zg, ty, tx)];
+                            if (nb >= 0) S->sv_nbr[id].push_back(nb);
+                        }
+                }
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev));
-    // every phase's task list lives on the device; the non-homogeneous
-    // selection gets a second list of the same capacity
-    std::vector<SvTask> flat;
-    S->sv_phase_off.assign(nphase + 1, 0);
-    for (int q = 0; q < nphase; q++) {
-        S->sv_phase_off[q] = (int)flat.size();
-        flat.insert(flat.end(), S->sv_phase[q].begin(), S->sv_phase[q].end());
+    // full-sweep launch lists, one per phase rotation
+    std::vector<int> buf;
+    S->sv_rot.assign(nphase, {});
+    for (int r = 0; r < nphase; r++) {
+        std::vector<int> ids(S->sv_all.size());
+        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
+        sv_sort(S, ids, r);
+        sv_build_list(S, ids, buf, S->sv_rot[r]);
     }
-    S->sv_phase_off[nphase] = (int)flat.size();
-    size_t maxt = 1;
-    for (auto &ph : S->sv_phase) maxt = std::max(maxt, ph.size());
-    dfree(S->d_sv_tasks);
+    // a non-homogeneous pass visits a subset: its list is never longer
+    size_t cap = 1;
+    for (int r = 0; r < nphase; r++)
+        cap = std::max(cap, (r + 1 < nphase ? S->sv_rot[r + 1][1] : buf.size()) - S->sv_rot[r][1]);
+    dfree(S->d_sv_all);
+    dfree(S->d_sv_done);
+    dfree(S->d_sv_lists);
     dfree(S->d_sv_sel);
     dfree(S->d_sv_out);
     dfree(S->d_scratch);
     dfree(S->d_queue);
-    S->d_sv_tasks = S->d_sv_sel = nullptr;
+    S->d_sv_all = nullptr;
+    S->d_sv_done = S->d_sv_lists = S->d_sv_sel = nullptr;
     S->d_sv_out = nullptr;
     S->d_scratch = nullptr;
     S->d_queue = nullptr;
-    CK(dalloc(&S->d_sv_tasks, flat.size()));
-    CK(dalloc(&S->d_sv_sel, flat.size()));
-    CK(cudaMemcpy(S->d_sv_tasks, flat.data(), flat.size() * sizeof(SvTask), cudaMemcpyHostToDevice));
-    const size_t ctas = std::min<size_t>(maxt, (size_t)S->sm_count);
+    CK(dalloc(&S->d_sv_all, S->sv_all.size()));
+    CK(cudaMemcpy(S->d_sv_all, S->sv_all.data(), S->sv_all.size() * sizeof(SvTask), cudaMemcpyHostToDevice));
+    CK(dalloc(&S->d_sv_done, S->sv_all.size()));
+    CK(cudaMemset(S->d_sv_done, 0, S->sv_all.size() * sizeof(int)));
+    S->sv_epoch = 0;
+    CK(dalloc(&S->d_sv_lists, buf.size()));
+    CK(cudaMemcpy(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(dalloc(&S->d_sv_sel, cap));
+    const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sm_count);
     CK(dalloc(&S->d_sv_out, 2));
     CK(dalloc(&S->d_scratch, ctas * sp.band_floats));
     CK(dalloc(&S->d_queue, kMaxLaunchesPerIter));
@@ -726,49 +804,50 @@ extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_si
     if (sv_side) *sv_side = S->sp.S;
     if (z_group) *z_group = S->gz;
     if (band_width) *band_width = S->sp.W;
-    if (phases) *phases = (int)S->sv_phase.size();
+    if (phases) *phases = S->sv_nphase;
     return 0;
 }
 
 // One launch of the SV kernel over `n` device-resident tasks; no host sync.
-static int sv_launch(MbirStage *S, const SvTask *d_tasks, int n, int iter, uint32_t seed, int qslot,
-                     SvTaskOut *acc)
+// One launch of the SV kernel over a launch list at `list` (device) with
+// layout meta; no host sync.
+static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> &meta, int iter, uint32_t seed,
+                     int qslot, SvTaskOut *acc)
 {
+    const int n = (int)meta[0];
     if (n <= 0) return 0;
     const int ctas = std::min(n, S->sv_ctas > 0 ? S->sv_ctas : S->sm_count);
     SvACache ac{S->d_acol};
-    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, ac, d_tasks, n, ctas, S->d_queue + qslot, S->d_scratch,
-                          acc, iter, seed, S->d_err, S->stream));
+    SvLaunch L{S->d_sv_all, list + meta[1], list + meta[2], list + meta[3], n, S->d_sv_done, ++S->sv_epoch};
+    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, ac, L, ctas, S->d_queue + qslot, S->d_scratch, acc, iter,
+                          seed, S->d_err, S->stream));
     S->launches++;
     S->icd_launches++;
     return 0;
 }
 
-// One outer iteration of the super-voxel schedule: a sweep over every SV,
-// colour phase by colour phase (phase order rotates with the iteration), a
-// ring-offset update, then (from the second iteration) a non-homogeneous pass
-// over the SVs whose lines changed most in the sweep, another ring-offset
-// update, and the variance update.  Convergence uses the reference's
-// criterion, with the ratio of summed |dx| to summed |x'| over the sweep
-// scaled by its 10 sub-iterations (XT_ICD_update.c:1066-1103).
+// One outer iteration of the super-voxel schedule: a sweep over every SV in
+// one launch, colour phase by colour phase (the phase order rotates with the
+// iteration; an SV starts as soon as the conflicting SVs before it have
+// finished), a ring-offset update, then (from the second iteration) a
+// non-homogeneous pass over the SVs whose lines changed most in the sweep,
+// another ring-offset update, and the variance update.  Convergence uses the
+// reference's criterion, with the ratio of summed |dx| to summed |x'| over
+// the sweep scaled by its 10 sub-iterations (XT_ICD_update.c:1066-1103).
 static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
-    const int P = (int)S->sv_phase.size();
-    int qslot = 0;
+    const int P = S->sv_nphase;
     if (S->d_acol && !S->acol_built) {
         CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
         S->acol_built = true;
     }
-    CK(cudaMemsetAsync(S->d_queue, 0, kMaxLaunchesPerIter * sizeof(int), S->stream));
+    CK(cudaMemsetAsync(S->d_queue, 0, 2 * sizeof(int), S->stream));
     CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
+    const int rot = iter % P;
     CK(cudaEventRecord(S->sv_ev[0], S->stream));
-    for (int q = 0; q < P; q++) {
-        const int ph = (q + iter) % P;
-        const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
-        if (sv_launch(S, S->d_sv_tasks + S->sv_phase_off[ph], S->sv_phase_off[ph + 1] - S->sv_phase_off[ph], iter,
-                      seed, qslot++, S->d_sv_out))
-            return -1;
-    }
+    if (sv_launch(S, S->d_sv_lists, S->sv_rot[rot], iter, (uint32_t)(S->rng.next() * 4294967295.0), 0,
+                  S->d_sv_out))
+        return -1;
     CK(cudaEventRecord(S->sv_ev[1], S->stream));
     if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
     bool nh = false;
@@ -790,34 +869,24 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
         const size_t nsel = (size_t)std::ceil(S->nh_fraction * score.size());
         std::partial_sort(score.begin(), score.begin() + nsel, score.end(),
                           [](const std::pair<float, int> &a, const std::pair<float, int> &b) { return a.first > b.first; });
-        std::vector<std::vector<SvTask>> sel(P);
+        std::vector<int> ids;
         for (size_t q = 0; q < nsel; q++) {
             if (score[q].first <= 0) break;
-            const int id = score[q].second;
-            sel[S->sv_all_phase[id]].push_back(S->sv_all[id]);
+            ids.push_back(score[q].second);
         }
-        std::vector<SvTask> flat;
-        std::vector<int> off(P + 1, 0);
-        for (int q = 0; q < P; q++) {
-            off[q] = (int)flat.size();
-            std::stable_sort(sel[q].begin(), sel[q].end(),
-                             [](const SvTask &a, const SvTask &b) { return a.nlines > b.nlines; });
-            flat.insert(flat.end(), sel[q].begin(), sel[q].end());
-        }
-        off[P] = (int)flat.size();
-        if (!flat.empty()) {
+        if (!ids.empty()) {
             nh = true;
-            CK(cudaMemcpyAsync(S->d_sv_sel, flat.data(), flat.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
-                               S->stream));
+            sv_sort(S, ids, rot);
+            std::array<size_t, 4> meta{};
+            S->sv_sel_host.clear();
+            sv_build_list(S, ids, S->sv_sel_host, meta);
+            // pageable source: the copy is staged before the call returns
+            CK(cudaMemcpyAsync(S->d_sv_sel, S->sv_sel_host.data(), S->sv_sel_host.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, S->stream));
             CK(cudaEventRecord(S->sv_ev[2], S->stream));
-            for (int q = 0; q < P; q++) {
-                const int ph = (q + iter) % P;
-                const uint32_t seed = (uint32_t)(S->rng.next() * 4294967295.0);
-                if (sv_launch(S, S->d_sv_sel + off[ph], off[ph + 1] - off[ph], iter, seed, qslot++, S->d_sv_out + 1))
-                    return -1;
-            }
+            if (sv_launch(S, S->d_sv_sel, meta, iter, (uint32_t)(S->rng.next() * 4294967295.0), 1, S->d_sv_out + 1))
+                return -1;
             CK(cudaEventRecord(S->sv_ev[3], S->stream));
-            CK(cudaStreamSynchronize(S->stream));  // keep `flat` alive until the copy ran
         }
         if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
     }
@@ -835,7 +904,8 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
         S->icd_ms += ms;
     }
     if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
-    if (err) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
+    if (err & 2) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
+    if (err & 4) return fail("super-voxel dependency wait timed out");
     for (int q = 0; q < (nh ? 2 : 1); q++) {
         S->updates += acc[q].updates;
         S->zero_skips += acc[q].zero_skips;

@@ -102,6 +102,17 @@ __device__ __forceinline__ void named_barrier(int id, int count)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d)
 {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
@@ -221,9 +232,8 @@ __global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__res
 // the error-sinogram update.
 template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
 __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp, SvACache ac,
-                                                  const SvTask *__restrict__ tasks, int ntasks, int *queue,
-                                                  float *__restrict__ scratch, SvTaskOut *__restrict__ out, int iter,
-                                                  uint32_t seed, int *err)
+                                                  SvLaunch L, int *queue, float *__restrict__ scratch,
+                                                  SvTaskOut *__restrict__ out, int iter, uint32_t seed, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
@@ -305,8 +315,9 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         }
         __syncthreads();
         const int tix = s_task;
-        if (tix >= ntasks) break;
-        const SvTask task = tasks[tix];
+        if (tix >= L.ntasks) break;
+        const int id = L.order[tix];
+        const SvTask task = L.tasks[id];
         const int nz = task.nz, rows = nz * mz;
         const int i = task.frame;
         const int Np = g.view_num[i];
@@ -397,6 +408,18 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 __syncwarp();
             }
             if (lane == 0) s_nlines = n;
+            // wait for the conflicting super-voxels earlier in this launch
+            // (bounded: a wait that gives up flags err and goes on)
+            for (int d = L.dep_off[tix] + lane; d < L.dep_off[tix + 1]; d += 32) {
+                const int *flag = L.done + L.deps[d];
+                for (int spins = 0; ld_acquire(flag) != L.epoch; spins++) {
+                    if (spins > (1 << 22)) {
+                        atomicOr(err, 4);
+                        break;
+                    }
+                    __nanosleep(100);
+                }
+            }
         }
         for (int q = tid; q < sp.max_nz * S * S; q += nthr) magl[q] = 0.0f;
         __syncthreads();
@@ -461,7 +484,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 const int xx = k0 + lx - 1, yy = j0 + ly - 1, zz = z0 + lz - 1;
                 float v = 0.0f;
                 if (xx >= 0 && xx < g.N_x && yy >= 0 && yy < g.N_y && zz >= 0 && zz < g.N_z)
-                    v = xf[(size_t)zz * plane + (size_t)yy * g.N_x + xx];
+                    v = __ldcg(xf + (size_t)zz * plane + (size_t)yy * g.N_x + xx);
                 xb[lz * S2 * S2 + q] = v;
             }
         for (int sz = warp; sz < 2 * nz; sz += nwarps) {
@@ -471,7 +494,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 const int lx = q % S, ly = q / S;
                 float v = 0.0f;
                 if (ti >= 0 && ti < g.N_time && lx < kx && ly < ky)
-                    v = dv.x[((size_t)ti * g.N_z + z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx];
+                    v = __ldcg(dv.x + ((size_t)ti * g.N_z + z0 + lz) * plane + (size_t)(j0 + ly) * g.N_x + k0 + lx);
                 tb[sz * S * S + q] = v;
             }
         }
@@ -752,6 +775,12 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 }
             }
         }
+        // publish: every thread's writes of this super-voxel, then its flag
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(L.done + id, L.epoch);
+        }
     }
     // ---- per-CTA statistics (lane 0 of each slice's first warp counts) ----
     if (lane == 0) {
@@ -778,14 +807,14 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
 
 template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
 cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
-                      const SvTask *tasks, int ntasks, int ctas, int threads, size_t sm, int *queue, float *scratch,
+                      const SvLaunch &L, int ctas, int threads, size_t sm, int *queue, float *scratch,
                       SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
 {
     cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_icd_sv<AMAXC, MZC, AC, MAXT, VU>
-        <<<ctas, threads, sm, s>>>(g, pr, dv, sp, ac, tasks, ntasks, queue, scratch, out, iter, seed, err);
+        <<<ctas, threads, sm, s>>>(g, pr, dv, sp, ac, L, queue, scratch, out, iter, seed, err);
     return cudaGetLastError();
 }
 
@@ -825,10 +854,10 @@ cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, in
 }
 
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               SvACache ac, const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
-                               SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
+                               SvACache ac, const SvLaunch &L, int ctas, int *queue, float *scratch, SvTaskOut *out,
+                               int iter, uint32_t seed, int *err, cudaStream_t s)
 {
-    if (ntasks <= 0) return cudaSuccess;
+    if (L.ntasks <= 0) return cudaSuccess;
     const bool cached = ac.a != nullptr;
     const size_t sm = mbir_sv_smem_bytes(sp, cached);
     const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
@@ -837,7 +866,7 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
     // fixed trip counts
     const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
     const bool full = sp.amax == 3 && g.m_z == 1 && vpl <= 4;
-#define MBIR_SV_ARGS g, pr, dv, sp, ac, tasks, ntasks, ctas, threads, sm, queue, scratch, out, iter, seed, err, s
+#define MBIR_SV_ARGS g, pr, dv, sp, ac, L, ctas, threads, sm, queue, scratch, out, iter, seed, err, s
 #define MBIR_SV_PICK(MAXT)                                                                                    \
     if (full && vpl <= 2)                                                                                     \
         return cached ? launch_sv<3, 1, true, MAXT, 2>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 2>(MBIR_SV_ARGS); \

@@ -47,9 +47,22 @@ size_t mbir_acache_bytes(const MbirGeom &g, int eq);
 // lines.  err |= 2 if a column has more than amax entries.
 cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
                               cudaStream_t s);
-// ctas persistent CTAs take the ntasks tasks from the queue counter (zero
-// before the launch); scratch holds ctas * sp.band_floats floats; the CTAs
-// add their statistics to *out.
+// One launch: the super-voxels order[0 .. ntasks) (ids into tasks[]) in
+// that order.  Super-voxel order[k] first waits until done[d] == epoch for
+// every id d in deps[dep_off[k] .. dep_off[k + 1]) (the conflicting ones
+// earlier in the order), and sets done[order[k]] = epoch when finished.
+struct SvLaunch {
+    const SvTask *tasks;
+    const int *order, *dep_off, *deps;
+    int ntasks;
+    int *done;
+    int epoch;
+};
+
+// ctas persistent CTAs take the launch's super-voxels from the queue counter
+// (zero before the launch); scratch holds ctas * sp.band_floats floats; the
+// CTAs add their statistics to *out.  err |= 1: a column outside the band,
+// 2: a column wider than amax, 4: a dependency wait gave up.
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
-                               SvACache ac, const SvTask *tasks, int ntasks, int ctas, int *queue, float *scratch,
-                               SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s);
+                               SvACache ac, const SvLaunch &L, int ctas, int *queue, float *scratch, SvTaskOut *out,
+                               int iter, uint32_t seed, int *err, cudaStream_t s);
