@@ -63,11 +63,7 @@ struct MbirTaskOut {
 };
 
 // ---- kernel launchers (mbir_kernels.cu) -------------------------------------
-// mode 0: out = y - A x - d; mode 1: out = A x.  frame_of_view[p] = frame of
-// view p, or -1 for a view outside every frame.
-cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
-                                const float *y, const float *d, float *out, int mode,
-                                cudaStream_t s);
+// (the forward projection is mbir_forward_rows in mbir_sv.cu)
 cudaError_t mbir_launch_icd_ref(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
                                 const MbirTask *tasks, int ntasks, MbirTaskOut *out, int iter,
                                 int threads, size_t acache_bytes, void *acache_global,

@@ -101,70 +101,6 @@ __device__ __forceinline__ T warp_sum(T v)
 }
 
 // ----------------------------------------------------------------------------
-// Error sinogram e = y - A x - d (XT_ICD_update.c:655-716 with the forward
-// projector of XT_ForwardProject.c:8-25).  One CTA per (view, group of up to
-// zc slices): each voxel line's A column at that view is computed once
-// (exact FP64 bins) and applied to every slice of the group, accumulating the
-// projections with float shared-memory atomics (the reference accumulates in
-// float too), then written to the m_z detector rows of each slice.  Voxels
-// are visited along the image axis closer to the detector direction, so the
-// lanes of a warp land on different bins.  Views that belong to no frame
-// project nothing (the reference never visits them).
-// mode 0: out = y - Ax - d (float arithmetic as the reference); mode 1: out = Ax.
-// ----------------------------------------------------------------------------
-__global__ void k_forward(MbirGeom g, const float *__restrict__ x, const int *__restrict__ frame_of_view,
-                          const float *__restrict__ y, const float *__restrict__ d,
-                          float *__restrict__ out, int mode, int zc)
-{
-    extern __shared__ float facc[];  // [zc][N_r]
-    const int p = blockIdx.x, z0 = blockIdx.y * zc;
-    const int nzc = min(zc, g.N_z - z0);
-    for (int q = threadIdx.x; q < nzc * g.N_r; q += blockDim.x) facc[q] = 0.0f;
-    __syncthreads();
-    const int f = frame_of_view[p];
-    const size_t plane = (size_t)g.N_y * g.N_x;
-    if (f >= 0) {
-        const float *xs = x + ((size_t)f * g.N_z + z0) * plane;
-        const int nxy = g.N_y * g.N_x;
-        const bool along_x = fabs(g.cosv[p]) >= fabs(g.sinv[p]);
-        for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-            int j, k;
-            if (along_x) {
-                j = q / g.N_x;
-                k = q - j * g.N_x;
-            } else {
-                k = q / g.N_y;
-                j = q - k * g.N_y;
-            }
-            const int v = j * g.N_x + k;
-            bool any = false;
-            for (int s = 0; s < nzc; s++) any |= xs[s * plane + v] != 0.0f;
-            if (!any) continue;
-            acol_visit(g, voxel_x(g, k), voxel_y(g, j), p, [&](int bin, double f1) {
-                const float a = (float)f1;
-                for (int s = 0; s < nzc; s++) {
-                    const float pix = xs[s * plane + v];
-                    if (pix != 0.0f) atomicAdd(&facc[s * g.N_r + bin], pix * a);
-                }
-            });
-        }
-    }
-    __syncthreads();
-    for (int s = 0; s < nzc; s++)
-        for (int rr = 0; rr < g.m_z; rr++) {
-            const int t = (z0 + s) * g.m_z + rr;
-            for (int r = threadIdx.x; r < g.N_r; r += blockDim.x) {
-                const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
-                const float ax = facc[s * g.N_r + r];
-                if (mode == 0)
-                    out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + r]);
-                else
-                    out[o] = ax;
-            }
-        }
-}
-
-// ----------------------------------------------------------------------------
 // Reference-schedule ICD (XT_VoxUpdate.c:43-281 inside the half-sweeps of
 // XT_ICD_update.c:974-1060).  One CTA per (frame, z-block) task; it walks the
 // task's voxel lines in list order and, per line, the slices of the block in
@@ -638,20 +574,6 @@ int mbir_amax(double delta_xy, double delta_r) { return (int)ceil(3 * delta_xy /
 cudaError_t mbir_launch_to_slice_major(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t s)
 {
     k_to_slice_major<<<1184, 256, 0, s>>>(in, out, N_p, N_t, N_r);
-    return cudaGetLastError();
-}
-
-cudaError_t mbir_launch_forward(const MbirGeom &g, const float *x, const int *frame_of_view,
-                                const float *y, const float *d, float *out, int mode, cudaStream_t s)
-{
-    // two slices per CTA (each A column serves both), within 96 KB of accumulators
-    const int zc = std::max(1, std::min(std::min(g.N_z, 2), (int)((96 * 1024) / (sizeof(float) * g.N_r))));
-    const size_t sm = sizeof(float) * (size_t)zc * g.N_r;
-    if (sm > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    dim3 grid(g.N_p, (g.N_z + zc - 1) / zc);
-    k_forward<<<grid, 256, sm, s>>>(g, x, frame_of_view, y, d, out, mode, zc);
     return cudaGetLastError();
 }
 

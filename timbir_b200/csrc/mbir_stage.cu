@@ -134,6 +134,8 @@ struct MbirStage {
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
     size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
     size_t nxy() const { return (size_t)st.N_y * st.N_x; }
+    // most detector columns of one A-matrix entry: 2 ceil(delta_xy / delta_r) + 1
+    int amax() const { return 2 * (int)std::ceil(st.delta_xy / sg.delta_r) + 1; }
     size_t nmag() const { return (size_t)sg.N_time * nblk * nxy(); }
     int max_views() const
     {
@@ -364,18 +366,20 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     const ScanGeom &sg = S->sg;
     if (compute_detector_response(S)) return -1;
     object_mask(sg, S->st, S->mask);
-    CK(cudaMemcpy(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice));
+    // uploads on the stage's stream, ahead of its kernels (pageable sources
+    // are staged before each call returns)
+    CK(cudaMemcpyAsync(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice, S->stream));
     if (object)
-        CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
     if (offset) {
         std::vector<float> d((size_t)sg.N_t * sg.N_r);
         for (int r = 0; r < sg.N_r; r++)
             for (int t = 0; t < sg.N_t; t++) d[(size_t)t * sg.N_r + r] = offset[(size_t)r * sg.N_t + t];
-        CK(cudaMemcpy(S->d_d, d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(S->d_d, d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
     }
     if (magmap)
-        CK(cudaMemcpy(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(mbir_launch_forward(S->g, S->d_x, S->d_fov, S->d_y, S->d_d, S->d_e, 0, S->stream));
+        CK(cudaMemcpyAsync(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+    CK(mbir_forward_rows(S->g, S->d_fov, S->d_x, S->d_y, S->d_d, S->d_e, 0, S->amax(), S->stream));
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
     S->prepared = 1;
@@ -643,7 +647,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         S->nblk = S->nzg;
         CK(dalloc(&S->d_mag, S->nmag()));
         CK(dalloc(&S->d_filt, S->nmag()));
-        CK(cudaMemset(S->d_mag, 0, S->nmag() * sizeof(float)));
+        CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
         S->dv.mag = S->d_mag;
         S->nr.assign((size_t)S->sg.N_time * S->nblk, 0);
         S->nn.assign((size_t)S->sg.N_time * S->nblk, 0);
@@ -737,19 +741,21 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     S->d_scratch = nullptr;
     S->d_queue = nullptr;
     CK(dalloc(&S->d_sv_all, S->sv_all.size()));
-    CK(cudaMemcpy(S->d_sv_all, S->sv_all.data(), S->sv_all.size() * sizeof(SvTask), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_sv_all, S->sv_all.data(), S->sv_all.size() * sizeof(SvTask), cudaMemcpyHostToDevice,
+                       S->stream));
     CK(dalloc(&S->d_sv_done, S->sv_all.size()));
-    CK(cudaMemset(S->d_sv_done, 0, S->sv_all.size() * sizeof(int)));
+    CK(cudaMemsetAsync(S->d_sv_done, 0, S->sv_all.size() * sizeof(int), S->stream));
     S->sv_epoch = 0;
     CK(dalloc(&S->d_sv_lists, buf.size()));
-    CK(cudaMemcpy(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
     CK(dalloc(&S->d_sv_sel, cap));
     const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sm_count);
     CK(dalloc(&S->d_sv_out, 2));
     CK(dalloc(&S->d_scratch, ctas * sp.band_floats));
     CK(dalloc(&S->d_queue, kMaxLaunchesPerIter));
     if (!S->d_err) CK(dalloc(&S->d_err, 1));
-    CK(cudaMemset(S->d_err, 0, sizeof(int)));
+    CK(cudaMemsetAsync(S->d_err, 0, sizeof(int), S->stream));
+    CK(cudaStreamSynchronize(S->stream));
     if (!S->sv_ev[0])
         for (auto &e : S->sv_ev) CK(cudaEventCreate(&e));
     S->schedule = 1;
@@ -840,6 +846,7 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     if (S->d_acol && !S->acol_built) {
         CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
         S->acol_built = true;
+        S->launches++;
     }
     CK(cudaMemsetAsync(S->d_queue, 0, 2 * sizeof(int), S->stream));
     CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
@@ -1093,7 +1100,7 @@ extern "C" int mbir_forward_project(MbirStage *S, const float *object, float *ou
 {
     if (!S->hr_ready && compute_detector_response(S)) return -1;
     CK(cudaMemcpy(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(mbir_launch_forward(S->g, S->d_x, S->d_fov, nullptr, nullptr, S->d_e, 1, S->stream));
+    CK(mbir_forward_rows(S->g, S->d_fov, S->d_x, nullptr, nullptr, S->d_e, 1, S->amax(), S->stream));
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
     const ScanGeom &sg = S->sg;

@@ -44,6 +44,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "mbir_internal.h"
 #include "mbir_sv.h"
 
@@ -166,7 +168,7 @@ __device__ __forceinline__ bool acol_entry(const MbirGeom &g, double x, double y
                         ok = false;
                         break;
                     }
-                    const float a = (float)num * inv_off_f;
+                    const float a = (float)__ddiv_rn(num, g.OffsetR);
                     if constexpr (AMAXC == 3) {
                         if (k == 0) a0 = a;
                         else if (k == 1) a1 = a;
@@ -221,6 +223,147 @@ __global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__res
         ok &= acol_entry<AMAXC>(g, x, y, g.cosv[p], g.sinv[p], g.H_r + (size_t)p * (MBIR_RESP_BINS + 1), inv_dr,
                                 inv_off, inv_off_f, amax, 4 * eq, reinterpret_cast<int *>(dst + (size_t)p * eq));
     if (!ok) atomicOr(err, 2);
+}
+
+// Forward projection (initErrorSinogam / forward_project_voxel_AMat1D,
+// XT_ICD_update.c:655-716, XT_ForwardProject.c:8-25), gathered and
+// deterministic: a CTA owns one view, a chunk of up to ZC slices and up to
+// BPT * Tg detector columns, and walks the image rows (or columns, whichever
+// the view's detector direction crosses faster), split over G thread groups
+// of Tg threads (rows g, g + G, ...).  For each of its rows a group first
+// computes the exact A-matrix column of every voxel with a non-zero value in
+// the chunk into its shared buffer, with the voxel values; then each thread
+// adds, for each of its detector columns j, a x over the row's voxels whose
+// column includes j -- candidates are the voxels whose centre projects within
+// delta_xy of column j's extent, widened by one voxel each side; the stored
+// column decides.  FP32 sums, as the reference accumulates the projection
+// into its float error sinogram (XT_ForwardProject.c:22); the groups' sums
+// are added in group order at the end.  No atomics.
+template <int AMAXC, int BPT, int ZC>
+__global__ void __launch_bounds__(512, 2) k_forward_rows(MbirGeom g, const int *__restrict__ frame_of_view,
+                                                       const float *__restrict__ x, const float *__restrict__ y,
+                                                       const float *__restrict__ d, float *__restrict__ out, int mode,
+                                                       int amax, int eq, int G)
+{
+    extern __shared__ __align__(16) unsigned char fsm[];
+    const int p = blockIdx.x, z0 = blockIdx.y * ZC, nzc = min(ZC, g.N_z - z0);
+    const int Tg = blockDim.x / G, grp = threadIdx.x / Tg, tid = threadIdx.x - grp * Tg;
+    const int jbase = blockIdx.z * Tg * BPT;
+    const double c = g.cosv[p], sn = g.sinv[p];
+    const bool rows = fabs(c) >= fabs(sn);
+    const int nouter = rows ? g.N_y : g.N_x, ninner = rows ? g.N_x : g.N_y;
+    const int nwd = 4 * eq;
+    const size_t gbytes = (sizeof(int4) * (size_t)eq + sizeof(float) * ZC) * ninner;  // one group's buffer
+    int4 *ent = reinterpret_cast<int4 *>(fsm + grp * gbytes);                     // [ninner][eq]
+    float *xsm = reinterpret_cast<float *>(fsm + grp * gbytes + sizeof(int4) * (size_t)eq * ninner);  // [ZC][ninner]
+    float acc[BPT][ZC];
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+#pragma unroll
+        for (int s = 0; s < ZC; s++) acc[b][s] = 0.0f;
+    const int f = frame_of_view[p];
+    if (f >= 0) {
+        const size_t plane = (size_t)g.N_y * g.N_x;
+        const float *xs = x + ((size_t)f * g.N_z + z0) * plane;
+        const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
+        const float *H = g.H_r + (size_t)p * (MBIR_RESP_BINS + 1);
+        for (int o = grp; o < nouter; o += G) {
+            const double oc = rows ? vy(g, o) : vx(g, o);
+            for (int i = tid; i < ninner; i += Tg) {
+                const int line = rows ? o * g.N_x + i : i * g.N_x + o;
+                bool any = false;
+#pragma unroll
+                for (int s = 0; s < ZC; s++) {
+                    const float v = s < nzc ? __ldg(xs + s * plane + line) : 0.0f;
+                    xsm[s * ninner + i] = v;
+                    any |= v != 0.0f;
+                }
+                int *dst = reinterpret_cast<int *>(ent + (size_t)i * eq);
+                if (!any)
+                    dst[0] = 0;
+                else if (!acol_entry<AMAXC>(g, rows ? vx(g, i) : oc, rows ? oc : vy(g, i), c, sn, H, inv_dr, inv_off,
+                                            0.0f, amax, nwd, dst))
+                    dst[0] = 0;  // wider than amax: cannot occur for 2 mult_xy + 1 columns
+            }
+            named_barrier(1 + grp, Tg);
+#pragma unroll
+            for (int b = 0; b < BPT; b++) {
+                const int j = jbase + b * Tg + tid;
+                if (j >= g.N_r) continue;
+                // rows: xc in [(lo + yc sin) / cos, (hi + yc sin) / cos];
+                // columns: yc in [(xc cos - hi) / sin, (xc cos - lo) / sin]
+                const double lo = g.R0 + (double)j * g.delta_r - g.delta_xy;
+                const double hi = g.R0 + (double)(j + 1) * g.delta_r + g.delta_xy;
+                double a0 = rows ? (lo + oc * sn) / c : (oc * c - hi) / sn;
+                double a1 = rows ? (hi + oc * sn) / c : (oc * c - lo) / sn;
+                if (a0 > a1) {
+                    const double t = a0;
+                    a0 = a1;
+                    a1 = t;
+                }
+                const double base = rows ? g.x0 : g.y0;
+                const int i0 = max((int)floor((a0 - base) / g.delta_xy - 0.5) - 1, 0);
+                const int i1 = min((int)ceil((a1 - base) / g.delta_xy - 0.5) + 1, ninner - 1);
+                for (int i = i0; i <= i1; i++) {
+                    const int *e = reinterpret_cast<const int *>(ent + (size_t)i * eq);
+                    const int h = e[0], k = j - (h & 0xffff);
+                    if (k < 0 || k >= (h >> 16)) continue;
+                    const float a = __int_as_float(e[1 + k]);
+#pragma unroll
+                    for (int s = 0; s < ZC; s++) acc[b][s] = fmaf(a, xsm[s * ninner + i], acc[b][s]);
+                }
+            }
+            named_barrier(1 + grp, Tg);
+        }
+    }
+    // groups' sums, added in group order
+    __syncthreads();
+    float *red = reinterpret_cast<float *>(fsm);  // [G][BPT][ZC][Tg]
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+#pragma unroll
+        for (int s = 0; s < ZC; s++) red[((size_t)(grp * BPT + b) * ZC + s) * Tg + tid] = acc[b][s];
+    __syncthreads();
+    if (grp != 0) return;
+#pragma unroll
+    for (int b = 0; b < BPT; b++) {
+        const int j = jbase + b * Tg + tid;
+        if (j >= g.N_r) continue;
+#pragma unroll
+        for (int s = 0; s < ZC; s++) {
+            if (s >= nzc) break;
+            float ax = 0.0f;
+            for (int q = 0; q < G; q++) ax += red[((size_t)(q * BPT + b) * ZC + s) * Tg + tid];
+            for (int rr = 0; rr < g.m_z; rr++) {
+                const int t = (z0 + s) * g.m_z + rr;
+                const size_t o = ((size_t)t * g.N_p + p) * g.N_r + j;
+                if (mode == 0)
+                    out[o] = __fsub_rn(__fsub_rn(y[o], ax), d[(size_t)t * g.N_r + j]);
+                else
+                    out[o] = ax;
+            }
+        }
+    }
+}
+
+template <int AMAXC, int BPT, int ZC>
+cudaError_t launch_forward_rows(const MbirGeom &g, const int *fov, const float *x, const float *y, const float *d,
+                                float *out, int mode, int amax, cudaStream_t s)
+{
+    const int eq = (1 + amax + 3) / 4;
+    const int per = BPT == 2 ? (g.N_r + 1) / 2 : g.N_r;
+    const int Tg = std::min(128, std::max(64, (per + 31) / 32 * 32));
+    const int ninner = std::max(g.N_x, g.N_y);
+    const size_t gbytes = (sizeof(int4) * (size_t)eq + sizeof(float) * ZC) * ninner;
+    // up to four groups whose row buffers fit 200 KB; the final sums reuse the space
+    const int G = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / gbytes));
+    const size_t sm = std::max(G * gbytes, sizeof(float) * G * BPT * ZC * Tg);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_forward_rows<AMAXC, BPT, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid(g.N_p, (g.N_z + ZC - 1) / ZC, (g.N_r + Tg * BPT - 1) / (Tg * BPT));
+    k_forward_rows<AMAXC, BPT, ZC><<<grid, G * Tg, sm, s>>>(g, fov, x, y, d, out, mode, amax, eq, G);
+    return cudaGetLastError();
 }
 
 // AMAXC: entries per (line, view) known at compile time (3 at full
@@ -834,6 +977,17 @@ size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached)
     b += sizeof(int) * NpS * 2;
     b += sizeof(int) * (S * S + 4);
     return (b + 15) & ~(size_t)15;
+}
+
+cudaError_t mbir_forward_rows(const MbirGeom &g, const int *frame_of_view, const float *x, const float *y,
+                              const float *d, float *out, int mode, int amax, cudaStream_t s)
+{
+    const bool full = amax == 3;
+    if (g.N_z <= 8)
+        return full ? launch_forward_rows<3, 2, 8>(g, frame_of_view, x, y, d, out, mode, amax, s)
+                    : launch_forward_rows<0, 2, 8>(g, frame_of_view, x, y, d, out, mode, amax, s);
+    return full ? launch_forward_rows<3, 2, 16>(g, frame_of_view, x, y, d, out, mode, amax, s)
+                : launch_forward_rows<0, 2, 16>(g, frame_of_view, x, y, d, out, mode, amax, s);
 }
 
 size_t mbir_acache_bytes(const MbirGeom &g, int eq)

@@ -47,6 +47,12 @@ size_t mbir_acache_bytes(const MbirGeom &g, int eq);
 // lines.  err |= 2 if a column has more than amax entries.
 cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
                               cudaStream_t s);
+// Forward projection, deterministic (FP32 sums in a fixed order, no
+// atomics): mode 0: out = y - A x - d; mode 1: out = A x.  amax: most
+// columns per A-matrix entry (2 mult_xy + 1).
+cudaError_t mbir_forward_rows(const MbirGeom &g, const int *frame_of_view, const float *x, const float *y,
+                              const float *d, float *out, int mode, int amax, cudaStream_t s);
+
 // One launch: the super-voxels order[0 .. ntasks) (ids into tasks[]) in
 // that order.  Super-voxel order[k] first waits until done[d] == epoch for
 // every id d in deps[dep_off[k] .. dep_off[k + 1]) (the conflicting ones
