@@ -166,3 +166,34 @@ def test_sv_cached_and_computed_columns_give_the_same_iterates(name):
     (x1, e1), (x0, e0) = out
     assert np.array_equal(x1, x0), float(np.abs(x1 - x0).max())
     assert np.array_equal(e1, e0), float(np.abs(e1 - e0).max())
+
+
+def test_sv_one_warp_per_slice_with_eight_views_per_lane():
+    # 192 views and one warp per slice: each lane holds 6 views of a slice in
+    # registers (the 8-views-per-lane variant); it must reach the same
+    # minimum as two warps per slice, and keep its error sinogram consistent
+    from timbir_b200 import synth
+    scan = synth.ellipsoid_scan(32, 4, 192, seed=9)
+    kw = dict(scenarios.BASE)
+    costs = []
+    for wps in (1, 2):
+        s = timbir_b200.Stage(scan, blocks=2, **kw)
+        s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0, wps)
+        assert s.schedule_info()["warps_per_slice"] == wps
+        s.prepare()
+        for it in range(1, 201):
+            s.iterate(it)
+        o = Oracle(scan, blocks=2, f64=True, **kw)
+        o.prepare(s.object(), s.offset())
+        costs.append(o.cost()[0])
+    assert abs(costs[0] - costs[1]) / abs(costs[1]) < 1e-6
+    # bookkeeping over 10 iterations, as the other consistency tests
+    s = timbir_b200.Stage(scan, blocks=2, **kw)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0, 1)
+    s.prepare()
+    for it in range(1, 11):
+        s.iterate(it)
+    f = timbir_b200.Stage(scan, blocks=2, **kw)
+    f.prepare(s.object(), s.offset())
+    scale = np.abs(f.errorsino()).max()
+    assert np.abs(s.errorsino() - f.errorsino()).max() < 2e-5 * scale

@@ -524,6 +524,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     sp.W = (int)floor((side - 1) * sqrt(2.0) * m + 2 * m + 1e-9) + 3;
     sp.amax = 2 * (int)ceil(m) + 1;
     sp.eq = (1 + sp.amax + 3) / 4;
+    sp.ring = 4;
     sp.max_views = S->max_views();
     sp.max_nz = nz;
     sp.max_rows = nz * S->st.m_z;

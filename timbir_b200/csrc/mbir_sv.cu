@@ -26,8 +26,8 @@
 // memory and a named barrier; one CTA barrier per line step hands the
 // updated voxels and the next line's A-matrix column to all warps.
 //
-// A-matrix columns reach a four-slot shared-memory ring either from the
-// stage's column cache in HBM (cp.async, two lines ahead, every thread
+// A-matrix columns reach a ring of R shared-memory slots either from the
+// stage's column cache in HBM (cp.async, R - 2 lines ahead, every thread
 // copying a share) or, when the cache does not fit, from producer warps that
 // compute the next line's column (exact FP64 bin arithmetic) while the
 // consumer warps update voxels.
@@ -115,6 +115,21 @@ __device__ __forceinline__ void st_release(int *p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// 2^x and 1/x by the SFU approximations (a few ulp; the prior's weights and
+// the surrogate step need no more)
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d)
 {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
@@ -127,8 +142,20 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// waits until at most n (0..6) of this thread's commit groups are pending
+__device__ __forceinline__ void cp_async_wait_upto(int n)
+{
+    switch (n) {
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+    }
+}
 
 // Exact A-matrix column of the voxel line centred at (x, y) for one view
 // (calcAMatrixColumnforAngle, XT_AMatrix.c:50-110): detector columns
@@ -392,7 +419,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
 
     // ---- carve shared memory (sizes fixed by the host in sp) ----
     unsigned char *p = smraw;
-    int4 *ring = reinterpret_cast<int4 *>(p); p += sizeof(int4) * 4 * (size_t)eq * NpS;
+    const int R = sp.ring, D = R - 2;  // ring slots; column prefetch distance (lines)
+    int4 *ring = reinterpret_cast<int4 *>(p); p += sizeof(int4) * (size_t)R * eq * NpS;
     float2 *band = reinterpret_cast<float2 *>(p); p += sizeof(float2) * (size_t)sp.max_rows * rowstride;
     double *cs = reinterpret_cast<double *>(p);
     double *sn = cs + NpS;
@@ -642,13 +670,13 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             }
         }
 
-        // ---- A-matrix column of line `li` into ring slot li & 3 ----
+        // ---- A-matrix column of line `li` into ring slot `slot` (li mod R) ----
         // from the cache: every thread copies a share (one commit group per call)
-        auto fetch = [&](int li) {
+        auto fetch = [&](int li, int slot) {
             if (li < nl && order[li] >= 0) {
                 const int o = order[li];
                 const size_t line = (size_t)(j0 + (o >> 8)) * g.N_x + k0 + (o & 0xff);
-                int4 *dst = ring + (size_t)(li & 3) * eq * NpS;
+                int4 *dst = ring + (size_t)slot * eq * NpS;
                 for (int q = tid; q < Np * eq; q += nthr) {
                     const int v = q / eq, w = q - v * eq;
                     cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
@@ -657,12 +685,12 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             cp_async_commit();
         };
         // computed: warps [w0, nwarps), av_lanes views per warp
-        auto acol = [&](int li, int w0, int av_lanes) {
+        auto acol = [&](int li, int slot, int w0, int av_lanes) {
             const int wr = warp - w0;
             const int o = order[li];
             if (wr < 0 || o < 0) return;
             const double x = vx(g, k0 + (o & 0xff)), y = vy(g, j0 + (o >> 8));
-            int *rw = reinterpret_cast<int *>(ring + (size_t)(li & 3) * eq * NpS);
+            int *rw = reinterpret_cast<int *>(ring + (size_t)slot * eq * NpS);
             for (int l = lane; l < av_lanes; l += 32) {
                 const int v = wr * av_lanes + l;
                 if (v >= Np) break;
@@ -675,16 +703,17 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         };
 
         if (AC) {
-            fetch(0);
-            fetch(1);
-            cp_async_wait1();
+            for (int q = 0; q < D; q++) fetch(q, q);
+            cp_async_wait_upto(D - 1);
         } else if (nl > 0) {
-            acol(0, 0, av_all);
+            acol(0, 0, 0, av_all);
         }
         __syncthreads();
 
-        for (int step = 0; step <= nl; step++) {
+        for (int step = 0, sl = 0; step <= nl; step++, sl = sl + 1 == R ? 0 : sl + 1) {
+            // sl = step mod R: the slot of line `step`; odd slices use line step - 1
             const int li = (zl & 1) ? step - 1 : step;
+            const int slot = (zl & 1) ? (sl == 0 ? R - 1 : sl - 1) : sl;
             const int o = li >= 0 && li < nl ? order[li] : -1;
             if (active && o >= 0) {
                 const int lx = o & 0xff, ly = o >> 8;
@@ -709,7 +738,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 } else {
                     // ---- data term over this slice's band rows, this warp's views ----
                     float th1 = 0.0f, th2 = 0.0f, th1b = 0.0f, th2b = 0.0f;
-                    const int4 *rq = ring + (size_t)(li & 3) * eq * NpS;
+                    const int4 *rq = ring + (size_t)slot * eq * NpS;
                     const float2 *bz = band + (size_t)zl * mz * rowstride;
                     // full resolution: per view three consecutive columns from
                     // j0 (clamped into the band; absent ones carry a = 0),
@@ -788,8 +817,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                     float p1 = 0.0f, p2 = 0.0f;
                     if (vh == 0 && valid) {
                         const float ad = fabsf(V - nbv);
-                        const float t1 = (ad > 0.0f ? exp2f(0.8f * __log2f(ad)) : 0.0f) * qpinv;
-                        const float rt3 = __frcp_rn(cc + t1);
+                        const float t1 = (ad > 0.0f ? ex2_approx(0.8f * __log2f(ad)) : 0.0f) * qpinv;
+                        const float rt3 = rcp_approx(cc + t1);
                         const float b = bw * (2.0f - 0.8f * t1 * rt3) * rt3 * qinv;
                         p1 = b * nbv;
                         p2 = b;
@@ -812,7 +841,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                         p1 = __shfl_sync(0xffffffffu, red, 16);
                         p2 = __shfl_sync(0xffffffffu, red, 24);
                     }
-                    const float u = (p1 + th2 * V - th1) / (p2 + th2);
+                    const float u = (p1 + th2 * V - th1) * rcp_approx(p2 + th2);
                     const float xn = V + alpha * (u - V);
                     const float dx = xn - V;
                     if (vh == 0) {
@@ -851,13 +880,14 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                 }
             }
             if (AC) {
-                fetch(step + 2);
-                cp_async_wait1();
+                fetch(step + D, sl + D >= R ? sl + D - R : sl + D);
+                cp_async_wait_upto(D - 1);
             } else if (step + 1 < nl) {
+                const int sn1 = sl + 1 == R ? 0 : sl + 1;
                 if (nprod > 0) {
-                    if (!consumer) acol(step + 1, ncons, av_prod);
+                    if (!consumer) acol(step + 1, sn1, ncons, av_prod);
                 } else {
-                    acol(step + 1, 0, av_all);
+                    acol(step + 1, sn1, 0, av_all);
                 }
             }
             __syncthreads();
@@ -967,7 +997,7 @@ size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached)
 {
     const size_t NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
     size_t b = 0;
-    b += 16 * 4 * (size_t)sp.eq * NpS;  // A-column ring, four slots
+    b += 16 * (size_t)sp.ring * sp.eq * NpS;  // A-column ring
     b += 8 * (size_t)sp.max_rows * sp.W * NpS;  // (e, sqrt(w)) band
     if (!cached) b += 2 * sizeof(double) * NpS;
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
@@ -1027,6 +1057,10 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
     if (full)                                                                                                 \
         return cached ? launch_sv<3, 1, true, MAXT, 4>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 4>(MBIR_SV_ARGS); \
     return cached ? launch_sv<0, 0, true, MAXT, 0>(MBIR_SV_ARGS) : launch_sv<0, 0, false, MAXT, 0>(MBIR_SV_ARGS);
+    // one warp per slice with up to 8 views per lane in registers (the
+    // cached path; 256 threads at most leave 255 registers per thread)
+    if (cached && threads <= 256 && sp.amax == 3 && g.m_z == 1 && vpl > 4 && vpl <= 8)
+        return launch_sv<3, 1, true, 256, 8>(MBIR_SV_ARGS);
     if (threads <= 512) {
         MBIR_SV_PICK(512)
     }

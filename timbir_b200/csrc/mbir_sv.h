@@ -16,6 +16,7 @@ struct SvParams {
     int max_rows;   // detector rows per CTA: max_nz * m_z
     int vsplit;     // warps per slice (1, 2 or 4; > 1 needs max_nz <= 15)
     int prod_warps; // warps computing the next line's A-matrix column (0 with a column cache)
+    int ring;       // A-column ring slots, 4..8 (the cache is read ring - 2 lines ahead)
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
 };
 
