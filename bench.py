@@ -80,6 +80,11 @@ W4D = Workload("4d", "4d two-phase microstructure 16 x 256x256x16, 1024 interlac
                "synthetic (seeded Gaussian-random-field two-phase frames, Poisson counts, zingers, rings)")
 WORKLOADS = {"3d": W3D, "4d": W4D}
 METRIC = "ICD voxel-updates/s"
+# DRAM bytes (read + write) per voxel update of the super-voxel kernel, from
+# one ncu capture of a full-sweep launch (profiles/k_icd_sv_3d_256x256x8.md:
+# 217.6 MB read + 5.8 MB written over the 411,744 in-mask voxels of the 3-D
+# workload); the line's roofline.traffic scales it to the average launch.
+DRAM_BYTES_PER_UPDATE = {"3d": (217.594e6 + 5.823e6) / 411744}
 
 
 def fourd_scan(w, seed_offset=0):
@@ -368,10 +373,16 @@ def gpu_arm(args, rank, world, local_rank):
     npf = w.views // w.frames
     b_vu = npf * (cbar * 1 * 12 + 2 * cbar + 2) + 29 * 4 + 4
     achieved = (updates * b_vu) / (icd_ms / 1e3) / 1e9 if icd_ms > 0 else 0.0
+    n_icd = max(n_icd1 - n_icd0, 1)
+    traffic, traffic_src = None, None
+    if sched and args.config in DRAM_BYTES_PER_UPDATE:
+        traffic = DRAM_BYTES_PER_UPDATE[args.config] * updates / n_icd
+        traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum per update of a sweep launch, x updates per launch"
     line = {
         "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 theta, prior and update)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (A-matrix bin indices exact in FP64; cost and convergence sums FP64)",
         "data": w.data,
         "config": {"workload": w.desc, "volume": [w.frames, w.rows, w.n_xy, w.n_xy],
                    "views": w.views,
@@ -381,7 +392,8 @@ def gpu_arm(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "bytes_per_update": b_vu, "mean_bins_per_view": cbar,
                      "kernel": "k_icd_sv" if sched else "k_icd_ref", "kernel_ms": icd_ms,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
