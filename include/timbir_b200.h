@@ -96,10 +96,20 @@ int mbir_get_schedule(MbirStage *stage, int32_t *schedule, int32_t *sv_side, int
  * Takes effect at the next mbir_set_schedule. */
 int mbir_set_acache(MbirStage *stage, int32_t mode);
 int mbir_get_acache(MbirStage *stage, int32_t *used, int64_t *bytes);
-/* Persistent CTAs per launch of schedule 1 (0, the default: one per SM).
- * With 1 the super-voxels of a launch run one after another, which makes
- * the schedule deterministic (a debugging and testing aid). */
+/* Persistent CTAs per launch of schedule 1 (0, the default: automatic, see
+ * mbir_get_sv_grid).  With 1 the super-voxels of a launch run one after
+ * another, which makes the schedule deterministic (a debugging and testing
+ * aid); more than the automatic count can make the iteration diverge. */
 int mbir_set_sv_ctas(MbirStage *stage, int32_t ctas);
+/* Slices per z-group of schedule 1 (0, the default: automatic); takes
+ * effect at the next mbir_set_schedule.  Z-groups have disjoint sinogram
+ * rows, so smaller groups allow more super-voxels in flight. */
+int mbir_set_sv_zgroup(MbirStage *stage, int32_t slices);
+/* The automatic launch size of schedule 1: persistent CTAs per launch, the
+ * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
+ * correct the same rays at once and the iteration diverges), and the CTAs
+ * that fit the GPU. */
+int mbir_get_sv_grid(MbirStage *stage, int32_t *ctas, int32_t *cap_per_group, int32_t *resident);
 /* The cached columns of in-mask voxel line (row, col) for every view:
  * N_p x 4 ceil((2 + 2 mult_xy) / 4) words; per view, word 0 = j0 | n << 16
  * (first detector column with a positive entry, number of columns from it),

@@ -197,3 +197,23 @@ def test_sv_one_warp_per_slice_with_eight_views_per_lane():
     f.prepare(s.object(), s.offset())
     scale = np.abs(f.errorsino()).max()
     assert np.abs(s.errorsino() - f.errorsino()).max() < 2e-5 * scale
+
+
+def test_sv_full_size_slices_converge_with_the_automatic_grid():
+    # 256 x 256 slices: super-voxels in flight on one sinogram each correct
+    # the rays they share; with too many at once (48 of side 6 here) the
+    # iteration diverges.  The automatic grid must keep the cost falling.
+    from timbir_b200 import synth
+    scan = synth.ellipsoid_scan(256, 8, 256, I0=1e4, seed=0)
+    kw = dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=0, quad_convex=1)
+    s = timbir_b200.Stage(scan, blocks=8, **kw)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0)
+    info = s.schedule_info()
+    assert info["ctas"] <= info["inflight_per_group"]
+    s.prepare(np.asarray(scan.phantom, np.float32) * 0.9)
+    costs = [s.cost()[0]]
+    for it in range(1, 11):
+        s.iterate(it)
+        costs.append(s.cost()[0])
+    assert all(np.isfinite(costs))
+    assert all(b < a for a, b in zip(costs, costs[1:])), costs

@@ -128,7 +128,12 @@ struct MbirStage {
     bool acol_built = false;
     int *d_err = nullptr, *d_queue = nullptr;
     int sm_count = 148;
-    int sv_ctas = 0;  // persistent CTAs per launch; 0 = one per SM
+    int sv_ctas = 0;    // persistent CTAs per launch requested; 0 = automatic
+    int sv_zgroup = 0;  // slices per z-group requested; 0 = automatic
+    int sv_grid = 1;    // persistent CTAs per launch (automatic)
+    int sv_cap = 0;     // concurrent super-voxels allowed per (frame, z-group)
+    int sv_fit = 1;     // CTAs resident on the GPU (all SMs)
+    std::vector<int> sv_rank;  // size rank of a super-voxel within its (phase, frame, z-group)
     double nh_fraction = 0.2;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
@@ -542,12 +547,16 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
 
 // Orders super-voxel ids for a sweep: colour phases starting from phase r,
 // the largest super-voxels of a phase first.
+// Orders super-voxel ids for a sweep: colour phases starting from phase r;
+// within a phase the (frame, z-group) groups take turns, largest super-voxels
+// first, so that the super-voxels in flight spread over the groups.
 static void sv_sort(const MbirStage *S, std::vector<int> &ids, int r)
 {
     const int P = S->sv_nphase;
     std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
         const int pa = (S->sv_all_phase[a] - r + P) % P, pb = (S->sv_all_phase[b] - r + P) % P;
         if (pa != pb) return pa < pb;
+        if (S->sv_rank[a] != S->sv_rank[b]) return S->sv_rank[a] < S->sv_rank[b];
         return S->sv_all[a].nlines > S->sv_all[b].nlines;
     });
 }
@@ -614,7 +623,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         S->acol_built = false;
     }
     const bool cached = S->d_acol != nullptr;
-    int gz = std::min(Nz, 32), side = sv_side;
+    int gz = S->sv_zgroup > 0 ? std::min(S->sv_zgroup, Nz) : std::min(Nz, 32), side = sv_side;
     SvParams sp{};
     for (;;) {
         if (side > 0) {
@@ -688,6 +697,21 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
                     S->sv_all_phase.push_back(phase_of[colour]);
                 }
     S->sv_nphase = nphase;
+    // size rank within (phase, frame, z-group)
+    {
+        std::vector<int> ids(S->sv_all.size());
+        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
+        auto key = [&](int a) {
+            return ((long long)S->sv_all_phase[a] * N_time + S->sv_all[a].frame) * S->nzg + S->sv_all[a].z0 / gz;
+        };
+        std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+            if (key(a) != key(b)) return key(a) < key(b);
+            return S->sv_all[a].nlines > S->sv_all[b].nlines;
+        });
+        S->sv_rank.assign(ids.size(), 0);
+        for (size_t q = 1; q < ids.size(); q++)
+            S->sv_rank[ids[q]] = key(ids[q]) == key(ids[q - 1]) ? S->sv_rank[ids[q - 1]] + 1 : 0;
+    }
     // conflicts: super-voxels sharing a prior neighbourhood -- x-y-z neighbours
     // in the same frame, the same block in adjacent frames
     S->sv_nbr.assign(S->sv_all.size(), {});
@@ -750,7 +774,27 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     CK(dalloc(&S->d_sv_lists, buf.size()));
     CK(cudaMemcpyAsync(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
     CK(dalloc(&S->d_sv_sel, cap));
-    const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sm_count);
+    // Concurrency.  Super-voxels that run at once each correct the residual of
+    // the rays they share as if alone, so their over-relaxed steps add up.  A
+    // ray of a (frame, z-group) sinogram crosses on average 2 n W / (pi R) of
+    // the n super-voxels in flight on it (band width W, object radius R, both
+    // in voxels).  Measured on 256 x 256 slices the iteration diverges once
+    // that exceeds about 2.1 (sides 4-10; e.g. side 6 converges with 33 in
+    // flight and diverges with 48), so n is capped at 1.8 pi R / (2 W) per
+    // sinogram.  The queue runs one colour phase at a time -- one z-group
+    // parity and one frame parity -- so half the z-groups and half the frames
+    // have super-voxels in flight; it interleaves those groups.
+    {
+        const double kMaxCrossings = 1.8;
+        const double Rv = S->sg.radius_obj / S->st.delta_xy;
+        const double Wv = sp.W * S->sg.delta_r / S->st.delta_xy;
+        S->sv_cap = std::max(4, (int)std::floor(kMaxCrossings * M_PI * Rv / (2.0 * Wv)));
+        S->sv_fit = mbir_sv_ctas_per_sm(S->g, sp, cached) * S->sm_count;
+        const long long active = (long long)(N_time > 1 ? (N_time + 1) / 2 : 1) * (S->nzg > 1 ? (S->nzg + 1) / 2 : 1);
+        S->sv_grid = (int)std::max<long long>(
+            1, std::min<long long>({(long long)S->sv_all.size(), (long long)S->sv_fit, S->sv_cap * active}));
+    }
+    const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sv_fit);
     CK(dalloc(&S->d_sv_out, 2));
     CK(dalloc(&S->d_scratch, ctas * sp.band_floats));
     CK(dalloc(&S->d_queue, kMaxLaunchesPerIter));
@@ -774,6 +818,21 @@ extern "C" int mbir_set_sv_ctas(MbirStage *S, int32_t ctas)
 {
     if (ctas < 0) return fail("negative CTA count");
     S->sv_ctas = ctas;
+    return 0;
+}
+
+extern "C" int mbir_set_sv_zgroup(MbirStage *S, int32_t slices)
+{
+    if (slices < 0) return fail("negative z-group size");
+    S->sv_zgroup = slices;
+    return 0;
+}
+
+extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_group, int32_t *resident)
+{
+    if (ctas) *ctas = S->sv_grid;
+    if (cap_per_group) *cap_per_group = S->sv_cap;
+    if (resident) *resident = S->sv_fit;
     return 0;
 }
 
@@ -823,7 +882,7 @@ static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> 
 {
     const int n = (int)meta[0];
     if (n <= 0) return 0;
-    const int ctas = std::min(n, S->sv_ctas > 0 ? S->sv_ctas : S->sm_count);
+    const int ctas = std::min(n, S->sv_ctas > 0 ? std::min(S->sv_ctas, S->sv_fit) : S->sv_grid);
     SvACache ac{S->d_acol};
     SvLaunch L{S->d_sv_all, list + meta[1], list + meta[2], list + meta[3], n, S->d_sv_done, ++S->sv_epoch};
     CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, ac, L, ctas, S->d_queue + qslot, S->d_scratch, acc, iter,

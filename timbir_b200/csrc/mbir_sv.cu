@@ -979,6 +979,19 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
 }
 
 template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
+int occupancy_sv(int threads, size_t sm)
+{
+    if (cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm) != cudaSuccess)
+        return 1;
+    int n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_icd_sv<AMAXC, MZC, AC, MAXT, VU>, threads, sm) !=
+        cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
+}
+
+template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
 cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
                       const SvLaunch &L, int ctas, int threads, size_t sm, int *queue, float *scratch,
                       SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
@@ -1037,6 +1050,45 @@ cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, in
     return cudaGetLastError();
 }
 
+// Instantiation of the super-voxel kernel for a configuration: F is called
+// with a tag carrying its template arguments.
+template <int A_, int M_, bool C_, int T_, int V_>
+struct SvInst {
+    static constexpr int AMAXC = A_, MZC = M_, MAXT = T_, VU = V_;
+    static constexpr bool AC = C_;
+};
+template <class F>
+auto sv_dispatch(const MbirGeom &g, const SvParams &sp, bool cached, int threads, F &&f)
+{
+    // full resolution (3 columns per entry, one detector row per slice) with
+    // at most 4 views per lane and slice has its own instantiations with
+    // fixed trip counts; one warp per slice with up to 8 views per lane in
+    // registers (the cached path; 256 threads leave 255 registers per thread)
+    const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
+    const bool full = sp.amax == 3 && g.m_z == 1 && vpl <= 4;
+    if (cached && threads <= 256 && sp.amax == 3 && g.m_z == 1 && vpl > 4 && vpl <= 8)
+        return f(SvInst<3, 1, true, 256, 8>{});
+#define MBIR_SV_PICK(T)                                                                                    \
+    if (full && vpl <= 2) return cached ? f(SvInst<3, 1, true, T, 2>{}) : f(SvInst<3, 1, false, T, 2>{}); \
+    if (full) return cached ? f(SvInst<3, 1, true, T, 4>{}) : f(SvInst<3, 1, false, T, 4>{});             \
+    return cached ? f(SvInst<0, 0, true, T, 0>{}) : f(SvInst<0, 0, false, T, 0>{});
+    if (threads <= 512) {
+        MBIR_SV_PICK(512)
+    }
+    MBIR_SV_PICK(1024)
+#undef MBIR_SV_PICK
+}
+
+int mbir_sv_ctas_per_sm(const MbirGeom &g, const SvParams &sp, bool cached)
+{
+    const size_t sm = mbir_sv_smem_bytes(sp, cached);
+    const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
+    return sv_dispatch(g, sp, cached, threads, [&](auto I) {
+        using In = decltype(I);
+        return occupancy_sv<In::AMAXC, In::MZC, In::AC, In::MAXT, In::VU>(threads, sm);
+    });
+}
+
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
                                SvACache ac, const SvLaunch &L, int ctas, int *queue, float *scratch, SvTaskOut *out,
                                int iter, uint32_t seed, int *err, cudaStream_t s)
@@ -1045,26 +1097,9 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
     const bool cached = ac.a != nullptr;
     const size_t sm = mbir_sv_smem_bytes(sp, cached);
     const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
-    // full resolution (3 columns per entry, one detector row per slice) with
-    // at most 4 views per lane and slice has its own instantiations with
-    // fixed trip counts
-    const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
-    const bool full = sp.amax == 3 && g.m_z == 1 && vpl <= 4;
-#define MBIR_SV_ARGS g, pr, dv, sp, ac, L, ctas, threads, sm, queue, scratch, out, iter, seed, err, s
-#define MBIR_SV_PICK(MAXT)                                                                                    \
-    if (full && vpl <= 2)                                                                                     \
-        return cached ? launch_sv<3, 1, true, MAXT, 2>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 2>(MBIR_SV_ARGS); \
-    if (full)                                                                                                 \
-        return cached ? launch_sv<3, 1, true, MAXT, 4>(MBIR_SV_ARGS) : launch_sv<3, 1, false, MAXT, 4>(MBIR_SV_ARGS); \
-    return cached ? launch_sv<0, 0, true, MAXT, 0>(MBIR_SV_ARGS) : launch_sv<0, 0, false, MAXT, 0>(MBIR_SV_ARGS);
-    // one warp per slice with up to 8 views per lane in registers (the
-    // cached path; 256 threads at most leave 255 registers per thread)
-    if (cached && threads <= 256 && sp.amax == 3 && g.m_z == 1 && vpl > 4 && vpl <= 8)
-        return launch_sv<3, 1, true, 256, 8>(MBIR_SV_ARGS);
-    if (threads <= 512) {
-        MBIR_SV_PICK(512)
-    }
-    MBIR_SV_PICK(1024)
-#undef MBIR_SV_PICK
-#undef MBIR_SV_ARGS
+    return sv_dispatch(g, sp, cached, threads, [&](auto I) {
+        using In = decltype(I);
+        return launch_sv<In::AMAXC, In::MZC, In::AC, In::MAXT, In::VU>(g, pr, dv, sp, ac, L, ctas, threads, sm, queue,
+                                                                       scratch, out, iter, seed, err, s);
+    });
 }

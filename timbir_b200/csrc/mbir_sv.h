@@ -66,6 +66,9 @@ struct SvLaunch {
     int epoch;
 };
 
+// CTAs of the super-voxel kernel that fit one SM for this configuration.
+int mbir_sv_ctas_per_sm(const MbirGeom &g, const SvParams &sp, bool cached);
+
 // ctas persistent CTAs take the launch's super-voxels from the queue counter
 // (zero before the launch); scratch holds ctas * sp.band_floats floats; the
 // CTAs add their statistics to *out.  err |= 1: a column outside the band,
