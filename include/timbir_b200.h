@@ -105,11 +105,18 @@ int mbir_set_sv_ctas(MbirStage *stage, int32_t ctas);
  * effect at the next mbir_set_schedule.  Z-groups have disjoint sinogram
  * rows, so smaller groups allow more super-voxels in flight. */
 int mbir_set_sv_zgroup(MbirStage *stage, int32_t slices);
+/* Over-relaxation of schedule 1's voxel steps, in (0, 2); 0 (the default)
+ * chooses it: the reference's 1.5 (XT_ICD_update.c:134-183) when the GPU can
+ * be kept busy with it, else the largest value down to 0.7 that allows enough
+ * super-voxels in flight (see mbir_get_sv_grid).  Takes effect at the next
+ * mbir_set_schedule.  The reference schedule always uses 1.5. */
+int mbir_set_sv_relaxation(MbirStage *stage, double alpha);
 /* The automatic launch size of schedule 1: persistent CTAs per launch, the
  * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
- * correct the same rays at once and the iteration diverges), and the CTAs
- * that fit the GPU. */
-int mbir_get_sv_grid(MbirStage *stage, int32_t *ctas, int32_t *cap_per_group, int32_t *resident);
+ * correct the same rays at once and the iteration diverges), the CTAs that
+ * fit the GPU, and the over-relaxation in use. */
+int mbir_get_sv_grid(MbirStage *stage, int32_t *ctas, int32_t *cap_per_group, int32_t *resident,
+                     double *relaxation);
 /* The cached columns of in-mask voxel line (row, col) for every view:
  * N_p x 4 ceil((2 + 2 mult_xy) / 4) words; per view, word 0 = j0 | n << 16
  * (first detector column with a positive entry, number of columns from it),

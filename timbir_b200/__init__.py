@@ -74,7 +74,8 @@ def load_library() -> C.CDLL:
     lib.mbir_get_acache_line.argtypes = [_VP, i32, i32, _i32p]
     lib.mbir_set_sv_ctas.argtypes = [_VP, i32]
     lib.mbir_set_sv_zgroup.argtypes = [_VP, i32]
-    lib.mbir_get_sv_grid.argtypes = [_VP] + [C.POINTER(i32)] * 3
+    lib.mbir_get_sv_grid.argtypes = [_VP] + [C.POINTER(i32)] * 3 + [C.POINTER(C.c_double)]
+    lib.mbir_set_sv_relaxation.argtypes = [_VP, C.c_double]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     lib.reconstruct.argtypes = [C.POINTER(C.POINTER(C.c_float))] + [_VP] * 5 + [i32] * 4 + [fl] * 7 + \
@@ -164,9 +165,16 @@ class Stage:
                      [x.value for x in v]))
         d["column_cache_bytes"] = int(nbytes.value) if used.value else 0
         g = [C.c_int32() for _ in range(3)]
-        self.lib.mbir_get_sv_grid(self.h, *[C.byref(x) for x in g])
+        rel = C.c_double()
+        self.lib.mbir_get_sv_grid(self.h, *[C.byref(x) for x in g], C.byref(rel))
         d["ctas"], d["inflight_per_group"], d["resident_ctas"] = [x.value for x in g]
+        d["relaxation"] = rel.value
         return d
+
+    def set_sv_relaxation(self, alpha: float):
+        """Over-relaxation of the super-voxel schedule in (0, 2); 0 = automatic.
+        Call before set_schedule."""
+        _check(self.lib.mbir_set_sv_relaxation(self.h, alpha))
 
     def set_sv_zgroup(self, slices: int):
         """Slices per z-group of the super-voxel schedule (0 = automatic); call

@@ -133,6 +133,8 @@ struct MbirStage {
     int sv_grid = 1;    // persistent CTAs per launch (automatic)
     int sv_cap = 0;     // concurrent super-voxels allowed per (frame, z-group)
     int sv_fit = 1;     // CTAs resident on the GPU (all SMs)
+    double sv_alpha = 0;      // over-relaxation of schedule 1 requested; 0 = automatic
+    double sv_alpha_eff = 1.5;  // over-relaxation schedule 1 uses
     std::vector<int> sv_rank;  // size rank of a super-voxel within its (phase, frame, z-group)
     double nh_fraction = 0.2;
 
@@ -775,24 +777,46 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     CK(cudaMemcpyAsync(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
     CK(dalloc(&S->d_sv_sel, cap));
     // Concurrency.  Super-voxels that run at once each correct the residual of
-    // the rays they share as if alone, so their over-relaxed steps add up.  A
-    // ray of a (frame, z-group) sinogram crosses on average 2 n W / (pi R) of
-    // the n super-voxels in flight on it (band width W, object radius R, both
-    // in voxels).  Measured on 256 x 256 slices the iteration diverges once
-    // that exceeds about 2.1 (sides 4-10; e.g. side 6 converges with 33 in
-    // flight and diverges with 48), so n is capped at 1.8 pi R / (2 W) per
-    // sinogram.  The queue runs one colour phase at a time -- one z-group
-    // parity and one frame parity -- so half the z-groups and half the frames
-    // have super-voxels in flight; it interleaves those groups.
+    // the rays they share as if alone, so their steps add up.  A ray of a
+    // (frame, z-group) sinogram crosses on average c = 2 n W / (pi R) of the n
+    // super-voxels in flight on it (band width W, object radius R, both in
+    // voxels).  With the reference's over-relaxation 1.5 the iteration
+    // diverges once c exceeds about 2.1 (measured on 256 x 256 slices, sides
+    // 4-10: side 6 converges with 33 in flight, diverges with 48); the limit
+    // behaves as (2 / alpha - 1) / 0.16, so a smaller alpha allows more in
+    // flight.  The cap keeps c at 1.8 x that limit / 2.1.  The queue runs one
+    // colour phase at a time -- one z-group parity and one frame parity -- so
+    // half the z-groups and half the frames have super-voxels in flight; it
+    // interleaves those groups.  Unless set, alpha is the reference's 1.5
+    // when the cap lets every resident CTA work, else the largest value
+    // (down to 0.7) that does, as long as the super-voxels in flight stay a
+    // small share (12 %) of their group's: measured on the 3-D workload, alpha
+    // 0.76 with all 148 CTAs (10 % of the super-voxels) reaches the MAP cost
+    // within 1e-5 in 21 iterations and 32 ms, alpha 1.5 with the 30 CTAs it
+    // allows in 26 iterations and 156 ms; on a 32 x 32 slice with 64
+    // super-voxels, 28 in flight at alpha 0.7 converged far more slowly.
     {
-        const double kMaxCrossings = 1.8;
         const double Rv = S->sg.radius_obj / S->st.delta_xy;
         const double Wv = sp.W * S->sg.delta_r / S->st.delta_xy;
-        S->sv_cap = std::max(4, (int)std::floor(kMaxCrossings * M_PI * Rv / (2.0 * Wv)));
+        const double ref_alpha = S->pr.alpha;
+        auto cap_for = [&](double alpha) {
+            const double crossings = 1.8 * (2.0 / alpha - 1.0) / (2.0 / 1.5 - 1.0);
+            return std::max(4, (int)std::floor(crossings * M_PI * Rv / (2.0 * Wv)));
+        };
         S->sv_fit = mbir_sv_ctas_per_sm(S->g, sp, cached) * S->sm_count;
         const long long active = (long long)(N_time > 1 ? (N_time + 1) / 2 : 1) * (S->nzg > 1 ? (S->nzg + 1) / 2 : 1);
-        S->sv_grid = (int)std::max<long long>(
-            1, std::min<long long>({(long long)S->sv_all.size(), (long long)S->sv_fit, S->sv_cap * active}));
+        const long long want = std::min<long long>((long long)S->sv_all.size(), (long long)S->sv_fit);
+        double alpha = S->sv_alpha > 0 ? S->sv_alpha : ref_alpha;
+        const double groups = (double)N_time * S->nzg;
+        const double per = std::min((double)want / (double)active,  // in flight per sinogram wanted
+                                    std::max(1.0, std::floor(0.12 * (double)S->sv_all.size() / groups)));
+        if (S->sv_alpha <= 0 && cap_for(ref_alpha) < per) {
+            const double g = per / cap_for(ref_alpha) * (2.0 / ref_alpha - 1.0);
+            alpha = std::min(ref_alpha, std::max(0.7, 2.0 / (1.0 + g)));
+        }
+        S->sv_alpha_eff = alpha;
+        S->sv_cap = cap_for(alpha);
+        S->sv_grid = (int)std::max<long long>(1, std::min<long long>(want, S->sv_cap * active));
     }
     const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sv_fit);
     CK(dalloc(&S->d_sv_out, 2));
@@ -828,11 +852,20 @@ extern "C" int mbir_set_sv_zgroup(MbirStage *S, int32_t slices)
     return 0;
 }
 
-extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_group, int32_t *resident)
+extern "C" int mbir_set_sv_relaxation(MbirStage *S, double alpha)
+{
+    if (!(alpha == 0 || (alpha > 0 && alpha < 2))) return fail("over-relaxation must lie in (0, 2), or be 0");
+    S->sv_alpha = alpha;
+    return 0;
+}
+
+extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_group, int32_t *resident,
+                                double *relaxation)
 {
     if (ctas) *ctas = S->sv_grid;
     if (cap_per_group) *cap_per_group = S->sv_cap;
     if (resident) *resident = S->sv_fit;
+    if (relaxation) *relaxation = S->sv_alpha_eff;
     return 0;
 }
 
@@ -885,7 +918,9 @@ static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> 
     const int ctas = std::min(n, S->sv_ctas > 0 ? std::min(S->sv_ctas, S->sv_fit) : S->sv_grid);
     SvACache ac{S->d_acol};
     SvLaunch L{S->d_sv_all, list + meta[1], list + meta[2], list + meta[3], n, S->d_sv_done, ++S->sv_epoch};
-    CK(mbir_launch_icd_sv(S->g, S->pr, S->dv, S->sp, ac, L, ctas, S->d_queue + qslot, S->d_scratch, acc, iter,
+    MbirPrior pr = S->pr;
+    pr.alpha = S->sv_alpha_eff;
+    CK(mbir_launch_icd_sv(S->g, pr, S->dv, S->sp, ac, L, ctas, S->d_queue + qslot, S->d_scratch, acc, iter,
                           seed, S->d_err, S->stream));
     S->launches++;
     S->icd_launches++;
