@@ -431,7 +431,8 @@ def gpu_arm(args, rank, world, local_rank):
                    "schedule_info": sched_info, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "step_ms": [round(v, 3) for v in e2e_ms],
+                "updates_per_step": e2e_upd / max(len(e2e_ms), 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "traffic_source": traffic_src,
