@@ -56,11 +56,18 @@ class Workload:
     def scan(self, seed_offset=0):
         if self.name == "3d":
             return synth.ellipsoid_scan(self.n_xy, self.rows, self.views, I0=1e4, seed=seed_offset)
+        if self.name == "c5":
+            # densities scaled by 256 / 2048 so that line integrals match the 3-D workload's
+            return synth.moving_ellipsoid_scan(self.n_xy, self.rows, self.frames, 1536, 32, 4, I0=1e4,
+                                               seed=seed_offset, vmax=0.02 * 256 / self.n_xy)
         return fourd_scan(self, seed_offset)
 
     def warm_start(self, scan):
         """The 2x-coarser phantom (mean over 2x2x2 cells) and its trilinear x2
         up-sampling onto the stage grid: the warm start both arms use."""
+        if scan.phantom is None:  # no phantom kept: the stage starts from zero
+            z = np.zeros((self.frames, self.rows, self.n_xy, self.n_xy), np.float32)
+            return z, z
         coarse, fine = [], []
         for ph in scan.phantom:
             c, f = coarse_start_frame(ph)
@@ -78,7 +85,14 @@ W4D = Workload("4d", "4d two-phase microstructure 16 x 256x256x16, 1024 interlac
                dict(sig_s=0.002, sig_t=0.004, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=2, quad_convex=0,
                     huber_delta=0.5, huber_T=4.0),
                "synthetic (seeded Gaussian-random-field two-phase frames, Poisson counts, zingers, rings)")
-WORKLOADS = {"3d": W3D, "4d": W4D}
+WC5 = Workload("c5", "large 4d z-subset: 32 x 2048x2048 x 4 of 64 detector rows, 6144 interlaced views "
+                "(K=32, 4 rotations of 1536, 192 per frame), densities 0-0.0025, I0=1e4, 0.1% zingers, rings, from "
+                "zero; the full "
+                "64-row configuration's time per iteration is this one's x 16 (extrapolated)", 2048, 4, 6144, 32,
+               dict(sig_s=0.00025, sig_t=0.0005, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=2, quad_convex=0,
+                    huber_delta=0.5, huber_T=4.0),
+               "synthetic (seeded drifting random ellipsoids, exact line integrals, Poisson counts, zingers, rings)")
+WORKLOADS = {"3d": W3D, "4d": W4D, "c5": WC5}
 METRIC = "ICD voxel-updates/s"
 # DRAM bytes (read + write) per voxel update of the super-voxel kernel, from
 # one ncu capture of a full-sweep launch (profiles/k_icd_sv_3d_256x256x8.md:
@@ -141,10 +155,14 @@ def mean_amatrix_count(stage, scan):
     x = R0 + (k + 0.5) * dr
     y = -n * dr / 2.0 + (k + 0.5) * dr
     X, Y = np.meshgrid(x, y)
-    m = stage.mask().astype(bool)
+    m = stage.mask().astype(bool).reshape(X.shape)
     X, Y = X[m], Y[m]
+    if len(X) > 20000:  # a seeded sample of lines on large images
+        pick = np.random.default_rng(0).choice(len(X), 20000, replace=False)
+        X, Y = X[pick], Y[pick]
+    vstep = max(4, scan.proj_num // 256)
     total = 0
-    for v in range(0, scan.proj_num, 4):
+    for v in range(0, scan.proj_num, vstep):
         c, s = np.cos(np.float64(scan.proj_angles[v])), np.sin(np.float64(scan.proj_angles[v]))
         r = X * c - Y * s
         imin = np.maximum(np.floor((r - dr - R0) / dr), 0).astype(int)
@@ -160,7 +178,7 @@ def mean_amatrix_count(stage, scan):
             w1 = dd - idc * off_r
             f = (off_r - w1) * hr[v, idc] + w1 * hr[v, idc + 1]
             total += int(np.count_nonzero(ok & (f > 0)))
-    return total / (len(X) * len(range(0, scan.proj_num, 4)))
+    return total / (len(X) * len(range(0, scan.proj_num, vstep)))
 
 
 class ClockSampler:
@@ -442,9 +460,12 @@ def gpu_arm(args, rank, world, local_rank):
         "gpu_launches": int(n_all1 - n_all0),
         "clocks": clk.summary(),
     }
-    if not args.no_ttm:
+    big = w.name == "c5"  # hundreds of iterations of about a second, ~100 s per reference iteration
+    if not args.no_ttm and not big:
         line["time_to_map"] = time_to_map(w, scan, fine, sched, args)
-    if not args.no_cpu:
+    if big:
+        line["cpu_baseline"] = {"unavailable": "the reference's CPU code needs minutes per iteration at this size"}
+    elif not args.no_cpu:
         v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, 1, 1, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                                 "sample": f"{n} ICD iteration(s) of the same stage after 1 warm-up, {secs:.1f} s"}

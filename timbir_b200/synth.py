@@ -195,6 +195,36 @@ def interlaced_angles(K: int, n_views: int, views_per_rotation: int) -> np.ndarr
     return out.astype(np.float32)
 
 
+def moving_ellipsoid_scan(n_xy: int, rows: int, frames: int, views_per_rotation: int, K: int, rotations: int,
+                          I0: float = 1e4, n_ell: int = 10, seed: int = 0, vmax: float = 0.02, drift: float = 0.05,
+                          zinger_frac: float = 0.001, ring_sigma: float = 0.02, oversample: int = 2) -> Scan:
+    """4-D scan of random ellipsoids whose inclusions drift in x-y over the
+    scan (by up to `drift` of the half-width), interlaced views (K sub-frames
+    per rotation of `views_per_rotation` views), `frames` frames of equal time.
+    The object is static within a frame: a frame's views see the ellipsoids at
+    the frame's mid time (the reconstruction's model).  Exact line integrals,
+    Poisson counts at I0, zingers and ring offsets as in counts_to_data.  No
+    phantom volume is kept (at this size it is not needed by the callers)."""
+    rng = np.random.default_rng(seed)
+    rc = n_xy / 2.0
+    ell = random_ellipsoids(n_ell, rng, vmax)
+    vel = rng.uniform(-drift, drift, size=(n_ell, 2))
+    vel[0] = 0.0
+    n_views = views_per_rotation * rotations
+    angles = interlaced_angles(K, n_views, views_per_rotation)
+    times = np.arange(n_views, dtype=np.float32)
+    recon_times = np.linspace(0, n_views, frames + 1).astype(np.float32)
+    li = np.zeros((n_views, rows, n_xy))
+    per = n_views // frames
+    for f in range(frames):
+        e = ell.copy()
+        e[:, 0:2] += vel * ((f + 0.5) / frames)
+        sl = slice(f * per, (f + 1) * per)
+        li[sl] = ellipsoid_sinogram(e, angles[sl], n_xy, rows, 1.0, rc, n_xy, oversample)
+    proj, wts = counts_to_data(li, I0, rng, zinger_frac, ring_sigma)
+    return Scan(proj, wts, angles, times, recon_times, rows, n_xy, n_views, frames, 1.0, rc, None)
+
+
 def two_phase_frames(n_xy: int, n_z: int, frames: int, seed: int, vmax: float = 0.02,
                      smooth: float = 6.0, flow_steps: int = 3) -> np.ndarray:
     """[frames][n_z][n_xy][n_xy] two-phase microstructure: a smoothed Gaussian
