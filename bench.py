@@ -303,7 +303,7 @@ def time_to_map(w, scan, fine, sched, args, max_iters=400):
 
     def stage():
         st = timbir_b200.Stage(scan, **w.prior, blocks=2 if w.rows < 8 else 8)
-        st.set_schedule(sched, args.sv_side, args.warps_per_slice)
+        st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
         st.prepare(fine)
         return st
 
@@ -348,7 +348,7 @@ def gpu_arm(args, rank, world, local_rank):
     coarse, fine = w.warm_start(scan)
     sched = 1 if args.schedule == "sv" else 0
     st = timbir_b200.Stage(scan, **w.prior, blocks=2 if w.rows < 8 else 8)
-    st.set_schedule(sched, args.sv_side, args.warps_per_slice)
+    st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
     sched_info = st.schedule_info()
     st.prepare(fine)
     for it in range(1, args.warmup + 1):
@@ -402,7 +402,7 @@ def gpu_arm(args, rank, world, local_rank):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
         s2 = timbir_b200.Stage(pscan, **w.prior, blocks=2 if w.rows < 8 else 8)
-        s2.set_schedule(sched, args.sv_side, args.warps_per_slice)
+        s2.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
         s2.prepare(pfine)
         s2.iterate(1)
         _ = s2.object()
@@ -441,7 +441,8 @@ def gpu_arm(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (A-matrix bin indices exact in FP64; cost and convergence sums FP64)",
+        "dtype": ("f32, A-matrix values fp16" if sched_info.get("column_cache_values") == "fp16" else "f32")
+        + " (A-matrix bin indices exact in FP64; cost and convergence sums FP64)",
         "data": w.data,
         "config": {"workload": w.desc, "volume": [w.frames, w.rows, w.n_xy, w.n_xy],
                    "views": w.views,
@@ -505,6 +506,8 @@ def main():
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
+    ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,
+                    help="A-matrix column cache with FP16 values (FP32 accumulation)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -92,8 +92,12 @@ int mbir_get_schedule(MbirStage *stage, int32_t *schedule, int32_t *sv_side, int
  * every view, 16 bytes per (line, view) at full resolution, built once per
  * stage at its first iteration.  mode -1 (default): used when it takes at
  * most a third of free device memory; 0: never (columns computed in the
- * kernel); 1: always (mbir_set_schedule fails if it cannot be allocated).
- * Takes effect at the next mbir_set_schedule. */
+ * kernel); 1: always (mbir_set_schedule fails if it cannot be allocated);
+ * 2: as -1, with FP16 values (8 bytes per entry; accumulation stays FP32;
+ * full-resolution stages of detectors up to 4096 columns, others keep FP32
+ * values): the iteration then minimises the cost of the A matrix rounded to
+ * FP16.  Takes effect at the next mbir_set_schedule.  mbir_get_acache's
+ * *used is 0 (no cache), 1 (FP32 values) or 2 (FP16 values). */
 int mbir_set_acache(MbirStage *stage, int32_t mode);
 int mbir_get_acache(MbirStage *stage, int32_t *used, int64_t *bytes);
 /* Persistent CTAs per launch of schedule 1 (0, the default: automatic, see

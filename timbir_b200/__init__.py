@@ -149,7 +149,7 @@ class Stage:
         """0: the reference's checkerboard z-block schedule; 1: super-voxel
         schedule (sv_side 0 = largest side whose band fits shared memory;
         warps_per_slice 0 = automatic; acache: A-matrix column cache, -1 when
-        it fits, 0 never, 1 always)."""
+        it fits, 0 never, 1 always, 2 when it fits with FP16 values)."""
         _check(self.lib.mbir_set_acache(self.h, acache))
         _check(self.lib.mbir_set_schedule(self.h, schedule, sv_side, warps_per_slice))
         d = np.zeros(9, np.int32)
@@ -164,6 +164,7 @@ class Stage:
         d = dict(zip(("schedule", "sv_side", "z_group", "band_width", "phases", "warps_per_slice"),
                      [x.value for x in v]))
         d["column_cache_bytes"] = int(nbytes.value) if used.value else 0
+        d["column_cache_values"] = {0: None, 1: "fp32", 2: "fp16"}[used.value]
         g = [C.c_int32() for _ in range(3)]
         rel = C.c_double()
         self.lib.mbir_get_sv_grid(self.h, *[C.byref(x) for x in g], C.byref(rel))

@@ -124,7 +124,8 @@ struct MbirStage {
     // filled at the first iteration after the prologue
     int4 *d_acol = nullptr;
     size_t acol_bytes = 0;
-    int acol_mode = -1;  // -1: when it fits in a third of free memory, 0: never, 1: always
+    int acol_mode = -1;  // -1: when it fits in a third of free memory, 0: never, 1: always, 2: FP16 values
+    bool acol_half = false;  // the cache holds FP16 values
     bool acol_built = false;
     int *d_err = nullptr, *d_queue = nullptr;
     int sm_count = 148;
@@ -532,6 +533,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     sp.amax = 2 * (int)ceil(m) + 1;
     sp.eq = (1 + sp.amax + 3) / 4;
     sp.ring = 4;
+    sp.ahalf = S->acol_half ? 1 : 0;
     sp.max_views = S->max_views();
     sp.max_nz = nz;
     sp.max_rows = nz * S->st.m_z;
@@ -605,10 +607,14 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     // the column cache: used when it fits (or always / never, as set)
     {
         const SvParams probe = sv_params(S, 4, 1, 1);
-        const size_t bytes = mbir_acache_bytes(S->g, probe.eq);
+        // FP16 values: full resolution (3 columns, one detector row per slice)
+        // and detectors of at most 4096 columns (12-bit column index)
+        const bool half = S->acol_mode == 2 && probe.amax == 3 && S->st.m_z == 1 && S->sg.N_r <= 4096;
+        const size_t bytes = mbir_acache_bytes(S->g, probe.eq, half);
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const bool want = S->acol_mode == 1 || (S->acol_mode == -1 && bytes <= fr / 3);
+        const bool want = S->acol_mode == 1 || ((S->acol_mode == -1 || S->acol_mode == 2) && bytes <= fr / 3);
+        S->acol_half = want && half;
         if (want && bytes != S->acol_bytes) {
             dfree(S->d_acol);
             S->d_acol = nullptr;
@@ -647,6 +653,12 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         }
         if (gz == 1) return fail("no super-voxel configuration fits shared memory");
         gz = std::max(1, gz / 2);
+    }
+    if (cached && sp.ahalf) {
+        const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
+        if (vpl > 4 || 32 * sp.max_nz * sp.vsplit > 512)
+            return fail("the FP16 column cache needs at most 4 views per lane and 512 threads per super-voxel "
+                        "(%d views per lane, %d threads)", vpl, 32 * sp.max_nz * sp.vsplit);
     }
     S->sp = sp;
     S->gz = gz;
@@ -833,7 +845,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
 
 extern "C" int mbir_set_acache(MbirStage *S, int32_t mode)
 {
-    if (mode < -1 || mode > 1) return fail("column cache mode must be -1, 0 or 1");
+    if (mode < -1 || mode > 2) return fail("column cache mode must be -1, 0, 1 or 2");
     S->acol_mode = mode;
     return 0;
 }
@@ -871,7 +883,7 @@ extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_gr
 
 extern "C" int mbir_get_acache(MbirStage *S, int32_t *used, int64_t *bytes)
 {
-    if (used) *used = S->d_acol != nullptr;
+    if (used) *used = S->d_acol != nullptr ? (S->acol_half ? 2 : 1) : 0;
     if (bytes) *bytes = (int64_t)S->acol_bytes;
     return 0;
 }
@@ -885,8 +897,27 @@ extern "C" int mbir_get_acache_line(MbirStage *S, int32_t row, int32_t col, int3
     if (row < 0 || row >= S->st.N_y || col < 0 || col >= S->st.N_x) return fail("line (%d, %d) outside the grid", row, col);
     if (!S->mask[(size_t)row * S->st.N_x + col]) return fail("line (%d, %d) outside the reconstruction mask", row, col);
     if (!S->acol_built) {
-        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
+        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->acol_half, S->d_acol, S->d_err, S->stream));
         S->acol_built = true;
+    }
+    if (S->acol_half) {
+        // 8-byte entries, unpacked into the FP32 layout
+        std::vector<uint32_t> h((size_t)S->g.N_p * 2);
+        CK(cudaMemcpyAsync(h.data(), reinterpret_cast<const uint2 *>(S->d_acol) + ((size_t)row * S->st.N_x + col) * S->g.N_p,
+                           h.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+        auto half_to_float = [](uint32_t b) {
+            const uint32_t sgn = (b >> 15) & 1u, ex = (b >> 10) & 31u, man = b & 1023u;
+            float v = ex == 0 ? std::ldexp((float)man, -24) : std::ldexp((float)(man | 1024u), (int)ex - 25);
+            return sgn ? -v : v;
+        };
+        for (int p = 0; p < S->g.N_p; p++) {
+            const uint32_t w0 = h[2 * p], w1 = h[2 * p + 1];
+            const float a[3] = {half_to_float(w0 >> 16), half_to_float(w1 & 0xffffu), half_to_float(w1 >> 16)};
+            words[4 * p] = (int32_t)((w0 & 0xfffu) | ((w0 >> 12) & 3u) << 16);
+            for (int k = 0; k < 3; k++) std::memcpy(&words[4 * p + 1 + k], &a[k], sizeof(float));
+        }
+        return 0;
     }
     const size_t n = (size_t)S->g.N_p * S->sp.eq;
     CK(cudaMemcpyAsync(words, S->d_acol + ((size_t)row * S->st.N_x + col) * n, n * sizeof(int4),
@@ -939,7 +970,7 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
     const int P = S->sv_nphase;
     if (S->d_acol && !S->acol_built) {
-        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->d_acol, S->d_err, S->stream));
+        CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->acol_half, S->d_acol, S->d_err, S->stream));
         S->acol_built = true;
         S->launches++;
     }

@@ -40,6 +40,7 @@
 // share error-sinogram entries, whose concurrent changes they see at their
 // next visit (the super-voxel ICD scheme of Wang et al., "High performance
 // model based image reconstruction", PPoPP 2016).
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -141,6 +142,11 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 // waits until at most n (0..6) of this thread's commit groups are pending
@@ -233,7 +239,8 @@ __device__ __forceinline__ void theta_acc(float2 es, float a, float hT, float hT
 }
 
 // Fills the column cache: one warp per in-mask line, lanes over views.
-template <int AMAXC>
+// HALF: the full-resolution entries in 8 bytes (see SvACache).
+template <int AMAXC, bool HALF>
 __global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__restrict__ mask, int amax, int eq,
                                                  int4 *__restrict__ cache, int *err)
 {
@@ -244,11 +251,25 @@ __global__ void __launch_bounds__(256) k_acache(MbirGeom g, const uint8_t *__res
     const double x = vx(g, col), y = vy(g, row);
     const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
     const float inv_off_f = (float)inv_off;
-    int4 *dst = cache + (size_t)line * g.N_p * eq;
     bool ok = true;
-    for (int p = lane; p < g.N_p; p += 32)
-        ok &= acol_entry<AMAXC>(g, x, y, g.cosv[p], g.sinv[p], g.H_r + (size_t)p * (MBIR_RESP_BINS + 1), inv_dr,
-                                inv_off, inv_off_f, amax, 4 * eq, reinterpret_cast<int *>(dst + (size_t)p * eq));
+    if constexpr (HALF) {
+        uint2 *dst = reinterpret_cast<uint2 *>(cache) + (size_t)line * g.N_p;
+        for (int p = lane; p < g.N_p; p += 32) {
+            int4 e;
+            ok &= acol_entry<3>(g, x, y, g.cosv[p], g.sinv[p], g.H_r + (size_t)p * (MBIR_RESP_BINS + 1), inv_dr,
+                                inv_off, inv_off_f, 3, 4, reinterpret_cast<int *>(&e));
+            const unsigned j0 = (unsigned)e.x & 0xfffu, n = ((unsigned)e.x >> 16) & 3u;
+            const unsigned h0 = __half_as_ushort(__float2half_rn(__int_as_float(e.y)));
+            const unsigned h1 = __half_as_ushort(__float2half_rn(__int_as_float(e.z)));
+            const unsigned h2 = __half_as_ushort(__float2half_rn(__int_as_float(e.w)));
+            dst[p] = make_uint2(j0 | n << 12 | h0 << 16, h1 | h2 << 16);
+        }
+    } else {
+        int4 *dst = cache + (size_t)line * g.N_p * eq;
+        for (int p = lane; p < g.N_p; p += 32)
+            ok &= acol_entry<AMAXC>(g, x, y, g.cosv[p], g.sinv[p], g.H_r + (size_t)p * (MBIR_RESP_BINS + 1), inv_dr,
+                                    inv_off, inv_off_f, amax, 4 * eq, reinterpret_cast<int *>(dst + (size_t)p * eq));
+    }
     if (!ok) atomicOr(err, 2);
 }
 
@@ -397,10 +418,11 @@ cudaError_t launch_forward_rows(const MbirGeom &g, const int *fov, const float *
 // resolution), 0 = runtime sp.amax.  MZC: detector rows per slice known at
 // compile time (1 at full resolution), 0 = runtime m_z.  AC: columns come
 // from the column cache (else from producer warps).  MAXT: most threads per
-// CTA (512 leaves 128 registers per thread).  VU (full-resolution path): a
+// CTA (512 leaves 128 registers per thread).  AC = 2: the cache holds FP16
+// values (8-byte entries, full resolution only).  VU (full-resolution path): a
 // lane's views per slice, at most VU, are held in registers from theta to
 // the error-sinogram update.
-template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
+template <int AMAXC, int MZC, int AC, int MAXT, int VU>
 __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp, SvACache ac,
                                                   SvLaunch L, int *queue, float *__restrict__ scratch,
                                                   SvTaskOut *__restrict__ out, int iter, uint32_t seed, int *err)
@@ -420,7 +442,9 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     // ---- carve shared memory (sizes fixed by the host in sp) ----
     unsigned char *p = smraw;
     const int R = sp.ring, D = R - 2;  // ring slots; column prefetch distance (lines)
-    int4 *ring = reinterpret_cast<int4 *>(p); p += sizeof(int4) * (size_t)R * eq * NpS;
+    constexpr int kHalf = AC == 2;
+    const int ent_bytes = kHalf ? 8 : 16 * eq;  // bytes per ring entry
+    int4 *ring = reinterpret_cast<int4 *>(p); p += (size_t)ent_bytes * R * NpS;
     float2 *band = reinterpret_cast<float2 *>(p); p += sizeof(float2) * (size_t)sp.max_rows * rowstride;
     double *cs = reinterpret_cast<double *>(p);
     double *sn = cs + NpS;
@@ -676,10 +700,16 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             if (li < nl && order[li] >= 0) {
                 const int o = order[li];
                 const size_t line = (size_t)(j0 + (o >> 8)) * g.N_x + k0 + (o & 0xff);
-                int4 *dst = ring + (size_t)slot * eq * NpS;
-                for (int q = tid; q < Np * eq; q += nthr) {
-                    const int v = q / eq, w = q - v * eq;
-                    cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
+                if constexpr (kHalf) {
+                    uint2 *dst = reinterpret_cast<uint2 *>(ring) + (size_t)slot * NpS;
+                    const uint2 *src = reinterpret_cast<const uint2 *>(ac.a) + line * g.N_p;
+                    for (int q = tid; q < Np; q += nthr) cp_async8(dst + q, src + vidx[q]);
+                } else {
+                    int4 *dst = ring + (size_t)slot * eq * NpS;
+                    for (int q = tid; q < Np * eq; q += nthr) {
+                        const int v = q / eq, w = q - v * eq;
+                        cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
+                    }
                 }
             }
             cp_async_commit();
@@ -756,15 +786,26 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
                             const int v = vh * 32 + lane + u * vstep;
                             const bool ok = v < Np;
                             const int vv = ok ? v : 0;
-                            int4 A = make_int4(0, 0, 0, 0);
-                            if (ok) A = rq[vv];
-                            const int off0 = max((A.x & 0xffff) - rlo[vv], 0);
+                            int j0c;
+                            if constexpr (kHalf) {
+                                uint2 A = make_uint2(0u, 0u);
+                                if (ok) A = reinterpret_cast<const uint2 *>(ring)[(size_t)slot * NpS + vv];
+                                j0c = (int)(A.x & 0xfffu);
+                                av[u][0] = __half2float(__ushort_as_half((unsigned short)(A.x >> 16)));
+                                av[u][1] = __half2float(__ushort_as_half((unsigned short)(A.y & 0xffffu)));
+                                av[u][2] = __half2float(__ushort_as_half((unsigned short)(A.y >> 16)));
+                            } else {
+                                int4 A = make_int4(0, 0, 0, 0);
+                                if (ok) A = rq[vv];
+                                j0c = A.x & 0xffff;
+                                av[u][0] = __int_as_float(A.y);
+                                av[u][1] = __int_as_float(A.z);
+                                av[u][2] = __int_as_float(A.w);
+                            }
+                            const int off0 = max(j0c - rlo[vv], 0);
                             cx[u][0] = off0 * NpS + vv;
                             cx[u][1] = min(off0 + 1, W - 1) * NpS + vv;
                             cx[u][2] = min(off0 + 2, W - 1) * NpS + vv;
-                            av[u][0] = __int_as_float(A.y);
-                            av[u][1] = __int_as_float(A.z);
-                            av[u][2] = __int_as_float(A.w);
                         }
 #pragma unroll
                         for (int u = 0; u < VR; u++)
@@ -978,7 +1019,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
     }
 }
 
-template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
+template <int AMAXC, int MZC, int AC, int MAXT, int VU>
 int occupancy_sv(int threads, size_t sm)
 {
     if (cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -991,7 +1032,7 @@ int occupancy_sv(int threads, size_t sm)
     return n > 0 ? n : 1;
 }
 
-template <int AMAXC, int MZC, bool AC, int MAXT, int VU>
+template <int AMAXC, int MZC, int AC, int MAXT, int VU>
 cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
                       const SvLaunch &L, int ctas, int threads, size_t sm, int *queue, float *scratch,
                       SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
@@ -1010,7 +1051,7 @@ size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached)
 {
     const size_t NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
     size_t b = 0;
-    b += 16 * (size_t)sp.ring * sp.eq * NpS;  // A-column ring
+    b += (size_t)(cached && sp.ahalf ? 8 : 16 * sp.eq) * sp.ring * NpS;  // A-column ring
     b += 8 * (size_t)sp.max_rows * sp.W * NpS;  // (e, sqrt(w)) band
     if (!cached) b += 2 * sizeof(double) * NpS;
     b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
@@ -1033,29 +1074,30 @@ cudaError_t mbir_forward_rows(const MbirGeom &g, const int *frame_of_view, const
                 : launch_forward_rows<0, 2, 16>(g, frame_of_view, x, y, d, out, mode, amax, s);
 }
 
-size_t mbir_acache_bytes(const MbirGeom &g, int eq)
+size_t mbir_acache_bytes(const MbirGeom &g, int eq, bool half)
 {
-    return (size_t)g.N_y * g.N_x * g.N_p * eq * 16;
+    return (size_t)g.N_y * g.N_x * g.N_p * (half ? 8 : eq * 16);
 }
 
-cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
-                              cudaStream_t s)
+cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, bool half, int4 *cache,
+                              int *err, cudaStream_t s)
 {
     const long long lines = (long long)g.N_y * g.N_x;
     const int blocks = (int)((lines + 7) / 8);
-    if (amax == 3)
-        k_acache<3><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
+    if (half)
+        k_acache<3, true><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
+    else if (amax == 3)
+        k_acache<3, false><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
     else
-        k_acache<0><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
+        k_acache<0, false><<<blocks, 256, 0, s>>>(g, dv.mask, amax, eq, cache, err);
     return cudaGetLastError();
 }
 
 // Instantiation of the super-voxel kernel for a configuration: F is called
 // with a tag carrying its template arguments.
-template <int A_, int M_, bool C_, int T_, int V_>
+template <int A_, int M_, int C_, int T_, int V_>
 struct SvInst {
-    static constexpr int AMAXC = A_, MZC = M_, MAXT = T_, VU = V_;
-    static constexpr bool AC = C_;
+    static constexpr int AMAXC = A_, MZC = M_, AC = C_, MAXT = T_, VU = V_;
 };
 template <class F>
 auto sv_dispatch(const MbirGeom &g, const SvParams &sp, bool cached, int threads, F &&f)
@@ -1066,12 +1108,18 @@ auto sv_dispatch(const MbirGeom &g, const SvParams &sp, bool cached, int threads
     // registers (the cached path; 256 threads leave 255 registers per thread)
     const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
     const bool full = sp.amax == 3 && g.m_z == 1 && vpl <= 4;
+    // FP16 cache: full resolution with at most 4 views per lane, 512 threads
+    // (the host asks for it only then)
+    if (cached && sp.ahalf && full && threads <= 512) {
+        if (vpl <= 2) return f(SvInst<3, 1, 2, 512, 2>{});
+        return f(SvInst<3, 1, 2, 512, 4>{});
+    }
     if (cached && threads <= 256 && sp.amax == 3 && g.m_z == 1 && vpl > 4 && vpl <= 8)
-        return f(SvInst<3, 1, true, 256, 8>{});
-#define MBIR_SV_PICK(T)                                                                                    \
-    if (full && vpl <= 2) return cached ? f(SvInst<3, 1, true, T, 2>{}) : f(SvInst<3, 1, false, T, 2>{}); \
-    if (full) return cached ? f(SvInst<3, 1, true, T, 4>{}) : f(SvInst<3, 1, false, T, 4>{});             \
-    return cached ? f(SvInst<0, 0, true, T, 0>{}) : f(SvInst<0, 0, false, T, 0>{});
+        return f(SvInst<3, 1, 1, 256, 8>{});
+#define MBIR_SV_PICK(T)                                                                              \
+    if (full && vpl <= 2) return cached ? f(SvInst<3, 1, 1, T, 2>{}) : f(SvInst<3, 1, 0, T, 2>{}); \
+    if (full) return cached ? f(SvInst<3, 1, 1, T, 4>{}) : f(SvInst<3, 1, 0, T, 4>{});             \
+    return cached ? f(SvInst<0, 0, 1, T, 0>{}) : f(SvInst<0, 0, 0, T, 0>{});
     if (threads <= 512) {
         MBIR_SV_PICK(512)
     }

@@ -17,6 +17,7 @@ struct SvParams {
     int vsplit;     // warps per slice (1, 2 or 4; > 1 needs max_nz <= 15)
     int prod_warps; // warps computing the next line's A-matrix column (0 with a column cache)
     int ring;       // A-column ring slots, 4..8 (the cache is read ring - 2 lines ahead)
+    int ahalf;      // the column cache holds FP16 values (8-byte entries; full resolution)
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
 };
 
@@ -27,6 +28,8 @@ struct SvParams {
 //
 // Column cache: the columns of every in-mask line for every view, laid out
 // [N_y * N_x][N_p][eq] (line-major, view next), computed once per stage.
+// FP16 variant (full resolution, N_r <= 4096): 8 bytes per entry, word 0 =
+// j0 | n << 12 | fp16(a0) << 16, word 1 = fp16(a1) | fp16(a2) << 16.
 struct SvACache {
     const int4 *a;  // nullptr: the kernel computes columns itself
 };
@@ -43,11 +46,11 @@ struct SvTaskOut {
 };
 
 size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached);
-size_t mbir_acache_bytes(const MbirGeom &g, int eq);
+size_t mbir_acache_bytes(const MbirGeom &g, int eq, bool half);
 // Fills the column cache (exact bin indices, FP32 values) for the in-mask
 // lines.  err |= 2 if a column has more than amax entries.
-cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, int4 *cache, int *err,
-                              cudaStream_t s);
+cudaError_t mbir_build_acache(const MbirGeom &g, const MbirDev &dv, int amax, int eq, bool half, int4 *cache,
+                              int *err, cudaStream_t s);
 // Forward projection, deterministic (FP32 sums in a fixed order, no
 // atomics): mode 0: out = y - A x - d; mode 1: out = A x.  amax: most
 // columns per A-matrix entry (2 mult_xy + 1).
