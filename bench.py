@@ -291,6 +291,187 @@ def cpu_measure(w, scan, coarse, fine, warm, steps, threads):
     return upd / secs, kind, cores, len(timed), secs
 
 
+# ------------------------------------------------------------ batched (c3) --
+C3_DESC = ("64 independent 3-D random-ellipsoid problems in one persistent launch per iteration (CUDA-graph "
+           "replays): side from {128,192,256,384,512}, 4-32 slices (even), 1.5 x side views over 180 degrees, "
+           "I0 log-uniform in [2e3, 5e4], seeds 0-63, from zero, plain ICD")
+C3_PRIOR = dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=1.0, remove_rings=0, quad_convex=1,
+                huber_delta=0.5, huber_T=4.0)
+C3_DATA = "synthetic (seeded random-ellipsoid phantoms, exact line integrals, Poisson counts)"
+
+
+def c3_sample_workload(specs):
+    """The CPU baseline's bounded sample: the smallest problem of the batch."""
+    k = min(range(len(specs)), key=lambda q: specs[q]["side"] ** 2 * specs[q]["slices"] * specs[q]["views"])
+    sp = specs[k]
+    prior = dict(C3_PRIOR, convg_thresh=0.0)
+    w = Workload("c3-sample", f"problem {k} of the batch: {sp['side']}x{sp['side']}x{sp['slices']}, "
+                 f"{sp['views']} views, I0={sp['I0']:.0f}", sp["side"], sp["slices"], sp["views"], 1, prior, C3_DATA)
+    return k, w
+
+
+def c3_build(specs, scans, tuned=None):
+    """Stages of the batch (column cache, super-voxel schedule, prepared from
+    zero); with `tuned` = {side: autotuner result} the schedule of each size
+    is the tuned one, otherwise the representative of each size (most slices)
+    is autotuned here and the others follow it."""
+    import timbir_b200
+    stages = [None] * len(specs)
+    tune = {}
+    reps = {}
+    for k, sp in enumerate(specs):
+        if sp["side"] not in reps or sp["slices"] > specs[reps[sp["side"]]]["slices"]:
+            reps[sp["side"]] = k
+    order = sorted(range(len(specs)), key=lambda k: (k not in reps.values(), k))
+    for k in order:
+        sp = specs[k]
+        st = timbir_b200.Stage(scans[k], **C3_PRIOR, blocks=2)
+        t = (tuned or tune).get(sp["side"])
+        if t is None:
+            st.set_batch_schedule(0, 1, 1)
+            st.prepare()
+            t = st.autotune()
+            tune[sp["side"]] = t
+        else:
+            st.set_batch_schedule(t["sv_side"], t["warps_per_slice"], 1)
+            st.prepare()
+        stages[k] = st
+    return stages, (tuned or tune)
+
+
+def c3_arm(args, rank, world, local_rank):
+    import torch
+    import timbir_b200
+    torch.cuda.set_device(local_rank)
+    specs = synth.batch_problem_specs(64, 0)
+    t0 = time.perf_counter()
+    scans = [synth.ellipsoid_scan_device(sp["side"], sp["slices"], sp["views"], I0=sp["I0"], seed=sp["seed"],
+                                         device="cuda") for sp in specs]
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    stages, tuned = c3_build(specs, scans)
+    setup_s = time.perf_counter() - t0
+    cbar = {}
+    for k, sp in enumerate(specs):
+        if sp["side"] not in cbar:
+            cbar[sp["side"]] = mean_amatrix_count(stages[k], scans[k])
+    b_vu = [sp["views"] * (cbar[sp["side"]] * 12 + 2 * cbar[sp["side"]] + 2) + 29 * 4 + 4 for sp in specs]
+    # throughput: every problem iterating (convergence test off)
+    for st in stages:
+        st.set_convergence_threshold(0.0)
+    batch = timbir_b200.Batch(stages)
+    binfo = batch.info()
+    for _ in range(args.warmup):
+        batch.iterate(1)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
+    u0 = batch.stats()["updates"].copy()
+    i0 = batch.info()
+    step_ms = []
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            m0 = batch.info()["ms"]
+            batch.iterate(1)
+            step_ms.append(batch.info()["ms"] - m0)
+    i1 = batch.info()
+    du = batch.stats()["updates"] - u0
+    updates = int(du.sum())
+    total_ms = sum(step_ms)
+    achieved = float(sum(int(du[k]) * b_vu[k] for k in range(len(specs)))) / (total_ms / 1e3) / 1e9
+    batch.close()
+    # time until every problem passes the reference's convergence test (1 %)
+    ttc = None
+    if not args.no_ttm:
+        for st in stages:
+            st.set_convergence_threshold(C3_PRIOR["convg_thresh"])
+            st.prepare()
+        batch = timbir_b200.Batch(stages)
+        left = batch.iterate(200, check_every=1)
+        bst = batch.stats()
+        ttc = {"value": batch.info()["ms"] / 1e3, "unit": "s", "iterations_max": int(bst["iterations"].max()),
+               "iterations_mean": float(bst["iterations"].mean()), "unconverged": int(left),
+               "target": "every problem's convergence ratio below convg_thresh = 1 % (XT_ICD_update.c:1066-1103)",
+               "start": "zero", "timed": "graph replays of the batched iterations (device events)"}
+        batch.close()
+    for st in stages:
+        st.close()
+    # end to end through the public API from pinned host buffers: stages,
+    # schedules (the tuned ones), prologue, one batched iteration, objects back
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    pscans = [synth.Scan(pin(s.projections), pin(s.weights), pin(s.proj_angles), pin(s.proj_times),
+                         pin(s.recon_times), s.proj_rows, s.proj_cols, s.proj_num, s.recon_num, s.vox_wid,
+                         s.rot_center) for s in scans]
+    h2d = sum(a.nbytes for s in pscans for a in (s.projections, s.weights, s.proj_angles, s.proj_times,
+                                                  s.recon_times))
+    d2h = sum(4 * sp["side"] ** 2 * sp["slices"] for sp in specs)
+    flush.fill_(0.0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    est, _ = c3_build(specs, pscans, tuned)
+    eb = timbir_b200.Batch(est)
+    eb.iterate(1)
+    e_upd = int(eb.stats()["updates"].sum())
+    eb.close()
+    for st in est:
+        _ = st.object()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    for st in est:
+        st.close()
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    sizes = {}
+    for sp, d in zip(specs, du):
+        z = sizes.setdefault(str(sp["side"]), {"problems": 0, "updates_per_iteration": 0})
+        z["problems"] += 1
+        z["updates_per_iteration"] += int(d) // max(args.steps, 1)
+    for side, t in tuned.items():
+        sizes[str(side)].update({"views": (3 * side) // 2, "sv_side": t["sv_side"], "band_width": t["band_width"],
+                                 "warps_per_slice": t["warps_per_slice"],
+                                 "threads_per_voxel": 32 * t["warps_per_slice"], "z_group": t["z_group"],
+                                 "ns_per_update_tuning": round(t["ns_per_update"], 3),
+                                 "mean_bins_per_view": cbar[side]})
+    line = {
+        "metric": METRIC, "value": updates / (total_ms / 1e3), "unit": "voxel-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (A-matrix bin indices exact in FP64; convergence sums FP64)", "data": C3_DATA,
+        "config": {"workload": C3_DESC, "problems": len(specs), "voxels": int(sum(sp["side"] ** 2 * sp["slices"]
+                                                                             for sp in specs)),
+                   "schedule": "batched super-voxel (one persistent launch + one end kernel per iteration, "
+                               "CUDA graph)", "ctas": binfo["ctas"], "smem_bytes_per_cta": binfo["smem_bytes"],
+                   "autotuned_per_size": sizes, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "setup_s": {"scan_generation": round(gen_s, 2), "stages_and_autotune": round(setup_s, 2)}},
+        "e2e": {"value": e_upd / (e2e_ms / 1e3), "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "step_ms": [round(e2e_ms, 3)], "updates_per_step": e_upd,
+                "includes": "64 stages from pinned host arrays, column caches, schedules, prologue, one batched "
+                            "iteration, 64 objects back"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "bytes_per_update": "views x (c-bar x 14 + 2) + 120 per problem",
+                     "kernel": "k_icd_sv (batched)", "kernel_ms": total_ms,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "gpu_launches": int(i1["launches"] - i0["launches"]),
+        "clocks": clk.summary(),
+    }
+    if ttc:
+        line["time_to_converge"] = ttc
+    if not args.no_cpu:
+        k, w = c3_sample_workload(specs)
+        z = np.zeros((1, w.rows // 2, w.n_xy // 2, w.n_xy // 2), np.float32)
+        zf = np.zeros((1, w.rows, w.n_xy, w.n_xy), np.float32)
+        v, kind, cores, n, secs = cpu_measure(w, scans[k], z, zf, 1, 1, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
+                                "sample": f"{w.desc}: {n} ICD iteration(s) after 1 warm-up, {secs:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------- GPU --
 def time_to_map(w, scan, fine, sched, args, max_iters=400):
     """Time-to-MAP of the GPU engine from the bench's warm start: device time of
@@ -336,6 +517,8 @@ def time_to_map(w, scan, fine, sched, args, max_iters=400):
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import timbir_b200
+    if args.config == "c3":
+        return c3_arm(args, rank, world, local_rank)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -476,9 +659,18 @@ def gpu_arm(args, rank, world, local_rank):
 def reference_arm(args, rank):
     if rank != 0:
         return
-    w = WORKLOADS[args.config]
-    scan = w.scan(0)
-    coarse, fine = w.warm_start(scan)
+    if args.config == "c3":
+        # the batch's smallest problem, one problem at a time as the reference runs
+        specs = synth.batch_problem_specs(64, 0)
+        k, w = c3_sample_workload(specs)
+        sp = specs[k]
+        scan = synth.ellipsoid_scan(sp["side"], sp["slices"], sp["views"], I0=sp["I0"], seed=sp["seed"])
+        coarse = np.zeros((1, w.rows // 2, w.n_xy // 2, w.n_xy // 2), np.float32)
+        fine = np.zeros((1, w.rows, w.n_xy, w.n_xy), np.float32)
+    else:
+        w = WORKLOADS[args.config]
+        scan = w.scan(0)
+        coarse, fine = w.warm_start(scan)
     threads = os.cpu_count() or 1
     v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, args.warmup, args.steps, threads)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "voxel-updates/s", "n_gpus": 0,
@@ -502,8 +694,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
-    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS),
-                    help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload")
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3"],
+                    help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
+                         "c3: 64 independent 3-D problems batched; c5: large 4-D z-subset")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
     ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,

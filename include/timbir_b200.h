@@ -31,6 +31,7 @@ extern "C" {
 #endif
 
 typedef struct MbirStage MbirStage;
+typedef struct MbirBatch MbirBatch;
 
 /* initStatStructures + initDynStructures for one stage whose voxels are
  * mult_xy detector columns wide and mult_z detector rows high
@@ -57,6 +58,10 @@ const char *mbir_last_error(void);
  * read from the previous stage (XT_Init.c:290-291, 327-330). */
 int mbir_set_stage_switches(MbirStage *stage, int32_t update_proj_offset, int32_t update_var,
                             double var_est);
+
+/* Convergence threshold of the stage's iterations, percent (the convg_thresh
+ * of reconstruct(); XT_ICD_update.c:1066-1103). */
+int mbir_set_convergence_threshold(MbirStage *stage, double convg_thresh);
 
 /* State of the voxel-line order generator (randlib.c srandom2/random2); one
  * stream runs through a whole reconstruct() call. */
@@ -195,10 +200,86 @@ int mbir_update_sinogram_offset_noalloc(float *e, const float *w, float *d, int3
                                         float huber_delta, float huber_T, void *stream);
 const char *mbir_noalloc_last_error(void);
 
+/* Filtered backprojection (ramp-filtered parallel-beam backprojection of
+ * each frame's views) of the stage's projections into out
+ * [N_time][N_z][N_y][N_x], zero outside the reconstruction mask: the start
+ * image of FBP-initialised ICD.  No counterpart in the reference, whose
+ * coarsest stage starts from zero. */
+int mbir_fbp(MbirStage *stage, float *out);
+
 /* A x of an object into a sinogram [proj_num][proj_rows][proj_cols], with the
  * forward projector of initErrorSinogam (XT_ForwardProject.c:8-25).  Meant
  * for a fresh stage: it overwrites the stage's object and error sinogram. */
 int mbir_forward_project(MbirStage *stage, const float *object, float *out);
+
+/* ---- batched super-voxel ICD (many independent problems per launch) -----
+ * No counterpart in the reference, which reconstructs one scan per process;
+ * each problem iterates exactly as updateVoxelsTimeSlices' HICD sweep with
+ * its convergence test (XT_ICD_update.c:936-1105), without the NHICD pass.
+ *
+ * mbir_batch_create: the stages must be prepared (mbir_icd_prepare) and use
+ * the super-voxel schedule with a column cache (mbir_set_schedule 1), plain
+ * ICD (no ring-offset or variance update), full resolution (3 detector
+ * columns per entry, one row per slice), at most 8 views per lane and 256
+ * threads per super-voxel.  The batch holds the stages' schedules as they are
+ * at creation and reads and writes the stages' objects and error sinograms;
+ * free it before changing or freeing a stage.  Each problem keeps its own
+ * over-relaxation and in-flight cap (uncapped = 1 drops the cap: timing
+ * runs only).  Every iteration is one replay of a captured CUDA graph: a
+ * persistent launch over every super-voxel of the problems still iterating,
+ * then a one-CTA kernel that applies each problem's convergence test
+ * (percentage below the stage's convg_thresh) and retires it. */
+int mbir_batch_create(MbirBatch **batch, MbirStage *const *stages, int32_t n, int32_t uncapped);
+void mbir_batch_free(MbirBatch *batch);
+/* Up to max_iters iterations; every check_every iterations the host reads
+ * how many problems are still active and stops at 0.  *active_left (may be
+ * NULL) = problems still iterating.  Adds the updates to each stage's count. */
+int mbir_batch_iterate(MbirBatch *batch, int32_t max_iters, int32_t check_every, int32_t *active_left);
+/* Per problem (arrays of n; any may be NULL): iterations done, 1 when the
+ * convergence test stopped it, voxel updates, zero-skipped voxels, the last
+ * iteration's convergence percentage. */
+int mbir_batch_stats(MbirBatch *batch, int32_t *iters, int32_t *converged, int64_t *updates,
+                     int64_t *zero_skips, double *pct);
+/* Device time of the batch's iterations (CUDA events on its stream), graph
+ * replays, kernels launched, persistent CTAs, shared memory per CTA. */
+int mbir_batch_info(MbirBatch *batch, double *ms, int64_t *replays, int64_t *launches, int32_t *ctas,
+                    int64_t *smem_bytes);
+/* Autotuner: times the batched kernel on this stage alone for super-voxel
+ * sides 4..8 and 1, 2 or 4 warps per slice (the z-group filling 256
+ * threads) and sets the stage's schedule to the fastest per voxel update.
+ * Call after mbir_icd_prepare and before iterating: the object and error
+ * sinogram are restored, the magnitude map cleared. */
+int mbir_autotune_stage(MbirStage *stage, int32_t *sv_side, int32_t *warps_per_slice, int32_t *z_group,
+                        double *ns_per_update);
+
+/* ---- learned warm start ------------------------------------------------
+ * A 3-D encoder-decoder convolutional network (4 levels, 16-128 channels,
+ * 3x3x3 convolutions, average-pool down, nearest up, additive skips; 1.33 M
+ * parameters) mapping a frame's filtered backprojection to an ICD start
+ * image: out = in + r(s in) / s.  BF16 weights and operands on the tensor
+ * cores with FP32 accumulation; FP32 master parameters and Adam state.
+ * Tensors are device float arrays [B][D][H][W] with D, H, W multiples of 8;
+ * stream is a cudaStream_t (NULL: the default stream); calls return after
+ * the stream has run them.  No counterpart in the reference. */
+typedef struct MbirNet MbirNet;
+int mbir_net_create(MbirNet **net, uint32_t seed);
+void mbir_net_free(MbirNet *net);
+const char *mbir_net_last_error(void);
+int64_t mbir_net_param_count(void);
+/* host float arrays of mbir_net_param_count() entries: per layer the weights
+ * [27 taps][in channels][out channels] (tap = 9 (dz+1) + 3 (dy+1) + dx+1),
+ * then the biases */
+int mbir_net_get_params(MbirNet *net, float *out);
+int mbir_net_set_params(MbirNet *net, const float *in);
+int mbir_net_get_grads(MbirNet *net, float *out);
+int mbir_net_forward(MbirNet *net, const float *in, float *out, int32_t B, int32_t D, int32_t H, int32_t W,
+                     float scale, void *stream);
+/* Parameter gradients of the loss mean((s in + r - s target)^2) into the
+ * network's gradient array; *loss (may be NULL) = the loss. */
+int mbir_net_gradients(MbirNet *net, const float *in, const float *target, int32_t B, int32_t D, int32_t H,
+                       int32_t W, float scale, double *loss, void *stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the last gradients. */
+int mbir_net_adam_step(MbirNet *net, float lr, void *stream);
 
 #ifdef __cplusplus
 }

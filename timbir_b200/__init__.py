@@ -46,6 +46,7 @@ def load_library() -> C.CDLL:
     lib.mbir_last_error.restype = C.c_char_p
     lib.mbir_set_stage_switches.argtypes = [_VP, i32, i32, C.c_double]
     lib.mbir_set_rng_state.argtypes = [_VP, C.c_uint32]
+    lib.mbir_set_convergence_threshold.argtypes = [_VP, C.c_double]
     lib.mbir_get_rng_state.argtypes = [_VP]
     lib.mbir_get_rng_state.restype = C.c_uint32
     lib.mbir_icd_prepare.argtypes = [_VP, _VP, _VP, _VP]
@@ -65,6 +66,7 @@ def load_library() -> C.CDLL:
     lib.mbir_get_update_count.argtypes = [_VP]
     lib.mbir_get_update_count.restype = C.c_longlong
     lib.mbir_forward_project.argtypes = [_VP, _f32p, _f32p]
+    lib.mbir_fbp.argtypes = [_VP, _f32p]
     lib.mbir_get_kernel_stats.argtypes = [_VP, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                           C.POINTER(C.c_longlong)]
     lib.mbir_set_schedule.argtypes = [_VP, i32, i32, i32]
@@ -78,6 +80,14 @@ def load_library() -> C.CDLL:
     lib.mbir_set_sv_relaxation.argtypes = [_VP, C.c_double]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
+    i64 = C.c_int64
+    lib.mbir_batch_create.argtypes = [C.POINTER(_VP), C.POINTER(_VP), i32, i32]
+    lib.mbir_batch_free.argtypes = [_VP]
+    lib.mbir_batch_iterate.argtypes = [_VP, i32, i32, C.POINTER(i32)]
+    lib.mbir_batch_stats.argtypes = [_VP, _VP, _VP, _VP, _VP, _VP]
+    lib.mbir_batch_info.argtypes = [_VP, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i32),
+                                    C.POINTER(i64)]
+    lib.mbir_autotune_stage.argtypes = [_VP] + [C.POINTER(i32)] * 3 + [C.POINTER(C.c_double)]
     lib.reconstruct.argtypes = [C.POINTER(C.POINTER(C.c_float))] + [_VP] * 5 + [i32] * 4 + [fl] * 7 + \
         [i32, i32, fl, fl, C.c_uint8, _VP]
     _lib = lib
@@ -135,6 +145,11 @@ class Stage:
     # --- driving -------------------------------------------------------
     def set_switches(self, update_proj_offset=0, update_var=0, var_est=0.0):
         _check(self.lib.mbir_set_stage_switches(self.h, update_proj_offset, update_var, var_est))
+
+    def set_convergence_threshold(self, convg_thresh: float):
+        """Convergence threshold of the iterations, percent (reconstruct()'s
+        convg_thresh)."""
+        _check(self.lib.mbir_set_convergence_threshold(self.h, convg_thresh))
 
     def set_rng_state(self, state: int):
         self.lib.mbir_set_rng_state(self.h, state)
@@ -280,10 +295,96 @@ class Stage:
         _check(self.lib.mbir_time_end(self.h, C.byref(ms)))
         return ms.value
 
+    def fbp(self) -> np.ndarray:
+        """Filtered backprojection of each frame [N_time][N_z][N_y][N_x]
+        (zero outside the reconstruction mask)."""
+        return self._get("mbir_fbp", (self.N_time, self.N_z, self.N_y, self.N_x))
+
     def forward_project(self, obj) -> np.ndarray:
         out = np.zeros((self.N_p, self.N_t, self.N_r), np.float32)
         _check(self.lib.mbir_forward_project(self.h, _f32(obj).reshape(-1), out.reshape(-1)))
         return out
+
+    def set_batch_schedule(self, sv_side: int = 0, warps_per_slice: int = 1, acache: int = 1):
+        """Super-voxel schedule that batched launches take: z-group and warps
+        per slice filling the batched kernel's 256 threads (batch_split)."""
+        wps, nz = batch_split(warps_per_slice, self.N_z)
+        self.set_sv_zgroup(nz)
+        self.set_schedule(self.SCHEDULE_SUPERVOXEL, sv_side, wps, acache)
+
+    def autotune(self) -> dict:
+        """Pick the super-voxel side, warps per slice and z-group of the
+        batched kernel for this stage by timing them (mbir_autotune_stage);
+        the stage keeps the winner.  Call after prepare, before iterating."""
+        side, wps, zg, ns = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _check(self.lib.mbir_autotune_stage(self.h, C.byref(side), C.byref(wps), C.byref(zg), C.byref(ns)))
+        info = self.schedule_info()
+        return {"sv_side": side.value, "warps_per_slice": wps.value, "z_group": zg.value,
+                "band_width": info["band_width"], "ns_per_update": ns.value}
+
+
+BATCH_WARPS = 8  # warps of the batched kernel's CTA (include/timbir_b200.h: 256 threads)
+
+
+def batch_split(warps_per_slice: int, slices: int, warps: int = BATCH_WARPS):
+    """(warps per slice, z-group) filling `warps` warps on a stack of
+    `slices` slices, starting from `warps_per_slice` and widening it (up to
+    4) when the stack is too short."""
+    wps = warps_per_slice
+    nz = min(warps // wps, slices)
+    while nz * wps < warps and wps < 4:
+        wps *= 2
+        nz = min(warps // wps, slices)
+    return wps, nz
+
+
+class Batch:
+    """Independent problems (prepared super-voxel stages with a column cache)
+    iterated together: one persistent launch per iteration over all their
+    super-voxels, replayed as a CUDA graph (include/timbir_b200.h,
+    mbir_batch_*).  Each problem stops at its own convergence test."""
+
+    def __init__(self, stages, uncapped: bool = False):
+        self.lib = load_library()
+        self.stages = list(stages)
+        arr = (_VP * len(self.stages))(*[s.h for s in self.stages])
+        h = _VP()
+        _check(self.lib.mbir_batch_create(C.byref(h), arr, len(self.stages), 1 if uncapped else 0))
+        self.h = h
+
+    def iterate(self, max_iters: int = 1, check_every: int = 1) -> int:
+        """Up to max_iters iterations (fewer once every problem has
+        converged); returns the problems still iterating."""
+        left = C.c_int32()
+        _check(self.lib.mbir_batch_iterate(self.h, max_iters, check_every, C.byref(left)))
+        return left.value
+
+    def stats(self) -> dict:
+        n = len(self.stages)
+        it, cv = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        up, zs = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        pct = np.zeros(n, np.float64)
+        _check(self.lib.mbir_batch_stats(self.h, it.ctypes.data, cv.ctypes.data, up.ctypes.data, zs.ctypes.data,
+                                         pct.ctypes.data))
+        return {"iterations": it, "converged": cv, "updates": up, "zero_skips": zs, "percent": pct}
+
+    def info(self) -> dict:
+        ms, rep, lau, ctas, sm = C.c_double(), C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()
+        _check(self.lib.mbir_batch_info(self.h, C.byref(ms), C.byref(rep), C.byref(lau), C.byref(ctas),
+                                        C.byref(sm)))
+        return {"ms": ms.value, "replays": rep.value, "launches": lau.value, "ctas": ctas.value,
+                "smem_bytes": sm.value}
+
+    def close(self):
+        if self.h:
+            self.lib.mbir_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _malloc_copy(a: np.ndarray) -> C.c_void_p:

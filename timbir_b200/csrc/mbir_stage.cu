@@ -12,12 +12,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/timbir_b200.h"
 #include "mbir_host.h"
 #include "mbir_internal.h"
+#include "mbir_fbp.h"
 #include "mbir_sv.h"
 
 using namespace mbir;
@@ -332,6 +334,12 @@ extern "C" int mbir_set_stage_switches(MbirStage *S, int32_t update_proj_offset,
     return 0;
 }
 
+extern "C" int mbir_set_convergence_threshold(MbirStage *S, double convg_thresh)
+{
+    S->stop_thresh = convg_thresh;
+    return 0;
+}
+
 extern "C" int mbir_set_rng_state(MbirStage *S, uint32_t state)
 {
     S->rng.state = state;
@@ -379,14 +387,20 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     CK(cudaMemcpyAsync(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice, S->stream));
     if (object)
         CK(cudaMemcpyAsync(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+    else
+        CK(cudaMemsetAsync(S->d_x, 0, S->nvox() * sizeof(float), S->stream));
     if (offset) {
         std::vector<float> d((size_t)sg.N_t * sg.N_r);
         for (int r = 0; r < sg.N_r; r++)
             for (int t = 0; t < sg.N_t; t++) d[(size_t)t * sg.N_r + r] = offset[(size_t)r * sg.N_t + t];
         CK(cudaMemcpyAsync(S->d_d, d.data(), d.size() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+    } else {
+        CK(cudaMemsetAsync(S->d_d, 0, (size_t)sg.N_t * sg.N_r * sizeof(float), S->stream));
     }
     if (magmap)
         CK(cudaMemcpyAsync(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+    else
+        CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
     CK(mbir_forward_rows(S->g, S->d_fov, S->d_x, S->d_y, S->d_d, S->d_e, 0, S->amax(), S->stream));
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
@@ -656,9 +670,10 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     }
     if (cached && sp.ahalf) {
         const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
-        if (vpl > 4 || 32 * sp.max_nz * sp.vsplit > 512)
-            return fail("the FP16 column cache needs at most 4 views per lane and 512 threads per super-voxel "
-                        "(%d views per lane, %d threads)", vpl, 32 * sp.max_nz * sp.vsplit);
+        const int thr = 32 * sp.max_nz * sp.vsplit;
+        if (!((vpl <= 4 && thr <= 512) || (vpl <= 8 && thr <= 256)))
+            return fail("the FP16 column cache needs at most 4 views per lane and 512 threads per super-voxel, or "
+                        "8 and 256 (%d views per lane, %d threads)", vpl, thr);
     }
     S->sp = sp;
     S->gz = gz;
@@ -1219,6 +1234,25 @@ extern "C" int mbir_get_kernel_stats(MbirStage *S, double *icd_ms, long long *ic
     return 0;
 }
 
+// Filtered backprojection of the stage's projections, frame by frame, into
+// out [N_time][N_z][N_y][N_x] (host); zero outside the reconstruction mask.
+extern "C" int mbir_fbp(MbirStage *S, float *out)
+{
+    if (S->mask.empty()) object_mask(S->sg, S->st, S->mask);
+    CK(cudaMemcpyAsync(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice, S->stream));
+    float *q = nullptr, *x = nullptr;
+    CK(dalloc(&q, S->nsino()));
+    CK(dalloc(&x, S->nvox()));
+    cudaError_t e = mbir_launch_fbp(S->g, S->d_mask, S->d_y, q, x, S->stream);
+    S->launches += 2;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, x, S->nvox() * sizeof(float), cudaMemcpyDeviceToHost, S->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    dfree(q);
+    dfree(x);
+    CK(e);
+    return 0;
+}
+
 // Forward projection A x of an object [N_time][N_z][N_y][N_x] into a
 // sinogram [view][row][col] (the layout reconstruct() takes), with this
 // stage's geometry.  Used to synthesise scans of voxelised phantoms.
@@ -1236,5 +1270,369 @@ extern "C" int mbir_forward_project(MbirStage *S, const float *object, float *ou
         for (int p = 0; p < sg.N_p; p++)
             for (int r = 0; r < sg.N_r; r++)
                 out[((size_t)p * sg.N_t + t) * sg.N_r + r] = tmp[((size_t)t * sg.N_p + p) * sg.N_r + r];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Batched super-voxel ICD: independent problems (stages) in one persistent
+// launch per iteration, each iteration one replay of a captured CUDA graph
+// ---------------------------------------------------------------------------
+struct MbirBatch {
+    std::vector<MbirStage *> stages;
+    int n = 0, ctas = 1, nrot = 1, ntasks = 0;
+    bool half = false;
+    size_t smem = 0;  // shared memory per CTA: the largest problem's plan
+    size_t scratch_floats = 0;
+    cudaStream_t stream = nullptr;
+    SvProblem *d_probs = nullptr;
+    SvBatchState *d_state = nullptr;
+    SvTask *d_tasks = nullptr;
+    int *d_lists = nullptr, *d_done = nullptr, *d_queue = nullptr, *d_err = nullptr, *d_ctl = nullptr;
+    float *d_scratch = nullptr;
+    int *h_ctl = nullptr;  // pinned copy of the control words
+    std::vector<cudaGraphExec_t> graphs;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double ms = 0;
+    long long replays = 0;
+    std::vector<long long> seen;  // updates already added to each stage's count
+    ~MbirBatch()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto g : graphs) cudaGraphExecDestroy(g);
+        void *bufs[] = {d_probs, d_state, d_tasks, d_lists, d_done, d_queue, d_err, d_ctl, d_scratch};
+        for (void *b : bufs) dfree(b);
+        if (h_ctl) cudaFreeHost(h_ctl);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// Launch lists of a batch for phase rotation r, appended to buf as
+// [order | dep_off | deps | seq]: each problem's full sweep in its own order
+// (its colour phases from phase r), the problems interleaved in proportion
+// to their super-voxel counts so that they all advance together; deps are
+// the conflicting super-voxels of the same problem earlier in the list, seq
+// the position in the problem's own order.
+static void batch_build_list(const std::vector<MbirStage *> &st, const std::vector<int> &base, int r,
+                             std::vector<int> &buf, std::array<size_t, 5> &meta)
+{
+    struct Ent {
+        double key;
+        int prob, k;
+    };
+    std::vector<std::vector<int>> ids(st.size());
+    std::vector<Ent> all;
+    for (size_t p = 0; p < st.size(); p++) {
+        const MbirStage *S = st[p];
+        ids[p].resize(S->sv_all.size());
+        for (size_t q = 0; q < ids[p].size(); q++) ids[p][q] = (int)q;
+        sv_sort(S, ids[p], r % std::max(1, S->sv_nphase));
+        const double n = (double)ids[p].size();
+        for (size_t k = 0; k < ids[p].size(); k++) all.push_back({(k + 0.5) / n, (int)p, (int)k});
+    }
+    std::stable_sort(all.begin(), all.end(), [](const Ent &a, const Ent &b) { return a.key < b.key; });
+    const size_t n = all.size();
+    meta[0] = n;
+    meta[1] = buf.size();
+    for (const Ent &e : all) buf.push_back(base[e.prob] + ids[e.prob][e.k]);
+    // position of each local id in its problem's order
+    std::vector<std::vector<int>> pos(st.size());
+    for (size_t p = 0; p < st.size(); p++) {
+        pos[p].assign(ids[p].size(), -1);
+        for (size_t k = 0; k < ids[p].size(); k++) pos[p][ids[p][k]] = (int)k;
+    }
+    meta[2] = buf.size();
+    buf.resize(buf.size() + n + 1);
+    std::vector<int> deps;
+    for (size_t t = 0; t < n; t++) {
+        const Ent &e = all[t];
+        buf[meta[2] + t] = (int)deps.size();
+        const int id = ids[e.prob][e.k];
+        for (int nb : st[e.prob]->sv_nbr[id])
+            if (pos[e.prob][nb] < e.k) deps.push_back(base[e.prob] + nb);
+    }
+    buf[meta[2] + n] = (int)deps.size();
+    meta[3] = buf.size();
+    buf.insert(buf.end(), deps.begin(), deps.end());
+    meta[4] = buf.size();
+    for (const Ent &e : all) buf.push_back(e.k);
+}
+
+extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int32_t n, int32_t uncapped)
+{
+    *out = nullptr;
+    if (n <= 0) return fail("a batch needs at least one stage");
+    auto B = std::make_unique<MbirBatch>();
+    B->stages.assign(stages, stages + n);
+    B->n = n;
+    for (int p = 0; p < n; p++) {
+        MbirStage *S = B->stages[p];
+        if (!S->prepared) return fail("batch problem %d: mbir_icd_prepare has not run", p);
+        if (S->schedule != 1 || !S->d_acol)
+            return fail("batch problem %d: the super-voxel schedule with a column cache is required", p);
+        if (S->upd_offset > 1 || S->upd_var == 1)
+            return fail("batch problem %d: batched iterations run plain ICD (no ring-offset or variance update)", p);
+        const SvParams &sp = S->sp;
+        const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
+        if (sp.amax != 3 || S->st.m_z != 1 || vpl > kSvBatchViewsPerLane ||
+            32 * sp.max_nz * sp.vsplit > kSvBatchThreads)
+            return fail("batch problem %d: needs 3 detector columns per entry, one row per slice, at most %d views "
+                        "per lane and %d threads per super-voxel (%d columns, %d rows, %d views per lane, %d "
+                        "threads)",
+                        p, kSvBatchViewsPerLane, kSvBatchThreads, sp.amax, S->st.m_z, vpl,
+                        32 * sp.max_nz * sp.vsplit);
+        if (p > 0 && S->acol_half != B->half) return fail("batch problem %d: mixed FP32 and FP16 column caches", p);
+        B->half = S->acol_half;
+        if (!S->acol_built) {
+            CK(mbir_build_acache(S->g, S->dv, sp.amax, sp.eq, S->acol_half, S->d_acol, S->d_err, S->stream));
+            S->acol_built = true;
+            S->launches++;
+        }
+        CK(cudaStreamSynchronize(S->stream));
+        B->smem = std::max(B->smem, mbir_sv_plan_bytes(mbir_sv_plan(sp, true)));
+        B->scratch_floats = std::max(B->scratch_floats, sp.band_floats);
+    }
+    if (B->smem > kSmemLimit) return fail("a batch problem needs %zu bytes of shared memory", B->smem);
+    // problems, tasks, launch lists
+    std::vector<SvProblem> probs(n);
+    std::vector<SvTask> tasks;
+    std::vector<int> base(n);
+    for (int p = 0; p < n; p++) {
+        MbirStage *S = B->stages[p];
+        SvProblem &P = probs[p];
+        P.g = S->g;
+        P.pr = S->pr;
+        P.pr.alpha = S->sv_alpha_eff;
+        P.dv = S->dv;
+        P.sp = S->sp;
+        P.ac = SvACache{S->d_acol};
+        P.plan = mbir_sv_plan(S->sp, true);
+        P.cap = uncapped ? (1 << 30) : std::max(1, S->sv_grid);
+        P.K = S->K;
+        P.stop = S->stop_thresh;
+        base[p] = (int)tasks.size();
+        for (SvTask t : S->sv_all) {
+            t.prob = p;
+            tasks.push_back(t);
+        }
+        B->nrot = std::max(B->nrot, S->sv_nphase);
+    }
+    B->ntasks = (int)tasks.size();
+    if (B->ntasks == 0) return fail("the batch has no super-voxels");
+    std::vector<int> buf;
+    std::vector<std::array<size_t, 5>> meta(B->nrot);
+    for (int r = 0; r < B->nrot; r++) batch_build_list(B->stages, base, r, buf, meta[r]);
+    CK(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&B->ev0));
+    CK(cudaEventCreate(&B->ev1));
+    int dev = 0, sms = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    B->ctas = std::max(1, std::min(B->ntasks, mbir_sv_batch_ctas_per_sm(B->smem, B->half) * sms));
+    CK(dalloc(&B->d_probs, n));
+    CK(dalloc(&B->d_state, n));
+    CK(dalloc(&B->d_tasks, tasks.size()));
+    CK(dalloc(&B->d_lists, buf.size()));
+    CK(dalloc(&B->d_done, tasks.size()));
+    CK(dalloc(&B->d_queue, 1));
+    CK(dalloc(&B->d_err, 1));
+    CK(dalloc(&B->d_ctl, 4));
+    CK(dalloc(&B->d_scratch, (size_t)B->ctas * B->scratch_floats));
+    CK(cudaMallocHost(&B->h_ctl, 4 * sizeof(int)));
+    std::vector<SvBatchState> state(n);
+    for (auto &s : state) s.active = 1;
+    const int ctl[4] = {1, n, 0, 0};
+    CK(cudaMemcpyAsync(B->d_probs, probs.data(), n * sizeof(SvProblem), cudaMemcpyHostToDevice, B->stream));
+    CK(cudaMemcpyAsync(B->d_state, state.data(), n * sizeof(SvBatchState), cudaMemcpyHostToDevice, B->stream));
+    CK(cudaMemcpyAsync(B->d_tasks, tasks.data(), tasks.size() * sizeof(SvTask), cudaMemcpyHostToDevice, B->stream));
+    CK(cudaMemcpyAsync(B->d_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, B->stream));
+    CK(cudaMemcpyAsync(B->d_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, B->stream));
+    CK(cudaMemsetAsync(B->d_done, 0, tasks.size() * sizeof(int), B->stream));
+    CK(cudaMemsetAsync(B->d_queue, 0, sizeof(int), B->stream));
+    CK(cudaMemsetAsync(B->d_err, 0, sizeof(int), B->stream));
+    CK(cudaStreamSynchronize(B->stream));
+    B->seen.assign(n, 0);
+    // one graph per phase rotation: the sweep, then the end of the iteration
+    CK(mbir_sv_batch_prepare(B->smem, B->half));
+    for (int r = 0; r < B->nrot; r++) {
+        SvLaunch L{B->d_tasks, B->d_lists + meta[r][1], B->d_lists + meta[r][2], B->d_lists + meta[r][3],
+                   (int)meta[r][0], B->d_done, 0, B->d_probs, B->d_lists + meta[r][4], B->d_state, B->d_ctl};
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = mbir_launch_icd_sv_batch(B->smem, B->half, L, B->ctas, B->d_queue, B->d_scratch,
+                                                  B->scratch_floats, 0x2545F491u + 977u * r, B->d_err, B->stream);
+        cudaError_t e2 = mbir_launch_sv_batch_end(B->d_probs, B->d_state, n, B->d_ctl, B->d_queue, B->stream);
+        cudaError_t e3 = cudaStreamEndCapture(B->stream, &g);
+        CK(e1);
+        CK(e2);
+        CK(e3);
+        cudaGraphExec_t ge = nullptr;
+        cudaError_t e4 = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        CK(e4);
+        B->graphs.push_back(ge);
+    }
+    *out = B.release();
+    return 0;
+}
+
+extern "C" void mbir_batch_free(MbirBatch *B) { delete B; }
+
+extern "C" int mbir_batch_iterate(MbirBatch *B, int32_t max_iters, int32_t check_every, int32_t *active_left)
+{
+    if (check_every <= 0) check_every = 1;
+    CK(cudaEventRecord(B->ev0, B->stream));
+    int left = B->n;
+    for (int k = 0; k < max_iters; k++) {
+        CK(cudaGraphLaunch(B->graphs[B->replays % B->nrot], B->stream));
+        B->replays++;
+        if ((k + 1) % check_every == 0 || k + 1 == max_iters) {
+            CK(cudaMemcpyAsync(B->h_ctl, B->d_ctl, 4 * sizeof(int), cudaMemcpyDeviceToHost, B->stream));
+            CK(cudaStreamSynchronize(B->stream));
+            left = B->h_ctl[1];
+            if (left == 0) break;
+        }
+    }
+    CK(cudaEventRecord(B->ev1, B->stream));
+    CK(cudaEventSynchronize(B->ev1));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, B->ev0, B->ev1));
+    B->ms += f;
+    int err = 0;
+    CK(cudaMemcpy(&err, B->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
+    if (err & 2) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
+    if (err & 4) return fail("super-voxel dependency wait timed out");
+    if (err & 8) return fail("super-voxel in-flight wait timed out");
+    // the stages' own counters
+    std::vector<SvBatchState> st(B->n);
+    CK(cudaMemcpy(st.data(), B->d_state, B->n * sizeof(SvBatchState), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < B->n; p++) {
+        MbirStage *S = B->stages[p];
+        S->updates += st[p].updates - B->seen[p];
+        B->seen[p] = st[p].updates;
+        S->last_pct = st[p].pct;
+    }
+    if (active_left) *active_left = left;
+    return 0;
+}
+
+// Per problem: iterations done, stopped by the convergence test, voxel
+// updates, zero-skipped voxels, last convergence ratio (percent).  Any
+// pointer may be null.
+extern "C" int mbir_batch_stats(MbirBatch *B, int32_t *iters, int32_t *converged, int64_t *updates,
+                                int64_t *zero_skips, double *pct)
+{
+    std::vector<SvBatchState> st(B->n);
+    CK(cudaMemcpy(st.data(), B->d_state, B->n * sizeof(SvBatchState), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < B->n; p++) {
+        if (iters) iters[p] = st[p].iters;
+        if (converged) converged[p] = st[p].converged;
+        if (updates) updates[p] = st[p].updates;
+        if (zero_skips) zero_skips[p] = st[p].zero_skips;
+        if (pct) pct[p] = st[p].pct;
+    }
+    return 0;
+}
+
+// Device time of the batch's iterations so far (CUDA events on its stream),
+// graph replays, kernels launched (two per replay), persistent CTAs, shared
+// memory per CTA.
+extern "C" int mbir_batch_info(MbirBatch *B, double *ms, int64_t *replays, int64_t *launches, int32_t *ctas,
+                               int64_t *smem_bytes)
+{
+    if (ms) *ms = B->ms;
+    if (replays) *replays = B->replays;
+    if (launches) *launches = 2 * B->replays;
+    if (ctas) *ctas = B->ctas;
+    if (smem_bytes) *smem_bytes = (int64_t)B->smem;
+    return 0;
+}
+
+// Autotuner: times the batched kernel on this stage alone (no in-flight cap,
+// every resident CTA busy) for super-voxel sides 4..8 and 1, 2 or 4 warps
+// per slice (with the z-group filling 256 threads), two iterations after one
+// warm-up from the stage's prepared state, and keeps the fastest per voxel
+// update.  The object and error sinogram are restored afterwards and the
+// magnitude map cleared; call after mbir_icd_prepare, before iterating.
+extern "C" int mbir_autotune_stage(MbirStage *S, int32_t *side, int32_t *warps_per_slice, int32_t *zgroup,
+                                   double *ns_per_update)
+{
+    if (!S->prepared) return fail("mbir_icd_prepare has not run");
+    const int Nz = S->st.N_z;
+    float *x0 = nullptr, *e0 = nullptr;
+    CK(dalloc(&x0, S->nvox()));
+    CK(dalloc(&e0, S->nsino()));
+    auto release = [&]() {
+        dfree(x0);
+        dfree(e0);
+    };
+    CK(cudaMemcpyAsync(x0, S->d_x, S->nvox() * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(e0, S->d_e, S->nsino() * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    auto restore = [&]() -> int {
+        CK(cudaMemcpyAsync(S->d_x, x0, S->nvox() * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->d_e, e0, S->nsino() * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+        return 0;
+    };
+    const int zg_saved = S->sv_zgroup;
+    double best = 1e300;
+    int bs = 0, bv = 0, bz = 0;
+    const int warps = kSvBatchThreads / 32;
+    for (int s = 4; s <= 8; s++)
+        for (int v = 1; v <= 4; v *= 2) {
+            const int nz = std::min(warps / v, Nz);
+            S->sv_zgroup = nz;
+            if (mbir_set_schedule(S, 1, s, v) != 0 || !S->d_acol) continue;
+            const SvParams &sp = S->sp;
+            if (sp.S != s || sp.vsplit != v || sp.max_nz != nz) continue;
+            if (restore()) return release(), -1;
+            MbirBatch *B = nullptr;
+            if (mbir_batch_create(&B, &S, 1, 1) != 0) continue;
+            int32_t left = 0;
+            int rc = mbir_batch_iterate(B, 1, 1, &left);
+            int64_t u0 = 0, u1 = 0;
+            double ms0 = 0, ms1 = 0;
+            if (!rc) {
+                mbir_batch_stats(B, nullptr, nullptr, &u0, nullptr, nullptr);
+                mbir_batch_info(B, &ms0, nullptr, nullptr, nullptr, nullptr);
+                rc = mbir_batch_iterate(B, 2, 2, &left);
+                mbir_batch_stats(B, nullptr, nullptr, &u1, nullptr, nullptr);
+                mbir_batch_info(B, &ms1, nullptr, nullptr, nullptr, nullptr);
+            }
+            mbir_batch_free(B);
+            if (rc) {
+                S->sv_zgroup = zg_saved;
+                release();
+                return -1;
+            }
+            const double ns = u1 > u0 ? (ms1 - ms0) * 1e6 / (double)(u1 - u0) : 1e300;
+            if (ns < best) {
+                best = ns;
+                bs = s;
+                bv = v;
+                bz = nz;
+            }
+        }
+    if (!bs) {
+        S->sv_zgroup = zg_saved;
+        release();
+        return fail("no super-voxel configuration of the batched kernel fits this stage");
+    }
+    S->sv_zgroup = bz;
+    if (mbir_set_schedule(S, 1, bs, bv) != 0 || restore()) {
+        release();
+        return -1;
+    }
+    // the stage's counters exclude the trial iterations
+    S->updates = 0;
+    S->zero_skips = 0;
+    release();
+    *side = bs;
+    *warps_per_slice = bv;
+    *zgroup = bz;
+    *ns_per_update = best;
     return 0;
 }

@@ -111,6 +111,14 @@ __device__ __forceinline__ int ld_acquire(const int *p)
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Once one wait of the launch has given up (err bits 4 or 8), the others
+// stop waiting too (checked every 1024 polls), so that a broken dependency
+// costs one wait limit, not one per super-voxel.
+__device__ __forceinline__ bool wait_abandoned(const int *err, int spins)
+{
+    return (spins & 1023) == 1023 && (*(volatile const int *)err & 12) != 0;
+}
+
 __device__ __forceinline__ void st_release(int *p, int v)
 {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -422,85 +430,67 @@ cudaError_t launch_forward_rows(const MbirGeom &g, const int *fov, const float *
 // values (8-byte entries, full resolution only).  VU (full-resolution path): a
 // lane's views per slice, at most VU, are held in registers from theta to
 // the error-sinogram update.
-template <int AMAXC, int MZC, int AC, int MAXT, int VU>
-__global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirDev dv, SvParams sp, SvACache ac,
-                                                  SvLaunch L, int *queue, float *__restrict__ scratch,
-                                                  SvTaskOut *__restrict__ out, int iter, uint32_t seed, int *err)
+// The problem a task runs on: the launch's own (a kernel parameter) or, in
+// a batched launch, the CTA's shared-memory copy of the task's problem.
+template <bool B>
+__device__ __forceinline__ const SvProblem *pick_problem(const unsigned char *shared_copy, const SvProblem *param)
+{
+    if constexpr (B)
+        return reinterpret_cast<const SvProblem *>(shared_copy);
+    else
+        return param;
+}
+
+template <int AMAXC, int MZC, int AC, int MAXT, int VU, bool BATCH>
+__global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProblem P0,
+                                                  const SvLaunch L, int *queue, float *__restrict__ scratch,
+                                                  size_t scratch_floats, SvTaskOut *__restrict__ out, int iter_arg,
+                                                  uint32_t seed_arg, int *err)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
-    const int amax = AMAXC > 0 ? AMAXC : sp.amax;
-    const int eq = AMAXC > 0 ? (AMAXC + 4) / 4 : sp.eq;
-    const int nwd = 4 * eq;  // words per ring entry
-    const int mz = MZC > 0 ? MZC : g.m_z;
-    const int NpS = sp.max_views;  // smem stride (views)
+    __shared__ __align__(16) unsigned char s_prob[BATCH ? sizeof(SvProblem) : 16];
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
-    const int S2 = S + 2;
-    const size_t rowstride = (size_t)W * NpS;  // band entries per detector row
-
-    // ---- carve shared memory (sizes fixed by the host in sp) ----
-    unsigned char *p = smraw;
-    const int R = sp.ring, D = R - 2;  // ring slots; column prefetch distance (lines)
     constexpr int kHalf = AC == 2;
-    const int ent_bytes = kHalf ? 8 : 16 * eq;  // bytes per ring entry
-    int4 *ring = reinterpret_cast<int4 *>(p); p += (size_t)ent_bytes * R * NpS;
-    float2 *band = reinterpret_cast<float2 *>(p); p += sizeof(float2) * (size_t)sp.max_rows * rowstride;
-    double *cs = reinterpret_cast<double *>(p);
-    double *sn = cs + NpS;
-    if (!AC) p += 2 * sizeof(double) * NpS;
-    float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
-    float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * 2 * sp.max_nz * S * S;
-    // |dx| of each (slice, line) at this visit; summed over the slices in
-    // slice order at write-back (the line's magnitude-map entry)
-    float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * sp.max_nz * S * S;
-    float *part = reinterpret_cast<float *>(p); p += sizeof(float) * 4 * 4 * sp.max_nz;
-    int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
-    int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * NpS;
-    // step sequence: lx | ly << 8 of the line, or -1 for an idle step
-    int *order = reinterpret_cast<int *>(p); p += sizeof(int) * (S * S + 4);
+
     __shared__ int s_nlines, s_task, s_bad;
     __shared__ float s_red[32][4];
 
-    const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
-    const float inv_off_f = (float)inv_off;
-    const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
-    const float sSQ_inv = (float)(1.0 / pr.sSQ), sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
-    const float sTQ_inv = (float)(1.0 / pr.sTQ), sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
-    // warps [0, ncons) update voxels (vsplit per slice); warps [ncons, nwarps)
-    // produce the next line's A-matrix column while they do
-    const int ncons = sp.max_nz * vsplit, nprod = nwarps - ncons;
-    const bool consumer = warp < ncons;
-    const int zl = consumer ? warp / vsplit : 0, vh = consumer ? warp - zl * vsplit : 0;
-    // neighbour of lane: spatial (dz, dy, dx) for lanes 0..25, temporal 26, 27
-    int ndz = 0, ndy = 0, ndx = 0;
-    float bw = 0.0f, qinv = 0.0f, qpinv = 0.0f, cc = 1.0f;
-    bool spatial = false, temporal = false;
-    int nboff = 0;  // offset of the spatial neighbour in the staged block
-    if (lane < 26) {
-        const int n = lane < 13 ? lane : lane + 1;  // skip the centre (13)
-        ndz = n / 9 - 1;
-        ndy = (n / 3) % 3 - 1;
-        ndx = n % 3 - 1;
-        nboff = (ndz * S2 + ndy) * S2 + ndx;
-        bw = (float)pr.SF[n];
-        qinv = sSQ_inv;
-        qpinv = sSQP_inv;
-        cc = cS;
-        spatial = true;
-    } else if (lane < 28) {
-        bw = (float)pr.TF;
-        qinv = sTQ_inv;
-        qpinv = sTQP_inv;
-        cc = cT;
-        temporal = true;
-    }
-    // views of the A-column computation: the producer warps' (all warps
-    // for the first line of a task, or when there are no producers)
-    const int av_all = (NpS + nwarps - 1) / nwarps;
-    const int av_prod = nprod > 0 ? (NpS + nprod - 1) / nprod : 0;
+    // a batched launch's iteration number comes from the device (so that one
+    // captured graph serves every iteration); it is also the epoch of the
+    // done flags and varies the line order
+    const int epoch = BATCH ? __ldcg(L.ctl) : L.epoch;
+    const int iter = BATCH ? epoch : iter_arg;
+    const uint32_t seed = BATCH ? hash32(seed_arg ^ ((uint32_t)epoch * 0x9E3779B9u)) : seed_arg;
     float sum_abs_dx = 0.0f, sum_abs_x = 0.0f;
     int n_upd = 0, n_skip = 0;
+    // statistics of the CTA's updates since the last call (lane 0 of each
+    // slice's first warp counts) into *o; every thread calls it
+    auto flush_stats = [&](SvTaskOut *o) {
+        if (lane == 0) {
+            s_red[warp][0] = sum_abs_dx;
+            s_red[warp][1] = sum_abs_x;
+            s_red[warp][2] = (float)n_upd;
+            s_red[warp][3] = (float)n_skip;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double d0 = 0, d1 = 0, d2 = 0, d3 = 0;
+            for (int w = 0; w < nwarps; w++) {
+                d0 += s_red[w][0];
+                d1 += s_red[w][1];
+                d2 += s_red[w][2];
+                d3 += s_red[w][3];
+            }
+            atomicAdd(&o->sum_abs_dx, d0);
+            atomicAdd(&o->sum_abs_x, d1);
+            atomicAdd((unsigned long long *)&o->updates, (unsigned long long)d2);
+            atomicAdd((unsigned long long *)&o->zero_skips, (unsigned long long)d3);
+        }
+        sum_abs_dx = sum_abs_x = 0.0f;
+        n_upd = n_skip = 0;
+    };
+    int cur = -1;  // problem held in s_prob (batched launches)
 
     for (;;) {
         __syncthreads();
@@ -513,6 +503,92 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         if (tix >= L.ntasks) break;
         const int id = L.order[tix];
         const SvTask task = L.tasks[id];
+        if constexpr (BATCH) {
+            if (task.prob != cur) {
+                cur = task.prob;
+                const long long *src = reinterpret_cast<const long long *>(L.problems + cur);
+                long long *dst = reinterpret_cast<long long *>(s_prob);
+                for (int q = tid; q < (int)(sizeof(SvProblem) / sizeof(long long)); q += nthr) dst[q] = src[q];
+                __syncthreads();
+            }
+            // a problem that has stopped iterating: skip its super-voxels
+            if (!__ldcg(&L.state[cur].active)) {
+                if (tid == 0) st_release(L.done + id, epoch);
+                continue;
+            }
+        }
+        const SvProblem &P = *pick_problem<BATCH>(s_prob, &P0);
+        const MbirGeom &g = P.g;
+        const MbirPrior &pr = P.pr;
+        const MbirDev &dv = P.dv;
+        const SvParams &sp = P.sp;
+        const SvACache ac = P.ac;
+        // ---- carve shared memory (the problem's region sizes) ----
+        const SvPlan &pl = P.plan;
+        unsigned char *p = smraw;
+        int4 *ring = reinterpret_cast<int4 *>(p); p += pl.ring_bytes;
+        float2 *band = reinterpret_cast<float2 *>(p); p += sizeof(float2) * (size_t)pl.band_pairs;
+        double *cs = reinterpret_cast<double *>(p);
+        double *sn = cs + pl.trig_views;
+        p += 2 * sizeof(double) * pl.trig_views;
+        float *xb = reinterpret_cast<float *>(p); p += sizeof(float) * pl.xb;
+        float *tb = reinterpret_cast<float *>(p); p += sizeof(float) * pl.tb;
+        // |dx| of each (slice, line) at this visit; summed over the slices in
+        // slice order at write-back (the line's magnitude-map entry)
+        float *magl = reinterpret_cast<float *>(p); p += sizeof(float) * pl.magl;
+        float *part = reinterpret_cast<float *>(p); p += sizeof(float) * pl.part;
+        int *vidx = reinterpret_cast<int *>(p); p += sizeof(int) * pl.views;
+        int *rlo = reinterpret_cast<int *>(p); p += sizeof(int) * pl.views;
+        // step sequence: lx | ly << 8 of the line, or -1 for an idle step
+        int *order = reinterpret_cast<int *>(p);
+        const int S = sp.S, W = sp.W, vsplit = sp.vsplit;
+        const int amax = AMAXC > 0 ? AMAXC : sp.amax;
+        const int eq = AMAXC > 0 ? (AMAXC + 4) / 4 : sp.eq;
+        const int nwd = 4 * eq;  // words per ring entry
+        const int mz = MZC > 0 ? MZC : g.m_z;
+        const int NpS = sp.max_views;  // smem stride (views)
+        const int S2 = S + 2;
+        const size_t rowstride = (size_t)W * NpS;  // band entries per detector row
+        const int R = sp.ring, D = R - 2;  // ring slots; column prefetch distance (lines)
+        const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
+        const float inv_off_f = (float)inv_off;
+        const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
+        const float sSQ_inv = (float)(1.0 / pr.sSQ), sSQP_inv = (float)(1.0 / pr.sSQP), cS = (float)pr.c_s;
+        const float sTQ_inv = (float)(1.0 / pr.sTQ), sTQP_inv = (float)(1.0 / pr.sTQP), cT = (float)pr.c_t;
+        // warps [0, ncons) update voxels (vsplit per slice); warps [ncons, nwarps)
+        // produce the next line's A-matrix column while they do (or, in a
+        // batched launch, idle when the problem needs fewer warps)
+        const int ncons = sp.max_nz * vsplit, nprod = nwarps - ncons;
+        const bool consumer = warp < ncons;
+        const int zl = consumer ? warp / vsplit : 0, vh = consumer ? warp - zl * vsplit : 0;
+        // neighbour of lane: spatial (dz, dy, dx) for lanes 0..25, temporal 26, 27
+        int ndz = 0, ndy = 0, ndx = 0;
+        float bw = 0.0f, qinv = 0.0f, qpinv = 0.0f, cc = 1.0f;
+        bool spatial = false, temporal = false;
+        int nboff = 0;  // offset of the spatial neighbour in the staged block
+        if (lane < 26) {
+            const int n = lane < 13 ? lane : lane + 1;  // skip the centre (13)
+            ndz = n / 9 - 1;
+            ndy = (n / 3) % 3 - 1;
+            ndx = n % 3 - 1;
+            nboff = (ndz * S2 + ndy) * S2 + ndx;
+            bw = (float)pr.SF[n];
+            qinv = sSQ_inv;
+            qpinv = sSQP_inv;
+            cc = cS;
+            spatial = true;
+        } else if (lane < 28) {
+            bw = (float)pr.TF;
+            qinv = sTQ_inv;
+            qpinv = sTQP_inv;
+            cc = cT;
+            temporal = true;
+        }
+        // views of the A-column computation: the producer warps' (all warps
+        // for the first line of a task, or when there are no producers)
+        const int av_all = (NpS + nwarps - 1) / nwarps;
+        const int av_prod = nprod > 0 ? (NpS + nprod - 1) / nprod : 0;
+
         const int nz = task.nz, rows = nz * mz;
         const int i = task.frame;
         const int Np = g.view_num[i];
@@ -605,10 +681,24 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
             if (lane == 0) s_nlines = n;
             // wait for the conflicting super-voxels earlier in this launch
             // (bounded: a wait that gives up flags err and goes on)
+            if constexpr (BATCH) {
+                // at most cap super-voxels of the problem in flight: those
+                // before this one in its order, less the finished ones
+                const int need = L.seq[tix] + 1 - P.cap;
+                if (lane == 0 && need > 0)
+                    for (int spins = 0; ld_acquire(&L.state[cur].fin) < need; spins++) {
+                        if (spins > (1 << 22) || wait_abandoned(err, spins)) {
+                            atomicOr(err, 8);
+                            break;
+                        }
+                        __nanosleep(100);
+                    }
+                __syncwarp();
+            }
             for (int d = L.dep_off[tix] + lane; d < L.dep_off[tix + 1]; d += 32) {
                 const int *flag = L.done + L.deps[d];
-                for (int spins = 0; ld_acquire(flag) != L.epoch; spins++) {
-                    if (spins > (1 << 22)) {
+                for (int spins = 0; ld_acquire(flag) != epoch; spins++) {
+                    if (spins > (1 << 22) || wait_abandoned(err, spins)) {
                         atomicOr(err, 4);
                         break;
                     }
@@ -625,7 +715,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         //      every fourth 16-byte-aligned word of the W columns (rows of
         //      N_r % 4 == 0 are 16-byte aligned; words starting past the row
         //      end stage zeros) ----
-        float *__restrict__ scr = scratch + (size_t)blockIdx.x * sp.band_floats;
+        float *__restrict__ scr = scratch + (size_t)blockIdx.x * scratch_floats;
         const bool vec = (g.N_r & 3) == 0;
         const int npairs = rows * Np;
         if (vec) {
@@ -993,75 +1083,101 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(MbirGeom g, MbirPrior pr, MbirD
         __syncthreads();
         if (tid == 0) {
             __threadfence();
-            st_release(L.done + id, L.epoch);
+            st_release(L.done + id, epoch);
+            if constexpr (BATCH) atomicAdd(&L.state[cur].fin, 1);
         }
+        if constexpr (BATCH) flush_stats(&L.state[cur].out);
     }
-    // ---- per-CTA statistics (lane 0 of each slice's first warp counts) ----
-    if (lane == 0) {
-        s_red[warp][0] = sum_abs_dx;
-        s_red[warp][1] = sum_abs_x;
-        s_red[warp][2] = (float)n_upd;
-        s_red[warp][3] = (float)n_skip;
-    }
+    if constexpr (!BATCH) flush_stats(out);
+}
+
+// End of a batched iteration (one CTA).
+__global__ void __launch_bounds__(256) k_sv_batch_end(const SvProblem *__restrict__ probs,
+                                                      SvBatchState *__restrict__ st, int n, int *ctl, int *queue)
+{
+    __shared__ int s_active;
+    if (threadIdx.x == 0) s_active = 0;
     __syncthreads();
-    if (tid == 0) {
-        double d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-        for (int w = 0; w < nwarps; w++) {
-            d0 += s_red[w][0];
-            d1 += s_red[w][1];
-            d2 += s_red[w][2];
-            d3 += s_red[w][3];
+    int act = 0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        SvBatchState &b = st[q];
+        if (b.active) {
+            b.iters++;
+            b.updates += b.out.updates;
+            b.zero_skips += b.out.zero_skips;
+            // the reference's convergence ratio (XT_ICD_update.c:1066-1103)
+            b.pct = b.out.sum_abs_x > 0 ? 100.0 * probs[q].K * b.out.sum_abs_dx / b.out.sum_abs_x : 0.0;
+            if (b.pct < probs[q].stop) {
+                b.active = 0;
+                b.converged = 1;
+            }
         }
-        atomicAdd(&out->sum_abs_dx, d0);
-        atomicAdd(&out->sum_abs_x, d1);
-        atomicAdd((unsigned long long *)&out->updates, (unsigned long long)d2);
-        atomicAdd((unsigned long long *)&out->zero_skips, (unsigned long long)d3);
+        act += b.active;
+        b.out = SvTaskOut{};
+        b.fin = 0;
+    }
+    if (act) atomicAdd(&s_active, act);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl[0]++;
+        ctl[1] = s_active;
+        *queue = 0;
     }
 }
 
-template <int AMAXC, int MZC, int AC, int MAXT, int VU>
+template <int AMAXC, int MZC, int AC, int MAXT, int VU, bool BATCH = false>
 int occupancy_sv(int threads, size_t sm)
 {
-    if (cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm) != cudaSuccess)
         return 1;
     int n = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_icd_sv<AMAXC, MZC, AC, MAXT, VU>, threads, sm) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_icd_sv<AMAXC, MZC, AC, MAXT, VU, BATCH>, threads, sm) !=
         cudaSuccess)
         return 1;
     return n > 0 ? n : 1;
 }
 
-template <int AMAXC, int MZC, int AC, int MAXT, int VU>
-cudaError_t launch_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp, SvACache ac,
-                      const SvLaunch &L, int ctas, int threads, size_t sm, int *queue, float *scratch,
-                      SvTaskOut *out, int iter, uint32_t seed, int *err, cudaStream_t s)
+template <int AMAXC, int MZC, int AC, int MAXT, int VU, bool BATCH = false>
+cudaError_t launch_sv(const SvProblem &P, const SvLaunch &L, int ctas, int threads, size_t sm, int *queue,
+                      float *scratch, size_t scratch_floats, SvTaskOut *out, int iter, uint32_t seed, int *err,
+                      cudaStream_t s)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU>,
+    cudaError_t e = cudaFuncSetAttribute(k_icd_sv<AMAXC, MZC, AC, MAXT, VU, BATCH>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_icd_sv<AMAXC, MZC, AC, MAXT, VU>
-        <<<ctas, threads, sm, s>>>(g, pr, dv, sp, ac, L, queue, scratch, out, iter, seed, err);
+    k_icd_sv<AMAXC, MZC, AC, MAXT, VU, BATCH>
+        <<<ctas, threads, sm, s>>>(P, L, queue, scratch, scratch_floats, out, iter, seed, err);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached)
+SvPlan mbir_sv_plan(const SvParams &sp, bool cached)
 {
-    const size_t NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
-    size_t b = 0;
-    b += (size_t)(cached && sp.ahalf ? 8 : 16 * sp.eq) * sp.ring * NpS;  // A-column ring
-    b += 8 * (size_t)sp.max_rows * sp.W * NpS;  // (e, sqrt(w)) band
-    if (!cached) b += 2 * sizeof(double) * NpS;
-    b += sizeof(float) * (sp.max_nz + 2) * S2 * S2;
-    b += sizeof(float) * 2 * sp.max_nz * S * S;
-    b += sizeof(float) * sp.max_nz * S * S;
-    b += sizeof(float) * 4 * 4 * sp.max_nz;
-    b += sizeof(int) * NpS * 2;
-    b += sizeof(int) * (S * S + 4);
+    const int NpS = sp.max_views, S = sp.S, S2 = sp.S + 2;
+    SvPlan pl{};
+    pl.ring_bytes = (cached && sp.ahalf ? 8 : 16 * sp.eq) * sp.ring * NpS;
+    pl.band_pairs = sp.max_rows * sp.W * NpS;
+    pl.trig_views = cached ? 0 : NpS;
+    pl.xb = (sp.max_nz + 2) * S2 * S2;
+    pl.tb = 2 * sp.max_nz * S * S;
+    pl.magl = sp.max_nz * S * S;
+    pl.part = 4 * 4 * sp.max_nz;
+    pl.views = NpS;
+    pl.order = S * S + 4;
+    return pl;
+}
+
+size_t mbir_sv_plan_bytes(const SvPlan &pl)
+{
+    size_t b = (size_t)pl.ring_bytes + 8 * (size_t)pl.band_pairs + 16 * (size_t)pl.trig_views;
+    b += sizeof(float) * ((size_t)pl.xb + pl.tb + pl.magl + pl.part);
+    b += sizeof(int) * (2 * (size_t)pl.views + pl.order);
     return (b + 15) & ~(size_t)15;
 }
+
+size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached) { return mbir_sv_plan_bytes(mbir_sv_plan(sp, cached)); }
 
 cudaError_t mbir_forward_rows(const MbirGeom &g, const int *frame_of_view, const float *x, const float *y,
                               const float *d, float *out, int mode, int amax, cudaStream_t s)
@@ -1115,7 +1231,7 @@ auto sv_dispatch(const MbirGeom &g, const SvParams &sp, bool cached, int threads
         return f(SvInst<3, 1, 2, 512, 4>{});
     }
     if (cached && threads <= 256 && sp.amax == 3 && g.m_z == 1 && vpl > 4 && vpl <= 8)
-        return f(SvInst<3, 1, 1, 256, 8>{});
+        return sp.ahalf ? f(SvInst<3, 1, 2, 256, 8>{}) : f(SvInst<3, 1, 1, 256, 8>{});
 #define MBIR_SV_PICK(T)                                                                              \
     if (full && vpl <= 2) return cached ? f(SvInst<3, 1, 1, T, 2>{}) : f(SvInst<3, 1, 0, T, 2>{}); \
     if (full) return cached ? f(SvInst<3, 1, 1, T, 4>{}) : f(SvInst<3, 1, 0, T, 4>{});             \
@@ -1143,11 +1259,54 @@ cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const Mbi
 {
     if (L.ntasks <= 0) return cudaSuccess;
     const bool cached = ac.a != nullptr;
-    const size_t sm = mbir_sv_smem_bytes(sp, cached);
+    SvProblem P{};
+    P.g = g;
+    P.pr = pr;
+    P.dv = dv;
+    P.sp = sp;
+    P.ac = ac;
+    P.plan = mbir_sv_plan(sp, cached);
+    const size_t sm = mbir_sv_plan_bytes(P.plan);
     const int threads = 32 * (sp.max_nz * sp.vsplit + (cached ? 0 : sp.prod_warps));
     return sv_dispatch(g, sp, cached, threads, [&](auto I) {
         using In = decltype(I);
-        return launch_sv<In::AMAXC, In::MZC, In::AC, In::MAXT, In::VU>(g, pr, dv, sp, ac, L, ctas, threads, sm, queue,
-                                                                       scratch, out, iter, seed, err, s);
+        return launch_sv<In::AMAXC, In::MZC, In::AC, In::MAXT, In::VU>(P, L, ctas, threads, sm, queue, scratch,
+                                                                       sp.band_floats, out, iter, seed, err, s);
     });
+}
+
+int mbir_sv_batch_ctas_per_sm(size_t smem_bytes, bool half)
+{
+    return half ? occupancy_sv<3, 1, 2, kSvBatchThreads, kSvBatchViewsPerLane, true>(kSvBatchThreads, smem_bytes)
+                : occupancy_sv<3, 1, 1, kSvBatchThreads, kSvBatchViewsPerLane, true>(kSvBatchThreads, smem_bytes);
+}
+
+cudaError_t mbir_sv_batch_prepare(size_t smem_bytes, bool half)
+{
+    const int sm = (int)smem_bytes;
+    return half ? cudaFuncSetAttribute(k_icd_sv<3, 1, 2, kSvBatchThreads, kSvBatchViewsPerLane, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sm)
+                : cudaFuncSetAttribute(k_icd_sv<3, 1, 1, kSvBatchThreads, kSvBatchViewsPerLane, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+cudaError_t mbir_launch_icd_sv_batch(size_t smem_bytes, bool half, const SvLaunch &L, int ctas, int *queue,
+                                     float *scratch, size_t scratch_floats, uint32_t seed, int *err, cudaStream_t s)
+{
+    // the problems come from L.problems; the parameter copy is unused
+    const SvProblem none{};
+    if (half)
+        k_icd_sv<3, 1, 2, kSvBatchThreads, kSvBatchViewsPerLane, true><<<ctas, kSvBatchThreads, smem_bytes, s>>>(
+            none, L, queue, scratch, scratch_floats, nullptr, 0, seed, err);
+    else
+        k_icd_sv<3, 1, 1, kSvBatchThreads, kSvBatchViewsPerLane, true><<<ctas, kSvBatchThreads, smem_bytes, s>>>(
+            none, L, queue, scratch, scratch_floats, nullptr, 0, seed, err);
+    return cudaGetLastError();
+}
+
+cudaError_t mbir_launch_sv_batch_end(const SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
+                                     cudaStream_t s)
+{
+    k_sv_batch_end<<<1, 256, 0, s>>>(probs, state, n, ctl, queue);
+    return cudaGetLastError();
 }

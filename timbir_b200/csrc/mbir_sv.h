@@ -38,6 +38,7 @@ struct SvTask {
     int frame, k0, j0, z0, nz;
     int nlines;  // in-mask voxel lines (host-side ordering of the work queue)
     float *mag;  // [N_y][N_x] plane of the magnitude map for (frame, z-group)
+    int prob;    // problem of a batched launch (0 otherwise)
 };
 
 struct SvTaskOut {
@@ -45,6 +46,20 @@ struct SvTaskOut {
     long long updates, zero_skips;
 };
 
+// Shared-memory regions of one CTA for one problem, in elements (a batched
+// launch carves them per task from its problem's plan, within the largest
+// plan's bytes).
+struct SvPlan {
+    int ring_bytes;    // A-column ring
+    int band_pairs;    // (e, sqrt(w)) float2 band entries
+    int trig_views;    // views with cos / sin (computed columns only)
+    int xb, tb, magl;  // voxel block, temporal neighbours, |dx| per (slice, line)
+    int part;          // per-slice theta partials (floats)
+    int views;         // view index / band origin entries
+    int order;         // step-sequence entries
+};
+SvPlan mbir_sv_plan(const SvParams &sp, bool cached);
+size_t mbir_sv_plan_bytes(const SvPlan &pl);
 size_t mbir_sv_smem_bytes(const SvParams &sp, bool cached);
 size_t mbir_acache_bytes(const MbirGeom &g, int eq, bool half);
 // Fills the column cache (exact bin indices, FP32 values) for the in-mask
@@ -61,12 +76,46 @@ cudaError_t mbir_forward_rows(const MbirGeom &g, const int *frame_of_view, const
 // that order.  Super-voxel order[k] first waits until done[d] == epoch for
 // every id d in deps[dep_off[k] .. dep_off[k + 1]) (the conflicting ones
 // earlier in the order), and sets done[order[k]] = epoch when finished.
+struct SvProblem;
+struct SvBatchState;
 struct SvLaunch {
     const SvTask *tasks;
     const int *order, *dep_off, *deps;
     int ntasks;
     int *done;
     int epoch;
+    // batched launches only: the problems, the position of each queue entry
+    // in its problem's own order (seq), per-problem state, and the control
+    // words ctl[0] = iteration number (also the epoch of the done flags)
+    const SvProblem *problems;
+    const int *seq;
+    SvBatchState *state;
+    const int *ctl;
+};
+
+// One problem of a batched launch: its stage's geometry, arrays, prior (the
+// over-relaxation it uses), schedule parameters and column cache.
+struct SvProblem {
+    MbirGeom g;
+    MbirPrior pr;
+    MbirDev dv;
+    SvParams sp;
+    SvACache ac;
+    SvPlan plan;  // shared-memory regions
+    int cap;      // super-voxels in flight at most
+    int K;        // sub-iterations per iteration (scales the convergence ratio)
+    double stop;  // convergence threshold, percent
+};
+
+// Per-problem state of a batched run (device).
+struct SvBatchState {
+    SvTaskOut out;   // this iteration's statistics
+    long long updates, zero_skips;
+    double pct;      // convergence ratio of the last iteration, percent
+    int active;      // still iterating
+    int iters;       // iterations done
+    int converged;   // stopped by the convergence test
+    int fin;         // super-voxels finished in this launch
 };
 
 // CTAs of the super-voxel kernel that fit one SM for this configuration.
@@ -79,3 +128,24 @@ int mbir_sv_ctas_per_sm(const MbirGeom &g, const SvParams &sp, bool cached);
 cudaError_t mbir_launch_icd_sv(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, const SvParams &sp,
                                SvACache ac, const SvLaunch &L, int ctas, int *queue, float *scratch, SvTaskOut *out,
                                int iter, uint32_t seed, int *err, cudaStream_t s);
+
+// Batched launches: every problem has a column cache (FP32 values, or FP16
+// when half), 3 detector columns per entry and one row per slice, at most
+// kSvBatchThreads / 32 warps per super-voxel and kSvBatchViewsPerLane views
+// per lane.  The super-voxel of queue entry k starts when its conflicting
+// super-voxels have finished (as above) and when at most cap - 1 super-voxels
+// of its problem before it are unfinished; super-voxels of problems no
+// longer active are skipped.  The CTA statistics go to state[prob].out;
+// err |= 8: an in-flight wait gave up.
+constexpr int kSvBatchThreads = 256;
+constexpr int kSvBatchViewsPerLane = 8;
+int mbir_sv_batch_ctas_per_sm(size_t smem_bytes, bool half);
+cudaError_t mbir_sv_batch_prepare(size_t smem_bytes, bool half);
+cudaError_t mbir_launch_icd_sv_batch(size_t smem_bytes, bool half, const SvLaunch &L, int ctas, int *queue,
+                                     float *scratch, size_t scratch_floats, uint32_t seed, int *err, cudaStream_t s);
+// End of a batched iteration: per active problem, the iteration's statistics
+// into the totals and the convergence test; then the statistics, in-flight
+// counters and queue counter are reset, ctl[0] (the iteration) advances and
+// ctl[1] = problems still active.
+cudaError_t mbir_launch_sv_batch_end(const SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
+                                     cudaStream_t s);

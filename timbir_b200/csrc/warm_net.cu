@@ -1,0 +1,784 @@
+// Learned warm start: a 3-D encoder-decoder convolutional network that maps a
+// frame's filtered backprojection to a start image for ICD, with its forward,
+// backward and Adam kernels.  No counterpart in the reference (which starts
+// its coarsest stage from zero); ICD still runs to its own convergence from
+// the network's output, so the answer is the MAP estimate either way.
+//
+// Network (channels-last FP32 activations [B][D][H][W][C], BF16 weights and
+// operands on the tensor cores, FP32 accumulation):
+//   level 0 (D x H x W):        conv 16->16, conv 16->16          -> e0
+//   level 1 (/2, average pool): conv 16->32, conv 32->32          -> e1
+//   level 2 (/4):               conv 32->64, conv 64->64          -> e2
+//   level 3 (/8):               conv 64->128, conv 128->128       -> e3
+//   up to level 2 (nearest):    conv 128->64 + e2, conv 64->64    -> d2
+//   up to level 1:              conv 64->32 + e1, conv 32->32     -> d1
+//   up to level 0:              conv 32->16 + e0, conv 16->16     -> d0
+//   output: conv 16->16 (channel 0 used): residual r
+// Every convolution is 3 x 3 x 3, stride 1, zero padding 1, with a bias, and
+// all but the last are followed by ReLU (after the skip addition).  The input
+// is s * fbp in channel 0 of 16 (the others zero), the prediction
+// s * fbp + r, the loss the mean over voxels of (prediction - s * target)^2;
+// s scales attenuation values to order one.
+//
+// Convolutions are implicit GEMMs on mma.sync m16n8k16 (BF16 in, FP32
+// accumulate): forward M = voxels, N = output channels, K = 27 taps x input
+// channels; the input gradient is the same kernel with the flipped,
+// transposed weights; the weight gradient is a GEMM over voxels
+// (M = input channels, N = output channels, K = voxels) split over CTAs and
+// reduced with FP32 atomics.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/timbir_b200.h"
+
+namespace {
+
+constexpr int kLayers = 15;
+constexpr int kCh[kLayers][2] = {{16, 16},  {16, 16},  {16, 32},  {32, 32}, {32, 64},
+                                 {64, 64},  {64, 128}, {128, 128}, {128, 64}, {64, 64},
+                                 {64, 32},  {32, 32},  {32, 16},  {16, 16}, {16, 16}};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct Shape {
+    int B, D, H, W;
+    __host__ __device__ long long voxels() const { return (long long)B * D * H * W; }
+};
+
+// voxel m -> (b, z, y, x); false past the end
+__device__ __forceinline__ bool decode(const Shape &s, long long m, int &b, int &z, int &y, int &x)
+{
+    if (m >= s.voxels()) return false;
+    x = (int)(m % s.W);
+    long long r = m / s.W;
+    y = (int)(r % s.H);
+    r /= s.H;
+    z = (int)(r % s.D);
+    b = (int)(r / s.D);
+    return true;
+}
+
+// Y[m][n] = act(sum over taps and input channels + bias[n] + add[m][n]), or
+// (accumulate) Y[m][n] += the sum.  Wp: packed B fragments, per (tap,
+// 16-channel input chunk, 8-channel output tile) one uint2 per lane.  A warp
+// computes 16 voxels x NT output tiles; a CTA 4 warps.
+template <int NT>
+__global__ void __launch_bounds__(128) k_conv3(const float *__restrict__ X, int Cin, const uint2 *__restrict__ Wp,
+                                               int Cout, const float *__restrict__ bias,
+                                               const float *__restrict__ add, int relu, int accumulate,
+                                               float *__restrict__ Y, Shape s)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long m0 = ((long long)blockIdx.x * 4 + warp) * 16;
+    if (m0 >= s.voxels()) return;
+    const int nt0 = blockIdx.y * NT, ntiles = Cout / 8, KC = Cin / 16;
+    const int g = lane >> 2, tq = lane & 3;
+    int vb[2], vz[2], vy[2], vx[2];
+    bool vin[2];
+    for (int r = 0; r < 2; r++) vin[r] = decode(s, m0 + g + 8 * r, vb[r], vz[r], vy[r], vx[r]);
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+    for (int tap = 0; tap < 27; tap++) {
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        const float *src[2];
+        bool ok[2];
+        for (int r = 0; r < 2; r++) {
+            const int z = vz[r] + dz, y = vy[r] + dy, x = vx[r] + dx;
+            ok[r] = vin[r] && z >= 0 && z < s.D && y >= 0 && y < s.H && x >= 0 && x < s.W;
+            src[r] = ok[r] ? X + ((((size_t)vb[r] * s.D + z) * s.H + y) * s.W + x) * Cin : X;
+        }
+        for (int kc = 0; kc < KC; kc++) {
+            const int c = kc * 16 + 2 * tq;
+            const float2 z2 = make_float2(0.0f, 0.0f);
+            const float2 p0 = ok[0] ? __ldg(reinterpret_cast<const float2 *>(src[0] + c)) : z2;
+            const float2 p1 = ok[1] ? __ldg(reinterpret_cast<const float2 *>(src[1] + c)) : z2;
+            const float2 p2 = ok[0] ? __ldg(reinterpret_cast<const float2 *>(src[0] + c + 8)) : z2;
+            const float2 p3 = ok[1] ? __ldg(reinterpret_cast<const float2 *>(src[1] + c + 8)) : z2;
+            const uint32_t a0 = pack_bf16(p0.x, p0.y), a1 = pack_bf16(p1.x, p1.y);
+            const uint32_t a2 = pack_bf16(p2.x, p2.y), a3 = pack_bf16(p3.x, p3.y);
+            const uint2 *wp = Wp + ((size_t)(tap * KC + kc) * ntiles + nt0) * 32 + lane;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const uint2 bb = __ldg(wp + j * 32);
+                mma_bf16(acc[j], a0, a1, a2, a3, bb.x, bb.y);
+            }
+        }
+    }
+    for (int r = 0; r < 2; r++) {
+        if (!vin[r]) continue;
+        const long long m = m0 + g + 8 * r;
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int n = (nt0 + j) * 8 + 2 * tq;
+            float v0 = acc[j][2 * r], v1 = acc[j][2 * r + 1];
+            if (bias) {
+                v0 += bias[n];
+                v1 += bias[n + 1];
+            }
+            float2 *y = reinterpret_cast<float2 *>(Y + (size_t)m * Cout + n);
+            if (add) {
+                const float2 a = *reinterpret_cast<const float2 *>(add + (size_t)m * Cout + n);
+                v0 += a.x;
+                v1 += a.y;
+            }
+            if (relu) {
+                v0 = fmaxf(v0, 0.0f);
+                v1 = fmaxf(v1, 0.0f);
+            }
+            if (accumulate) {
+                const float2 o = *y;
+                v0 += o.x;
+                v1 += o.y;
+            }
+            *y = make_float2(v0, v1);
+        }
+    }
+}
+
+// dW[tap][ci][co] += sum over voxels m of X[m shifted by tap][ci] dY[m][co],
+// tap = blockIdx.y, voxels [blockIdx.x * chunk, + chunk); warp w: input
+// channels 16 (w % (Cin / 16)) .. + 16, output tiles NT (w / (Cin / 16)) ...
+template <int NT>
+__global__ void __launch_bounds__(512) k_wgrad3(const float *__restrict__ X, int Cin,
+                                                const float *__restrict__ dY, int Cout, float *__restrict__ dW,
+                                                Shape s, long long chunk)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tap = blockIdx.y;
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int ci_tiles = Cin / 16;
+    const int ci0 = (warp % ci_tiles) * 16, nt0 = (warp / ci_tiles) * NT;
+    const int g = lane >> 2, tq = lane & 3;
+    const long long M = s.voxels();
+    const long long start = (long long)blockIdx.x * chunk, end = min(M, start + chunk);
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+    for (long long m0 = start; m0 < end; m0 += 16) {
+        // the four voxels of this thread's fragment columns: m0 + 2 tq + {0, 1, 8, 9}
+        float xa[4], xb[4];  // X at input channels ci0 + g, ci0 + g + 8
+        size_t yo[4];        // dY row offsets (unshifted)
+        bool yv[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const long long m = m0 + 2 * tq + (q & 1) + 8 * (q >> 1);
+            int b, z, y, x;
+            xa[q] = xb[q] = 0.0f;
+            yv[q] = m < end && decode(s, m, b, z, y, x);
+            yo[q] = (size_t)m * Cout;
+            if (yv[q]) {
+                const int zz = z + dz, yy = y + dy, xx = x + dx;
+                if (zz >= 0 && zz < s.D && yy >= 0 && yy < s.H && xx >= 0 && xx < s.W) {
+                    const float *p = X + ((((size_t)b * s.D + zz) * s.H + yy) * s.W + xx) * Cin + ci0 + g;
+                    xa[q] = __ldg(p);
+                    xb[q] = __ldg(p + 8);
+                }
+            }
+        }
+        // A[ci][m]: rows ci0 + g (a0, a1) and + 8 (a2, a3), columns 2 tq (+1)
+        // for a0..a3 and 2 tq + 8 (+1) for a4..a7
+        const uint32_t a0 = pack_bf16(xa[0], xa[1]), a1 = pack_bf16(xb[0], xb[1]);
+        const uint32_t a2 = pack_bf16(xa[2], xa[3]), a3 = pack_bf16(xb[2], xb[3]);
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int co = (nt0 + j) * 8 + g;
+            const float y0 = yv[0] ? __ldg(dY + yo[0] + co) : 0.0f, y1 = yv[1] ? __ldg(dY + yo[1] + co) : 0.0f;
+            const float y2 = yv[2] ? __ldg(dY + yo[2] + co) : 0.0f, y3 = yv[3] ? __ldg(dY + yo[3] + co) : 0.0f;
+            mma_bf16(acc[j], a0, a1, a2, a3, pack_bf16(y0, y1), pack_bf16(y2, y3));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        const int co = (nt0 + j) * 8 + 2 * tq;
+        float *w0 = dW + ((size_t)tap * Cin + ci0 + g) * Cout + co;
+        float *w1 = w0 + (size_t)8 * Cout;
+        atomicAdd(w0, acc[j][0]);
+        atomicAdd(w0 + 1, acc[j][1]);
+        atomicAdd(w1, acc[j][2]);
+        atomicAdd(w1 + 1, acc[j][3]);
+    }
+}
+
+// db[c] += sum over voxels of dY[m][c]
+__global__ void k_bias_grad(const float *__restrict__ dY, int C, long long M, long long chunk, float *__restrict__ db)
+{
+    const int c = threadIdx.x % C;
+    const int lanes = blockDim.x / C;
+    const int l = threadIdx.x / C;
+    if (l >= lanes) return;
+    const long long start = (long long)blockIdx.x * chunk, end = min(M, start + chunk);
+    float acc = 0.0f;
+    for (long long m = start + l; m < end; m += lanes) acc += dY[(size_t)m * C + c];
+    atomicAdd(db + c, acc);
+}
+
+// Packed B fragments of a layer: forward (K = cin, N = cout, element
+// W[tap][k][n]) or input gradient (K = cout, N = cin, element
+// W[26 - tap][n][k]: the flipped, transposed kernel).
+__global__ void k_pack(const float *__restrict__ W, int cin, int cout, int flip, uint2 *__restrict__ out)
+{
+    const int K = flip ? cout : cin, N = flip ? cin : cout;
+    const int KC = K / 16, NTL = N / 8;
+    const long long total = 27LL * KC * NTL * 32;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int lane = (int)(i % 32);
+    long long r = i / 32;
+    const int nt = (int)(r % NTL);
+    r /= NTL;
+    const int kc = (int)(r % KC);
+    const int tap = (int)(r / KC);
+    const int g = lane >> 2, tq = lane & 3;
+    const int n = nt * 8 + g, k = kc * 16 + 2 * tq;
+    auto val = [&](int kk) {
+        return flip ? W[((size_t)(26 - tap) * cin + n) * cout + kk] : W[((size_t)tap * cin + kk) * cout + n];
+    };
+    out[i] = make_uint2(pack_bf16(val(k), val(k + 1)), pack_bf16(val(k + 8), val(k + 9)));
+}
+
+// dA *= (A > 0): the ReLU's gradient mask
+__global__ void k_relu_mask(float *__restrict__ dA, const float *__restrict__ A, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !(A[i] > 0.0f)) dA[i] = 0.0f;
+}
+
+// 2 x 2 x 2 average pooling; forward fine -> coarse, backward coarse -> fine
+// (accumulate adds to the fine gradient)
+__global__ void k_pool(const float *__restrict__ X, float *__restrict__ Y, Shape c, int C)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.voxels() * C) return;
+    const int ch = (int)(i % C);
+    int b, z, y, x;
+    decode(c, i / C, b, z, y, x);
+    const Shape f{c.B, 2 * c.D, 2 * c.H, 2 * c.W};
+    float s = 0.0f;
+    for (int q = 0; q < 8; q++) {
+        const int zz = 2 * z + (q >> 2), yy = 2 * y + ((q >> 1) & 1), xx = 2 * x + (q & 1);
+        s += X[((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch];
+    }
+    Y[i] = 0.125f * s;
+}
+
+__global__ void k_pool_bwd(const float *__restrict__ dY, float *__restrict__ dX, Shape f, int C, int accumulate)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= f.voxels() * C) return;
+    const int ch = (int)(i % C);
+    int b, z, y, x;
+    decode(f, i / C, b, z, y, x);
+    const Shape c{f.B, f.D / 2, f.H / 2, f.W / 2};
+    const float v = 0.125f * dY[((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch];
+    dX[i] = accumulate ? dX[i] + v : v;
+}
+
+// nearest-neighbour x2 up-sampling; backward sums the 8 fine gradients
+__global__ void k_up(const float *__restrict__ X, float *__restrict__ Y, Shape f, int C)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= f.voxels() * C) return;
+    const int ch = (int)(i % C);
+    int b, z, y, x;
+    decode(f, i / C, b, z, y, x);
+    const Shape c{f.B, f.D / 2, f.H / 2, f.W / 2};
+    Y[i] = X[((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch];
+}
+
+__global__ void k_up_bwd(const float *__restrict__ dY, float *__restrict__ dX, Shape c, int C)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.voxels() * C) return;
+    const int ch = (int)(i % C);
+    int b, z, y, x;
+    decode(c, i / C, b, z, y, x);
+    const Shape f{c.B, 2 * c.D, 2 * c.H, 2 * c.W};
+    float s = 0.0f;
+    for (int q = 0; q < 8; q++) {
+        const int zz = 2 * z + (q >> 2), yy = 2 * y + ((q >> 1) & 1), xx = 2 * x + (q & 1);
+        s += dY[((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch];
+    }
+    dX[i] = s;
+}
+
+// network input: channel 0 = s * in, channels 1..15 = 0
+__global__ void k_input(const float *__restrict__ in, float s, float *__restrict__ X0, long long M)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M * 16) return;
+    X0[i] = (i % 16) == 0 ? s * in[i / 16] : 0.0f;
+}
+
+// out = in + r / s (r = channel 0 of the last layer)
+__global__ void k_output(const float *__restrict__ in, const float *__restrict__ Z, float s, float *__restrict__ out,
+                         long long M)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M) out[i] = in[i] + Z[(size_t)i * 16] / s;
+}
+
+// loss = mean (s in + r - s t)^2; dZ channel 0 = its gradient, others 0;
+// per-block partial sums (FP64) into part
+__global__ void __launch_bounds__(256) k_loss(const float *__restrict__ in, const float *__restrict__ t,
+                                              const float *__restrict__ Z, float s, float *__restrict__ dZ,
+                                              long long M, double *__restrict__ part)
+{
+    __shared__ double red[256];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (i < M) {
+        const float d = s * in[i] + Z[(size_t)i * 16] - s * t[i];
+        l = (double)d * d;
+        float *g = dZ + (size_t)i * 16;
+        g[0] = 2.0f * d / (float)M;
+        for (int c = 1; c < 16; c++) g[c] = 0.0f;
+    }
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// Adam (Kingma and Ba, 2015) on the FP32 master parameters
+__global__ void k_adam(float *__restrict__ p, const float *__restrict__ gr, float *__restrict__ m,
+                       float *__restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                       float c2)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = gr[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// He-normal initial weights (Box-Muller on a counter hash), zero biases
+__device__ __forceinline__ uint32_t mix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__global__ void k_init(float *__restrict__ W, long long n, float stdv, uint32_t seed)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t h1 = mix32(seed ^ mix32((uint32_t)i * 2u + 1u));
+    const uint32_t h2 = mix32(seed ^ mix32((uint32_t)i * 2u + 2u) ^ 0x9e3779b9u);
+    const float u1 = ((h1 >> 8) + 1.0f) * (1.0f / 16777217.0f);
+    const float u2 = (h2 >> 8) * (1.0f / 16777216.0f);
+    W[i] = stdv * sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+inline int blocks(long long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static thread_local char g_net_err[512];
+
+static int net_fail(const char *msg, cudaError_t e = cudaSuccess)
+{
+    snprintf(g_net_err, sizeof g_net_err, "%s%s%s", msg, e != cudaSuccess ? ": " : "",
+             e != cudaSuccess ? cudaGetErrorString(e) : "");
+    return -1;
+}
+
+#define NK(call)                                                             \
+    do {                                                                     \
+        cudaError_t _e = (call);                                             \
+        if (_e != cudaSuccess) return net_fail(#call, _e);                   \
+    } while (0)
+
+struct NetTensor {
+    float *p = nullptr;
+    size_t n = 0;
+};
+
+struct MbirNet {
+    size_t w_off[kLayers], b_off[kLayers], nparams = 0, pack_off[kLayers], dpack_off[kLayers], npack = 0;
+    float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
+    uint2 *pack = nullptr;  // forward and input-gradient fragments of every layer
+    long long step = 0;
+    Shape shape{0, 0, 0, 0};
+    // activations: X0 (input), A[k] (layer outputs), P1..P3 (pooled), U0..U2 (up-sampled)
+    std::vector<NetTensor> act, grad;
+    double *part = nullptr;
+    size_t npart = 0;
+    ~MbirNet()
+    {
+        for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)pack, (void *)part})
+            if (q) cudaFree(q);
+        for (auto &t : act)
+            if (t.p) cudaFree(t.p);
+        for (auto &t : grad)
+            if (t.p) cudaFree(t.p);
+    }
+};
+
+// tensor slots
+enum { T_X0 = 0, T_A0 = 1, /* A0..A14 = 1..15 */ T_P1 = 16, T_P2, T_P3, T_U2, T_U1, T_U0, T_COUNT };
+
+static Shape level_shape(const Shape &s, int lv) { return Shape{s.B, s.D >> lv, s.H >> lv, s.W >> lv}; }
+
+// level and channels of each tensor slot
+static void slot_info(int t, int &lv, int &C)
+{
+    static const int layer_level[kLayers] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0, 0};
+    if (t == T_X0) {
+        lv = 0;
+        C = 16;
+    } else if (t >= T_A0 && t < T_A0 + kLayers) {
+        lv = layer_level[t - T_A0];
+        C = kCh[t - T_A0][1];
+    } else if (t == T_P1 || t == T_P2 || t == T_P3) {
+        lv = t - T_P1 + 1;
+        C = kCh[2 * (t - T_P1) + 1][1];
+    } else {  // U2, U1, U0: up-sampled to levels 2, 1, 0
+        lv = 2 - (t - T_U2);
+        C = kCh[7 + 2 * (t - T_U2)][1];
+    }
+}
+
+static int net_shape(MbirNet *N, const Shape &s, bool train)
+{
+    if (s.B == N->shape.B && s.D == N->shape.D && s.H == N->shape.H && s.W == N->shape.W &&
+        (!train || !N->grad.empty()))
+        return 0;
+    if (s.D % 8 || s.H % 8 || s.W % 8 || s.B < 1)
+        return net_fail("network input sides must be multiples of 8");
+    for (auto &t : N->act)
+        if (t.p) cudaFree(t.p);
+    for (auto &t : N->grad)
+        if (t.p) cudaFree(t.p);
+    N->act.assign(T_COUNT, {});
+    N->grad.clear();
+    if (train) N->grad.assign(T_COUNT, {});
+    for (int t = 0; t < T_COUNT; t++) {
+        int lv, C;
+        slot_info(t, lv, C);
+        const size_t n = (size_t)level_shape(s, lv).voxels() * C;
+        NK(cudaMalloc(&N->act[t].p, n * sizeof(float)));
+        N->act[t].n = n;
+        if (train) {
+            NK(cudaMalloc(&N->grad[t].p, n * sizeof(float)));
+            N->grad[t].n = n;
+        }
+    }
+    const size_t np = (size_t)blocks(s.voxels());
+    if (np > N->npart) {
+        if (N->part) cudaFree(N->part);
+        NK(cudaMalloc(&N->part, np * sizeof(double)));
+        N->npart = np;
+    }
+    N->shape = s;
+    return 0;
+}
+
+static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, const float *bias, const float *add,
+                        int relu, int accumulate, float *Y, const Shape &s, cudaStream_t st)
+{
+    const int NT = std::min(cout / 8, 8);
+    const dim3 grid((unsigned)((s.voxels() + 63) / 64), (unsigned)(cout / 8 / NT));
+    switch (NT) {
+    case 1: k_conv3<1><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    case 2: k_conv3<2><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    case 4: k_conv3<4><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    default: k_conv3<8><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, float *dW, float *db, const Shape &s,
+                         cudaStream_t st)
+{
+    const int NT = std::min(cout / 8, 8);
+    const int warps = (cin / 16) * (cout / 8 / NT);
+    const long long M = s.voxels();
+    long long nch = std::max(1LL, std::min(M / 512, 160LL));
+    long long chunk = (M + nch - 1) / nch;
+    chunk = (chunk + 15) / 16 * 16;
+    nch = (M + chunk - 1) / chunk;
+    const dim3 grid((unsigned)nch, 27);
+    switch (NT) {
+    case 1: k_wgrad3<1><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
+    case 2: k_wgrad3<2><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
+    case 4: k_wgrad3<4><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
+    default: k_wgrad3<8><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const long long bch = std::max(1LL, std::min(M / 1024, 1024LL));
+    const long long bchunk = (M + bch - 1) / bch;
+    k_bias_grad<<<(unsigned)bch, 256, 0, st>>>(dY, cout, M, bchunk, db);
+    return cudaGetLastError();
+}
+
+static int pack_all(MbirNet *N, cudaStream_t st)
+{
+    for (int k = 0; k < kLayers; k++) {
+        const int ci = kCh[k][0], co = kCh[k][1];
+        const long long nf = 27LL * (ci / 16) * (co / 8) * 32;
+        k_pack<<<blocks(nf), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->pack + N->pack_off[k]);
+        NK(cudaGetLastError());
+        if (k > 0) {
+            const long long nb = 27LL * (co / 16) * (ci / 8) * 32;
+            k_pack<<<blocks(nb), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1, N->pack + N->dpack_off[k]);
+            NK(cudaGetLastError());
+        }
+    }
+    return 0;
+}
+
+static int forward(MbirNet *N, const float *in, float scale, cudaStream_t st)
+{
+    const Shape s = N->shape;
+    auto &A = N->act;
+    const long long M = s.voxels();
+    k_input<<<blocks(M * 16), 256, 0, st>>>(in, scale, A[T_X0].p, M);
+    NK(cudaGetLastError());
+    auto L = [&](int k, const float *x, const float *add, int relu, const Shape &sh) {
+        return conv(x, kCh[k][0], N->pack + N->pack_off[k], kCh[k][1], N->params + N->b_off[k], add, relu, 0,
+                    A[T_A0 + k].p, sh, st);
+    };
+    const Shape s1 = level_shape(s, 1), s2 = level_shape(s, 2), s3 = level_shape(s, 3);
+    NK(L(0, A[T_X0].p, nullptr, 1, s));
+    NK(L(1, A[T_A0 + 0].p, nullptr, 1, s));
+    k_pool<<<blocks(s1.voxels() * 16), 256, 0, st>>>(A[T_A0 + 1].p, A[T_P1].p, s1, 16);
+    NK(L(2, A[T_P1].p, nullptr, 1, s1));
+    NK(L(3, A[T_A0 + 2].p, nullptr, 1, s1));
+    k_pool<<<blocks(s2.voxels() * 32), 256, 0, st>>>(A[T_A0 + 3].p, A[T_P2].p, s2, 32);
+    NK(L(4, A[T_P2].p, nullptr, 1, s2));
+    NK(L(5, A[T_A0 + 4].p, nullptr, 1, s2));
+    k_pool<<<blocks(s3.voxels() * 64), 256, 0, st>>>(A[T_A0 + 5].p, A[T_P3].p, s3, 64);
+    NK(L(6, A[T_P3].p, nullptr, 1, s3));
+    NK(L(7, A[T_A0 + 6].p, nullptr, 1, s3));
+    k_up<<<blocks(s2.voxels() * 128), 256, 0, st>>>(A[T_A0 + 7].p, A[T_U2].p, s2, 128);
+    NK(L(8, A[T_U2].p, A[T_A0 + 5].p, 1, s2));
+    NK(L(9, A[T_A0 + 8].p, nullptr, 1, s2));
+    k_up<<<blocks(s1.voxels() * 64), 256, 0, st>>>(A[T_A0 + 9].p, A[T_U1].p, s1, 64);
+    NK(L(10, A[T_U1].p, A[T_A0 + 3].p, 1, s1));
+    NK(L(11, A[T_A0 + 10].p, nullptr, 1, s1));
+    k_up<<<blocks(s.voxels() * 32), 256, 0, st>>>(A[T_A0 + 11].p, A[T_U0].p, s, 32);
+    NK(L(12, A[T_U0].p, A[T_A0 + 1].p, 1, s));
+    NK(L(13, A[T_A0 + 12].p, nullptr, 1, s));
+    NK(L(14, A[T_A0 + 13].p, nullptr, 0, s));
+    return 0;
+}
+
+// Gradients of the loss with respect to every parameter into N->grads
+// (zeroed here); dZ of the last layer must already be in grad[A14].
+static int backward(MbirNet *N, cudaStream_t st)
+{
+    const Shape s = N->shape, s1 = level_shape(s, 1), s2 = level_shape(s, 2), s3 = level_shape(s, 3);
+    auto &A = N->act;
+    auto &G = N->grad;
+    NK(cudaMemsetAsync(N->grads, 0, N->nparams * sizeof(float), st));
+    // layer k: weight and bias gradients from its input x and output
+    // gradient dz; the input gradient (into dx, optionally accumulated)
+    auto layer = [&](int k, const float *x, const Shape &sh, float *dx, int acc) -> int {
+        const float *dz = G[T_A0 + k].p;
+        NK(wgrad(x, kCh[k][0], dz, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, st));
+        if (dx)
+            NK(conv(dz, kCh[k][1], N->pack + N->dpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, st));
+        return 0;
+    };
+    auto mask = [&](int t) -> int {  // dA -> dZ of a ReLU output
+        k_relu_mask<<<blocks((long long)A[t].n), 256, 0, st>>>(G[t].p, A[t].p, (long long)A[t].n);
+        NK(cudaGetLastError());
+        return 0;
+    };
+    if (layer(14, A[T_A0 + 13].p, s, G[T_A0 + 13].p, 0) || mask(T_A0 + 13)) return -1;
+    if (layer(13, A[T_A0 + 12].p, s, G[T_A0 + 12].p, 0) || mask(T_A0 + 12)) return -1;
+    // layer 12: input U0, skip from A1 (its gradient seeds dA1)
+    if (layer(12, A[T_U0].p, s, G[T_U0].p, 0)) return -1;
+    NK(cudaMemcpyAsync(G[T_A0 + 1].p, G[T_A0 + 12].p, A[T_A0 + 1].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s1.voxels() * 32), 256, 0, st>>>(G[T_U0].p, G[T_A0 + 11].p, s1, 32);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 11)) return -1;
+    if (layer(11, A[T_A0 + 10].p, s1, G[T_A0 + 10].p, 0) || mask(T_A0 + 10)) return -1;
+    if (layer(10, A[T_U1].p, s1, G[T_U1].p, 0)) return -1;
+    NK(cudaMemcpyAsync(G[T_A0 + 3].p, G[T_A0 + 10].p, A[T_A0 + 3].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s2.voxels() * 64), 256, 0, st>>>(G[T_U1].p, G[T_A0 + 9].p, s2, 64);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 9)) return -1;
+    if (layer(9, A[T_A0 + 8].p, s2, G[T_A0 + 8].p, 0) || mask(T_A0 + 8)) return -1;
+    if (layer(8, A[T_U2].p, s2, G[T_U2].p, 0)) return -1;
+    NK(cudaMemcpyAsync(G[T_A0 + 5].p, G[T_A0 + 8].p, A[T_A0 + 5].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s3.voxels() * 128), 256, 0, st>>>(G[T_U2].p, G[T_A0 + 7].p, s3, 128);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 7)) return -1;
+    if (layer(7, A[T_A0 + 6].p, s3, G[T_A0 + 6].p, 0) || mask(T_A0 + 6)) return -1;
+    if (layer(6, A[T_P3].p, s3, G[T_P3].p, 0)) return -1;
+    k_pool_bwd<<<blocks(s2.voxels() * 64), 256, 0, st>>>(G[T_P3].p, G[T_A0 + 5].p, s2, 64, 1);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 5)) return -1;
+    if (layer(5, A[T_A0 + 4].p, s2, G[T_A0 + 4].p, 0) || mask(T_A0 + 4)) return -1;
+    if (layer(4, A[T_P2].p, s2, G[T_P2].p, 0)) return -1;
+    k_pool_bwd<<<blocks(s1.voxels() * 32), 256, 0, st>>>(G[T_P2].p, G[T_A0 + 3].p, s1, 32, 1);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 3)) return -1;
+    if (layer(3, A[T_A0 + 2].p, s1, G[T_A0 + 2].p, 0) || mask(T_A0 + 2)) return -1;
+    if (layer(2, A[T_P1].p, s1, G[T_P1].p, 0)) return -1;
+    k_pool_bwd<<<blocks(s.voxels() * 16), 256, 0, st>>>(G[T_P1].p, G[T_A0 + 1].p, s, 16, 1);
+    NK(cudaGetLastError());
+    if (mask(T_A0 + 1)) return -1;
+    if (layer(1, A[T_A0 + 0].p, s, G[T_A0 + 0].p, 0) || mask(T_A0 + 0)) return -1;
+    if (layer(0, A[T_X0].p, s, nullptr, 0)) return -1;
+    return 0;
+}
+
+extern "C" {
+
+const char *mbir_net_last_error(void) { return g_net_err; }
+
+int64_t mbir_net_param_count(void)
+{
+    int64_t n = 0;
+    for (int k = 0; k < kLayers; k++) n += 27LL * kCh[k][0] * kCh[k][1] + kCh[k][1];
+    return n;
+}
+
+int mbir_net_create(MbirNet **out, uint32_t seed)
+{
+    *out = nullptr;
+    auto N = std::make_unique<MbirNet>();
+    size_t off = 0, poff = 0;
+    for (int k = 0; k < kLayers; k++) {
+        const int ci = kCh[k][0], co = kCh[k][1];
+        N->w_off[k] = off;
+        off += 27 * (size_t)ci * co;
+        N->b_off[k] = off;
+        off += co;
+        N->pack_off[k] = poff;
+        poff += 27 * (size_t)(ci / 16) * (co / 8) * 32;
+        N->dpack_off[k] = poff;
+        if (k > 0) poff += 27 * (size_t)(co / 16) * (ci / 8) * 32;
+    }
+    N->nparams = off;
+    N->npack = poff;
+    NK(cudaMalloc(&N->params, off * sizeof(float)));
+    NK(cudaMalloc(&N->grads, off * sizeof(float)));
+    NK(cudaMalloc(&N->m, off * sizeof(float)));
+    NK(cudaMalloc(&N->v, off * sizeof(float)));
+    NK(cudaMalloc(&N->pack, poff * sizeof(uint2)));
+    NK(cudaMemset(N->params, 0, off * sizeof(float)));
+    NK(cudaMemset(N->grads, 0, off * sizeof(float)));
+    NK(cudaMemset(N->m, 0, off * sizeof(float)));
+    NK(cudaMemset(N->v, 0, off * sizeof(float)));
+    for (int k = 0; k < kLayers; k++) {
+        const long long n = 27LL * kCh[k][0] * kCh[k][1];
+        // He initialisation for ReLU layers; the output layer starts small
+        // so that the untrained network returns about its input
+        const float stdv = k == kLayers - 1 ? 1e-3f : sqrtf(2.0f / (27.0f * kCh[k][0]));
+        k_init<<<blocks(n), 256>>>(N->params + N->w_off[k], n, stdv, seed * 2654435761u + (uint32_t)k);
+        NK(cudaGetLastError());
+    }
+    if (pack_all(N.get(), 0)) return -1;
+    NK(cudaDeviceSynchronize());
+    *out = N.release();
+    return 0;
+}
+
+void mbir_net_free(MbirNet *net) { delete net; }
+
+int mbir_net_get_params(MbirNet *N, float *out)
+{
+    NK(cudaMemcpy(out, N->params, N->nparams * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mbir_net_set_params(MbirNet *N, const float *in)
+{
+    NK(cudaMemcpy(N->params, in, N->nparams * sizeof(float), cudaMemcpyHostToDevice));
+    if (pack_all(N, 0)) return -1;
+    NK(cudaDeviceSynchronize());
+    return 0;
+}
+
+int mbir_net_get_grads(MbirNet *N, float *out)
+{
+    NK(cudaMemcpy(out, N->grads, N->nparams * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mbir_net_forward(MbirNet *N, const float *in, float *out, int32_t B, int32_t D, int32_t H, int32_t W,
+                     float scale, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (net_shape(N, Shape{B, D, H, W}, false) || forward(N, in, scale, st)) return -1;
+    const long long M = N->shape.voxels();
+    k_output<<<blocks(M), 256, 0, st>>>(in, N->act[T_A0 + 14].p, scale, out, M);
+    NK(cudaGetLastError());
+    NK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t B, int32_t D, int32_t H, int32_t W,
+                       float scale, double *loss, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (net_shape(N, Shape{B, D, H, W}, true) || forward(N, in, scale, st)) return -1;
+    const long long M = N->shape.voxels();
+    const int nb = blocks(M);
+    k_loss<<<nb, 256, 0, st>>>(in, target, N->act[T_A0 + 14].p, scale, N->grad[T_A0 + 14].p, M, N->part);
+    NK(cudaGetLastError());
+    if (backward(N, st)) return -1;
+    std::vector<double> part(nb);
+    NK(cudaMemcpyAsync(part.data(), N->part, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    NK(cudaStreamSynchronize(st));
+    double l = 0;
+    for (double v : part) l += v;
+    if (loss) *loss = l / (double)M;
+    return 0;
+}
+
+int mbir_net_adam_step(MbirNet *N, float lr, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const float b1 = 0.9f, b2 = 0.999f;
+    N->step++;
+    const float c1 = 1.0f - powf(b1, (float)N->step), c2 = 1.0f - powf(b2, (float)N->step);
+    k_adam<<<blocks((long long)N->nparams), 256, 0, st>>>(N->params, N->grads, N->m, N->v, (long long)N->nparams, lr,
+                                                          b1, b2, 1e-8f, c1, c2);
+    NK(cudaGetLastError());
+    if (pack_all(N, st)) return -1;
+    return 0;
+}
+
+}  // extern "C"

@@ -180,6 +180,102 @@ def ellipsoid_scan(n_xy: int = 64, rows: int = 4, views: int = 96, I0: float = 1
     return Scan(proj, wts, angles, times, recon_times, rows, n_xy, views, 1, vox_wid, rc, vol)
 
 
+def _torch_line_integrals(ell: np.ndarray, angles: np.ndarray, cols: int, rows: int, vox_wid: float,
+                          rot_center: float, n_xy: int, oversample: int, device: str) -> np.ndarray:
+    """ellipsoid_sinogram's exact line integrals evaluated with torch (FP64)
+    on `device`, a chunk of views at a time."""
+    import torch
+    half = n_xy * vox_wid / 2.0
+    scale_z = rows * vox_wid / 2.0
+    sub = (torch.arange(oversample, dtype=torch.float64, device=device) + 0.5) / oversample - 0.5
+    r = ((torch.arange(cols, dtype=torch.float64, device=device)[:, None] + 0.5 + sub[None, :] - rot_center)
+         * vox_wid).reshape(-1)
+    z = (torch.arange(rows, dtype=torch.float64, device=device) + 0.5) * vox_wid - scale_z
+    th_all = torch.as_tensor(angles.astype(np.float64), device=device)
+    out = np.zeros((len(angles), rows, cols))
+    chunk = max(1, int(2e7 // max(1, rows * cols * oversample)))
+    for v0 in range(0, len(angles), chunk):
+        th = th_all[v0:v0 + chunk, None]
+        nx, ny = torch.cos(th), -torch.sin(th)
+        acc = torch.zeros((th.shape[0], rows, cols * oversample), dtype=torch.float64, device=device)
+        for cx, cy, cz, a, b, c, phi, rho in ell:
+            zz = (z / scale_z - cz) / c
+            f = torch.clamp(1.0 - zz ** 2, min=0.0)
+            live = f > 0
+            if not bool(live.any()):
+                continue
+            A = a * half * torch.sqrt(f)
+            B = b * half * torch.sqrt(f)
+            nu = nx * np.cos(phi) + ny * np.sin(phi)
+            nv = -nx * np.sin(phi) + ny * np.cos(phi)
+            s0 = nx * (cx * half) + ny * (cy * half)
+            h2 = (A[None, :, None] ** 2) * (nu[:, :, None] ** 2) + (B[None, :, None] ** 2) * (nv[:, :, None] ** 2)
+            s = r[None, None, :] - s0[:, :, None]
+            val = 2.0 * (A * B)[None, :, None] / h2 * torch.sqrt(torch.clamp(h2 - s ** 2, min=0.0))
+            val = torch.nan_to_num(val) * live[None, :, None]
+            acc += rho * val
+        out[v0:v0 + chunk] = acc.reshape(th.shape[0], rows, cols, oversample).mean(dim=3).cpu().numpy()
+    return out
+
+
+def _torch_volume_max(ell: np.ndarray, n_xy: int, n_z: int, vox_wid: float, rot_center: float,
+                      device: str) -> float:
+    """Maximum of ellipsoid_volume's voxelised phantom, evaluated with torch
+    one slice at a time."""
+    import torch
+    half = n_xy * vox_wid / 2.0
+    k = torch.arange(n_xy, dtype=torch.float64, device=device)
+    x = (k + 0.5 - rot_center) * vox_wid
+    y = (k + 0.5) * vox_wid - half
+    Y, X = torch.meshgrid(y, x, indexing="ij")
+    scale_z = n_z * vox_wid / 2.0
+    best = 0.0
+    for iz in range(n_z):
+        zc = (iz + 0.5) * vox_wid - scale_z
+        vol = torch.zeros_like(X)
+        for cx, cy, cz, a, b, c, phi, rho in ell:
+            xr = X / half - cx
+            yr = Y / half - cy
+            zr = zc / scale_z - cz
+            u = xr * np.cos(phi) + yr * np.sin(phi)
+            v = -xr * np.sin(phi) + yr * np.cos(phi)
+            vol += rho * (((u / a) ** 2 + (v / b) ** 2 + (zr / c) ** 2) <= 1.0)
+        best = max(best, float(vol.max()))
+    return best
+
+
+def ellipsoid_scan_device(n_xy: int, rows: int, views: int, I0: float = 1e4, n_ell: int = 10, seed: int = 0,
+                          vmax: float = 0.02, device: str = "cuda") -> Scan:
+    """ellipsoid_scan's scan (same seeded ellipsoids, exact line integrals,
+    Poisson counts drawn on the host from the same generator) with the line
+    integrals and the density normalisation evaluated by torch on `device`;
+    no phantom volume is kept.  For the many-problem workloads, whose numpy
+    evaluation would take minutes."""
+    rng = np.random.default_rng(seed)
+    rc = n_xy / 2.0
+    ell = random_ellipsoids(n_ell, rng, vmax)
+    ell[:, 7] *= vmax / _torch_volume_max(ell, n_xy, rows, 1.0, rc, device)
+    angles = (np.arange(views) * np.pi / views).astype(np.float32)
+    li = _torch_line_integrals(ell, angles, n_xy, rows, 1.0, rc, n_xy, 4, device)
+    proj, wts = counts_to_data(li, I0, rng)
+    times = np.arange(views, dtype=np.float32)
+    recon_times = np.array([0.0, float(views)], dtype=np.float32)
+    return Scan(proj, wts, angles, times, recon_times, rows, n_xy, views, 1, 1.0, rc, None)
+
+
+def batch_problem_specs(n: int = 64, seed: int = 0, sides=(128, 192, 256, 384, 512)) -> list:
+    """Seeded sizes of a many-problem workload: side drawn uniformly from
+    `sides`, an even number of slices in [4, 32], views = 1.5 x side over
+    180 degrees, I0 log-uniform in [2e3, 5e4]; problem k uses seed k."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        side = int(rng.choice(sides))
+        out.append(dict(side=side, slices=2 * int(rng.integers(2, 17)), views=(3 * side) // 2,
+                        I0=float(np.exp(rng.uniform(np.log(2e3), np.log(5e4)))), seed=k))
+    return out
+
+
 def interlaced_angles(K: int, n_views: int, views_per_rotation: int) -> np.ndarray:
     """Interlaced view schedule: each rotation of `views_per_rotation` views is
     split in K sub-frames whose angular offsets follow the bit-reversal of the
