@@ -310,7 +310,7 @@ def c3_sample_workload(specs):
     return k, w
 
 
-def c3_build(specs, scans, tuned=None):
+def c3_build(specs, scans, tuned=None, autotune=True):
     """Stages of the batch (column cache, super-voxel schedule, prepared from
     zero); with `tuned` = {side: autotuner result} the schedule of each size
     is the tuned one, otherwise the representative of each size (most slices)
@@ -327,7 +327,14 @@ def c3_build(specs, scans, tuned=None):
         sp = specs[k]
         st = timbir_b200.Stage(scans[k], **C3_PRIOR, blocks=2)
         t = (tuned or tune).get(sp["side"])
-        if t is None:
+        if t is None and not autotune:
+            st.set_batch_schedule(0, 1, 1)
+            st.prepare()
+            info = st.schedule_info()
+            t = {"sv_side": info["sv_side"], "warps_per_slice": info["warps_per_slice"],
+                 "z_group": info["z_group"], "band_width": info["band_width"], "ns_per_update": 0.0}
+            tune[sp["side"]] = t
+        elif t is None:
             st.set_batch_schedule(0, 1, 1)
             st.prepare()
             t = st.autotune()
@@ -343,13 +350,13 @@ def c3_arm(args, rank, world, local_rank):
     import torch
     import timbir_b200
     torch.cuda.set_device(local_rank)
-    specs = synth.batch_problem_specs(64, 0)
+    specs = synth.batch_problem_specs(64, 0)[:args.problems]
     t0 = time.perf_counter()
     scans = [synth.ellipsoid_scan_device(sp["side"], sp["slices"], sp["views"], I0=sp["I0"], seed=sp["seed"],
                                          device="cuda") for sp in specs]
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    stages, tuned = c3_build(specs, scans)
+    stages, tuned = c3_build(specs, scans, autotune=not args.no_tune)
     setup_s = time.perf_counter() - t0
     cbar = {}
     for k, sp in enumerate(specs):
@@ -442,7 +449,8 @@ def c3_arm(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (A-matrix bin indices exact in FP64; convergence sums FP64)", "data": C3_DATA,
-        "config": {"workload": C3_DESC, "problems": len(specs), "voxels": int(sum(sp["side"] ** 2 * sp["slices"]
+        "config": {"workload": C3_DESC + ("" if len(specs) == 64 else f"; the first {len(specs)} problems only")
+                   + ("; default schedules, not autotuned" if args.no_tune else ""), "problems": len(specs), "voxels": int(sum(sp["side"] ** 2 * sp["slices"]
                                                                              for sp in specs)),
                    "schedule": "batched super-voxel (one persistent launch + one end kernel per iteration, "
                                "CUDA graph)", "ctas": binfo["ctas"], "smem_bytes_per_cta": binfo["smem_bytes"],
@@ -469,6 +477,164 @@ def c3_arm(args, rank, world, local_rank):
         v, kind, cores, n, secs = cpu_measure(w, scans[k], z, zf, 1, 1, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                                 "sample": f"{w.desc}: {n} ICD iteration(s) after 1 warm-up, {secs:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------ learned warm start --
+C4_DESC = ("learned warm start: 3-D encoder-decoder network (4 levels, 16-128 channels, 1.33 M parameters) trained "
+           "on (FBP, plain-ICD MBIR) pairs of seeded random-ellipsoid and two-phase Gaussian-random-field phantoms, "
+           "256x256x16, 384 views, I0 log-uniform in [2e3, 5e4]; ICD from its output vs from FBP to (1 + 1e-5) C*")
+C4_PRIOR = dict(W3D.prior)
+C4_DATA = ("synthetic (seeded random-ellipsoid phantoms with exact line integrals, and two-phase Gaussian-random-field "
+           "phantoms projected by the engine; Poisson counts)")
+
+
+def c4_scan(k, n_xy=256, rows=16, views=384):
+    """Scan k of the learned-warm-start workload: even k a random-ellipsoid
+    phantom, odd k a two-phase Gaussian-random-field phantom."""
+    import timbir_b200
+    rng = np.random.default_rng(5000 + k)
+    I0 = float(np.exp(rng.uniform(np.log(2e3), np.log(5e4))))
+    if k % 2 == 0:
+        return synth.ellipsoid_scan_device(n_xy, rows, views, I0=I0, seed=5000 + k)
+    ph = synth.two_phase_frames(n_xy, rows, 1, seed=5000 + k)
+    angles = (np.arange(views) * np.pi / views).astype(np.float32)
+    times = np.arange(views, dtype=np.float32)
+    rt = np.array([0.0, float(views)], np.float32)
+    zero = np.zeros((views, rows, n_xy), np.float32)
+    proto = synth.Scan(zero, np.ones_like(zero), angles, times, rt, rows, n_xy, views, 1, 1.0, n_xy / 2.0, ph)
+    st = timbir_b200.Stage(proto, **C4_PRIOR, blocks=2)
+    li = st.forward_project(ph)
+    st.close()
+    proj, wts = synth.counts_to_data(li.astype(np.float64), I0, rng)
+    return synth.Scan(proj, wts, angles, times, rt, rows, n_xy, views, 1, 1.0, n_xy / 2.0, ph)
+
+
+def c4_stage(scan, prior=None, blocks=2, acache=-1):
+    import timbir_b200
+    st = timbir_b200.Stage(scan, **(prior or C4_PRIOR), blocks=blocks)
+    st.set_schedule(1, 0, 0, acache)
+    return st
+
+
+def icd_from(scan, start, cstar=None, max_iters=600, flat=1e-10, prior=None, blocks=2, acache=-1):
+    """Plain GPU ICD from `start`: with cstar, device time and iterations
+    until the FP64 cost is within (1 + 1e-5) cstar; without, iterations until
+    two successive costs agree to `flat` (the converged cost C*).  Returns
+    (iterations, ms of the ICD iterations, last cost, object)."""
+    st = c4_stage(scan, prior, blocks, acache)
+    st.prepare(start)
+    ms, prev, c = 0.0, None, None
+    for it in range(1, max_iters + 1):
+        st.time_begin()
+        st.iterate(it)
+        ms += st.time_end()
+        c = st.cost()[0]
+        if cstar is not None and c <= (1.0 + 1e-5) * cstar:
+            break
+        if cstar is None and prev is not None and abs(prev - c) <= flat * abs(c):
+            break
+        prev = c
+    x = st.object()
+    st.close()
+    return it, ms, c, x
+
+
+def c4_arm(args, rank, world, local_rank, four_d=False, n_train=24, train_iters=100, steps=1500):
+    """Learned warm start: training pairs from the plain method, the network
+    trained on them, then ICD from its output against ICD from FBP on held-out
+    scans.  four_d: the 4-D workload (16 frames, 64 interlaced views per
+    frame, zingers and rings), trained on 4-D scans of other seeds, evaluated
+    on the bench's own 4-D scan, the warm run with FP16 A-matrix values."""
+    import torch
+    import timbir_b200
+    from timbir_b200 import warm
+    torch.cuda.set_device(local_rank)
+    if four_d:
+        w = W4D
+        prior, blocks = w.prior, 8
+        scan_of = lambda k: fourd_scan(w, 100 + k)  # noqa: E731
+        held_out = [(fourd_scan(w, 0), "two-phase microstructure, 16 frames (the 4-D workload's scan)")]
+        n_train, acache_warm = 4, -1
+    else:
+        prior, blocks, scan_of, acache_warm = C4_PRIOR, 2, c4_scan, -1
+        held_out = [(c4_scan(1000), "random ellipsoids"), (c4_scan(1001), "two-phase Gaussian random field")]
+    kw = dict(prior=prior, blocks=blocks)
+    t0 = time.perf_counter()
+    fbps, tgts = [], []
+    for k in range(n_train):
+        sc = scan_of(k)
+        st = c4_stage(sc, prior, blocks)
+        f = st.fbp()
+        st.prepare(f)
+        for it in range(1, train_iters + 1):
+            st.iterate(it)
+        fbps.extend(list(f))
+        tgts.extend(list(st.object()))
+        st.close()
+    data_s = time.perf_counter() - t0
+    X = torch.from_numpy(np.stack(fbps)).cuda()
+    T = torch.from_numpy(np.stack(tgts)).cuda()
+    net = warm.WarmNet(seed=7)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = warm.train(net, X, T, steps=steps, batch=4, patch=(16, 64, 64), lr=1e-3, seed=3)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    pairs = int(X.shape[0])
+    del X, T
+    results = []
+    for sc, name in held_out:
+        st = c4_stage(sc, prior, blocks)
+        mask = st.mask().astype(np.float32)
+        fbp = st.fbp()  # untimed first call
+        warm.warm_start(net, fbp, mask)  # the network's buffers, allocated once
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        fbp = st.fbp()
+        f1.record()
+        torch.cuda.synchronize()
+        fbp_ms = f0.elapsed_time(f1)
+        st.close()
+        f0.record()
+        ws = warm.warm_start(net, fbp, mask)
+        f1.record()
+        torch.cuda.synchronize()
+        net_ms = f0.elapsed_time(f1)
+        n_star, _, cstar, x_star = icd_from(sc, fbp, max_iters=800, **kw)
+        n_plain, ms_plain, c_plain, x_plain = icd_from(sc, fbp, cstar, **kw)
+        n_warm, ms_warm, c_warm, x_warm = icd_from(sc, ws, cstar, acache=acache_warm, **kw)
+        rng_ = float(x_star.max() - x_star.min())
+        rm = lambda a: float(np.sqrt(np.mean((a - x_star) ** 2))) / rng_  # noqa: E731
+        results.append({
+            "phantom": name, "cstar": cstar, "cstar_iterations": n_star,
+            "plain": {"iterations": n_plain, "icd_ms": round(ms_plain, 2), "start_ms": round(fbp_ms, 2),
+                      "total_ms": round(ms_plain + fbp_ms, 2), "a_matrix": "fp32"},
+            "warm": {"iterations": n_warm, "icd_ms": round(ms_warm, 2), "start_ms": round(fbp_ms + net_ms, 2),
+                     "total_ms": round(ms_warm + fbp_ms + net_ms, 2),
+                     "a_matrix": "fp16" if acache_warm == 2 else "fp32"},
+            "final_cost_over_cstar": {"plain": c_plain / cstar, "warm": c_warm / cstar},
+            "speedup_total": (ms_plain + fbp_ms) / (ms_warm + fbp_ms + net_ms),
+            "start_rmse_over_range": {"fbp": rm(fbp), "warm": rm(ws)},
+            "final_rmse_over_range": {"plain": rm(x_plain), "warm": rm(x_warm)},
+        })
+    net.close()
+    line = {
+        "metric": "time-to-MAP-cost (warm vs plain)", "value": float(np.mean([r["speedup_total"] for r in results])),
+        "unit": "x (plain time / warm time, start images included)", "n_gpus": world, "higher_is_better": True,
+        "config": {"workload": (W4D.desc + "; learned warm start (network trained on 4-D scans of other seeds)")
+                   if four_d else C4_DESC,
+                   "training_volumes": pairs, "pair_target": f"{train_iters} plain ICD iterations from FBP",
+                   "train_steps": steps, "train_batch": "4 patches 16x64x64", "params": int(net.n)},
+        "training": {"ms": round(train_ms, 1), "ms_per_step": round(train_ms / steps, 3),
+                     "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
+                     "pairs_s": round(data_s, 1)},
+        "held_out": results, "target": "FP64 MAP cost <= (1 + 1e-5) C*, C* = the plain FP32 run's converged cost",
+        "dtype": "network bf16 operands / fp32 accumulation; ICD f32",
+        "data": W4D.data if four_d else C4_DATA,
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -519,6 +685,8 @@ def gpu_arm(args, rank, world, local_rank):
     import timbir_b200
     if args.config == "c3":
         return c3_arm(args, rank, world, local_rank)
+    if args.config in ("c4", "4d-warm"):
+        return c4_arm(args, rank, world, local_rank, four_d=args.config == "4d-warm")
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -694,10 +862,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
-    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3"],
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm"],
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
-                         "c3: 64 independent 3-D problems batched; c5: large 4-D z-subset")
+                         "c3: 64 independent 3-D problems batched; c4: learned warm start (3-D); 4d-warm: learned warm "
+                         "start on the 4-D workload; c5: large 4-D z-subset")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
+    ap.add_argument("--problems", type=int, default=64, help="c3: the first N of the 64 problems")
+    ap.add_argument("--no-tune", action="store_true", help="c3: default schedules instead of the autotuner's")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
     ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,
                     help="A-matrix column cache with FP16 values (FP32 accumulation)")

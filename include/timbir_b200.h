@@ -120,6 +120,12 @@ int mbir_set_sv_zgroup(MbirStage *stage, int32_t slices);
  * super-voxels in flight (see mbir_get_sv_grid).  Takes effect at the next
  * mbir_set_schedule.  The reference schedule always uses 1.5. */
 int mbir_set_sv_relaxation(MbirStage *stage, double alpha);
+/* Times the super-voxel schedule's stability guard has halved the
+ * super-voxels in flight since the schedule was set: an iteration after
+ * which the MAP cost rose (by more than 1e-6 of it) is redone from the state
+ * before it with half as many in flight.  The guard evaluates the cost once
+ * per iteration (mbir_compute_cost) unless the CTA count was set. */
+int mbir_get_sv_adjustments(MbirStage *stage);
 /* The automatic launch size of schedule 1: persistent CTAs per launch, the
  * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
  * correct the same rays at once and the iteration diverges), the CTAs that
@@ -278,6 +284,11 @@ int mbir_net_forward(MbirNet *net, const float *in, float *out, int32_t B, int32
  * network's gradient array; *loss (may be NULL) = the loss. */
 int mbir_net_gradients(MbirNet *net, const float *in, const float *target, int32_t B, int32_t D, int32_t H,
                        int32_t W, float scale, double *loss, void *stream);
+/* Layer k's output (which 0; layer -1: the network input) or its gradient
+ * (which 1) from the last forward / gradient call, as host float
+ * [B][D][H][W][C] at the layer's level; *count (may be NULL) = elements,
+ * out may be NULL to ask for the count.  For tests. */
+int mbir_net_get_activation(MbirNet *net, int32_t layer, int32_t which, float *out, int64_t *count);
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the last gradients. */
 int mbir_net_adam_step(MbirNet *net, float lr, void *stream);
 

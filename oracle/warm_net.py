@@ -4,9 +4,9 @@ A numpy float64 restatement of the network in timbir_b200/csrc/warm_net.cu
 (no reference counterpart: TIMBIR has no learned part): the same layers,
 parameter layout and loss, with forward and backward passes written out by
 hand.  The GPU rounds the two operands of every tensor-core product to BF16
-(round to nearest even) and accumulates in FP32; the oracle rounds the same
-operands to BF16 and accumulates in FP64, so the two agree to FP32
-accumulation error.  ``finite_difference`` checks the oracle's own
+(round to nearest even) and accumulates in FP32 inside the tensor cores; the
+oracle rounds the same operands to BF16 and accumulates in FP64, so the two
+differ by the tensor cores' accumulation error only.  ``finite_difference`` checks the oracle's own
 gradients against its loss.
 
 Activations are channels-last [B][D][H][W][C]; parameters are flat, per
@@ -139,21 +139,32 @@ def predict(flat, fbp, s):
     return np.asarray(fbp, np.float64) + r / s
 
 
-def loss_and_grads(flat, fbp, target, s):
+def loss_and_grads(flat, fbp, target, s, trace=None, acts=None):
     """Loss mean((s fbp + r - s target)^2) and its gradient with respect to
-    the flat parameters."""
+    the flat parameters; trace (a dict), when given, receives each layer's
+    output gradient (after its ReLU's mask) under the layer's index.  acts,
+    when given, are the layer outputs to differentiate at ({"x0": input,
+    0..14: layer outputs}, channels-last), in place of the oracle's own
+    forward pass (so that a backward pass can be checked on its own)."""
     P = unpack(flat)
-    r, A = forward(flat, fbp, s)
+    if acts is None:
+        r, A = forward(flat, fbp, s)
+    else:
+        A = {k: np.asarray(v, np.float64) for k, v in acts.items()}
+        A["p1"], A["p2"], A["p3"] = pool(A[1]), pool(A[3]), pool(A[5])
+        A["u2"], A["u1"], A["u0"] = up(A[7]), up(A[9]), up(A[11])
+        r = A[14][..., 0]
     d = s * np.asarray(fbp, np.float64) + r - s * np.asarray(target, np.float64)
     M = d.size
     loss = float(np.mean(d * d))
-    G = {k: None for k in range(15)}
     dz14 = np.zeros(A[14].shape)
     dz14[..., 0] = 2.0 * d / M
     grads = [None] * 15
     mask = lambda g, a: g * (a > 0)  # noqa: E731
 
     def layer(k, x, dz, need_dx=True):
+        if trace is not None:
+            trace[k] = dz
         grads[k] = conv_weight_grad(x, dz)
         return conv_input_grad(dz, P[k][0]) if need_dx else None
 

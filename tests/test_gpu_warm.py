@@ -4,10 +4,13 @@ oracles (oracle/fbp.py, oracle/warm_net.py), and what a trained network
 gains over FBP-initialised ICD.
 
 Tolerances: the network's tensor-core products take BF16 operands (the
-oracle rounds the same operands to BF16) and accumulate in FP32 (the oracle
-in FP64); an activation that lands within an FP32 rounding of a BF16
-rounding boundary rounds differently on the two sides, so outputs and
-gradients are compared by relative L2 error (< 5e-3), not bit for bit.
+oracle rounds the same operands to BF16) and accumulate in FP32 inside the
+tensor cores, which is not IEEE round-to-nearest (measured: each layer's
+output differs from the FP64-accumulated oracle by about 2e-4 relative, the
+difference compounding over the 15 layers to about 3e-3 at the output).
+Outputs and gradients are therefore compared by relative L2 error, per
+layer, below 1e-2; the backward pass is checked at the GPU's own layer
+outputs.
 """
 import numpy as np
 import pytest
@@ -66,30 +69,48 @@ def test_network_forward_matches_the_oracle():
     fbp, _ = inputs(2)
     out = net.forward(torch.from_numpy(fbp).cuda()).cpu().numpy()
     r_gpu = (out.astype(np.float64) - fbp) * warm.SCALE
-    r_ref, _ = W.forward(p, fbp, warm.SCALE)
-    assert rel(r_gpu, r_ref) < 5e-3
+    r_ref, A = W.forward(p, fbp, warm.SCALE)
+    assert rel(r_gpu, r_ref) < 1e-2
+    for k in range(15):
+        assert rel(net.activation(k), A[k].reshape(-1)) < 1e-2, k
     net.close()
 
 
+LEVEL = [0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0, 0]
+
+
+def gpu_activations(net, shape):
+    """The network's stored layer outputs, channels-last, by layer."""
+    B, D, H, Wd = shape
+    acts = {"x0": net.activation(-1).reshape(B, D, H, Wd, 16)}
+    for k, (ci, co) in enumerate(W.LAYERS):
+        lv = LEVEL[k]
+        acts[k] = net.activation(k).reshape(B, D >> lv, H >> lv, Wd >> lv, co)
+    return acts
+
+
 def test_network_gradients_match_the_oracle():
+    # the backward pass on its own: the oracle differentiates at the GPU's
+    # own layer outputs (a forward difference near a ReLU's kink would
+    # otherwise flip its mask on one side only)
     net = warm.WarmNet(0)
     p = random_params(3)
     net.set_params(p)
     fbp, tgt = inputs(4)
     loss = net.gradients(torch.from_numpy(fbp).cuda(), torch.from_numpy(tgt).cuda())
     g = net.grads()
-    loss_ref, g_ref = W.loss_and_grads(p, fbp, tgt, warm.SCALE)
-    assert abs(loss - loss_ref) < 1e-3 * loss_ref
+    trace = {}
+    loss_ref, g_ref = W.loss_and_grads(p, fbp, tgt, warm.SCALE, trace, gpu_activations(net, fbp.shape))
+    assert abs(loss - loss_ref) < 1e-4 * loss_ref
+    for k in range(15):  # each layer's output gradient (after its ReLU's mask)
+        assert rel(net.activation(k, grad=True), trace[k].reshape(-1)) < 1e-2, k
     off = 0
     for k, (ci, co) in enumerate(W.LAYERS):
         nw = 27 * ci * co
-        gw, gw_ref = g[off:off + nw], g_ref[off:off + nw]
-        gb, gb_ref = g[off + nw:off + nw + co], g_ref[off + nw:off + nw + co]
+        for a, b in ((g[off:off + nw], g_ref[off:off + nw]), (g[off + nw:off + nw + co], g_ref[off + nw:off + nw + co])):
+            if np.linalg.norm(b) > 0:
+                assert rel(a, b) < 1e-2, k
         off += nw + co
-        if np.linalg.norm(gw_ref) > 0:
-            assert rel(gw, gw_ref) < 5e-3, (k, rel(gw, gw_ref))
-        if np.linalg.norm(gb_ref) > 0:
-            assert rel(gb, gb_ref) < 5e-3, (k, rel(gb, gb_ref))
     net.close()
 
 

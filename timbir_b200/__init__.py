@@ -78,6 +78,7 @@ def load_library() -> C.CDLL:
     lib.mbir_set_sv_zgroup.argtypes = [_VP, i32]
     lib.mbir_get_sv_grid.argtypes = [_VP] + [C.POINTER(i32)] * 3 + [C.POINTER(C.c_double)]
     lib.mbir_set_sv_relaxation.argtypes = [_VP, C.c_double]
+    lib.mbir_get_sv_adjustments.argtypes = [_VP]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     i64 = C.c_int64
@@ -185,6 +186,7 @@ class Stage:
         self.lib.mbir_get_sv_grid(self.h, *[C.byref(x) for x in g], C.byref(rel))
         d["ctas"], d["inflight_per_group"], d["resident_ctas"] = [x.value for x in g]
         d["relaxation"] = rel.value
+        d["stability_adjustments"] = int(self.lib.mbir_get_sv_adjustments(self.h))
         return d
 
     def set_sv_relaxation(self, alpha: float):

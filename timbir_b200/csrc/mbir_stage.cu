@@ -138,6 +138,12 @@ struct MbirStage {
     int sv_fit = 1;     // CTAs resident on the GPU (all SMs)
     double sv_alpha = 0;      // over-relaxation of schedule 1 requested; 0 = automatic
     double sv_alpha_eff = 1.5;  // over-relaxation schedule 1 uses
+    // stability guard of schedule 1: the state before the current iteration
+    // and the MAP cost there (have_cost: known)
+    float *d_snap_x = nullptr, *d_snap_e = nullptr, *d_snap_w = nullptr, *d_snap_d = nullptr;
+    double snap_var = 1.0, prev_cost = 0;
+    bool have_cost = false;
+    int stab_events = 0;
     std::vector<int> sv_rank;  // size rank of a super-voxel within its (phase, frame, z-group)
     double nh_fraction = 0.2;
 
@@ -158,7 +164,8 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_all, d_sv_done, d_sv_lists, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol};
+                        d_sv_all, d_sv_done, d_sv_lists, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol,
+                        d_snap_x, d_snap_e, d_snap_w, d_snap_d};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -405,6 +412,7 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
     S->prepared = 1;
+    S->have_cost = false;
     return 0;
 }
 
@@ -854,6 +862,8 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     CK(cudaStreamSynchronize(S->stream));
     if (!S->sv_ev[0])
         for (auto &e : S->sv_ev) CK(cudaEventCreate(&e));
+    S->stab_events = 0;
+    S->have_cost = false;
     S->schedule = 1;
     return 0;
 }
@@ -895,6 +905,10 @@ extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_gr
     if (relaxation) *relaxation = S->sv_alpha_eff;
     return 0;
 }
+
+// Times the stability guard of the super-voxel schedule has halved the
+// super-voxels in flight since the schedule was set.
+extern "C" int mbir_get_sv_adjustments(MbirStage *S) { return S->stab_events; }
 
 extern "C" int mbir_get_acache(MbirStage *S, int32_t *used, int64_t *bytes)
 {
@@ -984,6 +998,24 @@ static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> 
 static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
     const int P = S->sv_nphase;
+    // the state before this iteration, for the stability guard below
+    const size_t nsino = S->nsino(), nvox = S->nvox(), noff = (size_t)S->sg.N_t * S->sg.N_r;
+    if (!S->d_snap_x) {
+        CK(dalloc(&S->d_snap_x, nvox));
+        CK(dalloc(&S->d_snap_e, nsino));
+        CK(dalloc(&S->d_snap_w, nsino));
+        CK(dalloc(&S->d_snap_d, noff));
+    }
+    CK(cudaMemcpyAsync(S->d_snap_x, S->d_x, nvox * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->d_snap_e, S->d_e, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->d_snap_w, S->d_w, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->d_snap_d, S->d_d, noff * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    S->snap_var = S->var_est;
+    const bool adjustable = S->sv_ctas == 0 && S->sv_grid > 1;
+    if (adjustable && !S->have_cost) {
+        if (mbir_compute_cost(S, &S->prev_cost, nullptr, nullptr)) return -1;
+        S->have_cost = true;
+    }
     if (S->d_acol && !S->acol_built) {
         CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->acol_half, S->d_acol, S->d_err, S->stream));
         S->acol_built = true;
@@ -1054,11 +1086,36 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
     if (err & 2) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
     if (err & 4) return fail("super-voxel dependency wait timed out");
+    // Stability guard.  Super-voxels in flight together over-correct the
+    // rays they share; the in-flight cap bounds that for the geometries it
+    // was measured on.  Every step of an iteration (the voxel updates with
+    // over-relaxation below 2, the offset and variance updates) lowers the
+    // MAP cost, so a cost that rises by more than 1e-6 of its value means the
+    // super-voxels in flight diverged: the state before the iteration is
+    // restored and the iteration redone with half as many in flight.  Only
+    // the automatic grid is adjusted.
+    const double ax = acc[0].sum_abs_x;
+    const double pct = ax > 0 ? 100.0 * S->K * acc[0].sum_abs_dx / ax : 0.0;
+    if (adjustable && S->have_cost) {
+        double c = 0;
+        if (mbir_compute_cost(S, &c, nullptr, nullptr)) return -1;
+        if (!(c - S->prev_cost <= 1e-6 * std::fabs(S->prev_cost))) {
+            CK(cudaMemcpyAsync(S->d_x, S->d_snap_x, nvox * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+            CK(cudaMemcpyAsync(S->d_e, S->d_snap_e, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+            CK(cudaMemcpyAsync(S->d_w, S->d_snap_w, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+            CK(cudaMemcpyAsync(S->d_d, S->d_snap_d, noff * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+            S->var_est = S->snap_var;
+            S->sv_grid = std::max(1, S->sv_grid / 2);
+            S->stab_events++;
+            return sv_iterate(S, iter, converged);
+        }
+        S->prev_cost = c;
+    }
     for (int q = 0; q < (nh ? 2 : 1); q++) {
         S->updates += acc[q].updates;
         S->zero_skips += acc[q].zero_skips;
     }
-    S->last_pct = acc[0].sum_abs_x > 0 ? 100.0 * S->K * acc[0].sum_abs_dx / acc[0].sum_abs_x : 0.0;
+    S->last_pct = pct;
     *converged = S->last_pct < S->stop_thresh ? 1 : 0;
     return 0;
 }

@@ -1092,8 +1092,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
 }
 
 // End of a batched iteration (one CTA).
-__global__ void __launch_bounds__(256) k_sv_batch_end(const SvProblem *__restrict__ probs,
-                                                      SvBatchState *__restrict__ st, int n, int *ctl, int *queue)
+__global__ void __launch_bounds__(256) k_sv_batch_end(SvProblem *__restrict__ probs, SvBatchState *__restrict__ st,
+                                                      int n, int *ctl, int *queue)
 {
     __shared__ int s_active;
     if (threadIdx.x == 0) s_active = 0;
@@ -1106,7 +1106,16 @@ __global__ void __launch_bounds__(256) k_sv_batch_end(const SvProblem *__restric
             b.updates += b.out.updates;
             b.zero_skips += b.out.zero_skips;
             // the reference's convergence ratio (XT_ICD_update.c:1066-1103)
-            b.pct = b.out.sum_abs_x > 0 ? 100.0 * probs[q].K * b.out.sum_abs_dx / b.out.sum_abs_x : 0.0;
+            const double ax = b.out.sum_abs_x;
+            const double pct = ax > 0 ? 100.0 * probs[q].K * b.out.sum_abs_dx / ax : 0.0;
+            // stability guard: halve the problem's super-voxels in flight
+            // when a sweep's summed |x'| jumps (values blowing up)
+            if (b.iters >= 2 && b.prev_ax > 0 && ax > 2.0 * b.prev_ax && probs[q].cap > 1) {
+                probs[q].cap = max(1, probs[q].cap / 2);
+                b.adjustments++;
+            }
+            b.prev_ax = ax;
+            b.pct = pct;
             if (b.pct < probs[q].stop) {
                 b.active = 0;
                 b.converged = 1;
@@ -1304,7 +1313,7 @@ cudaError_t mbir_launch_icd_sv_batch(size_t smem_bytes, bool half, const SvLaunc
     return cudaGetLastError();
 }
 
-cudaError_t mbir_launch_sv_batch_end(const SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
+cudaError_t mbir_launch_sv_batch_end(SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
                                      cudaStream_t s)
 {
     k_sv_batch_end<<<1, 256, 0, s>>>(probs, state, n, ctl, queue);

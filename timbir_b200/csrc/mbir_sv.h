@@ -112,10 +112,12 @@ struct SvBatchState {
     SvTaskOut out;   // this iteration's statistics
     long long updates, zero_skips;
     double pct;      // convergence ratio of the last iteration, percent
+    double prev_ax;  // summed |x'| of the previous iteration's updates
     int active;      // still iterating
     int iters;       // iterations done
     int converged;   // stopped by the convergence test
     int fin;         // super-voxels finished in this launch
+    int adjustments; // times the in-flight cap was halved
 };
 
 // CTAs of the super-voxel kernel that fit one SM for this configuration.
@@ -144,8 +146,10 @@ cudaError_t mbir_sv_batch_prepare(size_t smem_bytes, bool half);
 cudaError_t mbir_launch_icd_sv_batch(size_t smem_bytes, bool half, const SvLaunch &L, int ctas, int *queue,
                                      float *scratch, size_t scratch_floats, uint32_t seed, int *err, cudaStream_t s);
 // End of a batched iteration: per active problem, the iteration's statistics
-// into the totals and the convergence test; then the statistics, in-flight
-// counters and queue counter are reset, ctl[0] (the iteration) advances and
-// ctl[1] = problems still active.
-cudaError_t mbir_launch_sv_batch_end(const SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
+// into the totals, the convergence test and the stability guard (a summed
+// |x'| above 2 x the previous iteration's halves the problem's in-flight
+// cap); then the
+// statistics, in-flight counters and queue counter are reset, ctl[0] (the
+// iteration) advances and ctl[1] = problems still active.
+cudaError_t mbir_launch_sv_batch_end(SvProblem *probs, SvBatchState *state, int n, int *ctl, int *queue,
                                      cudaStream_t s);

@@ -737,6 +737,20 @@ int mbir_net_get_grads(MbirNet *N, float *out)
     return 0;
 }
 
+// Activation (which = 0) or its gradient (which = 1) of layer k (0..14;
+// -1: the network input) from the last forward / gradient call, host
+// float [B][D][H][W][C] at the layer's level; *count = its elements.
+int mbir_net_get_activation(MbirNet *N, int32_t layer, int32_t which, float *out, int64_t *count)
+{
+    const int t = layer < 0 ? T_X0 : T_A0 + layer;
+    if (layer < -1 || layer >= kLayers || N->act.empty()) return net_fail("no such activation");
+    if (which == 1 && N->grad.empty()) return net_fail("no gradients computed");
+    const NetTensor &x = which == 1 ? N->grad[t] : N->act[t];
+    if (count) *count = (int64_t)x.n;
+    if (out) NK(cudaMemcpy(out, x.p, x.n * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
 int mbir_net_forward(MbirNet *N, const float *in, float *out, int32_t B, int32_t D, int32_t H, int32_t W,
                      float scale, void *stream)
 {

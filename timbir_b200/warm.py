@@ -32,6 +32,7 @@ def _lib():
         lib.mbir_net_forward.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, vp]
         lib.mbir_net_gradients.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.POINTER(C.c_double), vp]
         lib.mbir_net_adam_step.argtypes = [vp, C.c_float, vp]
+        lib.mbir_net_get_activation.argtypes = [vp, i32, i32, vp, C.POINTER(C.c_int64)]
         lib._net_bound = True
     return lib
 
@@ -80,6 +81,14 @@ class WarmNet:
     def grads(self) -> np.ndarray:
         out = np.zeros(self.n, np.float32)
         _check(self.lib.mbir_net_get_grads(self.h, out.ctypes.data))
+        return out
+
+    def activation(self, layer: int, grad: bool = False) -> np.ndarray:
+        """Layer `layer`'s output (or its gradient) from the last call, flat."""
+        n = C.c_int64()
+        _check(self.lib.mbir_net_get_activation(self.h, layer, 1 if grad else 0, None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        _check(self.lib.mbir_net_get_activation(self.h, layer, 1 if grad else 0, out.ctypes.data, None))
         return out
 
     def forward(self, x, scale: float = SCALE):
