@@ -121,11 +121,14 @@ int mbir_set_sv_zgroup(MbirStage *stage, int32_t slices);
  * mbir_set_schedule.  The reference schedule always uses 1.5. */
 int mbir_set_sv_relaxation(MbirStage *stage, double alpha);
 /* Times the super-voxel schedule's stability guard has halved the
- * super-voxels in flight since the schedule was set: an iteration after
- * which the MAP cost rose (by more than 1e-6 of it) is redone from the state
- * before it with half as many in flight.  The guard evaluates the cost once
- * per iteration (mbir_compute_cost) unless the CTA count was set. */
+ * super-voxels in flight since the schedule was set: when the MAP cost rose
+ * (by more than 1e-6 of it) over a window of iterations (one iteration for
+ * the first four windows, then eight), the state at the window's start is
+ * restored and the iteration redone with half as many in flight (the
+ * automatic grid, or the CTA count mbir_set_sv_ctas set). */
 int mbir_get_sv_adjustments(MbirStage *stage);
+/* The stability guard on (1, the default) or off (0). */
+int mbir_set_sv_guard(MbirStage *stage, int32_t on);
 /* The automatic launch size of schedule 1: persistent CTAs per launch, the
  * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
  * correct the same rays at once and the iteration diverges), the CTAs that

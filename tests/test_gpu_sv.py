@@ -250,3 +250,26 @@ def test_sv_fp16_columns_reach_the_map_within_the_fp64_oracle_bar():
           % (out[1] + out[2]))
     assert out[2][0] < 1e-3
     assert out[2][1] < 1e-4
+
+
+def test_stability_guard_recovers_from_too_many_supervoxels_in_flight():
+    # every super-voxel of the small scene in flight at once at the
+    # reference's over-relaxation 1.5 over-corrects the shared rays (about
+    # 19 super-voxels cross each ray); the guard sees the MAP cost rise,
+    # restores the state and halves the super-voxels in flight until the
+    # iteration converges, to the reference's MAP
+    g = np.load(os.path.join(GOLD, "converged_plain.npz"))
+    s = scenarios.make("plain", timbir_b200.Stage)
+    s.set_sv_relaxation(1.5)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 4, 0, 1)
+    s.set_sv_ctas(148)
+    s.prepare()
+    costs = [s.cost()[0]]
+    for it in range(1, 301):
+        s.iterate(it)
+        if it <= 4:
+            costs.append(s.cost()[0])
+    assert s.schedule_info()["stability_adjustments"] >= 1
+    assert all(b <= a * (1 + 1e-6) for a, b in zip(costs, costs[1:]))
+    c = fresh_cost_fp64("plain", s.object())
+    assert abs(c - float(g["ref_fresh_cost"])) / float(g["ref_fresh_cost"]) < 1e-5

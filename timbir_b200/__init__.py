@@ -79,6 +79,7 @@ def load_library() -> C.CDLL:
     lib.mbir_get_sv_grid.argtypes = [_VP] + [C.POINTER(i32)] * 3 + [C.POINTER(C.c_double)]
     lib.mbir_set_sv_relaxation.argtypes = [_VP, C.c_double]
     lib.mbir_get_sv_adjustments.argtypes = [_VP]
+    lib.mbir_set_sv_guard.argtypes = [_VP, i32]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     i64 = C.c_int64
@@ -199,6 +200,10 @@ class Stage:
         before set_schedule."""
         _check(self.lib.mbir_set_sv_zgroup(self.h, slices))
 
+    def set_sv_guard(self, on: bool):
+        """The super-voxel schedule's stability guard on (the default) or off."""
+        _check(self.lib.mbir_set_sv_guard(self.h, 1 if on else 0))
+
     def set_sv_ctas(self, ctas: int):
         """Persistent CTAs per super-voxel launch (0 = one per SM; 1 runs the
         super-voxels one after another, deterministically)."""
@@ -308,9 +313,15 @@ class Stage:
         return out
 
     def set_batch_schedule(self, sv_side: int = 0, warps_per_slice: int = 1, acache: int = 1):
-        """Super-voxel schedule that batched launches take: z-group and warps
-        per slice filling the batched kernel's 256 threads (batch_split)."""
-        wps, nz = batch_split(warps_per_slice, self.N_z)
+        """Super-voxel schedule that batched launches take: at least as many
+        warps per slice as keep a lane's views at 8 or fewer, and the z-group
+        and warps per slice filling the batched kernel's 256 threads
+        (batch_split)."""
+        views = -(-self.N_p // max(self.N_time, 1))  # views per frame (equal frames)
+        wps = max(1, warps_per_slice)
+        while wps < 4 and -(-views // (32 * wps)) > 8:
+            wps *= 2
+        wps, nz = batch_split(wps, self.N_z)
         self.set_sv_zgroup(nz)
         self.set_schedule(self.SCHEDULE_SUPERVOXEL, sv_side, wps, acache)
 

@@ -138,12 +138,13 @@ struct MbirStage {
     int sv_fit = 1;     // CTAs resident on the GPU (all SMs)
     double sv_alpha = 0;      // over-relaxation of schedule 1 requested; 0 = automatic
     double sv_alpha_eff = 1.5;  // over-relaxation schedule 1 uses
-    // stability guard of schedule 1: the state before the current iteration
-    // and the MAP cost there (have_cost: known)
+    // stability guard of schedule 1: the state at the start of the current
+    // window of iterations and the MAP cost there (have_cost: known), the
+    // window's iterations so far and the windows checked
     float *d_snap_x = nullptr, *d_snap_e = nullptr, *d_snap_w = nullptr, *d_snap_d = nullptr;
     double snap_var = 1.0, prev_cost = 0;
-    bool have_cost = false;
-    int stab_events = 0;
+    bool guard = true, have_cost = false, win_open = false;
+    int win_iters = 0, guard_checks = 0, stab_events = 0;
     std::vector<int> sv_rank;  // size rank of a super-voxel within its (phase, frame, z-group)
     double nh_fraction = 0.2;
 
@@ -412,7 +413,8 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
     S->prepared = 1;
-    S->have_cost = false;
+    S->have_cost = S->win_open = false;
+    S->guard_checks = 0;
     return 0;
 }
 
@@ -612,7 +614,9 @@ static void sv_build_list(const MbirStage *S, const std::vector<int> &ids, std::
     buf.insert(buf.end(), deps.begin(), deps.end());
 }
 
-static const size_t kSmemLimit = 227 * 1024;
+// dynamic shared memory per CTA: the 227 KB opt-in limit less the kernels' static
+// shared memory (at most 1.1 KB: the batched kernel's problem descriptor)
+static const size_t kSmemLimit = 227 * 1024 - 2048;
 static const int kMaxLaunchesPerIter = 64;
 
 // Super-voxel side 0 = choose the largest side (<= 16) whose band for a
@@ -863,7 +867,8 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     if (!S->sv_ev[0])
         for (auto &e : S->sv_ev) CK(cudaEventCreate(&e));
     S->stab_events = 0;
-    S->have_cost = false;
+    S->have_cost = S->win_open = false;
+    S->guard_checks = 0;
     S->schedule = 1;
     return 0;
 }
@@ -903,6 +908,13 @@ extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_gr
     if (cap_per_group) *cap_per_group = S->sv_cap;
     if (resident) *resident = S->sv_fit;
     if (relaxation) *relaxation = S->sv_alpha_eff;
+    return 0;
+}
+
+extern "C" int mbir_set_sv_guard(MbirStage *S, int32_t on)
+{
+    S->guard = on != 0;
+    S->win_open = false;
     return 0;
 }
 
@@ -998,23 +1010,29 @@ static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> 
 static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
 {
     const int P = S->sv_nphase;
-    // the state before this iteration, for the stability guard below
+    // the state at the start of a window of iterations, for the stability
+    // guard below
     const size_t nsino = S->nsino(), nvox = S->nvox(), noff = (size_t)S->sg.N_t * S->sg.N_r;
-    if (!S->d_snap_x) {
-        CK(dalloc(&S->d_snap_x, nvox));
-        CK(dalloc(&S->d_snap_e, nsino));
-        CK(dalloc(&S->d_snap_w, nsino));
-        CK(dalloc(&S->d_snap_d, noff));
-    }
-    CK(cudaMemcpyAsync(S->d_snap_x, S->d_x, nvox * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
-    CK(cudaMemcpyAsync(S->d_snap_e, S->d_e, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
-    CK(cudaMemcpyAsync(S->d_snap_w, S->d_w, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
-    CK(cudaMemcpyAsync(S->d_snap_d, S->d_d, noff * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
-    S->snap_var = S->var_est;
-    const bool adjustable = S->sv_ctas == 0 && S->sv_grid > 1;
-    if (adjustable && !S->have_cost) {
-        if (mbir_compute_cost(S, &S->prev_cost, nullptr, nullptr)) return -1;
-        S->have_cost = true;
+    const int grid_now = S->sv_ctas > 0 ? std::min(S->sv_ctas, S->sv_fit) : S->sv_grid;
+    const bool adjustable = S->guard && grid_now > 1;
+    if (adjustable && !S->win_open) {
+        if (!S->d_snap_x) {
+            CK(dalloc(&S->d_snap_x, nvox));
+            CK(dalloc(&S->d_snap_e, nsino));
+            CK(dalloc(&S->d_snap_w, nsino));
+            CK(dalloc(&S->d_snap_d, noff));
+        }
+        if (!S->have_cost) {
+            if (mbir_compute_cost(S, &S->prev_cost, nullptr, nullptr)) return -1;
+            S->have_cost = true;
+        }
+        CK(cudaMemcpyAsync(S->d_snap_x, S->d_x, nvox * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->d_snap_e, S->d_e, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->d_snap_w, S->d_w, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->d_snap_d, S->d_d, noff * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+        S->snap_var = S->var_est;
+        S->win_open = true;
+        S->win_iters = 0;
     }
     if (S->d_acol && !S->acol_built) {
         CK(mbir_build_acache(S->g, S->dv, S->sp.amax, S->sp.eq, S->acol_half, S->d_acol, S->d_err, S->stream));
@@ -1090,26 +1108,36 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     // rays they share; the in-flight cap bounds that for the geometries it
     // was measured on.  Every step of an iteration (the voxel updates with
     // over-relaxation below 2, the offset and variance updates) lowers the
-    // MAP cost, so a cost that rises by more than 1e-6 of its value means the
-    // super-voxels in flight diverged: the state before the iteration is
-    // restored and the iteration redone with half as many in flight.  Only
-    // the automatic grid is adjusted.
+    // MAP cost, so a cost that rose by more than 1e-6 of its value over a
+    // window of iterations means the super-voxels in flight diverged: the
+    // state at the window's start is restored and this iteration redone with
+    // half as many in flight.  The first four windows are one iteration long
+    // (divergence from a poor start shows at once), later ones eight (one
+    // FP64 cost evaluation per eight iterations).  mbir_set_sv_guard turns
+    // it off.
     const double ax = acc[0].sum_abs_x;
     const double pct = ax > 0 ? 100.0 * S->K * acc[0].sum_abs_dx / ax : 0.0;
-    if (adjustable && S->have_cost) {
+    if (adjustable && S->win_open && ++S->win_iters >= (S->guard_checks < 4 ? 1 : 8)) {
         double c = 0;
         if (mbir_compute_cost(S, &c, nullptr, nullptr)) return -1;
+        S->guard_checks++;
         if (!(c - S->prev_cost <= 1e-6 * std::fabs(S->prev_cost))) {
             CK(cudaMemcpyAsync(S->d_x, S->d_snap_x, nvox * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
             CK(cudaMemcpyAsync(S->d_e, S->d_snap_e, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
             CK(cudaMemcpyAsync(S->d_w, S->d_snap_w, nsino * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
             CK(cudaMemcpyAsync(S->d_d, S->d_snap_d, noff * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
             S->var_est = S->snap_var;
-            S->sv_grid = std::max(1, S->sv_grid / 2);
+            if (S->sv_ctas > 0)
+                S->sv_ctas = std::max(1, grid_now / 2);
+            else
+                S->sv_grid = std::max(1, S->sv_grid / 2);
             S->stab_events++;
+            S->win_iters = 0;  // the snapshot is the current state again
+            S->guard_checks = 0;
             return sv_iterate(S, iter, converged);
         }
         S->prev_cost = c;
+        S->win_open = false;
     }
     for (int q = 0; q < (nh ? 2 : 1); q++) {
         S->updates += acc[q].updates;
