@@ -827,6 +827,11 @@ def gpu_arm(args, rank, world, local_rank):
 def reference_arm(args, rank):
     if rank != 0:
         return
+    if args.config in ("c4", "4d-warm"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start (its coarsest "
+                          "stage starts from zero); the comparison is FBP-initialised ICD, in the same line"}),
+              flush=True)
+        return
     if args.config == "c3":
         # the batch's smallest problem, one problem at a time as the reference runs
         specs = synth.batch_problem_specs(64, 0)

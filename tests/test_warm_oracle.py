@@ -39,3 +39,17 @@ def test_bf16_rounds_to_nearest_even():
     # 1 + 2^-8 is half-way between 1 and 1 + 2^-7: ties to even (1)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == 1.0 and r[4] == -2.5
     assert abs(r[5] - 3.0e-3) / 3.0e-3 < 2 ** -8
+
+
+def test_fbp_oracle_reconstructs_the_phantom():
+    # the restatement is a reconstruction: within 6 % RMSE of the phantom's
+    # range on the small scan, zero outside the reconstruction disc
+    from oracle import fbp as F
+    from timbir_b200 import synth
+    scan = synth.ellipsoid_scan(32, 4, 48, seed=1)
+    x = F.fbp(scan)
+    assert x.shape == scan.phantom.shape
+    assert np.sqrt(np.mean((x - scan.phantom) ** 2)) < 0.06 * 0.02
+    k = np.arange(32) + 0.5 - 16
+    outside = (k[None, :] ** 2 + k[:, None] ** 2) >= 16 ** 2
+    assert np.all(x[..., outside] == 0)

@@ -616,6 +616,37 @@ static void sv_build_list(const MbirStage *S, const std::vector<int> &ids, std::
 
 // dynamic shared memory per CTA: the 227 KB opt-in limit less the kernels' static
 // shared memory (at most 1.1 KB: the batched kernel's problem descriptor)
+// Over-relaxation and in-flight cap of the super-voxel schedule for `want`
+// super-voxels wanted in flight at once (see the concurrency note in
+// mbir_set_schedule): alpha = the stage's (1.5 unless set) when the cap of
+// each active (frame, z-group) sinogram holds its share, else the largest
+// value down to 0.7 that does, as long as the share stays under 12 % of the
+// group's super-voxels.  *cap = super-voxels per sinogram, *grid = in total.
+static void sv_relaxation(const MbirStage *S, double want, double *alpha_out, int *cap_out, int *grid_out)
+{
+    const SvParams &sp = S->sp;
+    const int N_time = S->sg.N_time;
+    const double Rv = S->sg.radius_obj / S->st.delta_xy;
+    const double Wv = sp.W * S->sg.delta_r / S->st.delta_xy;
+    const double ref_alpha = S->pr.alpha;
+    auto cap_for = [&](double alpha) {
+        const double crossings = 1.8 * (2.0 / alpha - 1.0) / (2.0 / 1.5 - 1.0);
+        return std::max(4, (int)std::floor(crossings * M_PI * Rv / (2.0 * Wv)));
+    };
+    const long long active = (long long)(N_time > 1 ? (N_time + 1) / 2 : 1) * (S->nzg > 1 ? (S->nzg + 1) / 2 : 1);
+    double alpha = S->sv_alpha > 0 ? S->sv_alpha : ref_alpha;
+    const double groups = (double)N_time * S->nzg;
+    const double per = std::min(want / (double)active,  // in flight per sinogram wanted
+                                std::max(1.0, std::floor(0.12 * (double)S->sv_all.size() / groups)));
+    if (S->sv_alpha <= 0 && cap_for(ref_alpha) < per) {
+        const double g = per / cap_for(ref_alpha) * (2.0 / ref_alpha - 1.0);
+        alpha = std::min(ref_alpha, std::max(0.7, 2.0 / (1.0 + g)));
+    }
+    *alpha_out = alpha;
+    *cap_out = cap_for(alpha);
+    *grid_out = (int)std::max<double>(1.0, std::min<double>(std::ceil(want), (double)*cap_out * active));
+}
+
 static const size_t kSmemLimit = 227 * 1024 - 2048;
 static const int kMaxLaunchesPerIter = 64;
 
@@ -834,28 +865,10 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     // within 1e-5 in 21 iterations and 32 ms, alpha 1.5 with the 30 CTAs it
     // allows in 26 iterations and 156 ms; on a 32 x 32 slice with 64
     // super-voxels, 28 in flight at alpha 0.7 converged far more slowly.
+    S->sv_fit = mbir_sv_ctas_per_sm(S->g, sp, cached) * S->sm_count;
     {
-        const double Rv = S->sg.radius_obj / S->st.delta_xy;
-        const double Wv = sp.W * S->sg.delta_r / S->st.delta_xy;
-        const double ref_alpha = S->pr.alpha;
-        auto cap_for = [&](double alpha) {
-            const double crossings = 1.8 * (2.0 / alpha - 1.0) / (2.0 / 1.5 - 1.0);
-            return std::max(4, (int)std::floor(crossings * M_PI * Rv / (2.0 * Wv)));
-        };
-        S->sv_fit = mbir_sv_ctas_per_sm(S->g, sp, cached) * S->sm_count;
-        const long long active = (long long)(N_time > 1 ? (N_time + 1) / 2 : 1) * (S->nzg > 1 ? (S->nzg + 1) / 2 : 1);
         const long long want = std::min<long long>((long long)S->sv_all.size(), (long long)S->sv_fit);
-        double alpha = S->sv_alpha > 0 ? S->sv_alpha : ref_alpha;
-        const double groups = (double)N_time * S->nzg;
-        const double per = std::min((double)want / (double)active,  // in flight per sinogram wanted
-                                    std::max(1.0, std::floor(0.12 * (double)S->sv_all.size() / groups)));
-        if (S->sv_alpha <= 0 && cap_for(ref_alpha) < per) {
-            const double g = per / cap_for(ref_alpha) * (2.0 / ref_alpha - 1.0);
-            alpha = std::min(ref_alpha, std::max(0.7, 2.0 / (1.0 + g)));
-        }
-        S->sv_alpha_eff = alpha;
-        S->sv_cap = cap_for(alpha);
-        S->sv_grid = (int)std::max<long long>(1, std::min<long long>(want, S->sv_cap * active));
+        sv_relaxation(S, (double)want, &S->sv_alpha_eff, &S->sv_cap, &S->sv_grid);
     }
     const size_t ctas = std::min<size_t>(std::max<size_t>(S->sv_all.size(), 1), (size_t)S->sv_fit);
     CK(dalloc(&S->d_sv_out, 2));
@@ -1483,17 +1496,33 @@ extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int3
     std::vector<SvProblem> probs(n);
     std::vector<SvTask> tasks;
     std::vector<int> base(n);
+    // each problem's share of the batch's CTAs (the queue interleaves the
+    // problems in proportion to their super-voxel counts) sets its
+    // over-relaxation and in-flight cap, as the problem's own schedule sets
+    // them for the whole GPU
+    size_t nsv_all = 0;
+    for (MbirStage *S : B->stages) nsv_all += S->sv_all.size();
+    int dev0 = 0, sms0 = 148;
+    CK(cudaGetDevice(&dev0));
+    CK(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
+    const double batch_ctas = (double)mbir_sv_batch_ctas_per_sm(B->smem, B->half) * sms0;
     for (int p = 0; p < n; p++) {
         MbirStage *S = B->stages[p];
         SvProblem &P = probs[p];
+        double alpha = S->sv_alpha_eff;
+        int cap = 0, grid = std::max(1, S->sv_grid);
+        if (!uncapped) {
+            const double share = std::max(1.0, batch_ctas * (double)S->sv_all.size() / (double)std::max<size_t>(nsv_all, 1));
+            sv_relaxation(S, std::min(share, (double)S->sv_all.size()), &alpha, &cap, &grid);
+        }
         P.g = S->g;
         P.pr = S->pr;
-        P.pr.alpha = S->sv_alpha_eff;
+        P.pr.alpha = alpha;
         P.dv = S->dv;
         P.sp = S->sp;
         P.ac = SvACache{S->d_acol};
         P.plan = mbir_sv_plan(S->sp, true);
-        P.cap = uncapped ? (1 << 30) : std::max(1, S->sv_grid);
+        P.cap = uncapped ? (1 << 30) : std::max(1, grid);
         P.K = S->K;
         P.stop = S->stop_thresh;
         base[p] = (int)tasks.size();
