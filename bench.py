@@ -638,6 +638,56 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=24, train_iters=
     print(json.dumps(line), flush=True)
 
 
+def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
+    """Training-step throughput of the warm-start network (forward, loss,
+    backward, Adam) on a batch of patches of the training shape, random data;
+    the tensor-core roofline of its convolutions (algorithmic FLOPs: per 3x3x3
+    convolution 2 M 27 Cin Cout for the forward pass, the same again for the
+    input gradient (every layer but the first) and for the weight gradient)."""
+    import torch
+    from timbir_b200 import warm
+    torch.cuda.set_device(local_rank)
+    B, D, H, Wd = shape
+    flops = 0.0
+    for k, (ci, co, lv) in enumerate(warm.LAYERS):
+        M = B * (D >> lv) * (H >> lv) * (Wd >> lv)
+        f = 2.0 * M * 27 * ci * co
+        flops += f * (3 if k > 0 else 2)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand(shape, generator=g, device="cuda") * 0.02
+    t = x * 0.9
+    net = warm.WarmNet(seed=1)
+    for _ in range(args.warmup):
+        net.gradients(x, t)
+        net.adam_step(1e-4)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        net.gradients(x, t)
+        net.adam_step(1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    net.close()
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    tf = flops / (ms / 1e3) / 1e12
+    print(json.dumps({
+        "metric": "warm-start network training steps/s", "value": 1e3 / ms, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "dtype": "bf16 operands, fp32 accumulation (mma.sync m16n8k16)", "data": "synthetic (random patches)",
+        "config": {"workload": f"one training step on {B} patches {D}x{H}x{Wd} (forward, loss, backward, Adam)",
+                   "params": sum(27 * ci * co + co for ci, co, _ in warm.LAYERS)},
+        "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                     "flops_per_step": flops, "traffic": None,
+                     "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
+    }), flush=True)
+
+
 # --------------------------------------------------------------------- GPU --
 def time_to_map(w, scan, fine, sched, args, max_iters=400):
     """Time-to-MAP of the GPU engine from the bench's warm start: device time of
@@ -687,6 +737,8 @@ def gpu_arm(args, rank, world, local_rank):
         return c3_arm(args, rank, world, local_rank)
     if args.config in ("c4", "4d-warm"):
         return c4_arm(args, rank, world, local_rank, four_d=args.config == "4d-warm")
+    if args.config == "net":
+        return net_arm(args, rank, world, local_rank)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -827,7 +879,7 @@ def gpu_arm(args, rank, world, local_rank):
 def reference_arm(args, rank):
     if rank != 0:
         return
-    if args.config in ("c4", "4d-warm"):
+    if args.config in ("c4", "4d-warm", "net"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start (its coarsest "
                           "stage starts from zero); the comparison is FBP-initialised ICD, in the same line"}),
               flush=True)
@@ -867,10 +919,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
-    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm"],
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net"],
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
                          "c3: 64 independent 3-D problems batched; c4: learned warm start (3-D); 4d-warm: learned warm "
-                         "start on the 4-D workload; c5: large 4-D z-subset")
+                         "start on the 4-D workload; net: the network's training step; c5: large 4-D z-subset")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     ap.add_argument("--problems", type=int, default=64, help="c3: the first N of the 64 problems")
     ap.add_argument("--no-tune", action="store_true", help="c3: default schedules instead of the autotuner's")

@@ -53,3 +53,9 @@ def test_fbp_oracle_reconstructs_the_phantom():
     k = np.arange(32) + 0.5 - 16
     outside = (k[None, :] ** 2 + k[:, None] ** 2) >= 16 ** 2
     assert np.all(x[..., outside] == 0)
+
+
+def test_package_layer_table_matches_the_oracle():
+    from timbir_b200 import warm
+    assert [(ci, co) for ci, co, _ in warm.LAYERS] == W.LAYERS
+    assert sum(27 * ci * co + co for ci, co, _ in warm.LAYERS) == W.param_count() == 1327824

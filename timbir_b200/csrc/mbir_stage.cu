@@ -1496,33 +1496,17 @@ extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int3
     std::vector<SvProblem> probs(n);
     std::vector<SvTask> tasks;
     std::vector<int> base(n);
-    // each problem's share of the batch's CTAs (the queue interleaves the
-    // problems in proportion to their super-voxel counts) sets its
-    // over-relaxation and in-flight cap, as the problem's own schedule sets
-    // them for the whole GPU
-    size_t nsv_all = 0;
-    for (MbirStage *S : B->stages) nsv_all += S->sv_all.size();
-    int dev0 = 0, sms0 = 148;
-    CK(cudaGetDevice(&dev0));
-    CK(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
-    const double batch_ctas = (double)mbir_sv_batch_ctas_per_sm(B->smem, B->half) * sms0;
     for (int p = 0; p < n; p++) {
         MbirStage *S = B->stages[p];
         SvProblem &P = probs[p];
-        double alpha = S->sv_alpha_eff;
-        int cap = 0, grid = std::max(1, S->sv_grid);
-        if (!uncapped) {
-            const double share = std::max(1.0, batch_ctas * (double)S->sv_all.size() / (double)std::max<size_t>(nsv_all, 1));
-            sv_relaxation(S, std::min(share, (double)S->sv_all.size()), &alpha, &cap, &grid);
-        }
         P.g = S->g;
         P.pr = S->pr;
-        P.pr.alpha = alpha;
+        P.pr.alpha = S->sv_alpha_eff;
         P.dv = S->dv;
         P.sp = S->sp;
         P.ac = SvACache{S->d_acol};
         P.plan = mbir_sv_plan(S->sp, true);
-        P.cap = uncapped ? (1 << 30) : std::max(1, grid);
+        P.cap = uncapped ? (1 << 30) : std::max(1, S->sv_grid);
         P.K = S->K;
         P.stop = S->stop_thresh;
         base[p] = (int)tasks.size();

@@ -17,6 +17,11 @@ import numpy as np
 from . import MbirError, load_library
 
 SCALE = 50.0  # attenuation per voxel ~0.02 -> order one inside the network
+# (input channels, output channels, level) of the 15 convolutions, as in
+# timbir_b200/csrc/warm_net.cu; level l works at 1 / 2^l of the input's sides
+LAYERS = [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 128, 3),
+          (128, 128, 3), (128, 64, 2), (64, 64, 2), (64, 32, 1), (32, 32, 1), (32, 16, 0), (16, 16, 0),
+          (16, 16, 0)]
 
 
 def _lib():
