@@ -22,10 +22,11 @@
 //
 // Convolutions are implicit GEMMs on mma.sync m16n8k16 (BF16 in, FP32
 // accumulate): forward M = voxels, N = output channels, K = 27 taps x input
-// channels; the input gradient is the same kernel with the flipped,
-// transposed weights; the weight gradient is a GEMM over voxels
-// (M = input channels, N = output channels, K = voxels) split over CTAs and
-// reduced with FP32 atomics.
+// channels, the input block staged in shared memory per 16-channel chunk;
+// the input gradient is the same kernel with the flipped, transposed
+// weights; the weight gradient is a GEMM over voxels (M = input channels,
+// N = output channels, K = voxels) split over CTAs and reduced with FP32
+// atomics.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -68,93 +69,122 @@ struct Shape {
     __host__ __device__ long long voxels() const { return (long long)B * D * H * W; }
 };
 
-// voxel m -> (b, z, y, x); false past the end
+// voxel m -> (b, z, y, x); false past the end (32-bit arithmetic: tensors
+// hold fewer than 2^31 voxels, which net_shape checks)
 __device__ __forceinline__ bool decode(const Shape &s, long long m, int &b, int &z, int &y, int &x)
 {
     if (m >= s.voxels()) return false;
-    x = (int)(m % s.W);
-    long long r = m / s.W;
-    y = (int)(r % s.H);
-    r /= s.H;
-    z = (int)(r % s.D);
-    b = (int)(r / s.D);
+    unsigned r = (unsigned)m;
+    x = (int)(r % (unsigned)s.W);
+    r /= (unsigned)s.W;
+    y = (int)(r % (unsigned)s.H);
+    r /= (unsigned)s.H;
+    z = (int)(r % (unsigned)s.D);
+    b = (int)(r / (unsigned)s.D);
     return true;
 }
 
 // Y[m][n] = act(sum over taps and input channels + bias[n] + add[m][n]), or
 // (accumulate) Y[m][n] += the sum.  Wp: packed B fragments, per (tap,
-// 16-channel input chunk, 8-channel output tile) one uint2 per lane.  A warp
-// computes 16 voxels x NT output tiles; a CTA 4 warps.
+// 16-channel input chunk, 8-channel output tile) one uint2 per lane.  A CTA
+// computes a 2 x 4 x 16 block of output voxels (eight m-tiles of 16
+// consecutive x, two per warp) for NT output tiles; per 16-channel input
+// chunk it stages the block's input with a one-voxel halo (4 x 6 x 18
+// voxels, BF16, 13.8 KB) in shared memory once, and every tap takes its A
+// fragments from there.
+constexpr int TZ = 2, TY = 4, TX = 16, HZ = TZ + 2, HY = TY + 2, HX = TX + 2, HV = HZ * HY * HX;
+
 template <int NT>
-__global__ void __launch_bounds__(128) k_conv3(const float *__restrict__ X, int Cin, const uint2 *__restrict__ Wp,
-                                               int Cout, const float *__restrict__ bias,
-                                               const float *__restrict__ add, int relu, int accumulate,
-                                               float *__restrict__ Y, Shape s)
+__global__ void __launch_bounds__(128) k_conv3t(const float *__restrict__ X, int Cin, const uint2 *__restrict__ Wp,
+                                                int Cout, const float *__restrict__ bias,
+                                                const float *__restrict__ add, int relu, int accumulate,
+                                                float *__restrict__ Y, Shape s)
 {
+    __shared__ __align__(16) uint2 tile[HV * 4];  // per voxel 16 BF16 channels = 4 x uint2
+    const uint32_t *tw = reinterpret_cast<const uint32_t *>(tile);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long m0 = ((long long)blockIdx.x * 4 + warp) * 16;
-    if (m0 >= s.voxels()) return;
-    const int nt0 = blockIdx.y * NT, ntiles = Cout / 8, KC = Cin / 16;
     const int g = lane >> 2, tq = lane & 3;
-    int vb[2], vz[2], vy[2], vx[2];
-    bool vin[2];
-    for (int r = 0; r < 2; r++) vin[r] = decode(s, m0 + g + 8 * r, vb[r], vz[r], vy[r], vx[r]);
-    float acc[NT][4];
+    const int ntx = (s.W + TX - 1) / TX, nty = (s.H + TY - 1) / TY, ntz = (s.D + TZ - 1) / TZ;
+    int t = blockIdx.x;
+    const int bx = t % ntx;
+    t /= ntx;
+    const int by = t % nty;
+    t /= nty;
+    const int bz = t % ntz;
+    const int b = t / ntz;
+    const int x0 = bx * TX, y0 = by * TY, z0 = bz * TZ;
+    const int nt0 = blockIdx.y * NT, ntiles = Cout / 8, KC = Cin / 16;
+    float acc[2][NT][4];
 #pragma unroll
-    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    for (int tap = 0; tap < 27; tap++) {
-        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        const float *src[2];
-        bool ok[2];
-        for (int r = 0; r < 2; r++) {
-            const int z = vz[r] + dz, y = vy[r] + dy, x = vx[r] + dx;
-            ok[r] = vin[r] && z >= 0 && z < s.D && y >= 0 && y < s.H && x >= 0 && x < s.W;
-            src[r] = ok[r] ? X + ((((size_t)vb[r] * s.D + z) * s.H + y) * s.W + x) * Cin : X;
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int j = 0; j < NT; j++) acc[mt][j][0] = acc[mt][j][1] = acc[mt][j][2] = acc[mt][j][3] = 0.0f;
+    for (int kc = 0; kc < KC; kc++) {
+        __syncthreads();  // the previous chunk's tile is consumed
+        for (int q = threadIdx.x; q < HV * 4; q += blockDim.x) {
+            const int v = q >> 2, part = q & 3;
+            const int lx = v % HX, ly = (v / HX) % HY, lz = v / (HX * HY);
+            const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
+                f = __ldg(reinterpret_cast<const float4 *>(
+                    X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
+            tile[q] = make_uint2(pack_bf16(f.x, f.y), pack_bf16(f.z, f.w));
         }
-        for (int kc = 0; kc < KC; kc++) {
-            const int c = kc * 16 + 2 * tq;
-            const float2 z2 = make_float2(0.0f, 0.0f);
-            const float2 p0 = ok[0] ? __ldg(reinterpret_cast<const float2 *>(src[0] + c)) : z2;
-            const float2 p1 = ok[1] ? __ldg(reinterpret_cast<const float2 *>(src[1] + c)) : z2;
-            const float2 p2 = ok[0] ? __ldg(reinterpret_cast<const float2 *>(src[0] + c + 8)) : z2;
-            const float2 p3 = ok[1] ? __ldg(reinterpret_cast<const float2 *>(src[1] + c + 8)) : z2;
-            const uint32_t a0 = pack_bf16(p0.x, p0.y), a1 = pack_bf16(p1.x, p1.y);
-            const uint32_t a2 = pack_bf16(p2.x, p2.y), a3 = pack_bf16(p3.x, p3.y);
+        __syncthreads();
+        for (int tap = 0; tap < 27; tap++) {
+            const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
             const uint2 *wp = Wp + ((size_t)(tap * KC + kc) * ntiles + nt0) * 32 + lane;
+            uint2 bb[NT];
 #pragma unroll
-            for (int j = 0; j < NT; j++) {
-                const uint2 bb = __ldg(wp + j * 32);
-                mma_bf16(acc[j], a0, a1, a2, a3, bb.x, bb.y);
+            for (int j = 0; j < NT; j++) bb[j] = __ldg(wp + j * 32);
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                const int m = warp * 2 + mt;  // m-tile: output row (oz, oy), x = 0..15
+                const int oz = m / TY, oy = m % TY;
+                const int vb = ((oz + 1 + dz) * HY + (oy + 1 + dy)) * HX + 1 + dx;
+                const uint32_t *r0 = tw + (size_t)(vb + g) * 8, *r1 = tw + (size_t)(vb + g + 8) * 8;
+                const uint32_t a0 = r0[tq], a1 = r1[tq], a2 = r0[4 + tq], a3 = r1[4 + tq];
+#pragma unroll
+                for (int j = 0; j < NT; j++) mma_bf16(acc[mt][j], a0, a1, a2, a3, bb[j].x, bb[j].y);
             }
         }
     }
-    for (int r = 0; r < 2; r++) {
-        if (!vin[r]) continue;
-        const long long m = m0 + g + 8 * r;
 #pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const int n = (nt0 + j) * 8 + 2 * tq;
-            float v0 = acc[j][2 * r], v1 = acc[j][2 * r + 1];
-            if (bias) {
-                v0 += bias[n];
-                v1 += bias[n + 1];
+    for (int mt = 0; mt < 2; mt++) {
+        const int m = warp * 2 + mt;
+        const int oz = m / TY, oy = m % TY;
+        const int z = z0 + oz, y = y0 + oy;
+        if (z >= s.D || y >= s.H) continue;
+        for (int r = 0; r < 2; r++) {
+            const int x = x0 + g + 8 * r;
+            if (x >= s.W) continue;
+            const size_t mo = (((size_t)b * s.D + z) * s.H + y) * s.W + x;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const int n = (nt0 + j) * 8 + 2 * tq;
+                float v0 = acc[mt][j][2 * r], v1 = acc[mt][j][2 * r + 1];
+                if (bias) {
+                    v0 += bias[n];
+                    v1 += bias[n + 1];
+                }
+                float2 *yp = reinterpret_cast<float2 *>(Y + mo * Cout + n);
+                if (add) {
+                    const float2 a = *reinterpret_cast<const float2 *>(add + mo * Cout + n);
+                    v0 += a.x;
+                    v1 += a.y;
+                }
+                if (relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                if (accumulate) {
+                    const float2 o = *yp;
+                    v0 += o.x;
+                    v1 += o.y;
+                }
+                *yp = make_float2(v0, v1);
             }
-            float2 *y = reinterpret_cast<float2 *>(Y + (size_t)m * Cout + n);
-            if (add) {
-                const float2 a = *reinterpret_cast<const float2 *>(add + (size_t)m * Cout + n);
-                v0 += a.x;
-                v1 += a.y;
-            }
-            if (relu) {
-                v0 = fmaxf(v0, 0.0f);
-                v1 = fmaxf(v1, 0.0f);
-            }
-            if (accumulate) {
-                const float2 o = *y;
-                v0 += o.x;
-                v1 += o.y;
-            }
-            *y = make_float2(v0, v1);
         }
     }
 }
@@ -482,6 +512,7 @@ static int net_shape(MbirNet *N, const Shape &s, bool train)
         return 0;
     if (s.D % 8 || s.H % 8 || s.W % 8 || s.B < 1)
         return net_fail("network input sides must be multiples of 8");
+    if (s.voxels() >= (1LL << 31)) return net_fail("network input above 2^31 voxels");
     for (auto &t : N->act)
         if (t.p) cudaFree(t.p);
     for (auto &t : N->grad)
@@ -514,12 +545,13 @@ static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, cons
                         int relu, int accumulate, float *Y, const Shape &s, cudaStream_t st)
 {
     const int NT = std::min(cout / 8, 8);
-    const dim3 grid((unsigned)((s.voxels() + 63) / 64), (unsigned)(cout / 8 / NT));
+    const long long tiles = (long long)s.B * ((s.D + TZ - 1) / TZ) * ((s.H + TY - 1) / TY) * ((s.W + TX - 1) / TX);
+    const dim3 grid((unsigned)tiles, (unsigned)(cout / 8 / NT));
     switch (NT) {
-    case 1: k_conv3<1><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    case 2: k_conv3<2><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    case 4: k_conv3<4><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    default: k_conv3<8><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    case 1: k_conv3t<1><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    case 2: k_conv3t<2><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    case 4: k_conv3t<4><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
+    default: k_conv3t<8><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
     }
     return cudaGetLastError();
 }
