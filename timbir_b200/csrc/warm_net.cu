@@ -25,8 +25,8 @@
 // channels, the input block staged in shared memory per 16-channel chunk;
 // the input gradient is the same kernel with the flipped, transposed
 // weights; the weight gradient is a GEMM over voxels (M = input channels,
-// N = output channels, K = voxels) split over CTAs and reduced with FP32
-// atomics.
+// N = output channels, K = voxels) over staged blocks, reduced over CTAs
+// with FP32 atomics.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -189,67 +189,113 @@ __global__ void __launch_bounds__(128) k_conv3t(const float *__restrict__ X, int
     }
 }
 
-// dW[tap][ci][co] += sum over voxels m of X[m shifted by tap][ci] dY[m][co],
-// tap = blockIdx.y, voxels [blockIdx.x * chunk, + chunk); warp w: input
-// channels 16 (w % (Cin / 16)) .. + 16, output tiles NT (w / (Cin / 16)) ...
+// Weight gradient, tiled: a CTA owns one 16-channel input chunk and NT
+// output tiles and walks 2 x 4 x 16 voxel blocks; per block it stages the
+// input with a one-voxel halo as [channel][voxel] BF16 (twice: aligned and
+// shifted by one voxel, so that every tap's pair of consecutive voxels is one
+// aligned 32-bit word) and the block's output gradient as [channel][voxel]
+// BF16; warp w accumulates taps w, w + 9, w + 18 over the blocks (K = voxels,
+// 16 per step), then adds its sums to dW with FP32 atomics.
+constexpr int kWgWarps = 9;
+
 template <int NT>
-__global__ void __launch_bounds__(512) k_wgrad3(const float *__restrict__ X, int Cin,
-                                                const float *__restrict__ dY, int Cout, float *__restrict__ dW,
-                                                Shape s, long long chunk)
+__global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restrict__ X, int Cin,
+                                                          const float *__restrict__ dY, int Cout,
+                                                          float *__restrict__ dW, Shape s)
 {
+    __shared__ __align__(16) __nv_bfloat16 xs[2][16][HV];
+    __shared__ __align__(16) __nv_bfloat16 ys[NT * 8][TZ * TY * TX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tap = blockIdx.y;
-    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-    const int ci_tiles = Cin / 16;
-    const int ci0 = (warp % ci_tiles) * 16, nt0 = (warp / ci_tiles) * NT;
     const int g = lane >> 2, tq = lane & 3;
-    const long long M = s.voxels();
-    const long long start = (long long)blockIdx.x * chunk, end = min(M, start + chunk);
-    float acc[NT][4];
+    const int ci0 = blockIdx.y * 16, co0 = blockIdx.z * NT * 8;
+    const int ntx = (s.W + TX - 1) / TX, nty = (s.H + TY - 1) / TY, ntz = (s.D + TZ - 1) / TZ;
+    const int nblocks = s.B * ntz * nty * ntx;
+    float acc[3][NT][4];
 #pragma unroll
-    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    for (long long m0 = start; m0 < end; m0 += 16) {
-        // the four voxels of this thread's fragment columns: m0 + 2 tq + {0, 1, 8, 9}
-        float xa[4], xb[4];  // X at input channels ci0 + g, ci0 + g + 8
-        size_t yo[4];        // dY row offsets (unshifted)
-        bool yv[4];
+    for (int u = 0; u < 3; u++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const long long m = m0 + 2 * tq + (q & 1) + 8 * (q >> 1);
-            int b, z, y, x;
-            xa[q] = xb[q] = 0.0f;
-            yv[q] = m < end && decode(s, m, b, z, y, x);
-            yo[q] = (size_t)m * Cout;
-            if (yv[q]) {
-                const int zz = z + dz, yy = y + dy, xx = x + dx;
-                if (zz >= 0 && zz < s.D && yy >= 0 && yy < s.H && xx >= 0 && xx < s.W) {
-                    const float *p = X + ((((size_t)b * s.D + zz) * s.H + yy) * s.W + xx) * Cin + ci0 + g;
-                    xa[q] = __ldg(p);
-                    xb[q] = __ldg(p + 8);
-                }
+        for (int j = 0; j < NT; j++) acc[u][j][0] = acc[u][j][1] = acc[u][j][2] = acc[u][j][3] = 0.0f;
+    for (int blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+        int t = blk;
+        const int bx = t % ntx;
+        t /= ntx;
+        const int by = t % nty;
+        t /= nty;
+        const int bz = t % ntz;
+        const int b = t / ntz;
+        const int x0 = bx * TX, y0 = by * TY, z0 = bz * TZ;
+        __syncthreads();  // the previous block's tiles are consumed
+        for (int q = threadIdx.x; q < HV * 4; q += blockDim.x) {
+            const int v = q >> 2, part = q & 3;
+            const int lx = v % HX, ly = (v / HX) % HY, lz = v / (HX * HY);
+            const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
+                f = __ldg(reinterpret_cast<const float4 *>(
+                    X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + ci0 + part * 4));
+            const float fv[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(fv[c]);
+                xs[0][part * 4 + c][v] = h;
+                if (v > 0) xs[1][part * 4 + c][v - 1] = h;
             }
-        }
-        // A[ci][m]: rows ci0 + g (a0, a1) and + 8 (a2, a3), columns 2 tq (+1)
-        // for a0..a3 and 2 tq + 8 (+1) for a4..a7
-        const uint32_t a0 = pack_bf16(xa[0], xa[1]), a1 = pack_bf16(xb[0], xb[1]);
-        const uint32_t a2 = pack_bf16(xa[2], xa[3]), a3 = pack_bf16(xb[2], xb[3]);
+            if (v == HV - 1)
 #pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const int co = (nt0 + j) * 8 + g;
-            const float y0 = yv[0] ? __ldg(dY + yo[0] + co) : 0.0f, y1 = yv[1] ? __ldg(dY + yo[1] + co) : 0.0f;
-            const float y2 = yv[2] ? __ldg(dY + yo[2] + co) : 0.0f, y3 = yv[3] ? __ldg(dY + yo[3] + co) : 0.0f;
-            mma_bf16(acc[j], a0, a1, a2, a3, pack_bf16(y0, y1), pack_bf16(y2, y3));
+                for (int c = 0; c < 4; c++) xs[1][part * 4 + c][HV - 1] = __float2bfloat16_rn(0.0f);
+        }
+        for (int q = threadIdx.x; q < TZ * TY * TX * NT * 2; q += blockDim.x) {
+            const int i = q / (NT * 2), part = q % (NT * 2);  // block voxel, 4 output channels
+            const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
+            const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (x < s.W && y < s.H && z < s.D)
+                f = __ldg(reinterpret_cast<const float4 *>(
+                    dY + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cout + co0 + part * 4));
+            ys[part * 4 + 0][i] = __float2bfloat16_rn(f.x);
+            ys[part * 4 + 1][i] = __float2bfloat16_rn(f.y);
+            ys[part * 4 + 2][i] = __float2bfloat16_rn(f.z);
+            ys[part * 4 + 3][i] = __float2bfloat16_rn(f.w);
+        }
+        __syncthreads();
+        const uint32_t *yw = reinterpret_cast<const uint32_t *>(&ys[0][0]);
+#pragma unroll 1
+        for (int r = 0; r < TZ * TY; r++) {  // k-step: the 16 voxels of block row r
+            const int oz = r / TY, oy = r % TY;
+            uint32_t b0[NT], b1[NT];
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const int w0 = ((j * 8 + g) * (TZ * TY * TX) + r * TX + 2 * tq) >> 1;
+                b0[j] = yw[w0];
+                b1[j] = yw[w0 + 4];
+            }
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                const int tap = warp + kWgWarps * u;
+                const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                const int v0 = ((oz + 1 + dz) * HY + (oy + 1 + dy)) * HX + 1 + dx;
+                const int par = v0 & 1;
+                const uint32_t *xw = reinterpret_cast<const uint32_t *>(&xs[par][0][0]);
+                const int wa = (g * HV + v0 - par + 2 * tq) >> 1, wb = ((g + 8) * HV + v0 - par + 2 * tq) >> 1;
+                const uint32_t a0 = xw[wa], a1 = xw[wb], a2 = xw[wa + 4], a3 = xw[wb + 4];
+#pragma unroll
+                for (int j = 0; j < NT; j++) mma_bf16(acc[u][j], a0, a1, a2, a3, b0[j], b1[j]);
+            }
         }
     }
 #pragma unroll
-    for (int j = 0; j < NT; j++) {
-        const int co = (nt0 + j) * 8 + 2 * tq;
-        float *w0 = dW + ((size_t)tap * Cin + ci0 + g) * Cout + co;
-        float *w1 = w0 + (size_t)8 * Cout;
-        atomicAdd(w0, acc[j][0]);
-        atomicAdd(w0 + 1, acc[j][1]);
-        atomicAdd(w1, acc[j][2]);
-        atomicAdd(w1 + 1, acc[j][3]);
+    for (int u = 0; u < 3; u++) {
+        const int tap = warp + kWgWarps * u;
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int co = co0 + j * 8 + 2 * tq;
+            float *w0 = dW + ((size_t)tap * Cin + ci0 + g) * Cout + co;
+            float *w1 = w0 + (size_t)8 * Cout;
+            atomicAdd(w0, acc[u][j][0]);
+            atomicAdd(w0 + 1, acc[u][j][1]);
+            atomicAdd(w1, acc[u][j][2]);
+            atomicAdd(w1 + 1, acc[u][j][3]);
+        }
     }
 }
 
@@ -559,22 +605,17 @@ static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, cons
 static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, float *dW, float *db, const Shape &s,
                          cudaStream_t st)
 {
-    const int NT = std::min(cout / 8, 8);
-    const int warps = (cin / 16) * (cout / 8 / NT);
-    const long long M = s.voxels();
-    long long nch = std::max(1LL, std::min(M / 512, 160LL));
-    long long chunk = (M + nch - 1) / nch;
-    chunk = (chunk + 15) / 16 * 16;
-    nch = (M + chunk - 1) / chunk;
-    const dim3 grid((unsigned)nch, 27);
+    const int NT = std::min(cout / 8, 4);
+    const long long blocks_ = (long long)s.B * ((s.D + TZ - 1) / TZ) * ((s.H + TY - 1) / TY) * ((s.W + TX - 1) / TX);
+    const dim3 grid((unsigned)std::min<long long>(blocks_, 128), (unsigned)(cin / 16), (unsigned)(cout / 8 / NT));
     switch (NT) {
-    case 1: k_wgrad3<1><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
-    case 2: k_wgrad3<2><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
-    case 4: k_wgrad3<4><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
-    default: k_wgrad3<8><<<grid, 32 * warps, 0, st>>>(X, cin, dY, cout, dW, s, chunk); break;
+    case 1: k_wgrad3t<1><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
+    case 2: k_wgrad3t<2><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
+    default: k_wgrad3t<4><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    const long long M = s.voxels();
     const long long bch = std::max(1LL, std::min(M / 1024, 1024LL));
     const long long bchunk = (M + bch - 1) / bch;
     k_bias_grad<<<(unsigned)bch, 256, 0, st>>>(dY, cout, M, bchunk, db);
