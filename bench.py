@@ -95,9 +95,9 @@ WC5 = Workload("c5", "large 4d z-subset: 32 x 2048x2048 x 4 of 64 detector rows,
 WORKLOADS = {"3d": W3D, "4d": W4D, "c5": WC5}
 METRIC = "ICD voxel-updates/s"
 # DRAM bytes (read + write) per voxel update of the super-voxel kernel, from
-# one ncu capture of a full-sweep launch (profiles/k_icd_sv_3d_256x256x8.md:
-# 217.6 MB read + 5.8 MB written over the 411,744 in-mask voxels of the 3-D
-# workload); the line's roofline.traffic scales it to the average launch.
+# one ncu capture of a full-sweep launch on the 3-D workload (217.6 MB read +
+# 5.8 MB written over its 411,744 in-mask voxels); the line's roofline.traffic
+# scales it to the average launch.
 DRAM_BYTES_PER_UPDATE = {"3d": (217.594e6 + 5.823e6) / 411744}
 
 

@@ -187,9 +187,11 @@ int mbir_time_end(MbirStage *stage, double *ms);
 /* Ring-offset update that allocates no device memory.  No counterpart in the
  * reference: it is mbir_update_sinogram_offset's computation (the reference's
  * update_Sinogram_Offset) on device arrays the caller owns, for callers that
- * must not allocate device memory -- code running while a CUDA graph is
- * captured, where an allocation breaks the capture, or a host framework that
- * owns every device allocation and forbids libraries to call cudaMalloc.
+ * cannot allocate device memory -- an application or acquisition framework
+ * that reserves all of the GPU's memory for its own pool at start-up (so
+ * cudaMalloc fails) and forbids libraries to allocate behind its back, or a
+ * processing loop that must not take cudaMalloc's implicit device-wide
+ * synchronisation.
  *   e  device float [N_t][N_p][N_r]  error sinogram, updated in place
  *   w  device float [N_t][N_p][N_r]  weights
  *   d  device float [N_t][N_r]       ring offsets, updated in place
@@ -199,10 +201,11 @@ int mbir_time_end(MbirStage *stage, double *ms);
  * device array of MBIR_NOALLOC_MAX_ELEMS detector elements (16 MiB, held by
  * every GPU that loads the library until exit); larger detectors are rejected
  * with an error (-1, message from mbir_noalloc_last_error()).  The first call
- * on a device looks the array's address up, so make that first call before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU (other streams, other host threads) race and must be serialised by the
- * caller.  Nothing in the array needs to start at zero. */
+ * on a device looks the array's address up and caches it for the process's
+ * life, so make that first call before any stream capture, and do not call
+ * it on a device after cudaDeviceReset.  All calls share the array: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller.  Nothing in the array needs to start at zero. */
 #define MBIR_NOALLOC_MAX_ELEMS (1 << 20)
 int mbir_update_sinogram_offset_noalloc(float *e, const float *w, float *d, int32_t N_p, int32_t N_r,
                                         int32_t N_t, int32_t remove_rings, int32_t quad_convex,

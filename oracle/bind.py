@@ -36,9 +36,16 @@ def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
 
 
-def build_reference(ref_src: str = "/root/reference/src") -> bool:
-    """Compile the reference where its sources lie; False if they are absent."""
-    if not os.path.isdir(os.path.join(ref_src, "MBIR_4D")):
+def reference_src() -> str:
+    """The reference tree's src/ directory, from TIMBIR_REFERENCE_SRC ('' if unset)."""
+    return os.environ.get("TIMBIR_REFERENCE_SRC", "")
+
+
+def build_reference(ref_src: str = "") -> bool:
+    """Compile the reference where its sources lie (ref_src, else
+    TIMBIR_REFERENCE_SRC); False if they are absent."""
+    ref_src = ref_src or reference_src()
+    if not ref_src or not os.path.isdir(os.path.join(ref_src, "MBIR_4D")):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_src}"], check=True)
     return True

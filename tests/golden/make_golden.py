@@ -1,9 +1,11 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Needs the reference library built from its own sources (``make -C oracle ref``,
-which needs the TIMBIR tree).  Run from the repository root:
+which needs the TIMBIR tree) and, for the generator's known-answer table, the
+environment variable TIMBIR_REFERENCE_SRC set to the tree's src directory.
+Run from the repository root:
 
-    python tests/golden/make_golden.py
+    TIMBIR_REFERENCE_SRC=<reference>/src python tests/golden/make_golden.py
 
 Outputs (committed):
   park_miller_seed1.json   the known-answer table of the reference's generator,
@@ -30,12 +32,12 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-from oracle.bind import REF_BIN, Reference  # noqa: E402
+from oracle.bind import REF_BIN, Reference, reference_src  # noqa: E402
 from timbir_b200 import synth  # noqa: E402
 
 import scenarios  # noqa: E402
 
-REF_SRC = "/root/reference/src"
+REF_SRC = reference_src()  # TIMBIR_REFERENCE_SRC: the reference tree's src directory
 
 
 def park_miller_table():

@@ -1,7 +1,6 @@
 """GPU tests of the learned warm start: the filtered backprojection and the
 network's forward pass, parameter gradients and Adam step against the CPU
-oracles (oracle/fbp.py, oracle/warm_net.py), and what a trained network
-gains over FBP-initialised ICD.
+oracles (oracle/fbp.py, oracle/warm_net.py).
 
 Tolerances: the network's tensor-core products take BF16 operands (the
 oracle rounds the same operands to BF16) and accumulate in FP32 inside the

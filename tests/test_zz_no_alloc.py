@@ -1,7 +1,8 @@
 """The ring-offset update that allocates no device memory.
 
-Callers that must not allocate device memory -- code running inside a CUDA
-graph capture, or a host framework that owns all device allocations -- use
+Callers that cannot allocate device memory -- an application that reserves
+all of the GPU's memory for its own pool at start-up, or a loop that must not
+take cudaMalloc's device-wide synchronisation -- use
 mbir_update_sinogram_offset_noalloc() on device arrays they own; its scratch
 is a fixed array inside the library.  This test gives it the state of a stage
 (the test itself may allocate: it plays the caller's framework, with torch as
@@ -38,7 +39,7 @@ def bind():
     return lib, f
 
 
-@pytest.mark.parametrize("name", ["rings2", "zinger_var"])
+@pytest.mark.parametrize("name", ["rings1", "rings2", "rings3", "zinger_var"])
 def test_noalloc_offset_update_matches_stage_entry_point(name):
     import torch
     lib, noalloc = bind()

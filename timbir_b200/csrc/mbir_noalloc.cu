@@ -4,11 +4,16 @@
 // stage-level ring-offset update, on device arrays the caller owns, with its
 // scratch (per-detector-element numerators and denominators and the partial
 // sums of the zero-mean constraint) in a file-scope device array instead of
-// memory from cudaMalloc.  It is meant for callers that must not allocate
-// device memory: code that runs while a CUDA graph is being captured (an
-// allocation would break the capture), or a host framework that owns every
-// device allocation through its own allocator and forbids libraries to call
-// cudaMalloc behind its back.
+// memory from cudaMalloc.  It is meant for callers that cannot allocate
+// device memory: a host application or acquisition framework that reserves
+// all of the GPU's memory for its own pool at start-up (cudaMalloc would then
+// fail) and forbids libraries to allocate behind its back, or a processing
+// loop that must not take cudaMalloc's implicit device-wide synchronisation.
+//
+// The array's device address is looked up once per device (the first call
+// with that device current) and cached for the life of the process; after
+// cudaDeviceReset the cached address is stale, so a process that resets a
+// device must not call this entry point on it again.
 #include <cuda_runtime.h>
 
 #include <mutex>
