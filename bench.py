@@ -92,7 +92,46 @@ WC5 = Workload("c5", "large 4d z-subset: 32 x 2048x2048 x 4 of 64 detector rows,
                dict(sig_s=0.00025, sig_t=0.0005, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=2, quad_convex=0,
                     huber_delta=0.5, huber_T=4.0),
                "synthetic (seeded drifting random ellipsoids, exact line integrals, Poisson counts, zingers, rings)")
-WORKLOADS = {"3d": W3D, "4d": W4D, "c5": WC5}
+W4DC = Workload("4dc", "4d two-phase microstructure 16 x 256x256x16 as the 4d workload, convex model: quadratic "
+                "data term (quad_convex=1), zero-mean ring offsets (remove_rings=2), finest stage", 256, 16, 1024, 16,
+                dict(W4D.prior, quad_convex=1), W4D.data)
+WORKLOADS = {"3d": W3D, "4d": W4D, "4dc": W4DC, "c5": WC5}
+
+
+def finest_stage_switches(prior):
+    """Stage switches of the finest multi-resolution stage (XT_Init.c:245-266,
+    XT_Engine.c:111-141): ring offsets updated (mode 3, starting from the
+    offsets handed over) when remove_rings > 0, the variance re-estimated
+    when quad_convex = 0."""
+    sw = {}
+    if prior["remove_rings"]:
+        sw["update_proj_offset"] = 3
+    if not prior["quad_convex"]:
+        sw["update_var"] = 1
+        sw["var_est"] = 1.0
+    return sw
+
+
+def zero_offsets(scan):
+    """Ring offsets [N_r][N_t] handed to the finest stage: zero (as
+    PROJ_OFFSET_INIT leaves them on the reference's first stage)."""
+    return np.zeros((scan.proj_cols, scan.proj_rows), np.float32)
+
+
+def workload_stage(w, scan, sched, args, prior=None):
+    """A finest-stage Stage of workload w with its schedule and switches."""
+    import timbir_b200
+    prior = prior or w.prior
+    st = timbir_b200.Stage(scan, **prior, blocks=2 if w.rows < 8 else 8)
+    st.set_switches(**finest_stage_switches(prior))
+    if args.zgroup:
+        st.set_sv_zgroup(args.zgroup)
+    st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
+    if sched and getattr(args, "nhicd", -1.0) >= 0:
+        st.set_sv_nhicd(args.nhicd)
+    return st
+
+
 METRIC = "ICD voxel-updates/s"
 # DRAM bytes (read + write) per voxel update of the super-voxel kernel, from
 # one ncu capture of a full-sweep launch on the 3-D workload (217.6 MB read +
@@ -104,23 +143,17 @@ DRAM_BYTES_PER_UPDATE = {"3d": (217.594e6 + 5.823e6) / 411744}
 def fourd_scan(w, seed_offset=0):
     """Config-2 stand-in: thresholded smoothed Gaussian random field coarsened
     by curvature-flow steps, 16 frames; views interlaced in K = 16 sub-frames,
-    8 rotations of 128 views, 64 views per frame; projected with the engine's
-    own forward projector (the reconstruction's model), Poisson counts at
-    I0 = 5e3, 0.1% of readings x10 (zingers), per-(row, column) log offsets
+    8 rotations of 128 views, 64 views per frame; line integrals of the
+    voxelised frames (synth.project_frames, float64 on the CPU), Poisson counts
+    at I0 = 5e3, 0.1% of readings x10 (zingers), per-(row, column) log offsets
     ~ N(0, 0.02) (rings)."""
-    import timbir_b200
     rng = np.random.default_rng(100 + seed_offset)
     frames = synth.two_phase_frames(w.n_xy, w.rows, w.frames, seed=seed_offset)
     angles = synth.interlaced_angles(16, w.views, 128)
     times = np.arange(w.views, dtype=np.float32)
     rt = np.linspace(0, w.views, w.frames + 1).astype(np.float32)
-    zero = np.zeros((w.views, w.rows, w.n_xy), np.float32)
-    proto = synth.Scan(zero, np.ones_like(zero), angles, times, rt, w.rows, w.n_xy, w.views, w.frames, 1.0,
-                       w.n_xy / 2.0, frames)
-    st = timbir_b200.Stage(proto, **w.prior, blocks=2)
-    li = st.forward_project(frames)
-    st.close()
-    proj, wts = synth.counts_to_data(li.astype(np.float64), 5e3, rng, zinger_frac=0.001, ring_sigma=0.02)
+    li = synth.project_frames(frames, angles, rt, times, w.n_xy)
+    proj, wts = synth.counts_to_data(li, 5e3, rng, zinger_frac=0.001, ring_sigma=0.02)
     return synth.Scan(proj, wts, angles, times, rt, w.rows, w.n_xy, w.views, w.frames, 1.0, w.n_xy / 2.0, frames)
 
 
@@ -288,7 +321,29 @@ def cpu_measure(w, scan, coarse, fine, warm, steps, threads):
     timed = its[warm:] if len(its) > warm else its
     secs = sum(t for t, _ in timed)
     upd = sum(u for _, u in timed)
+    cpu_measure.iterations = its  # every iteration's (seconds, updates), warm-up included
     return upd / secs, kind, cores, len(timed), secs
+
+
+def reference_time_to_map(w, scan, its, kind):
+    """The reference's time-to-MAP on this host: its iterations to (1 + 1e-5) C*
+    from the bench's warm start (counted where the fixture was made, from a
+    fresh FP64 cost after each iteration of the reference library) times the
+    iteration times this run measured -- the sum of the first ones when the run
+    went that far, else their mean x the count (labelled extrapolated)."""
+    ref = reference_map(w, scan)
+    if not ref or not ref["ref_iterations"] or ref["ref_iterations"] < 0 or kind != "reference":
+        return None
+    n = ref["ref_iterations"]
+    secs = [t for t, _ in its]
+    if len(secs) >= n:
+        v, how = sum(secs[:n]), f"measured: the first {n} iterations of this run"
+    else:
+        v, how = n * sum(secs) / len(secs), f"extrapolated: {n} x the mean of {len(secs)} measured iterations"
+    return {"value": v, "unit": "s", "iterations": n, "target": "FP64 MAP cost <= (1 + 1e-5) C*",
+            "cstar": ref["cstar"], "timed": how,
+            "iterations_source": "reference library from the same warm start, fresh FP64 cost after each iteration "
+                                 "(tests/golden/converged_%s.npz)" % w.name}
 
 
 # ------------------------------------------------------------ batched (c3) --
@@ -486,13 +541,12 @@ C4_DESC = ("learned warm start: 3-D encoder-decoder network (4 levels, 16-128 ch
            "256x256x16, 384 views, I0 log-uniform in [2e3, 5e4]; ICD from its output vs from FBP to (1 + 1e-5) C*")
 C4_PRIOR = dict(W3D.prior)
 C4_DATA = ("synthetic (seeded random-ellipsoid phantoms with exact line integrals, and two-phase Gaussian-random-field "
-           "phantoms projected by the engine; Poisson counts)")
+           "phantoms projected on the CPU; Poisson counts)")
 
 
 def c4_scan(k, n_xy=256, rows=16, views=384):
     """Scan k of the learned-warm-start workload: even k a random-ellipsoid
     phantom, odd k a two-phase Gaussian-random-field phantom."""
-    import timbir_b200
     rng = np.random.default_rng(5000 + k)
     I0 = float(np.exp(rng.uniform(np.log(2e3), np.log(5e4))))
     if k % 2 == 0:
@@ -501,12 +555,8 @@ def c4_scan(k, n_xy=256, rows=16, views=384):
     angles = (np.arange(views) * np.pi / views).astype(np.float32)
     times = np.arange(views, dtype=np.float32)
     rt = np.array([0.0, float(views)], np.float32)
-    zero = np.zeros((views, rows, n_xy), np.float32)
-    proto = synth.Scan(zero, np.ones_like(zero), angles, times, rt, rows, n_xy, views, 1, 1.0, n_xy / 2.0, ph)
-    st = timbir_b200.Stage(proto, **C4_PRIOR, blocks=2)
-    li = st.forward_project(ph)
-    st.close()
-    proj, wts = synth.counts_to_data(li.astype(np.float64), I0, rng)
+    li = synth.project_frames(ph, angles, rt, times, n_xy)
+    proj, wts = synth.counts_to_data(li, I0, rng)
     return synth.Scan(proj, wts, angles, times, rt, rows, n_xy, views, 1, 1.0, n_xy / 2.0, ph)
 
 
@@ -689,34 +739,57 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
 
 
 # --------------------------------------------------------------------- GPU --
+def reference_map(w, scan):
+    """The converged MAP cost C* of workload w's scan from the reference library
+    and the FP64 oracle (tests/golden/converged_<name>.npz, made by
+    tests/golden/make_converged_full.py), with the reference's iterations to
+    (1 + 1e-5) C* from the bench's warm start; None when there is no fixture
+    for w or it was made for another scan (SHA-256 of projections and
+    weights)."""
+    import hashlib
+    path = os.path.join(ROOT, "tests", "golden", f"converged_{w.name}.npz")
+    if not os.path.exists(path):
+        return None
+    g = np.load(path)
+    dig = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()  # noqa: E731
+    if dig(scan.projections) != str(g["proj_sha256"]) or dig(scan.weights) != str(g["weight_sha256"]):
+        return None
+    n = int(g["ref_iterations_to_target"]) if "ref_iterations_to_target" in g.files else None
+    return {"cstar": float(g["cstar"]), "ref_iterations": n, "ref_fresh_cost": float(g["ref_fresh_cost"]),
+            "f64_fresh_cost": float(g["f64_fresh_cost"])}
+
+
 def time_to_map(w, scan, fine, sched, args, max_iters=400):
     """Time-to-MAP of the GPU engine from the bench's warm start: device time of
     the ICD iterations (CUDA events on the stage's stream, host work inside an
     iteration included) until the MAP cost -- evaluated in FP64 on the GPU after
-    each iteration, not timed -- is within (1 + 1e-5) of C*, the cost the same
-    schedule converges to (iterated until two successive costs agree to 1e-10
-    relative, at most max_iters iterations)."""
-    import timbir_b200
-
+    each iteration, not timed -- is within (1 + 1e-5) of C*.  C* is the
+    reference's converged cost (reference library to a flat cost, then the
+    FP64 oracle; costs evaluated afresh in FP64) where a fixture exists for the
+    workload, else the cost this schedule converges to (iterated until two
+    successive costs agree to 1e-10 relative, at most max_iters iterations)."""
     def stage():
-        st = timbir_b200.Stage(scan, **w.prior, blocks=2 if w.rows < 8 else 8)
-        st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
-        st.prepare(fine)
+        st = workload_stage(w, scan, sched, args)
+        st.prepare(fine, zero_offsets(scan) if w.prior["remove_rings"] else None)
         return st
 
+    ref = reference_map(w, scan)
+    if ref:
+        cstar, n_star, source = ref["cstar"], None, "reference library + FP64 oracle, converged (fixture)"
+    else:
+        st = stage()
+        prev, n_star = None, max_iters
+        for it in range(1, max_iters + 1):
+            st.iterate(it)
+            c = st.cost()[0]
+            if prev is not None and abs(prev - c) <= 1e-10 * abs(c):
+                n_star = it
+                break
+            prev = c
+        cstar, source = c, "this schedule's own converged cost"
+        st.close()
     st = stage()
-    prev, n_star = None, max_iters
-    for it in range(1, max_iters + 1):
-        st.iterate(it)
-        c = st.cost()[0]
-        if prev is not None and abs(prev - c) <= 1e-10 * abs(c):
-            n_star = it
-            break
-        prev = c
-    cstar = c
-    st.close()
-    st = stage()
-    ms, n = 0.0, max_iters
+    ms, n = 0.0, None
     for it in range(1, max_iters + 1):
         st.time_begin()
         st.iterate(it)
@@ -725,9 +798,15 @@ def time_to_map(w, scan, fine, sched, args, max_iters=400):
             n = it
             break
     st.close()
-    return {"value": ms / 1e3, "unit": "s", "iterations": n, "target": "FP64 MAP cost <= (1 + 1e-5) C*",
-            "cstar": cstar, "cstar_iterations": n_star, "start": "2x-coarser phantom up-sampled (the stage's warm start)",
-            "timed": "ICD iterations only (cost evaluations excluded)"}
+    out = {"value": ms / 1e3 if n else None, "unit": "s", "iterations": n, "target": "FP64 MAP cost <= (1 + 1e-5) C*",
+           "cstar": cstar, "cstar_source": source,
+           "start": "2x-coarser phantom up-sampled (the stage's warm start)",
+           "timed": "ICD iterations only (cost evaluations excluded)"}
+    if n_star is not None:
+        out["cstar_iterations"] = n_star
+    if n is None:
+        out["not_reached_in"] = max_iters
+    return out
 
 
 def gpu_arm(args, rank, world, local_rank):
@@ -750,10 +829,9 @@ def gpu_arm(args, rank, world, local_rank):
     scan = w.scan(rank)
     coarse, fine = w.warm_start(scan)
     sched = 1 if args.schedule == "sv" else 0
-    st = timbir_b200.Stage(scan, **w.prior, blocks=2 if w.rows < 8 else 8)
-    st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
+    st = workload_stage(w, scan, sched, args)
     sched_info = st.schedule_info()
-    st.prepare(fine)
+    st.prepare(fine, zero_offsets(scan) if w.prior["remove_rings"] else None)
     for it in range(1, args.warmup + 1):
         st.iterate(it)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
@@ -795,8 +873,9 @@ def gpu_arm(args, rank, world, local_rank):
                        pin(scan.recon_times), scan.proj_rows, scan.proj_cols, scan.proj_num, scan.recon_num,
                        scan.vox_wid, scan.rot_center)
     pfine = pin(fine)
+    pzero = pin(zero_offsets(scan)) if w.prior["remove_rings"] else None
     h2d = sum(a.nbytes for a in (pscan.projections, pscan.weights, pscan.proj_angles, pscan.proj_times,
-                                 pscan.recon_times, pfine))
+                                 pscan.recon_times, pfine) + ((pzero,) if pzero is not None else ()))
     d2h = fine.nbytes
     for k in range(max(1, min(args.steps, 3))):
         flush.fill_(0.0)
@@ -804,9 +883,8 @@ def gpu_arm(args, rank, world, local_rank):
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        s2 = timbir_b200.Stage(pscan, **w.prior, blocks=2 if w.rows < 8 else 8)
-        s2.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
-        s2.prepare(pfine)
+        s2 = workload_stage(w, pscan, sched, args)
+        s2.prepare(pfine, pzero)
         s2.iterate(1)
         _ = s2.object()
         t1.record()
@@ -873,6 +951,9 @@ def gpu_arm(args, rank, world, local_rank):
         v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, 1, 1, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                                 "sample": f"{n} ICD iteration(s) of the same stage after 1 warm-up, {secs:.1f} s"}
+        rt = reference_time_to_map(w, scan, cpu_measure.iterations, kind)
+        if rt:
+            line["cpu_baseline"]["time_to_map"] = rt
     print(json.dumps(line), flush=True)
 
 
@@ -898,6 +979,7 @@ def reference_arm(args, rank):
         coarse, fine = w.warm_start(scan)
     threads = os.cpu_count() or 1
     v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, args.warmup, args.steps, threads)
+    ttm = reference_time_to_map(w, scan, cpu_measure.iterations, kind) if args.config != "c3" else None
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "voxel-updates/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(n, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 scalars)",
@@ -907,6 +989,8 @@ def reference_arm(args, rank):
             "cpu_baseline": {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
                              "sample": f"{n} ICD iterations after {args.warmup} warm-up, {secs:.1f} s"},
             "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if ttm:
+        line["time_to_map"] = ttm
     print(json.dumps(line), flush=True)
 
 
@@ -927,6 +1011,9 @@ def main():
     ap.add_argument("--problems", type=int, default=64, help="c3: the first N of the 64 problems")
     ap.add_argument("--no-tune", action="store_true", help="c3: default schedules instead of the autotuner's")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
+    ap.add_argument("--zgroup", type=int, default=0, help="slices per super-voxel z-group (0: automatic)")
+    ap.add_argument("--nhicd", type=float, default=-1.0,
+                    help="share of each plane's lines the NHICD pass selects (default: the library's 0.1)")
     ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,
                     help="A-matrix column cache with FP16 values (FP32 accumulation)")
     args = ap.parse_args()

@@ -129,6 +129,23 @@ int mbir_set_sv_relaxation(MbirStage *stage, double alpha);
 int mbir_get_sv_adjustments(MbirStage *stage);
 /* The stability guard on (1, the default) or off (0). */
 int mbir_set_sv_guard(MbirStage *stage, int32_t on);
+/* Non-homogeneous pass of schedule 1 (the reference's NHICD, XT_NHICD.c:
+ * 164-216, XT_ICD_update.c:1015-1058): from the second iteration, after the
+ * sweep, the lines whose 5x5 Hamming-filtered update magnitude is above each
+ * (frame, z-group) plane's order statistic -- `fraction` of the plane's
+ * in-mask lines (the reference takes 0.1: lines / NHICD iterations) -- are
+ * updated once more, chosen on the device.  0, the default, turns the pass
+ * off (the sweep alone reached the MAP cost sooner on the measured
+ * workloads); reconstruct() reads the fraction from TIMBIR_SV_NHICD. */
+int mbir_set_sv_nhicd(MbirStage *stage, double fraction);
+/* The NHICD line selection on the device, for testing against the
+ * reference's VSC_based_Voxel_Line_Select (XT_NHICD.c:164-216): mag host
+ * float [planes][N_y][N_x] magnitude maps, nsel[plane] lines wanted; sel
+ * (host, same shape) = 1 where the filtered magnitude (ComputeVSC) exceeds the
+ * plane's (N_y N_x - nsel)-th smallest filtered value, thresh[plane] (may be
+ * NULL) = that value. */
+int mbir_nhicd_select(const float *mag, int32_t planes, int32_t N_y, int32_t N_x, const int32_t *nsel,
+                      uint8_t *sel, float *thresh);
 /* The automatic launch size of schedule 1: persistent CTAs per launch, the
  * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
  * correct the same rays at once and the iteration diverges), the CTAs that

@@ -15,6 +15,8 @@ Outputs (committed):
                            after ICD iterations 1 and 3 of the reference schedule
   recon_small.npz          a full reconstruct() run of the reference driver
                            binary (object, cost trace) on a seeded 32x32x4 scan
+  recon_rings.npz          the same with ring offsets in the data and
+                           remove_rings 2 (object, offsets, cost trace)
 """
 from __future__ import annotations
 
@@ -93,9 +95,34 @@ def recon_fixture():
     print("recon", obj.shape, cost[-3:])
 
 
+def recon_rings_fixture():
+    """A full reference-driver run with ring correction (zero-mean offsets,
+    remove_rings 2) and the quadratic data term: object, offsets, cost trace."""
+    scan = synth.ellipsoid_scan(32, 4, 48, seed=13, ring_sigma=0.02)
+    wd = tempfile.mkdtemp()
+    scan.write_bin(wd)
+    a = dict(RECON_ARGS, remove_rings=2)
+    cmd = [REF_BIN, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
+           str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
+           str(scan.rot_center), "--sig_s", str(a["sig_s"]), "--sig_t", str(a["sig_t"]), "--c_s", str(a["c_s"]),
+           "--c_t", str(a["c_t"]), "--convg_thresh", str(a["convg_thresh"]), "--remove_rings", "2", "--quad_convex"]
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    subprocess.run(cmd, cwd=wd, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    obj = np.fromfile(os.path.join(wd, "object_time_0.bin"), np.float32).reshape(4, 32, 32)
+    off = np.fromfile(os.path.join(wd, "proj_offset.bin"), np.float32)
+    cost = np.fromfile(os.path.join(wd, "cost.bin"), np.float64)
+    np.savez_compressed(os.path.join(HERE, "recon_rings.npz"), object=obj, offset=off, cost=cost,
+                        threads=np.int32(4))
+    print("recon rings", obj.shape, off.shape, cost[-3:])
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "recon_rings":
+        recon_rings_fixture()
+        sys.exit(0)
     if not Reference.available():
         sys.exit("build the reference first: make -C oracle ref")
     park_miller_table()
     stage_fixtures()
     recon_fixture()
+    recon_rings_fixture()

@@ -1,0 +1,74 @@
+"""The drop-in test: the reference's own driver, linked against this library.
+
+oracle/_ref/XT_Main_gpu is src/reconstruct/bin_data/XT_Main.c, unmodified,
+compiled with this repository's include/mbir4d.h and linked against
+timbir_b200/libtimbir_b200.so instead of the reference's libmbir4d.a (the
+link line INTEGRATION.md gives; oracle/Makefile builds it where the
+reference sources are).  It reads the bin_data file set, calls reconstruct()
+and leaves the output files in its working directory.  Its results are
+compared with full runs of the reference's driver on the same inputs
+(tests/golden/recon_small.npz, recon_rings.npz): MAP cost of the final
+object (and offsets) evaluated afresh in FP64 within 5e-5 relative, object
+RMSE below 1e-3 of the phantom's 0.02 range, ring-offset RMSE below 1e-3,
+and the reference's output file set.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.bind import Oracle
+from timbir_b200 import synth
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "XT_Main_gpu")
+ARGS = dict(sig_s=0.002, sig_t=1.0, c_s=1e-3, c_t=1e-3, convg_thresh=0.005, huber_delta=0.5, huber_T=4.0)
+
+CASES = {
+    "plain": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=11), 0, "recon_small.npz"),
+    "rings": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=13, ring_sigma=0.02), 2, "recon_rings.npz"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_reference_driver_linked_against_the_library(tmp_path, case):
+    if not os.path.exists(DRIVER):
+        pytest.skip("oracle/_ref/XT_Main_gpu not built (make -C oracle ref with the reference sources)")
+    factory, rings, fixture = CASES[case]
+    g = np.load(os.path.join(GOLD, fixture))
+    scan = factory()
+    scan.write_bin(str(tmp_path))
+    cmd = [DRIVER, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
+           str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
+           str(scan.rot_center), "--sig_s", str(ARGS["sig_s"]), "--sig_t", str(ARGS["sig_t"]), "--c_s",
+           str(ARGS["c_s"]), "--c_t", str(ARGS["c_t"]), "--convg_thresh", str(ARGS["convg_thresh"]),
+           "--remove_rings", str(rings), "--quad_convex"]
+    r = subprocess.run(cmd, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    x = np.fromfile(tmp_path / "object_time_0.bin", np.float32).reshape(1, 4, 32, 32)
+    xr = g["object"].reshape(1, 4, 32, 32)
+    d = np.fromfile(tmp_path / "proj_offset.bin", np.float32).reshape(32, 4)  # [N_r][N_t]
+    prior = dict(ARGS, remove_rings=rings, quad_convex=1)
+
+    def fresh(obj, off):
+        o = Oracle(scan, blocks=2, f64=True, **prior)
+        o.prepare(obj, off)
+        c = o.cost()[0]
+        o.close()
+        return c
+
+    dr = g["offset"].reshape(32, 4) if rings else None
+    c, cr = fresh(x, d if rings else None), fresh(xr, dr)
+    assert abs(c - cr) / cr < 5e-5
+    assert float(np.sqrt(np.mean((x - xr) ** 2))) < 1e-3 * 0.02
+    if rings:
+        assert np.any(d != 0)
+        assert float(np.sqrt(np.mean((d - dr) ** 2))) < 1e-3
+    for name, size in (("proj_offset.bin", 32 * 4 * 4), ("variance_estimate.bin", 8), ("status.bin", 4),
+                       ("projs_runtime.bin", 48 * 32 * 4 * 4), ("weights_runtime.bin", 48 * 32 * 4 * 4)):
+        assert (tmp_path / name).stat().st_size == size, name
+    assert np.fromfile(tmp_path / "status.bin", np.int32)[0] == 1
+    assert (tmp_path / "mag_update.bin").exists()

@@ -80,6 +80,8 @@ def load_library() -> C.CDLL:
     lib.mbir_set_sv_relaxation.argtypes = [_VP, C.c_double]
     lib.mbir_get_sv_adjustments.argtypes = [_VP]
     lib.mbir_set_sv_guard.argtypes = [_VP, i32]
+    lib.mbir_set_sv_nhicd.argtypes = [_VP, C.c_double]
+    lib.mbir_nhicd_select.argtypes = [_f32p, i32, i32, i32, _i32p, _u8p, _f32p]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     i64 = C.c_int64
@@ -203,6 +205,11 @@ class Stage:
     def set_sv_guard(self, on: bool):
         """The super-voxel schedule's stability guard on (the default) or off."""
         _check(self.lib.mbir_set_sv_guard(self.h, 1 if on else 0))
+
+    def set_sv_nhicd(self, fraction: float):
+        """Share of each plane's in-mask lines the super-voxel schedule's NHICD
+        pass selects (the reference's is 0.1; 0, the default, turns it off)."""
+        _check(self.lib.mbir_set_sv_nhicd(self.h, fraction))
 
     def set_sv_ctas(self, ctas: int):
         """Persistent CTAs per super-voxel launch (0 = one per SM; 1 runs the
@@ -398,6 +405,19 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def nhicd_select(mag: np.ndarray, nsel) -> tuple:
+    """The device NHICD line selection (mbir_nhicd_select) of magnitude maps
+    mag [planes][N_y][N_x]: (selected-line byte map, per-plane thresholds)."""
+    lib = load_library()
+    mag = np.ascontiguousarray(mag, np.float32)
+    planes, ny, nx = mag.shape
+    nsel = np.ascontiguousarray(np.broadcast_to(np.asarray(nsel, np.int32), (planes,)))
+    sel = np.zeros(mag.shape, np.uint8)
+    th = np.zeros(planes, np.float32)
+    _check(lib.mbir_nhicd_select(mag.reshape(-1), planes, ny, nx, nsel, sel.reshape(-1), th))
+    return sel, th
 
 
 def _malloc_copy(a: np.ndarray) -> C.c_void_p:

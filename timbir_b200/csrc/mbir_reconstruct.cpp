@@ -268,6 +268,13 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
                 in.release_all();
                 return -1;
             }
+            const char *nh = getenv("TIMBIR_SV_NHICD");
+            if (nh && *nh && mbir_set_sv_nhicd(S, atof(nh))) {
+                LOG_ERR(log, "NHICD fraction: %s\n", mbir_last_error());
+                mbir_free_stage(S);
+                in.release_all();
+                return -1;
+            }
             int32_t d[9];
             mbir_stage_dims(S, d);
             nblk_stage = d[7];

@@ -115,10 +115,9 @@ struct MbirStage {
     int *d_sv_done = nullptr;  // per id: epoch of its last finished visit
     int sv_epoch = 0;
     // launch lists [order | dep_off | deps] of the full sweep for each phase
-    // rotation (d_sv_lists), and of the non-homogeneous pass (d_sv_sel)
+    // rotation (the non-homogeneous pass visits a subset of one of them)
     std::vector<std::array<size_t, 4>> sv_rot;  // {n, order, dep_off, deps offsets}
-    int *d_sv_lists = nullptr, *d_sv_sel = nullptr;
-    std::vector<int> sv_sel_host;
+    int *d_sv_lists = nullptr;
     cudaEvent_t sv_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     SvTaskOut *d_sv_out = nullptr;
     float *d_scratch = nullptr;
@@ -146,7 +145,17 @@ struct MbirStage {
     bool guard = true, have_cost = false, win_open = false;
     int win_iters = 0, guard_checks = 0, stab_events = 0;
     std::vector<int> sv_rank;  // size rank of a super-voxel within its (phase, frame, z-group)
-    double nh_fraction = 0.2;
+    // NHICD pass of schedule 1: per (frame, z-group) plane, the lines whose
+    // filtered update magnitude is above the plane's order statistic (a
+    // fraction nh_fraction of its in-mask lines), chosen on the device; off
+    // unless set (on the 3-D workload every fraction tried made the time to
+    // the MAP cost longer: each selected super-voxel stages and commits its
+    // whole band for a few lines)
+    double nh_fraction = 0.0;
+    uint8_t *d_nh_sel = nullptr;  // [planes][N_y][N_x] selected lines
+    int *d_nh_nsel = nullptr, *d_nh_count = nullptr, *d_nh_pos = nullptr, *d_nh_nt = nullptr;
+    float *d_nh_thresh = nullptr;
+    std::vector<int> nh_nsel;  // host copy of d_nh_nsel
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
     size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
@@ -165,8 +174,9 @@ struct MbirStage {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
                         d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
-                        d_sv_all, d_sv_done, d_sv_lists, d_sv_sel, d_sv_out, d_scratch, d_err, d_queue, d_acol,
-                        d_snap_x, d_snap_e, d_snap_w, d_snap_d};
+                        d_sv_all, d_sv_done, d_sv_lists, d_sv_out, d_scratch, d_err, d_queue, d_acol,
+                        d_snap_x, d_snap_e, d_snap_w, d_snap_d, d_nh_sel, d_nh_nsel, d_nh_count, d_nh_pos,
+                        d_nh_nt, d_nh_thresh};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
@@ -616,6 +626,19 @@ static void sv_build_list(const MbirStage *S, const std::vector<int> &ids, std::
 
 // dynamic shared memory per CTA: the 227 KB opt-in limit less the kernels' static
 // shared memory (at most 1.1 KB: the batched kernel's problem descriptor)
+// Lines the NHICD pass selects per plane: nh_fraction of the in-mask lines.
+static int sv_upload_nsel(MbirStage *S)
+{
+    if (!S->d_nh_nsel) return 0;
+    size_t in_mask = 0;
+    for (uint8_t m : S->mask) in_mask += m == 1;
+    S->nh_nsel.assign((size_t)S->sg.N_time * S->nzg, (int)std::floor(S->nh_fraction * (double)in_mask));
+    CK(cudaMemcpyAsync(S->d_nh_nsel, S->nh_nsel.data(), S->nh_nsel.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
 // Over-relaxation and in-flight cap of the super-voxel schedule for `want`
 // super-voxels wanted in flight at once (see the concurrency note in
 // mbir_set_schedule): alpha = the stage's (1.5 unless set) when the cap of
@@ -764,6 +787,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
                     t.nz = std::min(gz, Nz - t.z0);
                     t.nlines = lines;
                     t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
+                    t.plane = i * S->nzg + zg;
                     cell[cell_of(i, zg, ty, tx)] = (int)S->sv_all.size();
                     S->sv_all.push_back(t);
                     S->sv_all_phase.push_back(phase_of[colour]);
@@ -821,19 +845,14 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         sv_sort(S, ids, r);
         sv_build_list(S, ids, buf, S->sv_rot[r]);
     }
-    // a non-homogeneous pass visits a subset: its list is never longer
-    size_t cap = 1;
-    for (int r = 0; r < nphase; r++)
-        cap = std::max(cap, (r + 1 < nphase ? S->sv_rot[r + 1][1] : buf.size()) - S->sv_rot[r][1]);
     dfree(S->d_sv_all);
     dfree(S->d_sv_done);
     dfree(S->d_sv_lists);
-    dfree(S->d_sv_sel);
     dfree(S->d_sv_out);
     dfree(S->d_scratch);
     dfree(S->d_queue);
     S->d_sv_all = nullptr;
-    S->d_sv_done = S->d_sv_lists = S->d_sv_sel = nullptr;
+    S->d_sv_done = S->d_sv_lists = nullptr;
     S->d_sv_out = nullptr;
     S->d_scratch = nullptr;
     S->d_queue = nullptr;
@@ -845,7 +864,27 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     S->sv_epoch = 0;
     CK(dalloc(&S->d_sv_lists, buf.size()));
     CK(cudaMemcpyAsync(S->d_sv_lists, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
-    CK(dalloc(&S->d_sv_sel, cap));
+    // NHICD selection buffers; n_sel per plane = nh_fraction of the in-mask
+    // lines (XT_NHICD.c:171: the lines updated / NHICD iterations)
+    {
+        const int planes = N_time * S->nzg;
+        dfree(S->d_nh_sel);
+        dfree(S->d_nh_nsel);
+        dfree(S->d_nh_count);
+        dfree(S->d_nh_pos);
+        dfree(S->d_nh_nt);
+        dfree(S->d_nh_thresh);
+        S->d_nh_sel = nullptr;
+        S->d_nh_nsel = S->d_nh_count = S->d_nh_pos = S->d_nh_nt = nullptr;
+        S->d_nh_thresh = nullptr;
+        CK(dalloc(&S->d_nh_sel, (size_t)planes * S->nxy()));
+        CK(dalloc(&S->d_nh_nsel, planes));
+        CK(dalloc(&S->d_nh_count, planes));
+        CK(dalloc(&S->d_nh_thresh, planes));
+        CK(dalloc(&S->d_nh_pos, std::max<size_t>(S->sv_all.size(), 1)));
+        CK(dalloc(&S->d_nh_nt, 1));
+        if (sv_upload_nsel(S)) return -1;
+    }
     // Concurrency.  Super-voxels that run at once each correct the residual of
     // the rays they share as if alone, so their steps add up.  A ray of a
     // (frame, z-group) sinogram crosses on average c = 2 n W / (pi R) of the n
@@ -924,6 +963,46 @@ extern "C" int mbir_get_sv_grid(MbirStage *S, int32_t *ctas, int32_t *cap_per_gr
     return 0;
 }
 
+extern "C" int mbir_set_sv_nhicd(MbirStage *S, double fraction)
+{
+    if (!(fraction >= 0.0 && fraction <= 1.0)) return fail("NHICD fraction must lie in [0, 1]");
+    S->nh_fraction = fraction;
+    return sv_upload_nsel(S);
+}
+
+extern "C" int mbir_nhicd_select(const float *mag, int32_t planes, int32_t N_y, int32_t N_x, const int32_t *nsel,
+                                 uint8_t *sel, float *thresh)
+{
+    if (planes <= 0 || N_y <= 0 || N_x <= 0) return fail("non-positive dimensions");
+    const size_t n = (size_t)planes * N_y * N_x;
+    float *d_mag = nullptr, *d_filt = nullptr, *d_th = nullptr;
+    int *d_nsel = nullptr, *d_cnt = nullptr;
+    uint8_t *d_sel = nullptr;
+    auto release = [&]() {
+        dfree(d_mag);
+        dfree(d_filt);
+        dfree(d_th);
+        dfree(d_nsel);
+        dfree(d_cnt);
+        dfree(d_sel);
+    };
+    cudaError_t e = dalloc(&d_mag, n);
+    if (e == cudaSuccess) e = dalloc(&d_filt, n);
+    if (e == cudaSuccess) e = dalloc(&d_th, (size_t)planes);
+    if (e == cudaSuccess) e = dalloc(&d_nsel, (size_t)planes);
+    if (e == cudaSuccess) e = dalloc(&d_cnt, (size_t)planes);
+    if (e == cudaSuccess) e = dalloc(&d_sel, n);
+    if (e == cudaSuccess) e = cudaMemcpy(d_mag, mag, n * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_nsel, nsel, planes * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = mbir_launch_vsc_filter(d_mag, d_filt, planes, N_y, N_x, 0);
+    if (e == cudaSuccess) e = mbir_launch_vsc_threshold(d_filt, planes, N_y * N_x, d_nsel, d_th, d_sel, d_cnt, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(sel, d_sel, n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && thresh) e = cudaMemcpy(thresh, d_th, planes * sizeof(float), cudaMemcpyDeviceToHost);
+    release();
+    if (e != cudaSuccess) return fail("NHICD selection: %s", cudaGetErrorString(e));
+    return 0;
+}
+
 extern "C" int mbir_set_sv_guard(MbirStage *S, int32_t on)
 {
     S->guard = on != 0;
@@ -992,23 +1071,47 @@ extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_si
     return 0;
 }
 
-// One launch of the SV kernel over `n` device-resident tasks; no host sync.
 // One launch of the SV kernel over a launch list at `list` (device) with
-// layout meta; no host sync.
+// layout meta; no host sync.  subset: the NHICD pass -- queue entries are
+// the positions in d_nh_pos, their count in d_nh_nt, and only the lines
+// selected in d_nh_sel are visited.
 static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> &meta, int iter, uint32_t seed,
-                     int qslot, SvTaskOut *acc)
+                     int qslot, SvTaskOut *acc, bool subset = false)
 {
     const int n = (int)meta[0];
     if (n <= 0) return 0;
     const int ctas = std::min(n, S->sv_ctas > 0 ? std::min(S->sv_ctas, S->sv_fit) : S->sv_grid);
     SvACache ac{S->d_acol};
     SvLaunch L{S->d_sv_all, list + meta[1], list + meta[2], list + meta[3], n, S->d_sv_done, ++S->sv_epoch};
+    if (subset) {
+        L.pos = S->d_nh_pos;
+        L.ntasks_dev = S->d_nh_nt;
+        L.sel = S->d_nh_sel;
+    }
     MbirPrior pr = S->pr;
     pr.alpha = S->sv_alpha_eff;
     CK(mbir_launch_icd_sv(S->g, pr, S->dv, S->sp, ac, L, ctas, S->d_queue + qslot, S->d_scratch, acc, iter,
                           seed, S->d_err, S->stream));
     S->launches++;
     S->icd_launches++;
+    return 0;
+}
+
+// NHICD selection of schedule 1 on the device, for the sweep of rotation
+// `rot`: the VSC filter of the magnitude map, each plane's order statistic
+// and selected lines, and the sweep's order compacted to the super-voxels
+// holding a selected line (the others marked finished for the pass's epoch).
+static int sv_nh_select(MbirStage *S, int rot)
+{
+    const int planes = S->sg.N_time * S->nzg;
+    CK(mbir_launch_vsc_filter(S->d_mag, S->d_filt, planes, S->st.N_y, S->st.N_x, S->stream));
+    CK(mbir_launch_vsc_threshold(S->d_filt, planes, (int)S->nxy(), S->d_nh_nsel, S->d_nh_thresh, S->d_nh_sel,
+                                 S->d_nh_count, S->stream));
+    const auto &m = S->sv_rot[rot];
+    CK(mbir_launch_sv_nh_list(S->d_sv_lists + m[1], (int)m[0], S->d_sv_all, S->sp.S, S->st.N_x, S->st.N_y,
+                              S->d_nh_sel, S->d_mask, S->sv_epoch + 1, S->d_sv_done, S->d_nh_pos, S->d_nh_nt,
+                              S->stream));
+    S->launches += 3;
     return 0;
 }
 
@@ -1063,42 +1166,15 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
     bool nh = false;
     if (iter > 1 && S->nh_fraction > 0) {
-        // score = summed last-visit magnitude over the SV's lines
-        std::vector<float> mag(S->nmag());
-        CK(cudaMemcpyAsync(mag.data(), S->d_mag, mag.size() * sizeof(float), cudaMemcpyDeviceToHost, S->stream));
-        CK(cudaStreamSynchronize(S->stream));
-        const int side = S->sp.S, N_x = S->st.N_x, N_y = S->st.N_y;
-        std::vector<std::pair<float, int>> score(S->sv_all.size());
-        for (size_t q = 0; q < S->sv_all.size(); q++) {
-            const SvTask &t = S->sv_all[q];
-            const float *pl = mag.data() + ((size_t)t.frame * S->nzg + t.z0 / S->gz) * S->nxy();
-            double sc = 0;
-            for (int y = t.j0; y < std::min(N_y, t.j0 + side); y++)
-                for (int x = t.k0; x < std::min(N_x, t.k0 + side); x++) sc += pl[(size_t)y * N_x + x];
-            score[q] = {(float)sc, (int)q};
-        }
-        const size_t nsel = (size_t)std::ceil(S->nh_fraction * score.size());
-        std::partial_sort(score.begin(), score.begin() + nsel, score.end(),
-                          [](const std::pair<float, int> &a, const std::pair<float, int> &b) { return a.first > b.first; });
-        std::vector<int> ids;
-        for (size_t q = 0; q < nsel; q++) {
-            if (score[q].first <= 0) break;
-            ids.push_back(score[q].second);
-        }
-        if (!ids.empty()) {
-            nh = true;
-            sv_sort(S, ids, rot);
-            std::array<size_t, 4> meta{};
-            S->sv_sel_host.clear();
-            sv_build_list(S, ids, S->sv_sel_host, meta);
-            // pageable source: the copy is staged before the call returns
-            CK(cudaMemcpyAsync(S->d_sv_sel, S->sv_sel_host.data(), S->sv_sel_host.size() * sizeof(int),
-                               cudaMemcpyHostToDevice, S->stream));
-            CK(cudaEventRecord(S->sv_ev[2], S->stream));
-            if (sv_launch(S, S->d_sv_sel, meta, iter, (uint32_t)(S->rng.next() * 4294967295.0), 1, S->d_sv_out + 1))
-                return -1;
-            CK(cudaEventRecord(S->sv_ev[3], S->stream));
-        }
+        // non-homogeneous pass over the lines the sweep changed most
+        // (VSC_based_Voxel_Line_Select, XT_NHICD.c:164-216), chosen on the device
+        if (sv_nh_select(S, rot)) return -1;
+        nh = true;
+        CK(cudaEventRecord(S->sv_ev[2], S->stream));
+        if (sv_launch(S, S->d_sv_lists, S->sv_rot[rot], iter, (uint32_t)(S->rng.next() * 4294967295.0), 1,
+                      S->d_sv_out + 1, true))
+            return -1;
+        CK(cudaEventRecord(S->sv_ev[3], S->stream));
         if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
     }
     if (S->upd_var == 1 && mbir_update_variance_parameter(S)) return -1;

@@ -491,6 +491,9 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         n_upd = n_skip = 0;
     };
     int cur = -1;  // problem held in s_prob (batched launches)
+    // a subset pass takes its length from the device (written by the kernel
+    // that chose the subset, earlier on the stream)
+    const int ntasks = L.ntasks_dev ? min(*L.ntasks_dev, L.ntasks) : L.ntasks;
 
     for (;;) {
         __syncthreads();
@@ -499,8 +502,10 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             s_bad = 0;
         }
         __syncthreads();
-        const int tix = s_task;
-        if (tix >= L.ntasks) break;
+        const int tix0 = s_task;
+        if (tix0 >= ntasks) break;
+        // position in the order / dependency lists
+        const int tix = L.pos ? L.pos[tix0] : tix0;
         const int id = L.order[tix];
         const SvTask task = L.tasks[id];
         if constexpr (BATCH) {
@@ -627,12 +632,15 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         }
         // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
         if (warp == 0) {
-            // in-mask bit of line q = 32 k + lane in bit k (all loads in flight at once)
+            // in-mask bit of line q = 32 k + lane in bit k (all loads in flight
+            // at once); a subset pass keeps the selected lines only
+            const uint8_t *lsel = L.sel ? L.sel + (size_t)task.plane * g.N_y * g.N_x : nullptr;
             unsigned mbits = 0;
             for (int k = 0; 32 * k < S * S; k++) {
                 const int q = 32 * k + lane;
                 const int lx = q % S, ly = q / S;
-                if (q < S * S && lx < kx && ly < ky && dv.mask[(size_t)(j0 + ly) * g.N_x + k0 + lx] == 1)
+                const size_t l = (size_t)(j0 + ly) * g.N_x + k0 + lx;
+                if (q < S * S && lx < kx && ly < ky && dv.mask[l] == 1 && (!lsel || lsel[l]))
                     mbits |= 1u << k;
             }
             int n = 0;
@@ -648,14 +656,36 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     n += __popc(bal);
                 }
                 __syncwarp();
-                if (lane == 0 && n > base) {
-                    for (int q = n - 1; q > base; q--) {
-                        const uint32_t h = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)q));
-                        const int r = base + (int)(h % (uint32_t)(q - base + 1));
-                        const int t = order[q];
-                        order[q] = order[r];
-                        order[r] = t;
+                // random order within the class: each line's rank among the
+                // class's per-visit hash keys (ties by position), computed by
+                // the whole warp; classes of more than 64 lines (sides above
+                // 16) are shuffled by lane 0
+                const int m = n - base;
+                if (m > 1 && m <= 64) {
+                    const int oa = lane < m ? order[base + lane] : 0;
+                    const int ob = lane + 32 < m ? order[base + lane + 32] : 0;
+                    const uint32_t ka = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)oa));
+                    const uint32_t kb = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)ob));
+                    int ra = 0, rb = 0;
+                    for (int j = 0; j < m; j++) {
+                        const uint32_t kj = __shfl_sync(0xffffffffu, j < 32 ? ka : kb, j & 31);
+                        ra += kj < ka || (kj == ka && j < lane);
+                        rb += kj < kb || (kj == kb && j < lane + 32);
                     }
+                    __syncwarp();
+                    if (lane < m) order[base + ra] = oa;
+                    if (lane + 32 < m) order[base + rb] = ob;
+                    __syncwarp();
+                }
+                if (lane == 0 && n > base) {
+                    if (m > 64)
+                        for (int q = n - 1; q > base; q--) {
+                            const uint32_t h = hash32(seed ^ hash32((uint32_t)tix * 1315423911u + (uint32_t)q));
+                            const int r = base + (int)(h % (uint32_t)(q - base + 1));
+                            const int t = order[q];
+                            order[q] = order[r];
+                            order[r] = t;
+                        }
                     // the odd slices lag one step: keep the previous class's last
                     // line and this class's first line apart
                     auto adjacent = [](int a, int b) {
@@ -719,31 +749,64 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         const bool vec = (g.N_r & 3) == 0;
         const int npairs = rows * Np;
         if (vec) {
-            for (int pqc = warp * 32 + lane; pqc < 4 * npairs; pqc += nwarps * 32) {
-                const int pq = pqc >> 2, row = pq / Np, v = pq - row * Np;
-                const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
-                for (int c = pqc & 3; 4 * c < sh + W; c += 4) {
-                    const int col0 = a0 + 4 * c;
-                    const size_t rbase = ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
-                    float4 ev = make_float4(0.0f, 0.0f, 0.0f, 0.0f), wv = ev;
-                    if (col0 < g.N_r) {
-                        ev = __ldcg(reinterpret_cast<const float4 *>(dv.e + rbase + col0));
-                        wv = __ldg(reinterpret_cast<const float4 *>(dv.w + rbase + col0));
-                    }
-                    const float ee[4] = {ev.x, ev.y, ev.z, ev.w};
-                    const float ww[4] = {wv.x, wv.y, wv.z, wv.w};
-                    float2 *bd = band + (size_t)row * rowstride + v;
-                    float *sc = scr + (size_t)row * rowstride + v;
+            // one 16-byte word of a (row, view): pqc = 4 (row Np + v) + c
+            auto stage_word = [&](int pq, int c, float4 ev, float4 wv) {
+                const int row = pq / Np, v = pq - row * Np;
+                const int sh = rlo[v] & 3;
+                const float ee[4] = {ev.x, ev.y, ev.z, ev.w};
+                const float ww[4] = {wv.x, wv.y, wv.z, wv.w};
+                float2 *bd = band + (size_t)row * rowstride + v;
+                float *sc = scr + (size_t)row * rowstride + v;
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int off = 4 * c + j - sh;
-                        if (off >= 0 && off < W) {
-                            bd[(size_t)off * NpS] = make_float2(ee[j], sqrtf(ww[j]));
-                            sc[(size_t)off * NpS] = ee[j];
-                        }
+                for (int j = 0; j < 4; j++) {
+                    const int off = 4 * c + j - sh;
+                    if (off >= 0 && off < W) {
+                        bd[(size_t)off * NpS] = make_float2(ee[j], sqrtf(ww[j]));
+                        sc[(size_t)off * NpS] = ee[j];
                     }
                 }
+            };
+            // global address of word c of pair pq (-1: past the band or the row)
+            auto word_at = [&](int pq, int c) -> long long {
+                const int row = pq / Np, v = pq - row * Np;
+                const int lo = rlo[v], a0 = lo & ~3;
+                if (4 * c >= (lo - a0) + W || a0 + 4 * c >= g.N_r) return -1;
+                return (long long)((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r + a0 + 4 * c;
+            };
+            // words 0-3 of every pair, four per thread in flight at once
+            constexpr int U = 4;
+            const int stride = nwarps * 32, total = 4 * npairs;
+            for (int b = tid; b < total; b += U * stride) {
+                float4 ev[U], wv[U];
+                long long at[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int pqc = b + u * stride;
+                    at[u] = pqc < total ? word_at(pqc >> 2, pqc & 3) : -2;
+                    ev[u] = wv[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (at[u] >= 0) {
+                        ev[u] = __ldcg(reinterpret_cast<const float4 *>(dv.e + at[u]));
+                        wv[u] = __ldg(reinterpret_cast<const float4 *>(dv.w + at[u]));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int pqc = b + u * stride;
+                    if (at[u] != -2) stage_word(pqc >> 2, pqc & 3, ev[u], wv[u]);
+                }
             }
+            // words 4 and up (bands wider than 13 columns)
+            if (W + 3 > 16)
+                for (int pqc = tid; pqc < total; pqc += stride)
+                    for (int c = (pqc & 3) + 4; 4 * c < W + 3; c += 4) {
+                        const long long a = word_at(pqc >> 2, c);
+                        float4 ev = make_float4(0.0f, 0.0f, 0.0f, 0.0f), wv = ev;
+                        if (a >= 0) {
+                            ev = __ldcg(reinterpret_cast<const float4 *>(dv.e + a));
+                            wv = __ldg(reinterpret_cast<const float4 *>(dv.w + a));
+                        }
+                        stage_word(pqc >> 2, c, ev, wv);
+                    }
         } else {
             for (int pq = tid; pq < npairs; pq += nthr) {
                 const int row = pq / Np, v = pq - row * Np;
@@ -830,6 +893,17 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         }
         __syncthreads();
 
+        // full resolution: this lane's views (vh * 32 + lane + 32 vsplit u, u
+        // < VU) as a mask of those the frame has, and their band origins
+        constexpr int VRL = VU > 0 ? VU : 1;
+        int rl[VRL];
+        unsigned okm = 0;
+#pragma unroll
+        for (int u = 0; u < VRL; u++) {
+            const int v = vh * 32 + lane + u * 32 * vsplit;
+            rl[u] = v < Np ? rlo[v] : 0;
+            okm |= v < Np ? 1u << u : 0u;
+        }
         for (int step = 0, sl = 0; step <= nl; step++, sl = sl + 1 == R ? 0 : sl + 1) {
             // sl = step mod R: the slot of line `step`; odd slices use line step - 1
             const int li = (zl & 1) ? step - 1 : step;
@@ -862,15 +936,18 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     const float2 *bz = band + (size_t)zl * mz * rowstride;
                     // full resolution: per view three consecutive columns from
                     // j0 (clamped into the band; absent ones carry a = 0),
-                    // e kept in registers for the update; the weight is w for
-                    // every entry unless some lane of the warp holds an entry
-                    // with |e sqrt(w)| >= T, which then gets T delta sqrt(w)/|e|
+                    // e kept in registers for the update.  Every entry is
+                    // first summed with weight w, tracking the largest
+                    // |e sqrt(w)|; only when some lane of the warp holds an
+                    // entry with |e sqrt(w)| >= T (generalized Huber,
+                    // XT_VoxUpdate.c:62-84) are the warp's sums recomputed
+                    // with T delta sqrt(w) / |e| for those entries
                     constexpr int VR = VU > 0 ? VU : 1;
                     float ev[VR][3], av[VR][3];
                     int cx[VR][3];
                     if constexpr (AMAXC == 3 && MZC == 1) {
                         const int vstep = 32 * vsplit;
-                        unsigned big = 0;
+                        float pmax = 0.0f;
 #pragma unroll
                         for (int u = 0; u < VR; u++) {
                             const int v = vh * 32 + lane + u * vstep;
@@ -892,7 +969,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                                 av[u][1] = __int_as_float(A.z);
                                 av[u][2] = __int_as_float(A.w);
                             }
-                            const int off0 = max(j0c - rlo[vv], 0);
+                            const int off0 = max(j0c - rl[u], 0);
                             cx[u][0] = off0 * NpS + vv;
                             cx[u][1] = min(off0 + 1, W - 1) * NpS + vv;
                             cx[u][2] = min(off0 + 2, W - 1) * NpS + vv;
@@ -904,9 +981,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                                 const float2 es = bz[cx[u][k]];
                                 ev[u][k] = es.x;
                                 const float pe = es.x * es.y;
-                                const bool sel = fabsf(pe) < hT;
-                                const float q = sel ? av[u][k] * es.y : 0.0f;
-                                big |= sel ? 0u : 1u << (3 * u + k);
+                                const float q = av[u][k] * es.y;
+                                pmax = fmaxf(pmax, fabsf(pe));
                                 if (u & 1) {
                                     th2b = fmaf(q, q, th2b);
                                     th1b = fmaf(-q, pe, th1b);
@@ -915,18 +991,15 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                                     th1 = fmaf(-q, pe, th1);
                                 }
                             }
-                        if (__any_sync(0xffffffffu, big != 0u)) {
+                        if (__any_sync(0xffffffffu, !(pmax < hT))) {
+                            // exact sums: w where |e sqrt(w)| < T, else T delta sqrt(w) / |e|
+                            th1 = th2 = th1b = th2b = 0.0f;
 #pragma unroll
                             for (int u = 0; u < VR; u++)
 #pragma unroll
                                 for (int k = 0; k < 3; k++)
-                                    if (big & (1u << (3 * u + k))) {
-                                        const float e = ev[u][k], a = av[u][k];
-                                        const float om = __fdividef(hTd * bz[cx[u][k]].y, fabsf(e));
-                                        const float ao = a * om;
-                                        th2 = fmaf(a, ao, th2);
-                                        th1 = fmaf(-e, ao, th1);
-                                    }
+                                    theta_acc(make_float2(ev[u][k], bz[cx[u][k]].y), av[u][k], hT, hTd,
+                                              (u & 1) ? th1b : th1, (u & 1) ? th2b : th2);
                         }
                     } else {
                         const int *rw = reinterpret_cast<const int *>(rq);
@@ -988,11 +1061,16 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     // ---- error sinogram: e -= a dx over this slice's rows ----
                     float *bzf = reinterpret_cast<float *>(band + (size_t)zl * mz * rowstride);
                     if constexpr (AMAXC == 3 && MZC == 1) {
+                        // absent columns (a = 0) rewrite their own value; a
+                        // clamped one can share the slot of a real column of
+                        // the same view at a lower k, so the writes go from
+                        // k = 2 down to k = 0 and the real column's is last
 #pragma unroll
                         for (int u = 0; u < VR; u++)
+                            if (okm & (1u << u)) {
 #pragma unroll
-                            for (int k = 0; k < 3; k++)
-                                if (av[u][k] != 0.0f) bzf[2 * cx[u][k]] = fmaf(-av[u][k], dx, ev[u][k]);
+                                for (int k = 2; k >= 0; k--) bzf[2 * cx[u][k]] = fmaf(-av[u][k], dx, ev[u][k]);
+                            }
                     } else {
                         const int *rw = reinterpret_cast<const int *>(rq);
                         for (int v = vh * 32 + lane; v < Np; v += 32 * vsplit) {
@@ -1046,24 +1124,46 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         // outside the band), one lane per (row, view), so that the atomics of
         // one instruction go to different rows
         if (vec) {
-            for (int pq = tid; pq < npairs; pq += nthr) {
+            // word c of pair pq: its change (zeros outside the band) and its
+            // global address (-1: past the band or the row); the reads of a
+            // batch of four words are issued before any of their atomics
+            auto commit_word = [&](int pq, int c, float *d) -> long long {
                 const int row = pq / Np, v = pq - row * Np;
                 const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
+                if (4 * c >= sh + W || a0 + 4 * c >= g.N_r) return -1;
                 const float2 *bd = band + (size_t)row * rowstride + v;
                 const float *sc = scr + (size_t)row * rowstride + v;
-                float *erow = dv.e + ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
-                for (int c = 0; 4 * c < sh + W && a0 + 4 * c < g.N_r; c++) {
-                    float d[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int off = 4 * c + j - sh;
-                        d[j] = 0.0f;
-                        if (off >= 0 && off < W) d[j] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
-                    }
-                    if (d[0] != 0.0f || d[1] != 0.0f || d[2] != 0.0f || d[3] != 0.0f)
-                        red_add_v4(erow + a0 + 4 * c, d[0], d[1], d[2], d[3]);
+                for (int j = 0; j < 4; j++) {
+                    const int off = 4 * c + j - sh;
+                    d[j] = 0.0f;
+                    if (off >= 0 && off < W) d[j] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
                 }
+                return (long long)((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r + a0 + 4 * c;
+            };
+            constexpr int U = 3;
+            const int total = 4 * npairs;
+            for (int b = tid; b < total; b += U * nthr) {
+                float d[U][4];
+                long long at[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int pqc = b + u * nthr;
+                    at[u] = pqc < total ? commit_word(pqc >> 2, pqc & 3, d[u]) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (at[u] >= 0 && (d[u][0] != 0.0f || d[u][1] != 0.0f || d[u][2] != 0.0f || d[u][3] != 0.0f))
+                        red_add_v4(dv.e + at[u], d[u][0], d[u][1], d[u][2], d[u][3]);
             }
+            if (W + 3 > 16)
+                for (int pqc = tid; pqc < total; pqc += nthr)
+                    for (int c = (pqc & 3) + 4; 4 * c < W + 3; c += 4) {
+                        float d[4];
+                        const long long a = commit_word(pqc >> 2, c, d);
+                        if (a >= 0 && (d[0] != 0.0f || d[1] != 0.0f || d[2] != 0.0f || d[3] != 0.0f))
+                            red_add_v4(dv.e + a, d[0], d[1], d[2], d[3]);
+                    }
         } else {
             for (int pq = tid; pq < npairs; pq += nthr) {
                 const int row = pq / Np, v = pq - row * Np;

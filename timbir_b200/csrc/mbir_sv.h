@@ -39,6 +39,7 @@ struct SvTask {
     int nlines;  // in-mask voxel lines (host-side ordering of the work queue)
     float *mag;  // [N_y][N_x] plane of the magnitude map for (frame, z-group)
     int prob;    // problem of a batched launch (0 otherwise)
+    int plane;   // index of that plane: frame * z-groups + z-group
 };
 
 struct SvTaskOut {
@@ -91,6 +92,13 @@ struct SvLaunch {
     const int *seq;
     SvBatchState *state;
     const int *ctl;
+    // a pass over a device-chosen subset (NHICD): queue entry k is position
+    // pos[k] of the order / dependency lists, *ntasks_dev entries in all,
+    // and only the lines with sel[plane][line] != 0 are visited (all three
+    // null: every entry of the lists, every in-mask line)
+    const int *pos;
+    const int *ntasks_dev;
+    const uint8_t *sel;
 };
 
 // One problem of a batched launch: its stage's geometry, arrays, prior (the
@@ -119,6 +127,19 @@ struct SvBatchState {
     int fin;         // super-voxels finished in this launch
     int adjustments; // times the in-flight cap was halved
 };
+
+// NHICD selection on the device (mbir_nhicd.cu).  Per plane of `filt`
+// (planes x n values, the VSC-filtered magnitude map): thresh[plane] = the
+// (n - nsel[plane])-th smallest value, sel[plane][q] = filt > thresh,
+// count[plane] = lines selected (XT_NHICD.c:164-216).
+cudaError_t mbir_launch_vsc_threshold(const float *filt, int planes, int n, const int *nsel, float *thresh,
+                                      uint8_t *sel, int *count, cudaStream_t s);
+// The positions k of a sweep's order[0 .. n) whose super-voxel holds a
+// selected in-mask line, kept in order, into pos[0 .. *ntasks); the others
+// get done[id] = epoch.
+cudaError_t mbir_launch_sv_nh_list(const int *order, int n, const SvTask *tasks, int S, int N_x, int N_y,
+                                   const uint8_t *sel, const uint8_t *mask, int epoch, int *done, int *pos,
+                                   int *ntasks, cudaStream_t s);
 
 // CTAs of the super-voxel kernel that fit one SM for this configuration.
 int mbir_sv_ctas_per_sm(const MbirGeom &g, const SvParams &sp, bool cached);

@@ -321,6 +321,42 @@ def moving_ellipsoid_scan(n_xy: int, rows: int, frames: int, views_per_rotation:
     return Scan(proj, wts, angles, times, recon_times, rows, n_xy, n_views, frames, 1.0, rc, None)
 
 
+def project_frames(frames: np.ndarray, angles: np.ndarray, recon_times: np.ndarray, proj_times: np.ndarray,
+                   cols: int, vox_wid: float = 1.0, rot_center: float | None = None) -> np.ndarray:
+    """Line integrals [views][rows][cols] of a voxelised 4-D object
+    frames [N_time][rows][n_xy][n_xy] (z, y, x): each view sees the frame whose
+    time interval [recon_times[t], recon_times[t+1]) holds its time.  Each
+    voxel's mass goes to the two detector columns nearest its centre's
+    projection r = x cos(theta) - y sin(theta), by linear interpolation
+    (geometry as in the module docstring).  Float64 numpy on the CPU, so the
+    data are the same on every machine; the reconstruction's own A matrix is
+    not used."""
+    import scipy.sparse as sp
+    n_t, rows, n_xy, _ = frames.shape
+    rc = n_xy / 2.0 if rot_center is None else rot_center
+    live = np.flatnonzero(frames.reshape(n_t * rows, -1).any(axis=0))  # voxel lines ever non-zero
+    yi, xi = np.divmod(live, n_xy)
+    X = (xi + 0.5 - rc) * vox_wid
+    Y = (yi + 0.5) * vox_wid - n_xy * vox_wid / 2.0
+    col = np.arange(len(live))
+    out = np.zeros((len(angles), rows, cols))
+    dense = [frames[t].reshape(rows, -1)[:, live].T.astype(np.float64) for t in range(n_t)]  # [lines][rows]
+    for v, th in enumerate(angles.astype(np.float64)):
+        t = int(np.searchsorted(recon_times, proj_times[v], side="right")) - 1
+        if t < 0 or t >= n_t:
+            continue
+        u = (X * np.cos(th) - Y * np.sin(th)) / vox_wid + rc - 0.5  # fractional detector column
+        j0 = np.floor(u).astype(np.int64)
+        f1 = u - j0
+        ok0 = (j0 >= 0) & (j0 < cols)
+        ok1 = (j0 + 1 >= 0) & (j0 + 1 < cols)
+        M = sp.csr_matrix((np.concatenate([1.0 - f1[ok0], f1[ok1]]),
+                           (np.concatenate([j0[ok0], j0[ok1] + 1]), np.concatenate([col[ok0], col[ok1]]))),
+                          shape=(cols, len(live)))
+        out[v] = (M @ dense[t]).T * vox_wid
+    return out
+
+
 def two_phase_frames(n_xy: int, n_z: int, frames: int, seed: int, vmax: float = 0.02,
                      smooth: float = 6.0, flow_steps: int = 3) -> np.ndarray:
     """[frames][n_z][n_xy][n_xy] two-phase microstructure: a smoothed Gaussian
