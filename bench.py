@@ -92,9 +92,9 @@ WC5 = Workload("c5", "large 4d z-subset: 32 x 2048x2048 x 4 of 64 detector rows,
                dict(sig_s=0.00025, sig_t=0.0005, c_s=1.0, c_t=1.0, convg_thresh=0.0, remove_rings=2, quad_convex=0,
                     huber_delta=0.5, huber_T=4.0),
                "synthetic (seeded drifting random ellipsoids, exact line integrals, Poisson counts, zingers, rings)")
-W4DC = Workload("4dc", "4d two-phase microstructure 16 x 256x256x16 as the 4d workload, convex model: quadratic "
-                "data term (quad_convex=1), zero-mean ring offsets (remove_rings=2), finest stage", 256, 16, 1024, 16,
-                dict(W4D.prior, quad_convex=1), W4D.data)
+W4DC = Workload("4dc", "4d two-phase microstructure 16 x 256x256x16 as the 4d workload (zingers and rings in the "
+                "data), convex model: quadratic data term (quad_convex=1), no ring correction (remove_rings=0), "
+                "finest stage", 256, 16, 1024, 16, dict(W4D.prior, quad_convex=1, remove_rings=0), W4D.data)
 WORKLOADS = {"3d": W3D, "4d": W4D, "4dc": W4DC, "c5": WC5}
 
 
@@ -738,6 +738,66 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     }), flush=True)
 
 
+# ------------------------------------------------------ auxiliary kernels --
+def kernels_arm(args, rank, world, local_rank):
+    """Each kernel of the path besides the super-voxel sweep, run on the 4-D
+    workload's sizes (sinogram-shaped arrays of 67 MB each, volume 67 MB:
+    larger than L2 together) so that one command covers them for a profiler:
+    the prologue's forward projection (k_forward_rows) and column cache
+    (k_acache), the ring-offset update (k_offset_terms / k_offset_apply), the
+    windowed ring-offset solve (k_offset_windows), the variance update
+    (k_variance / k_variance_apply), the MAP cost (k_cost / k_sum_partials),
+    the NHICD selection (k_vsc_filter / k_vsc_threshold / k_sv_nh_list) and
+    pass, the stage hand-off up-sampling (k_upsample_xy / _xyz), the
+    filtered backprojection (k_ramp / k_backproject) and, on the 3-D
+    workload, one iteration of the reference schedule (k_icd_ref).  Prints
+    the wall time of each call (the profiler gives per-kernel times)."""
+    import torch
+    import timbir_b200
+    torch.cuda.set_device(local_rank)
+    w = W4D
+    scan = w.scan(0)
+    _, fine = w.warm_start(scan)
+    out = {}
+
+    def timed(name, fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        out[name] = round((time.perf_counter() - t0) * 1e3, 3)
+        return r
+
+    st = workload_stage(w, scan, 1, args)
+    timed("prologue (forward projection)", lambda: st.prepare(fine, zero_offsets(scan)))
+    st.set_sv_nhicd(0.1)
+    timed("iteration 1 (column cache, sweep, offsets, variance)", lambda: st.iterate(1))
+    timed("iteration 2 (sweep, NHICD selection and pass, offsets, variance)", lambda: st.iterate(2))
+    timed("MAP cost", st.cost)
+    timed("ring-offset update (mode 2)", st.offset_update)
+    timed("variance update", st.variance_update)
+    x = st.object()
+    st.close()
+    s3 = workload_stage(w, scan, 1, args, prior=dict(w.prior, remove_rings=3))
+    s3.set_offset_windows(True)
+    s3.prepare(fine, zero_offsets(scan))
+    timed("ring-offset update (mode 3, %d windows)" % s3.offset_window_count(), s3.offset_update)
+    timed("filtered backprojection", s3.fbp)
+    s3.close()
+    coarse = np.ascontiguousarray(x[0, ::2, ::2, ::2])
+    timed("up-sampling x2 (x, y)", lambda: timbir_b200.upsample(x[0], False))
+    timed("up-sampling x2 (x, y, z)", lambda: timbir_b200.upsample(coarse, True))
+    w3 = W3D
+    scan3 = w3.scan(0)
+    _, fine3 = w3.warm_start(scan3)
+    sr = timbir_b200.Stage(scan3, **w3.prior, blocks=8)
+    sr.prepare(fine3)
+    timed("reference-schedule iteration (3-D workload)", lambda: sr.iterate(1))
+    sr.close()
+    print(json.dumps({"metric": "wall ms per call (profile for per-kernel device times)", "calls": out,
+                      "config": {"workload": w.desc + "; reference schedule on " + w3.desc}}), flush=True)
+
+
 # --------------------------------------------------------------------- GPU --
 def reference_map(w, scan):
     """The converged MAP cost C* of workload w's scan from the reference library
@@ -818,6 +878,8 @@ def gpu_arm(args, rank, world, local_rank):
         return c4_arm(args, rank, world, local_rank, four_d=args.config == "4d-warm")
     if args.config == "net":
         return net_arm(args, rank, world, local_rank)
+    if args.config == "kernels":
+        return kernels_arm(args, rank, world, local_rank)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -864,34 +926,50 @@ def gpu_arm(args, rank, world, local_rank):
     cbar = mean_amatrix_count(st, scan) if rank == 0 else 0.0
     st.close()
 
-    # end to end through the C ABI with host buffers: set-up from host arrays
-    # (H2D), prologue, one ICD iteration, object back to the host (D2H)
-    e2e_ms, e2e_upd = [], 0
-    # the step's inputs from pinned host memory
+    # time to the MAP target (every rank: its iteration count sizes the e2e solve)
+    big = w.name == "c5"  # hundreds of iterations of about a second, ~100 s per reference iteration
+    ttm = time_to_map(w, scan, fine, sched, args) if not args.no_ttm and not big else None
+    n_solve = ttm["iterations"] if ttm and ttm["iterations"] else args.steps
+
+    # end to end through the public API with host buffers: every step is the
+    # call a user makes -- the stage reconstructed from pinned host arrays
+    # (set-up and H2D copies, prologue, n_solve ICD iterations: the iterations
+    # the GPU needed to reach the MAP target) and its object read back into
+    # pinned host memory (D2H); the same with one iteration reported beside it
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     pscan = synth.Scan(pin(scan.projections), pin(scan.weights), pin(scan.proj_angles), pin(scan.proj_times),
                        pin(scan.recon_times), scan.proj_rows, scan.proj_cols, scan.proj_num, scan.recon_num,
                        scan.vox_wid, scan.rot_center)
     pfine = pin(fine)
     pzero = pin(zero_offsets(scan)) if w.prior["remove_rings"] else None
+    pout = pin(np.zeros_like(fine))
     h2d = sum(a.nbytes for a in (pscan.projections, pscan.weights, pscan.proj_angles, pscan.proj_times,
                                  pscan.recon_times, pfine) + ((pzero,) if pzero is not None else ()))
     d2h = fine.nbytes
-    for k in range(max(1, min(args.steps, 3))):
-        flush.fill_(0.0)
-        torch.cuda.synchronize()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record()
-        s2 = workload_stage(w, pscan, sched, args)
-        s2.prepare(pfine, pzero)
-        s2.iterate(1)
-        _ = s2.object()
-        t1.record()
-        torch.cuda.synchronize()
-        e2e_ms.append(t0.elapsed_time(t1))
-        e2e_upd += s2.update_count()
-        s2.close()
+
+    def e2e_run(n_iter, reps):
+        times, upd = [], 0
+        for _ in range(reps):
+            flush.fill_(0.0)
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            s2 = workload_stage(w, pscan, sched, args)
+            s2.prepare(pfine, pzero)
+            for it in range(1, n_iter + 1):
+                s2.iterate(it)
+            s2.object(out=pout)
+            t1.record()
+            torch.cuda.synchronize()
+            times.append(t0.elapsed_time(t1))
+            upd += s2.update_count()
+            s2.close()
+        return times, upd
+
+    reps = max(1, min(args.steps, 3))
+    e2e_ms, e2e_upd = e2e_run(n_solve, reps)
+    one_ms, one_upd = e2e_run(1, reps)
     if dist:
         t = torch.tensor([sum(e2e_ms), float(e2e_upd)], dtype=torch.float64, device="cuda")
         mx = t.clone()
@@ -932,7 +1010,12 @@ def gpu_arm(args, rank, world, local_rank):
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "step_ms": [round(v, 3) for v in e2e_ms],
-                "updates_per_step": e2e_upd / max(len(e2e_ms), 1)},
+                "updates_per_step": e2e_upd / max(len(e2e_ms), 1),
+                "step": f"stage reconstructed from pinned host arrays: set-up, prologue, {n_solve} ICD iterations "
+                        f"({'the GPU iterations to the MAP target' if ttm and ttm['iterations'] else 'steps'}), "
+                        "object read back into pinned memory",
+                "single_iteration": {"value": one_upd / (sum(one_ms) / 1e3), "step_ms": [round(v, 3) for v in one_ms],
+                                     "updates_per_step": one_upd / max(len(one_ms), 1)}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "traffic_source": traffic_src,
@@ -942,9 +1025,8 @@ def gpu_arm(args, rank, world, local_rank):
         "gpu_launches": int(n_all1 - n_all0),
         "clocks": clk.summary(),
     }
-    big = w.name == "c5"  # hundreds of iterations of about a second, ~100 s per reference iteration
-    if not args.no_ttm and not big:
-        line["time_to_map"] = time_to_map(w, scan, fine, sched, args)
+    if ttm:
+        line["time_to_map"] = ttm
     if big:
         line["cpu_baseline"] = {"unavailable": "the reference's CPU code needs minutes per iteration at this size"}
     elif not args.no_cpu:
@@ -959,6 +1041,10 @@ def gpu_arm(args, rank, world, local_rank):
 
 def reference_arm(args, rank):
     if rank != 0:
+        return
+    if args.config == "kernels":
+        print(json.dumps({"impl": "reference", "unavailable": "a profiling helper of this library's kernels; no "
+                          "reference counterpart"}), flush=True)
         return
     if args.config in ("c4", "4d-warm", "net"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start (its coarsest "
@@ -1003,10 +1089,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
-    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net"],
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net", "kernels"],
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
                          "c3: 64 independent 3-D problems batched; c4: learned warm start (3-D); 4d-warm: learned warm "
-                         "start on the 4-D workload; net: the network's training step; c5: large 4-D z-subset")
+                         "start on the 4-D workload; net: the network's training step; c5: large 4-D z-subset; "
+                         "kernels: each auxiliary kernel once, for a profiler")
     ap.add_argument("--sv-side", type=int, default=0, help="super-voxel side (0: largest that fits)")
     ap.add_argument("--problems", type=int, default=64, help="c3: the first N of the 64 problems")
     ap.add_argument("--no-tune", action="store_true", help="c3: default schedules instead of the autotuner's")

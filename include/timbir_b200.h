@@ -146,6 +146,13 @@ int mbir_set_sv_nhicd(MbirStage *stage, double fraction);
  * NULL) = that value. */
 int mbir_nhicd_select(const float *mag, int32_t planes, int32_t N_y, int32_t N_x, const int32_t *nsel,
                       uint8_t *sel, float *thresh);
+/* The x2 up-sampling that hands a stage's object and magnitude map to the
+ * next multi-resolution stage on the device (upsample_object_bilinear_2D /
+ * _3D, upsample_bilinear_2D / _3D, XT_ICD_update.c:323-498): host float in
+ * [n_z][n_y][n_x] -> out [n_z or 2 n_z][2 n_y][2 n_x] (z_too = 1: also along
+ * z), computed by the same GPU kernels reconstruct() uses between stages.
+ * For testing; n_y, n_x >= 2, n_z >= 2 with z_too. */
+int mbir_upsample(const float *in, float *out, int32_t n_z, int32_t n_y, int32_t n_x, int32_t z_too);
 /* The automatic launch size of schedule 1: persistent CTAs per launch, the
  * super-voxels allowed in flight per (frame, z-group) sinogram (more of them
  * correct the same rays at once and the iteration diverges), the CTAs that
@@ -170,6 +177,18 @@ int mbir_compute_cost(MbirStage *stage, double *total, double *forward, double *
 
 /* update_Sinogram_Offset (XT_ICD_update.c:919-927), by remove_rings. */
 int mbir_update_sinogram_offset(MbirStage *stage);
+/* Rectangular-patch constraint windows for ring-offset mode 3 (remove_rings
+ * 3): on = 1 builds them as gen_offset_constraint_windows does
+ * (XT_OffsetError.c:46-96; overlapping windows of 2 N_r / round(sqrt N_r)
+ * columns by 2 N_t / round(sqrt N_t) rows with tent weights), and mode 3
+ * then solves the constrained problem of update_d_offset_rect_patch_constraint
+ * / constrained_quad_opt (XT_ICD_update.c:753-800, XT_OffsetError.c:99-168):
+ * the offsets minimise the data term subject to a zero weighted sum over
+ * every window, through an M x M FP64 system solved on the GPU.  on = 0 (the
+ * default, and the reference's reconstruct path, which builds no windows)
+ * leaves mode 3 unconstrained.  mbir_get_offset_windows = windows built. */
+int mbir_set_offset_windows(MbirStage *stage, int32_t on);
+int mbir_get_offset_windows(MbirStage *stage);
 
 /* update_variance_parameter (XT_ICD_update.c:720-751). */
 int mbir_update_variance_parameter(MbirStage *stage);

@@ -76,6 +76,9 @@ class _Lib:
         f("amatrix").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _i32p, _f64p, C.c_int]
         f("functional_substitution").argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _f64p, _u8p, _f64p, _u8p]
         f("functional_substitution").restype = C.c_double
+        f("build_offset_windows").argtypes = [C.c_void_p]
+        f("get_offset_windows").argtypes = [C.c_void_p, C.c_void_p]
+        f("get_offset_windows").restype = C.c_int
         f("var_est").argtypes = [C.c_void_p]
         f("var_est").restype = C.c_double
         f("num_z_blocks").argtypes = [C.c_void_p]
@@ -201,6 +204,18 @@ class _Lib:
             self.h, V, th1, th2, np.ascontiguousarray(sn, np.float64).reshape(-1),
             np.ascontiguousarray(sf, np.uint8).reshape(-1), np.ascontiguousarray(tn, np.float64),
             np.ascontiguousarray(tf, np.uint8))
+
+    def build_offset_windows(self):
+        """Build the rectangular-patch constraint windows of offset mode 3."""
+        self._f("build_offset_windows")(self.h)
+
+    def offset_windows(self):
+        """The constraint windows [M][N_r][N_t] (M = 0: none built)."""
+        m = self._f("get_offset_windows")(self.h, None)
+        out = np.zeros((m, self.N_r, self.N_t), np.float32)
+        if m:
+            self._f("get_offset_windows")(self.h, out.ctypes.data)
+        return out
 
     def var_est(self):
         return self._f("var_est")(self.h)

@@ -58,6 +58,9 @@ typedef struct {
 	uint8_t *mask;
 	double last_pct, fwd_cost, prior_cost, err_cost;
 	long long updates;
+	/* rectangular-patch constraint windows of the ring offsets, [nwin][N_r][N_t] */
+	int nwin;
+	oarr_t *win;
 } orc_t;
 
 #define SINO(c, p, r, t) ((((size_t)(p) * (c)->N_r) + (r)) * (c)->N_t + (t))
@@ -298,7 +301,7 @@ void orc_destroy(void *h)
 	free(c->angles); free(c->ptimes); free(c->rtimes);
 	free(c->y); free(c->w); free(c->e); free(c->d); free(c->sel); free(c->obj);
 	free(c->xr); free(c->yr); free(c->xn); free(c->yn); free(c->nr); free(c->nn);
-	free(c->mag); free(c->mask); free(c->H_r);
+	free(c->mag); free(c->mask); free(c->H_r); free(c->win);
 	free(c);
 }
 
@@ -787,6 +790,151 @@ static void orc_apply_shift(orc_t *c, int i, int j, double shift)
  * (XT_ICD_update.c:753-814, XT_OffsetError.c:99-168); on the reconstruct path
  * the constraint windows are never built, so the solve has M = 0 constraints
  * and reduces to x = b/Lambda with b = sum (e + d) w-terms. */
+/* ------------------------------------------- offset constraint windows -- */
+/* Overlapping rectangular windows over the detector (gen_offset_constraint_windows,
+ * XT_OffsetError.c:46-96): sides r_size = 2 N_r / round(sqrt(N_r)) and
+ * t_size = 2 N_t / round(sqrt(N_t)), origins every half side, wrapping
+ * around the detector edges, separable tent weights. */
+void orc_build_offset_windows(void *h)
+{
+	orc_t *c = (orc_t *)h;
+	int rs = 2 * c->N_r / (int)(sqrt(c->N_r) + 0.5), ts = 2 * c->N_t / (int)(sqrt(c->N_t) + 0.5);
+	int i, j, k, l, m = 0;
+	for (i = 0; i <= c->N_r - rs / 2; i += rs / 2)
+		for (j = 0; j <= c->N_t - ts / 2; j += ts / 2)
+			m++;
+	free(c->win);
+	c->nwin = m;
+	c->win = (oarr_t *)calloc((size_t)m * c->N_r * c->N_t, sizeof(oarr_t));
+	m = 0;
+	for (i = 0; i <= c->N_r - rs / 2; i += rs / 2)
+		for (j = 0; j <= c->N_t - ts / 2; j += ts / 2) {
+			for (k = i; k < i + rs; k++)
+				for (l = j; l < j + ts; l++) {
+					double a = (k - i) < rs / 2 ? (k - i + 1) : rs - (k - i);
+					a *= (l - j) < ts / 2 ? (l - j + 1) : ts - (l - j);
+					c->win[((size_t)m * c->N_r + k % c->N_r) * c->N_t + l % c->N_t] = (oarr_t)a;
+				}
+			m++;
+		}
+}
+
+int orc_get_offset_windows(void *h, float *out)
+{
+	orc_t *c = (orc_t *)h;
+	size_t q, n = (size_t)c->nwin * c->N_r * c->N_t;
+	if (out)
+		for (q = 0; q < n; q++)
+			out[q] = (float)c->win[q];
+	return c->nwin;
+}
+
+/* In-place inverse of the n x n matrix a (row-major) by LU decomposition with
+ * partial pivoting (rows scaled by their largest entry for the pivot choice)
+ * and forward / back substitution of each unit vector, as invert2 does
+ * (invert.c:110-140). */
+static void lu_inverse(double *a, int n)
+{
+	int i, j, k, imax = 0, *piv = (int *)malloc(sizeof(int) * n);
+	double *scale = (double *)malloc(sizeof(double) * n), *col = (double *)malloc(sizeof(double) * n);
+	double *y = (double *)malloc(sizeof(double) * n * n);
+	for (i = 0; i < n; i++) {
+		double big = 0;
+		for (j = 0; j < n; j++)
+			if (fabs(a[i * n + j]) > big)
+				big = fabs(a[i * n + j]);
+		scale[i] = big > 0 ? 1.0 / big : 0.0;
+	}
+	for (j = 0; j < n; j++) {
+		double big = 0;
+		for (i = 0; i < j; i++) {
+			double sum = a[i * n + j];
+			for (k = 0; k < i; k++)
+				sum -= a[i * n + k] * a[k * n + j];
+			a[i * n + j] = sum;
+		}
+		for (i = j; i < n; i++) {
+			double sum = a[i * n + j];
+			for (k = 0; k < j; k++)
+				sum -= a[i * n + k] * a[k * n + j];
+			a[i * n + j] = sum;
+			if (scale[i] * fabs(sum) >= big) {
+				big = scale[i] * fabs(sum);
+				imax = i;
+			}
+		}
+		if (j != imax) {
+			for (k = 0; k < n; k++) {
+				double t = a[imax * n + k];
+				a[imax * n + k] = a[j * n + k];
+				a[j * n + k] = t;
+			}
+			scale[imax] = scale[j];
+		}
+		piv[j] = imax;
+		if (a[j * n + j] == 0.0)
+			a[j * n + j] = 1e-20;
+		for (i = j + 1; i < n; i++)
+			a[i * n + j] /= a[j * n + j];
+	}
+	for (j = 0; j < n; j++) {
+		int first = -1;
+		for (i = 0; i < n; i++)
+			col[i] = i == j ? 1.0 : 0.0;
+		for (i = 0; i < n; i++) {
+			double sum = col[piv[i]];
+			col[piv[i]] = col[i];
+			if (first >= 0)
+				for (k = first; k < i; k++)
+					sum -= a[i * n + k] * col[k];
+			else if (sum != 0.0)
+				first = i;
+			col[i] = sum;
+		}
+		for (i = n - 1; i >= 0; i--) {
+			double sum = col[i];
+			for (k = i + 1; k < n; k++)
+				sum -= a[i * n + k] * col[k];
+			col[i] = sum / a[i * n + i];
+		}
+		for (i = 0; i < n; i++)
+			y[i * n + j] = col[i];
+	}
+	memcpy(a, y, sizeof(double) * n * n);
+	free(piv); free(scale); free(col); free(y);
+}
+
+/* Offsets x minimising sum Lambda (x - b / Lambda)^2 subject to A x = 0 for
+ * the constraint windows A (constrained_quad_opt, XT_OffsetError.c:99-168):
+ * D = A Lambda^-1 A^T, t = D^-1 A (b / Lambda), x = (b - A^T t) / Lambda. */
+static void orc_constrained_offsets(orc_t *c, const double *b, const double *L, oarr_t *x)
+{
+	const int M = c->nwin, Nr = c->N_r, Nt = c->N_t;
+	const size_t ne = (size_t)Nr * Nt;
+	double *D = (double *)calloc((size_t)M * M, sizeof(double));
+	double *t2 = (double *)calloc(M, sizeof(double)), *t = (double *)calloc(M, sizeof(double));
+	int i, j;
+	size_t q;
+	for (i = 0; i < M; i++)
+		for (j = 0; j < M; j++)
+			for (q = 0; q < ne; q++)
+				D[i * M + j] += (double)c->win[i * ne + q] * (double)c->win[j * ne + q] / L[q];
+	lu_inverse(D, M);
+	for (i = 0; i < M; i++)
+		for (q = 0; q < ne; q++)
+			t2[i] += (double)c->win[i * ne + q] * b[q] / L[q];
+	for (i = 0; i < M; i++)
+		for (j = 0; j < M; j++)
+			t[i] += D[i * M + j] * t2[j];
+	for (q = 0; q < ne; q++) {
+		oarr_t v = 0;
+		for (i = 0; i < M; i++)
+			v += (double)c->win[i * ne + q] * t[i];
+		x[q] = (oarr_t)((b[q] - v) / L[q]);
+	}
+	free(D); free(t2); free(t);
+}
+
 void orc_offset_update(void *h)
 {
 	orc_t *c = (orc_t *)h;
@@ -817,18 +965,27 @@ void orc_offset_update(void *h)
 				num[q] = b;
 				den[q] = L;
 			}
-		for (k = 0; k < c->N_p; k++)
-			for (i = 0; i < c->N_r; i++)
-				for (j = 0; j < c->N_t; j++) {
-					oarr_t x;
-					q = (size_t)i * c->N_t + j;
-					x = (oarr_t)((num[q] - 0.0) / den[q]);
-					o = SINO(c, k, i, j);
-					c->e[o] += c->d[q] - x;
-					c->sel[o] = fabs(c->e[o] * sqrt(c->w[o])) < c->hT;
-				}
-		for (q = 0; q < n; q++)
-			c->d[q] = (oarr_t)((num[q] - 0.0) / den[q]);
+		{
+			/* without windows (the reference's reconstruct path: none are
+			 * built) the constraint is empty and x = b / Lambda */
+			oarr_t *xs = (oarr_t *)malloc(sizeof(oarr_t) * n);
+			if (c->nwin > 0)
+				orc_constrained_offsets(c, num, den, xs);
+			else
+				for (q = 0; q < n; q++)
+					xs[q] = (oarr_t)((num[q] - 0.0) / den[q]);
+			for (k = 0; k < c->N_p; k++)
+				for (i = 0; i < c->N_r; i++)
+					for (j = 0; j < c->N_t; j++) {
+						q = (size_t)i * c->N_t + j;
+						o = SINO(c, k, i, j);
+						c->e[o] += c->d[q] - xs[q];
+						c->sel[o] = fabs(c->e[o] * sqrt(c->w[o])) < c->hT;
+					}
+			for (q = 0; q < n; q++)
+				c->d[q] = xs[q];
+			free(xs);
+		}
 		free(num);
 		free(den);
 		return;

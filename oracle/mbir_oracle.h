@@ -40,6 +40,8 @@ int orc_prepare(void *h, const float *object, const float *offset);
 int orc_iterate(void *h, int iter);
 double orc_cost(void *h, double *forward, double *prior, double *errsino);
 void orc_offset_update(void *h);
+void orc_build_offset_windows(void *h);
+int orc_get_offset_windows(void *h, float *out);
 void orc_variance_update(void *h);
 void orc_random_select(void *h);
 void orc_vsc_select(void *h);

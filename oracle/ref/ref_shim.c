@@ -25,6 +25,7 @@
 #include "XT_AMatrix.h"
 #include "XT_NHICD.h"
 #include "XT_ICD_update.h"
+#include "XT_OffsetError.h"
 #include "randlib.h"
 #include "allocate.h"
 
@@ -371,4 +372,51 @@ double ref_random2(void) { return random2(); }
 double ref_randomized_select(float *a, uint32_t n, uint32_t i)
 {
 	return RandomizedSelect(a, 0, n - 1, i);
+}
+
+/* Builds the rectangular-patch constraint windows of the ring offsets with
+ * the reference's own gen_offset_constraint_windows (XT_OffsetError.c:46-96),
+ * which only its phantom set-up calls (XT_Init.c:772); afterwards offset mode
+ * 3 solves the constrained problem (constrained_quad_opt). */
+void ref_build_offset_windows(void *h)
+{
+	ref_ctx *c = (ref_ctx *)h;
+	c->T->Write2Tiff = 0;
+	gen_offset_constraint_windows(c->S, c->T);
+}
+
+/* The windows [M][N_r][N_t] into out (may be NULL); returns M. */
+int ref_get_offset_windows(void *h, float *out)
+{
+	ref_ctx *c = (ref_ctx *)h;
+	int M = c->S->off_constraint_num;
+	size_t n = (size_t)M * c->S->N_r * c->S->N_t, q;
+	if (out && M > 0)
+		for (q = 0; q < n; q++)
+			out[q] = (float)(&(c->S->off_constraint[0][0][0]))[q];
+	return M;
+}
+
+/* The reference's x2 up-sampling of an object between resolution stages
+ * (upsample_object_bilinear_2D / _3D, XT_ICD_update.c:359-498) on flat arrays:
+ * in [n_z][n_y][n_x], out [n_z or 2 n_z][2 n_y][2 n_x].  The reference writes
+ * into slices 1.. of a halo-padded object; the halo is dropped here. */
+void upsample_object_bilinear_2D(Real_arr_t ***, Real_arr_t ***, int32_t, int32_t, int32_t);
+void upsample_object_bilinear_3D(Real_arr_t ***, Real_arr_t ***, int32_t, int32_t, int32_t);
+void ref_upsample(const float *in, float *out, int n_z, int n_y, int n_x, int z_too)
+{
+	const int oz = z_too ? 2 * n_z : n_z;
+	Real_arr_t ***I = (Real_arr_t ***)multialloc(sizeof(Real_arr_t), 3, n_z, n_y, n_x);
+	Real_arr_t ***O = (Real_arr_t ***)multialloc(sizeof(Real_arr_t), 3, oz + 2, 2 * n_y, 2 * n_x);
+	size_t q, pl = (size_t)4 * n_y * n_x;
+	for (q = 0; q < (size_t)n_z * n_y * n_x; q++)
+		(&I[0][0][0])[q] = in[q];
+	if (z_too)
+		upsample_object_bilinear_3D(O, I, n_z, n_y, n_x);
+	else
+		upsample_object_bilinear_2D(O, I, n_z, n_y, n_x);
+	for (q = 0; q < (size_t)oz * pl; q++)
+		out[q] = (&O[1][0][0])[q];
+	multifree(I, 3);
+	multifree(O, 3);
 }

@@ -17,6 +17,8 @@ Outputs (committed):
                            binary (object, cost trace) on a seeded 32x32x4 scan
   recon_rings.npz          the same with ring offsets in the data and
                            remove_rings 2 (object, offsets, cost trace)
+  upsample.npz             the reference's x2 up-sampling between stages
+                           (upsample_object_bilinear_2D / _3D) of seeded slices
 """
 from __future__ import annotations
 
@@ -34,7 +36,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-from oracle.bind import REF_BIN, Reference, reference_src  # noqa: E402
+from oracle.bind import REF_BIN, REF_SO, Reference, reference_src  # noqa: E402
 from timbir_b200 import synth  # noqa: E402
 
 import scenarios  # noqa: E402
@@ -51,8 +53,8 @@ def park_miller_table():
         json.dump({"seed": 1, "values": nums, "source": "src/MBIR_4D/randlib.c:69-90"}, f, indent=1)
 
 
-def stage_fixtures():
-    for name in scenarios.SCENARIOS:
+def stage_fixtures(names=None):
+    for name in names or scenarios.SCENARIOS:
         wd = tempfile.mkdtemp()
         R = scenarios.make(name, Reference, workdir=wd)
         R.prepare()
@@ -116,9 +118,34 @@ def recon_rings_fixture():
     print("recon rings", obj.shape, off.shape, cost[-3:])
 
 
+def upsample_fixture():
+    """The reference's x2 up-sampling between stages on seeded random slices."""
+    import ctypes as C
+    lib = C.CDLL(REF_SO)
+    lib.ref_upsample.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+    rng = np.random.default_rng(31)
+    out = {}
+    for k, (nz, ny, nx) in enumerate([(4, 8, 8), (3, 5, 7), (2, 16, 2), (2, 2, 6)]):
+        x = (rng.random((nz, ny, nx)) * 0.02).astype(np.float32)
+        out[f"in{k}"] = x
+        for z_too in (0, 1):
+            oz = 2 * nz if z_too else nz
+            y = np.zeros((oz, 2 * ny, 2 * nx), np.float32)
+            lib.ref_upsample(x.ctypes.data, y.ctypes.data, nz, ny, nx, z_too)
+            out[f"out{k}_{z_too}"] = y
+    np.savez_compressed(os.path.join(HERE, "upsample.npz"), **out)
+    print("upsample", sorted(out))
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "upsample":
+        upsample_fixture()
+        sys.exit(0)
     if len(sys.argv) > 1 and sys.argv[1] == "recon_rings":
         recon_rings_fixture()
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[1] == "stage":  # named scenarios only
+        stage_fixtures(sys.argv[2:])
         sys.exit(0)
     if not Reference.available():
         sys.exit("build the reference first: make -C oracle ref")
@@ -126,3 +153,4 @@ if __name__ == "__main__":
     stage_fixtures()
     recon_fixture()
     recon_rings_fixture()
+    upsample_fixture()

@@ -28,6 +28,9 @@ SCENARIOS = {
                dict(remove_rings=2), dict(update_proj_offset=2), 2, 1, 1),
     "rings3": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=3, ring_sigma=0.02),
                dict(remove_rings=3), dict(update_proj_offset=3), 2, 1, 1),
+    # mode 3 with the rectangular-patch constraint windows built
+    "rings3w": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=3, ring_sigma=0.02),
+                dict(remove_rings=3), dict(update_proj_offset=3), 2, 1, 1),
     "zinger_var": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=4, zinger_frac=0.003),
                    dict(remove_rings=2, quad_convex=0), dict(update_proj_offset=2, update_var=1, var_est=1.3),
                    2, 1, 1),
@@ -48,4 +51,6 @@ def make(name, cls, **extra):
     obj = cls(scan, blocks=blocks, mult_xy=mxy, mult_z=mz, **args, **extra)
     if sw:
         obj.set_switches(**sw)
+    if name.endswith("w"):
+        obj.build_offset_windows()
     return obj

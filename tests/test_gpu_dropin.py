@@ -7,10 +7,21 @@ link line INTEGRATION.md gives; oracle/Makefile builds it where the
 reference sources are).  It reads the bin_data file set, calls reconstruct()
 and leaves the output files in its working directory.  Its results are
 compared with full runs of the reference's driver on the same inputs
-(tests/golden/recon_small.npz, recon_rings.npz): MAP cost of the final
-object (and offsets) evaluated afresh in FP64 within 5e-5 relative, object
-RMSE below 1e-3 of the phantom's 0.02 range, ring-offset RMSE below 1e-3,
-and the reference's output file set.
+(tests/golden/recon_small.npz, recon_rings.npz), by the MAP cost of the final
+object (and offsets) evaluated afresh in FP64, the object's RMSE against the
+reference's (below 1e-3 of the phantom's 0.02 range), the offsets' RMSE,
+and the reference's output file set:
+  * plain scan, default (super-voxel) schedule: cost within 5e-5 relative;
+  * scan with ring offsets, remove_rings 2, the reference schedule
+    (TIMBIR_SCHEDULE=reference): the reference's 1000 iterations (its
+    convergence test does not stop it), cost within 5e-5, offsets RMSE
+    below 1e-3;
+  * the same scan, default schedule with convg_thresh 1e-6 and up to 3000
+    iterations per stage: the joint image-offset cost is nearly flat along
+    ring patterns (a ring-shaped image component and a per-detector offset
+    explain the data almost equally well), so the reference's 1000-iteration
+    result is not its minimum; this run must end at least as low (cost at
+    most 5e-5 above the reference's).
 """
 import os
 import subprocess
@@ -28,8 +39,12 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "XT_Main_gpu")
 ARGS = dict(sig_s=0.002, sig_t=1.0, c_s=1e-3, c_t=1e-3, convg_thresh=0.005, huber_delta=0.5, huber_T=4.0)
 
 CASES = {
-    "plain": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=11), 0, "recon_small.npz"),
-    "rings": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=13, ring_sigma=0.02), 2, "recon_rings.npz"),
+    # name: scan, remove_rings, fixture, schedule, convg_thresh, comparison
+    "plain": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=11), 0, "recon_small.npz", "sv", 0.005, "match"),
+    "rings_reference_schedule": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=13, ring_sigma=0.02), 2,
+                                 "recon_rings.npz", "reference", 0.005, "match"),
+    "rings_sv_converged": (lambda: synth.ellipsoid_scan(32, 4, 48, seed=13, ring_sigma=0.02), 2, "recon_rings.npz",
+                           "sv", 1e-6, "at_most"),
 }
 
 
@@ -37,16 +52,21 @@ CASES = {
 def test_reference_driver_linked_against_the_library(tmp_path, case):
     if not os.path.exists(DRIVER):
         pytest.skip("oracle/_ref/XT_Main_gpu not built (make -C oracle ref with the reference sources)")
-    factory, rings, fixture = CASES[case]
+    factory, rings, fixture, schedule, convg, how = CASES[case]
     g = np.load(os.path.join(GOLD, fixture))
     scan = factory()
     scan.write_bin(str(tmp_path))
     cmd = [DRIVER, "--proj_rows", str(scan.proj_rows), "--proj_cols", str(scan.proj_cols), "--proj_num",
            str(scan.proj_num), "--recon_num", "1", "--vox_wid", str(scan.vox_wid), "--rot_center",
            str(scan.rot_center), "--sig_s", str(ARGS["sig_s"]), "--sig_t", str(ARGS["sig_t"]), "--c_s",
-           str(ARGS["c_s"]), "--c_t", str(ARGS["c_t"]), "--convg_thresh", str(ARGS["convg_thresh"]),
+           str(ARGS["c_s"]), "--c_t", str(ARGS["c_t"]), "--convg_thresh", str(convg),
            "--remove_rings", str(rings), "--quad_convex"]
-    r = subprocess.run(cmd, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    env = dict(os.environ, TIMBIR_SCHEDULE=schedule)
+    if how == "at_most":
+        env["TIMBIR_MAX_ITERS"] = "3000"
+    if schedule == "reference":
+        env["TIMBIR_Z_BLOCK_THREADS"] = str(int(g["threads"]))
+    r = subprocess.run(cmd, cwd=tmp_path, capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     x = np.fromfile(tmp_path / "object_time_0.bin", np.float32).reshape(1, 4, 32, 32)
     xr = g["object"].reshape(1, 4, 32, 32)
@@ -62,11 +82,16 @@ def test_reference_driver_linked_against_the_library(tmp_path, case):
 
     dr = g["offset"].reshape(32, 4) if rings else None
     c, cr = fresh(x, d if rings else None), fresh(xr, dr)
-    assert abs(c - cr) / cr < 5e-5
-    assert float(np.sqrt(np.mean((x - xr) ** 2))) < 1e-3 * 0.02
+    print(f"{case}: fresh FP64 cost {c:.10g}, reference driver's {cr:.10g}, relative {(c - cr) / cr:.3g}")
+    if how == "match":
+        assert abs(c - cr) / cr < 5e-5
+        assert float(np.sqrt(np.mean((x - xr) ** 2))) < 1e-3 * 0.02
+        if rings:
+            assert float(np.sqrt(np.mean((d - dr) ** 2))) < 1e-3
+    else:
+        assert (c - cr) / cr < 5e-5
     if rings:
         assert np.any(d != 0)
-        assert float(np.sqrt(np.mean((d - dr) ** 2))) < 1e-3
     for name, size in (("proj_offset.bin", 32 * 4 * 4), ("variance_estimate.bin", 8), ("status.bin", 4),
                        ("projs_runtime.bin", 48 * 32 * 4 * 4), ("weights_runtime.bin", 48 * 32 * 4 * 4)):
         assert (tmp_path / name).stat().st_size == size, name

@@ -70,7 +70,7 @@ def _load_state(stage, oracle, seed):
     oracle.prepare(x, off)
 
 
-@pytest.mark.parametrize("name", ["rings1", "rings2", "rings3", "zinger_var"])
+@pytest.mark.parametrize("name", ["rings1", "rings2", "rings3", "rings3w", "zinger_var"])
 def test_offset_update_matches_oracle(name):
     s = scenarios.make(name, timbir_b200.Stage)
     o = scenarios.make(name, Oracle)
@@ -80,6 +80,28 @@ def test_offset_update_matches_oracle(name):
         o.offset_update()
     assert rel(s.offset(), o.offset()) < 1e-5
     assert rel(s.errorsino(), o.errorsino()) < 1e-5
+
+
+def test_windowed_offsets_meet_every_window_constraint():
+    # ring-offset mode 3 with the rectangular-patch windows built: the
+    # offsets solve min sum Lambda (d - b / Lambda)^2 subject to A d = 0 for
+    # every window A (constrained_quad_opt, XT_OffsetError.c:99-168); the
+    # GPU's must satisfy the constraints to FP32 rounding of d, use the
+    # reference's windows, and differ from the unconstrained mode-3 update
+    s = scenarios.make("rings3w", timbir_b200.Stage)
+    o = scenarios.make("rings3w", Oracle)
+    u = scenarios.make("rings3", timbir_b200.Stage)
+    A = o.offset_windows()  # [M][N_r][N_t]
+    assert s.offset_window_count() == A.shape[0] > 0 and u.offset_window_count() == 0
+    _load_state(s, o, 11)
+    _load_state(u, o, 11)
+    s.offset_update()
+    u.offset_update()
+    d = s.offset().astype(np.float64)
+    sums = np.tensordot(A.astype(np.float64), d, axes=([1, 2], [0, 1]))
+    scale = np.tensordot(A.astype(np.float64), np.abs(d), axes=([1, 2], [0, 1]))
+    assert np.abs(sums).max() < 1e-5 * scale.max()
+    assert rel(u.offset(), s.offset()) > 1e-3
 
 
 @pytest.mark.parametrize("name", ["zinger_var", "frames4"])

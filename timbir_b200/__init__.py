@@ -53,6 +53,8 @@ def load_library() -> C.CDLL:
     lib.mbir_update_voxels_time_slices.argtypes = [_VP, i32, C.POINTER(i32)]
     lib.mbir_compute_cost.argtypes = [_VP] + [C.POINTER(C.c_double)] * 3
     lib.mbir_update_sinogram_offset.argtypes = [_VP]
+    lib.mbir_set_offset_windows.argtypes = [_VP, i32]
+    lib.mbir_get_offset_windows.argtypes = [_VP]
     lib.mbir_update_variance_parameter.argtypes = [_VP]
     lib.mbir_stage_dims.argtypes = [_VP, _i32p]
     for n in ("mbir_get_object", "mbir_set_object", "mbir_get_errorsino", "mbir_get_weight", "mbir_get_offset",
@@ -82,6 +84,7 @@ def load_library() -> C.CDLL:
     lib.mbir_set_sv_guard.argtypes = [_VP, i32]
     lib.mbir_set_sv_nhicd.argtypes = [_VP, C.c_double]
     lib.mbir_nhicd_select.argtypes = [_f32p, i32, i32, i32, _i32p, _u8p, _f32p]
+    lib.mbir_upsample.argtypes = [_f32p, _f32p, i32, i32, i32, i32]
     lib.mbir_time_begin.argtypes = [_VP]
     lib.mbir_time_end.argtypes = [_VP, C.POINTER(C.c_double)]
     i64 = C.c_int64
@@ -245,6 +248,17 @@ class Stage:
     def offset_update(self):
         _check(self.lib.mbir_update_sinogram_offset(self.h))
 
+    def set_offset_windows(self, on: bool = True):
+        """Rectangular-patch constraint windows for ring-offset mode 3
+        (mbir_set_offset_windows)."""
+        _check(self.lib.mbir_set_offset_windows(self.h, 1 if on else 0))
+
+    def build_offset_windows(self):
+        self.set_offset_windows(True)
+
+    def offset_window_count(self) -> int:
+        return int(self.lib.mbir_get_offset_windows(self.h))
+
     def variance_update(self):
         _check(self.lib.mbir_update_variance_parameter(self.h))
 
@@ -254,8 +268,15 @@ class Stage:
         _check(getattr(self.lib, fn)(self.h, out.reshape(-1)))
         return out
 
-    def object(self):
-        return self._get("mbir_get_object", (self.N_time, self.N_z, self.N_y, self.N_x))
+    def object(self, out=None):
+        """The object [N_time][N_z][N_y][N_x]; `out` (float32, C-contiguous, e.g.
+        pinned host memory) receives it when given."""
+        if out is None:
+            return self._get("mbir_get_object", (self.N_time, self.N_z, self.N_y, self.N_x))
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.N_time * self.N_z * self.N_y * self.N_x:
+            raise ValueError("out must be a C-contiguous float32 array of the object's size")
+        _check(self.lib.mbir_get_object(self.h, out.reshape(-1)))
+        return out
 
     def set_object(self, x):
         _check(self.lib.mbir_set_object(self.h, _f32(x).reshape(-1)))
@@ -418,6 +439,17 @@ def nhicd_select(mag: np.ndarray, nsel) -> tuple:
     th = np.zeros(planes, np.float32)
     _check(lib.mbir_nhicd_select(mag.reshape(-1), planes, ny, nx, nsel, sel.reshape(-1), th))
     return sel, th
+
+
+def upsample(x: np.ndarray, z_too: bool) -> np.ndarray:
+    """The GPU's x2 up-sampling between multi-resolution stages (mbir_upsample)
+    of x [n_z][n_y][n_x]."""
+    lib = load_library()
+    x = np.ascontiguousarray(x, np.float32)
+    nz, ny, nx = x.shape
+    out = np.zeros(((2 if z_too else 1) * nz, 2 * ny, 2 * nx), np.float32)
+    _check(lib.mbir_upsample(x.reshape(-1), out.reshape(-1), nz, ny, nx, 1 if z_too else 0))
+    return out
 
 
 def _malloc_copy(a: np.ndarray) -> C.c_void_p:

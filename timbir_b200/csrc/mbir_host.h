@@ -62,3 +62,9 @@ void upsample_xy(const float *in, float *out, int n_z, int n_y, int n_x);
 void upsample_xyz(const float *in, float *out, int n_z, int n_y, int n_x);
 
 }  // namespace mbir
+
+// The prologue of a stage that follows `prev` in one multi-resolution run,
+// with the start object and magnitude map up-sampled from prev's on the
+// device (mbir_stage.cu); *mag_carried = 1 when the magnitude map was carried.
+struct MbirStage;
+int mbir_icd_prepare_from(MbirStage *S, MbirStage *prev, int initICD, const float *offset, int *mag_carried);

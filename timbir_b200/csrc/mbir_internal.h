@@ -70,9 +70,26 @@ cudaError_t mbir_launch_icd_ref(const MbirGeom &g, const MbirPrior &pr, const Mb
                                 cudaStream_t s);
 cudaError_t mbir_launch_cost(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
                              double *partials, int nparts, double *result, cudaStream_t s);
+// Rectangular-patch constraint windows of offset type 3 (device arrays; the
+// element index is q = t N_r + r): per window m its elements win_el /
+// weights win_a in [win_off[m], win_off[m+1]); per overlapping window pair
+// (pair_i <= pair_j) the shared elements and both weights; per element its
+// windows el_m / weights el_a.  D (M x M), y (M), x (nel) are scratch.
+struct OffsetWindows {
+    int M, nel, npairs;
+    const int *win_off, *win_el;
+    const float *win_a;
+    const int *pair_off, *pair_i, *pair_j, *pair_el;
+    const float *pair_ai, *pair_aj;
+    const int *el_off, *el_m;
+    const float *el_a;
+    double *D, *y, *x;
+};
+// Ring-offset update of the given type; with type 3 and windows (M > 0) the
+// constrained solve (err |= 16 if its system is not positive definite).
 cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
                                double *num, double *den, double *partials, int nparts,
-                               cudaStream_t s);
+                               cudaStream_t s, const OffsetWindows *win = nullptr, int *err = nullptr);
 cudaError_t mbir_launch_variance(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
                                  double var_est, double *partials, int nparts, double *result,
                                  cudaStream_t s);
@@ -84,6 +101,9 @@ cudaError_t mbir_launch_select_stats(const float *mag, const int *xs, const int 
                                      const int *counts, int planes, int stride, double *out,
                                      cudaStream_t s);
 int mbir_amax(double delta_xy, double delta_r);
+// x2 up-sampling of n_z coarse [n_y][n_x] slices into [n_z or 2 n_z][2 n_y][2 n_x]
+// (z_too: also along z), as the host hand-off between stages computes it.
+cudaError_t mbir_launch_upsample(const float *in, float *out, int n_z, int n_y, int n_x, bool z_too, cudaStream_t s);
 // [view][row][col] -> [row][view][col].
 cudaError_t mbir_launch_to_slice_major(const float *in, float *out, int N_p, int N_t, int N_r, cudaStream_t s);
 // Detector response table H_r [N_p][65] from the host-computed trapezoids and beam.

@@ -415,7 +415,7 @@ __global__ void k_offset_terms(MbirGeom g, MbirPrior pr, MbirDev dv, int type, d
 }
 
 __global__ void k_offset_apply(MbirGeom g, MbirDev dv, int type, const double *num, const double *den,
-                               const double *sums)
+                               const double *sums, const double *xw)
 {
     const size_t nel = (size_t)g.N_t * g.N_r;
     const double gamma = type == 2 ? sums[0] / sums[1] : 0.0;
@@ -423,7 +423,7 @@ __global__ void k_offset_apply(MbirGeom g, MbirDev dv, int type, const double *n
     if (q >= nel) return;
     const int t = (int)(q / g.N_r), r = (int)(q % g.N_r);
     if (type == 3) {
-        const float xn = (float)((num[q] - 0.0) / den[q]);
+        const float xn = xw ? (float)xw[q] : (float)((num[q] - 0.0) / den[q]);
         const float dd = __fsub_rn(dv.d[q], xn);
         for (int p = 0; p < g.N_p; p++) {
             const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
@@ -439,6 +439,185 @@ __global__ void k_offset_apply(MbirGeom g, MbirDev dv, int type, const double *n
         }
     }
 }
+
+// ----------------------------------------------------------------------------
+// Ring offsets of type 3 with rectangular-patch constraint windows
+// (constrained_quad_opt, XT_OffsetError.c:99-168): minimise
+// sum Lambda (x - b / Lambda)^2 subject to A x = 0 for the M windows A.
+// With D = A Lambda^-1 A^T (symmetric positive definite) and
+// c = A (b / Lambda): D y = c, x = (b - A^T y) / Lambda.  One CTA, FP64: c per
+// window and D per overlapping window pair as fixed-order sums over the
+// (host-built) element lists, Cholesky factorisation of D in place
+// (column by column), forward and back substitution, then x per element.
+// The reference inverts D by LU decomposition; the solution is the same up
+// to FP64 rounding.  err |= 16 if D is not positive definite.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(1024) k_offset_windows(OffsetWindows W, const double *__restrict__ b,
+                                                         const double *__restrict__ L, double *__restrict__ xw,
+                                                         int *err)
+{
+    const int M = W.M, tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5,
+              nw = nthr >> 5;
+    double *D = W.D, *y = W.y;
+    for (int q = tid; q < M * M; q += nthr) D[q] = 0.0;
+    __syncthreads();
+    for (int m = warp; m < M; m += nw) {
+        double s = 0.0;
+        for (int k = W.win_off[m] + lane; k < W.win_off[m + 1]; k += 32) {
+            const int q = W.win_el[k];
+            s += (double)W.win_a[k] * b[q] / L[q];
+        }
+        s = warp_sum_d(s);
+        if (lane == 0) y[m] = s;
+    }
+    for (int p = warp; p < W.npairs; p += nw) {
+        double s = 0.0;
+        for (int k = W.pair_off[p] + lane; k < W.pair_off[p + 1]; k += 32) {
+            const int q = W.pair_el[k];
+            s += (double)W.pair_ai[k] * (double)W.pair_aj[k] / L[q];
+        }
+        s = warp_sum_d(s);
+        if (lane == 0) {
+            D[W.pair_i[p] * M + W.pair_j[p]] = s;
+            D[W.pair_j[p] * M + W.pair_i[p]] = s;
+        }
+    }
+    __syncthreads();
+    // D = L L^T, L in the lower triangle
+    for (int k = 0; k < M; k++) {
+        if (tid == 0) {
+            double v = D[k * M + k];
+            if (!(v > 0.0)) {
+                atomicOr(err, 16);
+                v = 1.0;
+            }
+            D[k * M + k] = sqrt(v);
+        }
+        __syncthreads();
+        const double dk = D[k * M + k];
+        for (int i = k + 1 + tid; i < M; i += nthr) D[i * M + k] /= dk;
+        __syncthreads();
+        const int n = M - k - 1;
+        for (int q = tid; q < n * n; q += nthr) {
+            const int i = k + 1 + q / n, j = k + 1 + q % n;
+            if (j <= i) D[i * M + j] -= D[i * M + k] * D[j * M + k];
+        }
+        __syncthreads();
+    }
+    // L z = c, then L^T y = z (y holds c on entry)
+    for (int k = 0; k < M; k++) {
+        if (tid == 0) y[k] /= D[k * M + k];
+        __syncthreads();
+        for (int i = k + 1 + tid; i < M; i += nthr) y[i] -= D[i * M + k] * y[k];
+        __syncthreads();
+    }
+    for (int k = M - 1; k >= 0; k--) {
+        if (tid == 0) y[k] /= D[k * M + k];
+        __syncthreads();
+        for (int i = tid; i < k; i += nthr) y[i] -= D[k * M + i] * y[k];
+        __syncthreads();
+    }
+    for (int q = tid; q < W.nel; q += nthr) {
+        double v = 0.0;
+        for (int k = W.el_off[q]; k < W.el_off[q + 1]; k++) v += (double)W.el_a[k] * y[W.el_m[k]];
+        xw[q] = (b[q] - v) / L[q];
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Multi-resolution hand-off on the device: the x2 up-samplings of the object
+// and the update-magnitude map between stages (initObject / upsample_*,
+// XT_ICD_update.c:323-651), in the operation order of the host versions
+// (mbir_setup.cpp upsample_xy / upsample_xyz), so the results are identical.
+// Interior samples are (a + 3 b) / 4 and (3 b + c) / 4 of the two nearest
+// coarse ones, edge samples repeat the edge value.
+// ----------------------------------------------------------------------------
+// x-pass value at fine column X of coarse row r (length n_x), in double
+__device__ __forceinline__ double up_x(const float *r, int n_x, int X)
+{
+    const int ox = 2 * n_x;
+    if (X == 0) return (double)r[0];
+    if (X == 1) return __ddiv_rn(__dadd_rn(__dmul_rn(3.0, (double)r[0]), (double)r[1]), 4.0);
+    if (X == ox - 1) return (double)r[n_x - 1];
+    if (X == ox - 2) return __ddiv_rn(__dadd_rn((double)r[n_x - 2], __dmul_rn(3.0, (double)r[n_x - 1])), 4.0);
+    const int k = X >> 1;
+    if ((X & 1) == 0) return __ddiv_rn(__dadd_rn((double)r[k - 1], __dmul_rn(3.0, (double)r[k])), 4.0);
+    return __ddiv_rn(__dadd_rn(__dmul_rn(3.0, (double)r[k]), (double)r[k + 1]), 4.0);
+}
+
+// slices up-sampled in x and y only (same slice count)
+__global__ void k_upsample_xy(const float *__restrict__ in, float *__restrict__ out, int n_z, int n_y, int n_x)
+{
+    const int ox = 2 * n_x, oy = 2 * n_y;
+    const size_t n = (size_t)n_z * oy * ox;
+    const size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int X = (int)(o % ox), Y = (int)((o / ox) % oy), s = (int)(o / ((size_t)ox * oy));
+    const float *I = in + (size_t)s * n_y * n_x;
+    // the x-pass rows are stored as float
+    auto b = [&](int j) { return (float)up_x(I + (size_t)j * n_x, n_x, X); };
+    float v;
+    if (Y == 0)
+        v = b(0);
+    else if (Y == 1)
+        v = (float)__ddiv_rn(__dadd_rn(__dmul_rn(3.0, (double)b(0)), (double)b(1)), 4.0);
+    else if (Y == oy - 1)
+        v = b(n_y - 1);
+    else if (Y == oy - 2)
+        v = (float)__ddiv_rn(__dadd_rn((double)b(n_y - 2), __dmul_rn(3.0, (double)b(n_y - 1))), 4.0);
+    else {
+        const int j = Y >> 1;
+        if ((Y & 1) == 0)
+            v = (float)__ddiv_rn(__dadd_rn((double)b(j - 1), __dmul_rn(3.0, (double)b(j))), 4.0);
+        else  // float arithmetic for 3 b + c, as the host version
+            v = (float)__ddiv_rn((double)__fadd_rn(__fmul_rn(3.0f, b(j)), b(j + 1)), 4.0);
+    }
+    out[o] = v;
+}
+
+// up-sampled in x, y and z (twice the slices); every pass in double
+__global__ void k_upsample_xyz(const float *__restrict__ in, float *__restrict__ out, int n_z, int n_y, int n_x)
+{
+    const int ox = 2 * n_x, oy = 2 * n_y, oz = 2 * n_z;
+    const size_t n = (size_t)oz * oy * ox;
+    const size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int X = (int)(o % ox), Y = (int)((o / ox) % oy), Z = (int)(o / ((size_t)ox * oy));
+    auto b2 = [&](int s, int j) { return up_x(in + ((size_t)s * n_y + j) * n_x, n_x, X); };
+    auto b3 = [&](int s) {
+        if (Y == 0) return b2(s, 0);
+        if (Y == 1) return __ddiv_rn(__dadd_rn(__dmul_rn(3.0, b2(s, 0)), b2(s, 1)), 4.0);
+        if (Y == oy - 1) return b2(s, n_y - 1);
+        if (Y == oy - 2) return __ddiv_rn(__dadd_rn(b2(s, n_y - 2), __dmul_rn(3.0, b2(s, n_y - 1))), 4.0);
+        const int j = Y >> 1;
+        if ((Y & 1) == 0) return __ddiv_rn(__dadd_rn(b2(s, j - 1), __dmul_rn(3.0, b2(s, j))), 4.0);
+        return __ddiv_rn(__dadd_rn(__dmul_rn(3.0, b2(s, j)), b2(s, j + 1)), 4.0);
+    };
+    double v;
+    if (Z == 0)
+        v = b3(0);
+    else if (Z == 1)
+        v = __ddiv_rn(__dadd_rn(__dmul_rn(3.0, b3(0)), b3(1)), 4.0);
+    else if (Z == oz - 1)
+        v = b3(n_z - 1);
+    else if (Z == oz - 2)
+        v = __ddiv_rn(__dadd_rn(__dmul_rn(3.0, b3(n_z - 1)), b3(n_z - 2)), 4.0);
+    else {
+        const int s = Z >> 1;
+        if ((Z & 1) == 0)
+            v = __ddiv_rn(__dadd_rn(b3(s - 1), __dmul_rn(3.0, b3(s))), 4.0);
+        else
+            v = __ddiv_rn(__dadd_rn(__dmul_rn(3.0, b3(s)), b3(s + 1)), 4.0);
+    }
+    out[o] = (float)v;
+}
+
 
 // ----------------------------------------------------------------------------
 // Variance (XT_ICD_update.c:720-751).  Pass 1 restores w_orig = w * sigma^2
@@ -560,6 +739,16 @@ __global__ void k_to_slice_major(const float *__restrict__ in, float *__restrict
 
 }  // namespace
 
+cudaError_t mbir_launch_upsample(const float *in, float *out, int n_z, int n_y, int n_x, bool z_too, cudaStream_t s)
+{
+    const size_t n = (size_t)(z_too ? 2 * n_z : n_z) * 4 * n_y * n_x;
+    if (z_too)
+        k_upsample_xyz<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n_z, n_y, n_x);
+    else
+        k_upsample_xy<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n_z, n_y, n_x);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- launchers --
 cudaError_t mbir_launch_detector_response(const double *trap, const double *beam, int N_p, double OffsetR,
                                           double delta_xy, double r0, double step, double tc, float *H_r,
@@ -615,13 +804,18 @@ cudaError_t mbir_launch_cost(const MbirGeom &g, const MbirPrior &pr, const MbirD
 
 cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
                                double *num, double *den, double *partials, int nparts,
-                               cudaStream_t s)
+                               cudaStream_t s, const OffsetWindows *win, int *err)
 {
     k_offset_terms<<<nparts, 128, 0, s>>>(g, pr, dv, type, num, den, partials, nparts);
     double *sums = partials + 2 * (size_t)nparts;
     k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, sums);
     const size_t nel = (size_t)g.N_t * g.N_r;
-    k_offset_apply<<<(unsigned)((nel + 127) / 128), 128, 0, s>>>(g, dv, type, num, den, sums);
+    const double *xw = nullptr;
+    if (type == 3 && win && win->M > 0) {
+        k_offset_windows<<<1, 1024, 0, s>>>(*win, num, den, win->x, err);
+        xw = win->x;
+    }
+    k_offset_apply<<<(unsigned)((nel + 127) / 128), 128, 0, s>>>(g, dv, type, num, den, sums, xw);
     return cudaGetLastError();
 }
 

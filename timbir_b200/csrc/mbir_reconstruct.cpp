@@ -31,6 +31,7 @@
 #include <cstring>
 #include <ctime>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/mbir4d.h"
@@ -179,6 +180,9 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
     uint32_t rng_state = 761521u;
     std::vector<float> carried_offset;  // ring offsets kept in memory between stages
     const size_t nsino = (size_t)proj_num * proj_rows * proj_cols;
+    // the previous stage of this call, kept on the device until the next
+    // stage has taken its object and magnitude map (freed on every exit)
+    std::unique_ptr<MbirStage, void (*)(MbirStage *)> prev_stage(nullptr, mbir_free_stage);
 
     for (int i = last; i < multres; i++) {
         LOG_INFO(log, "Running multi-resolution stage %d with x-y voxel scale = %d and z voxel scale = %d.\n",
@@ -202,11 +206,12 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
             in.release_all();
             return -1;
         }
-        // inputs: the caller's arrays at the first stage run, the runtime copies
-        // (reference layout [view][col][row]) afterwards (XT_Init.c:296-315)
+        // inputs: the caller's arrays for the stages of this call; a restarted
+        // call's first stage reads the runtime copies (reference layout
+        // [view][col][row], XT_Init.c:296-315) as the reference does
         std::vector<float> pr_in, wt_in;
         const float *P = projections, *W = weights;
-        if (i != 0) {
+        if (i != 0 && i == last) {
             std::vector<float> a(nsino), b(nsino);
             if (read_bin("projs_runtime", a.data(), sizeof(float), nsino) ||
                 read_bin("weights_runtime", b.data(), sizeof(float), nsino)) {
@@ -224,7 +229,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
                     }
             P = pr_in.data();
             W = wt_in.data();
-        } else {
+        } else if (i == 0) {
             std::vector<float> a(nsino), b(nsino);
             for (int p = 0; p < proj_num; p++)
                 for (int t = 0; t < proj_rows; t++)
@@ -258,7 +263,6 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
             in.release_all();
             return -1;
         }
-        if (i == last) in.release();
         mbir_set_rng_state(S, rng_state);
         int nblk_stage = nblk;
         if (use_sv) {
@@ -297,7 +301,22 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
         const size_t nvox = (size_t)recon_num * N_z * N_y * N_x, nxy = (size_t)N_y * N_x;
         std::vector<float> obj(nvox, 0.0f), mag((size_t)recon_num * nblk_stage * nxy, 0.0f);
         bool have_mag = false;
-        if (initICD == 2 || initICD == 3) {
+        const bool on_device = prev_stage && (initICD == 2 || initICD == 3);
+        if (on_device) {
+            // the previous stage of this call is still on the device: its object
+            // and magnitude map are up-sampled there, nothing is read back
+            int carried = 0;
+            if (mbir_icd_prepare_from(S, prev_stage.get(), initICD, offp, &carried)) {
+                LOG_ERR(log, "Stage prologue failed: %s\n", mbir_last_error());
+                mbir_free_stage(S);
+                in.release_all();
+                return -1;
+            }
+            if (!carried)
+                LOG_INFO(log, "Number of axial blocks is incompatible with previous stage; "
+                              "initializing the multi-resolution map to zeros.\n");
+            prev_stage.reset();
+        } else if (initICD == 2 || initICD == 3) {
             const int cz = initICD == 3 ? N_z / 2 : N_z;
             std::vector<float> coarse((size_t)cz * (N_y / 2) * (N_x / 2));
             for (int f = 0; f < recon_num; f++) {
@@ -336,7 +355,7 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
                 }
             }
         }
-        if (mbir_icd_prepare(S, obj.data(), offp, have_mag ? mag.data() : nullptr)) {
+        if (!on_device && mbir_icd_prepare(S, obj.data(), offp, have_mag ? mag.data() : nullptr)) {
             LOG_ERR(log, "Stage prologue failed: %s\n", mbir_last_error());
             mbir_free_stage(S);
             in.release_all();
@@ -400,7 +419,10 @@ extern "C" int reconstruct(float **object, float *projections, float *weights, f
             rng_state = mbir_get_rng_state(S);
         }
         LOG_INFO(log, "Time elapsed is %f minutes.\n", difftime(time(nullptr), start) / 60.0);
-        mbir_free_stage(S);
+        if (failed)
+            mbir_free_stage(S);
+        else
+            prev_stage.reset(S);
         if (failed) {
             LOG_ERR(log, "Reconstruction failed!\n");
             in.release_all();

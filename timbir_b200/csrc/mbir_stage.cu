@@ -12,8 +12,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/timbir_b200.h"
@@ -156,6 +159,9 @@ struct MbirStage {
     int *d_nh_nsel = nullptr, *d_nh_count = nullptr, *d_nh_pos = nullptr, *d_nh_nt = nullptr;
     float *d_nh_thresh = nullptr;
     std::vector<int> nh_nsel;  // host copy of d_nh_nsel
+    // rectangular-patch constraint windows of offset mode 3 (win.M = 0: none)
+    OffsetWindows win{};
+    std::vector<void *> win_bufs;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
     size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
@@ -179,6 +185,7 @@ struct MbirStage {
                         d_nh_nt, d_nh_thresh};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
+        for (void *b : win_bufs) dfree(b);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (tev0) cudaEventDestroy(tev0);
@@ -310,6 +317,10 @@ extern "C" int mbir_init_stage(MbirStage **out, const float *projections, const 
         CKS(cudaMemcpy(S->d_vnum, vnum.data(), vnum.size() * sizeof(int), cudaMemcpyHostToDevice));
         CKS(cudaMemcpy(S->d_fov, sg.frame_of_view.data(), sg.N_p * sizeof(int), cudaMemcpyHostToDevice));
     }
+    // error flags of the stage's kernels (super-voxel waits, column widths,
+    // the windowed offset solve)
+    CKS(dalloc(&S->d_err, 1));
+    CKS(cudaMemsetAsync(S->d_err, 0, sizeof(int), S->stream));
 #undef CKS
     // device-side views of the geometry and prior
     MbirGeom &g = S->g;
@@ -394,8 +405,12 @@ static int compute_detector_response(MbirStage *S)
 // detector response, initial object (zero unless given, [N_time][N_z][N_y][N_x]),
 // ring offsets (zero unless given, [N_r][N_t] as the reference stores them),
 // update-magnitude map (zero unless given) and the error sinogram.
-extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *offset,
-                                const float *magmap)
+// The stage prologue (ICD_BackProject, XT_ICD_update.c:1134-1159): detector
+// response, mask, start object, offsets and magnitude map, error sinogram.
+// fill_object / fill_mag enqueue the start object and magnitude map on the
+// stage's stream.
+template <class FO, class FM>
+static int icd_prepare_with(MbirStage *S, const float *offset, FO &&fill_object, FM &&fill_mag)
 {
     const ScanGeom &sg = S->sg;
     if (compute_detector_response(S)) return -1;
@@ -403,10 +418,7 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     // uploads on the stage's stream, ahead of its kernels (pageable sources
     // are staged before each call returns)
     CK(cudaMemcpyAsync(S->d_mask, S->mask.data(), S->mask.size(), cudaMemcpyHostToDevice, S->stream));
-    if (object)
-        CK(cudaMemcpyAsync(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
-    else
-        CK(cudaMemsetAsync(S->d_x, 0, S->nvox() * sizeof(float), S->stream));
+    if (fill_object()) return -1;
     if (offset) {
         std::vector<float> d((size_t)sg.N_t * sg.N_r);
         for (int r = 0; r < sg.N_r; r++)
@@ -415,10 +427,7 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     } else {
         CK(cudaMemsetAsync(S->d_d, 0, (size_t)sg.N_t * sg.N_r * sizeof(float), S->stream));
     }
-    if (magmap)
-        CK(cudaMemcpyAsync(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
-    else
-        CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
+    if (fill_mag()) return -1;
     CK(mbir_forward_rows(S->g, S->d_fov, S->d_x, S->d_y, S->d_d, S->d_e, 0, S->amax(), S->stream));
     S->launches++;
     CK(cudaStreamSynchronize(S->stream));
@@ -426,6 +435,64 @@ extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *
     S->have_cost = S->win_open = false;
     S->guard_checks = 0;
     return 0;
+}
+
+extern "C" int mbir_icd_prepare(MbirStage *S, const float *object, const float *offset,
+                                const float *magmap)
+{
+    return icd_prepare_with(
+        S, offset,
+        [&]() -> int {
+            if (object)
+                CK(cudaMemcpyAsync(S->d_x, object, S->nvox() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+            else
+                CK(cudaMemsetAsync(S->d_x, 0, S->nvox() * sizeof(float), S->stream));
+            return 0;
+        },
+        [&]() -> int {
+            if (magmap)
+                CK(cudaMemcpyAsync(S->d_mag, magmap, S->nmag() * sizeof(float), cudaMemcpyHostToDevice, S->stream));
+            else
+                CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
+            return 0;
+        });
+}
+
+// The prologue of the stage after `prev` in one multi-resolution run, with
+// the hand-off on the device (initObject, XT_ICD_update.c:540-651): the start
+// object is prev's object up-sampled x2 in x and y (initICD 2) or in x, y
+// and z (initICD 3), the magnitude map prev's up-sampled likewise when its
+// planes per frame allow (the same count, or half), else zero.  prev must
+// have finished its iterations.
+int mbir_icd_prepare_from(MbirStage *S, MbirStage *prev, int initICD, const float *offset, int *mag_carried)
+{
+    const int Nt = S->sg.N_time, cNz = prev->st.N_z, cNy = prev->st.N_y, cNx = prev->st.N_x;
+    if (2 * cNy != S->st.N_y || 2 * cNx != S->st.N_x || (initICD == 3 ? 2 * cNz : cNz) != S->st.N_z)
+        return fail("stage hand-off: the previous stage is not half this one's size");
+    const int pb = prev->nblk, nb = S->nblk;
+    const bool mag_ok = pb == nb || 2 * pb == nb;
+    if (mag_carried) *mag_carried = mag_ok ? 1 : 0;
+    return icd_prepare_with(
+        S, offset,
+        [&]() -> int {
+            for (int f = 0; f < Nt; f++)
+                CK(mbir_launch_upsample(prev->d_x + (size_t)f * prev->st.N_z * prev->nxy(),
+                                        S->d_x + (size_t)f * S->st.N_z * S->nxy(), cNz, cNy, cNx, initICD == 3,
+                                        S->stream));
+            S->launches += Nt;
+            return 0;
+        },
+        [&]() -> int {
+            if (!mag_ok) {
+                CK(cudaMemsetAsync(S->d_mag, 0, S->nmag() * sizeof(float), S->stream));
+                return 0;
+            }
+            for (int f = 0; f < Nt; f++)
+                CK(mbir_launch_upsample(prev->d_mag + (size_t)f * pb * prev->nxy(),
+                                        S->d_mag + (size_t)f * nb * S->nxy(), pb, cNy, cNx, pb != nb, S->stream));
+            S->launches += Nt;
+            return 0;
+        });
 }
 
 // ---------------------------------------------------------------------------
@@ -482,14 +549,153 @@ static int run_half(MbirStage *S, int j, int second, int nhicd, int iter, double
     return 0;
 }
 
-extern "C" int mbir_update_sinogram_offset(MbirStage *S)
+// The ring-offset update enqueued on the stage's stream (no host sync).
+static int offset_update_async(MbirStage *S)
 {
     CK(mbir_launch_offset(S->g, S->pr, S->dv, S->offset_type, S->d_num, S->d_den, S->d_partials,
-                          S->nparts, S->stream));
-    S->launches += 3;
-    CK(cudaStreamSynchronize(S->stream));
+                          S->nparts, S->stream, &S->win, S->d_err));
+    S->launches += S->offset_type == 3 && S->win.M > 0 ? 4 : 3;
     return 0;
 }
+
+extern "C" int mbir_update_sinogram_offset(MbirStage *S)
+{
+    if (offset_update_async(S)) return -1;
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    if (err & 16) return fail("ring-offset constraint system is not positive definite");
+    return 0;
+}
+
+// Constraint windows of offset mode 3 (gen_offset_constraint_windows,
+// XT_OffsetError.c:46-96): sides r_size = 2 N_r / round(sqrt(N_r)) and
+// t_size = 2 N_t / round(sqrt(N_t)), origins every half side, wrapping
+// around the detector, tent weights; a later assignment to an element of the
+// same window replaces an earlier one, as in the reference's loop.  Lists are
+// in the reference's element order (detector column major, row inner).
+extern "C" int mbir_set_offset_windows(MbirStage *S, int32_t on)
+{
+    CK(cudaStreamSynchronize(S->stream));
+    for (void *b : S->win_bufs) dfree(b);
+    S->win_bufs.clear();
+    S->win = OffsetWindows{};
+    if (!on) return 0;
+    if (!S->d_err) CK(dalloc(&S->d_err, 1));
+    const int Nr = S->sg.N_r, Nt = S->sg.N_t, nel = Nr * Nt;
+    const int rs = 2 * Nr / (int)(std::sqrt((double)Nr) + 0.5), ts = 2 * Nt / (int)(std::sqrt((double)Nt) + 0.5);
+    // per window: its elements (q = t N_r + r) in reference order and weights
+    std::vector<std::vector<std::pair<int, float>>> wins;
+    std::vector<float> val(nel, 0.0f);
+    std::vector<int> seen(nel, -1);
+    for (int i = 0; i <= Nr - rs / 2; i += rs / 2)
+        for (int j = 0; j <= Nt - ts / 2; j += ts / 2) {
+            const int m = (int)wins.size();
+            std::vector<int> touched;
+            for (int k = i; k < i + rs; k++)
+                for (int l = j; l < j + ts; l++) {
+                    double a = (k - i) < rs / 2 ? (k - i + 1) : rs - (k - i);
+                    a *= (l - j) < ts / 2 ? (l - j + 1) : ts - (l - j);
+                    const int q = (l % Nt) * Nr + k % Nr;
+                    if (seen[q] != m) {
+                        seen[q] = m;
+                        touched.push_back(q);
+                    }
+                    val[q] = (float)a;
+                }
+            std::sort(touched.begin(), touched.end(), [&](int a, int b) {
+                const int ra = a % Nr, rb = b % Nr;
+                return ra != rb ? ra < rb : a / Nr < b / Nr;
+            });
+            std::vector<std::pair<int, float>> w;
+            for (int q : touched) w.push_back({q, val[q]});
+            wins.push_back(std::move(w));
+        }
+    const int M = (int)wins.size();
+    if (M == 0) return 0;
+    // per element its windows; per overlapping pair the shared elements
+    std::vector<std::vector<std::pair<int, float>>> els(nel);
+    for (int m = 0; m < M; m++)
+        for (auto &p : wins[m]) els[p.first].push_back({m, p.second});
+    std::map<std::pair<int, int>, std::vector<int>> pairs;  // (i <= j) -> element list (reference order)
+    std::vector<int> order(nel);
+    for (int q = 0; q < nel; q++) order[q] = q;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ra = a % Nr, rb = b % Nr;
+        return ra != rb ? ra < rb : a / Nr < b / Nr;
+    });
+    for (int q : order)
+        for (size_t u = 0; u < els[q].size(); u++)
+            for (size_t v = u; v < els[q].size(); v++) {
+                int a = els[q][u].first, b = els[q][v].first;
+                if (a > b) std::swap(a, b);
+                pairs[{a, b}].push_back(q);
+            }
+    std::vector<int> win_off(M + 1, 0), win_el, pair_off(1, 0), pair_i, pair_j, pair_el, el_off(nel + 1, 0), el_m;
+    std::vector<float> win_a, pair_ai, pair_aj, el_a;
+    for (int m = 0; m < M; m++) {
+        for (auto &p : wins[m]) {
+            win_el.push_back(p.first);
+            win_a.push_back(p.second);
+        }
+        win_off[m + 1] = (int)win_el.size();
+    }
+    auto weight = [&](int m, int q) {
+        for (auto &p : els[q])
+            if (p.first == m) return p.second;
+        return 0.0f;
+    };
+    for (auto &kv : pairs) {
+        pair_i.push_back(kv.first.first);
+        pair_j.push_back(kv.first.second);
+        for (int q : kv.second) {
+            pair_el.push_back(q);
+            pair_ai.push_back(weight(kv.first.first, q));
+            pair_aj.push_back(weight(kv.first.second, q));
+        }
+        pair_off.push_back((int)pair_el.size());
+    }
+    for (int q = 0; q < nel; q++) {
+        for (auto &p : els[q]) {
+            el_m.push_back(p.first);
+            el_a.push_back(p.second);
+        }
+        el_off[q + 1] = (int)el_m.size();
+    }
+    auto up = [&](auto &vec, auto **dst) -> int {
+        using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+        T *d = nullptr;
+        CK(dalloc(&d, std::max<size_t>(vec.size(), 1)));
+        S->win_bufs.push_back(d);
+        if (!vec.empty())
+            CK(cudaMemcpyAsync(d, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice, S->stream));
+        *dst = d;
+        return 0;
+    };
+    OffsetWindows W{};
+    W.M = M;
+    W.nel = nel;
+    W.npairs = (int)pair_i.size();
+    if (up(win_off, &W.win_off) || up(win_el, &W.win_el) || up(win_a, &W.win_a) || up(pair_off, &W.pair_off) ||
+        up(pair_i, &W.pair_i) || up(pair_j, &W.pair_j) || up(pair_el, &W.pair_el) || up(pair_ai, &W.pair_ai) ||
+        up(pair_aj, &W.pair_aj) || up(el_off, &W.el_off) || up(el_m, &W.el_m) || up(el_a, &W.el_a))
+        return -1;
+    double *D = nullptr, *y = nullptr, *x = nullptr;
+    CK(dalloc(&D, (size_t)M * M));
+    CK(dalloc(&y, (size_t)M));
+    CK(dalloc(&x, (size_t)nel));
+    S->win_bufs.push_back(D);
+    S->win_bufs.push_back(y);
+    S->win_bufs.push_back(x);
+    W.D = D;
+    W.y = y;
+    W.x = x;
+    CK(cudaStreamSynchronize(S->stream));
+    S->win = W;
+    return 0;
+}
+
+extern "C" int mbir_get_offset_windows(MbirStage *S) { return S->win.M; }
 
 extern "C" int mbir_update_variance_parameter(MbirStage *S)
 {
@@ -566,7 +772,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     sp.W = (int)floor((side - 1) * sqrt(2.0) * m + 2 * m + 1e-9) + 3;
     sp.amax = 2 * (int)ceil(m) + 1;
     sp.eq = (1 + sp.amax + 3) / 4;
-    sp.ring = 4;
+    sp.ring = kSvRing;
     sp.ahalf = S->acol_half ? 1 : 0;
     sp.max_views = S->max_views();
     sp.max_nz = nz;
@@ -622,6 +828,148 @@ static void sv_build_list(const MbirStage *S, const std::vector<int> &ids, std::
     buf[meta[2] + ids.size()] = (int)deps.size();
     meta[3] = buf.size();
     buf.insert(buf.end(), deps.begin(), deps.end());
+}
+
+// The super-voxels of schedule 1 (tasks, colour phases, size ranks,
+// conflicts) and the full-sweep launch lists of every phase rotation, into
+// S and buf.  They depend only on the geometry (grid, z-groups, side, mask),
+// so they are kept in a small process-wide cache: stages of the same
+// geometry set up one after another (a scan series, the stages of repeated
+// reconstructions) reuse them instead of rebuilding them on the host.
+namespace {
+struct SvScheduleCache {
+    std::vector<SvTask> all;
+    std::vector<int> phase, rank, buf;
+    std::vector<std::vector<int>> nbr;
+    std::vector<std::array<size_t, 4>> rot;
+    int nphase = 1;
+};
+std::mutex g_sched_mu;
+std::vector<std::pair<std::string, std::shared_ptr<const SvScheduleCache>>> g_sched_cache;  // most recent last
+}  // namespace
+
+static void sv_schedule_build(MbirStage *S, const SvParams &sp, int gz, std::vector<int> &buf)
+{
+    const int Nz = S->st.N_z;
+    // super-voxels, coloured by SV x / y parity, z-group parity, frame parity
+    const int side_ = sp.S, N_x = S->st.N_x, N_y = S->st.N_y, N_time = S->sg.N_time;
+    const int ntx = (N_x + side_ - 1) / side_, nty = (N_y + side_ - 1) / side_;
+    std::vector<int> phase_of(16, -1), cell((size_t)N_time * S->nzg * nty * ntx, -1);
+    auto cell_of = [&](int i, int zg, int ty, int tx) { return (((size_t)i * S->nzg + zg) * nty + ty) * ntx + tx; };
+    int nphase = 0;
+    S->sv_all.clear();
+    S->sv_all_phase.clear();
+    for (int i = 0; i < N_time; i++)
+        for (int zg = 0; zg < S->nzg; zg++)
+            for (int ty = 0; ty < nty; ty++)
+                for (int tx = 0; tx < ntx; tx++) {
+                    const int k0 = tx * side_, j0 = ty * side_;
+                    int lines = 0;
+                    for (int y = j0; y < std::min(N_y, j0 + side_); y++)
+                        for (int x = k0; x < std::min(N_x, k0 + side_); x++)
+                            if (S->mask[(size_t)y * N_x + x]) lines++;
+                    if (!lines) continue;
+                    const int colour = (tx & 1) | ((ty & 1) << 1) | ((S->nzg > 1 ? (zg & 1) : 0) << 2) |
+                                       ((N_time > 1 ? (i & 1) : 0) << 3);
+                    if (phase_of[colour] < 0) phase_of[colour] = nphase++;
+                    SvTask t{};
+                    t.frame = i;
+                    t.k0 = k0;
+                    t.j0 = j0;
+                    t.z0 = zg * gz;
+                    t.nz = std::min(gz, Nz - t.z0);
+                    t.nlines = lines;
+                    t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
+                    t.plane = i * S->nzg + zg;
+                    cell[cell_of(i, zg, ty, tx)] = (int)S->sv_all.size();
+                    S->sv_all.push_back(t);
+                    S->sv_all_phase.push_back(phase_of[colour]);
+                }
+    S->sv_nphase = nphase;
+    // size rank within (phase, frame, z-group)
+    {
+        std::vector<int> ids(S->sv_all.size());
+        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
+        auto key = [&](int a) {
+            return ((long long)S->sv_all_phase[a] * N_time + S->sv_all[a].frame) * S->nzg + S->sv_all[a].z0 / gz;
+        };
+        std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+            if (key(a) != key(b)) return key(a) < key(b);
+            return S->sv_all[a].nlines > S->sv_all[b].nlines;
+        });
+        S->sv_rank.assign(ids.size(), 0);
+        for (size_t q = 1; q < ids.size(); q++)
+            S->sv_rank[ids[q]] = key(ids[q]) == key(ids[q - 1]) ? S->sv_rank[ids[q - 1]] + 1 : 0;
+    }
+    // conflicts: super-voxels sharing a prior neighbourhood -- x-y-z neighbours
+    // in the same frame, the same block in adjacent frames
+    S->sv_nbr.assign(S->sv_all.size(), {});
+    for (int i = 0; i < N_time; i++)
+        for (int zg = 0; zg < S->nzg; zg++)
+            for (int ty = 0; ty < nty; ty++)
+                for (int tx = 0; tx < ntx; tx++) {
+                    const int id = cell[cell_of(i, zg, ty, tx)];
+                    if (id < 0) continue;
+                    for (int dz = -1; dz <= 1; dz++)
+                        for (int dy = -1; dy <= 1; dy++)
+                            for (int dx = -1; dx <= 1; dx++) {
+                                const int z2 = zg + dz, y2 = ty + dy, x2 = tx + dx;
+                                if ((dz | dy | dx) == 0 || z2 < 0 || z2 >= S->nzg || y2 < 0 || y2 >= nty || x2 < 0 ||
+                                    x2 >= ntx)
+                                    continue;
+                                const int nb = cell[cell_of(i, z2, y2, x2)];
+                                if (nb >= 0) S->sv_nbr[id].push_back(nb);
+                            }
+                    for (int di = -1; di <= 1; di += 2)
+                        if (i + di >= 0 && i + di < N_time) {
+                            const int nb = cell[cell_of(i + di, zg, ty, tx)];
+                            if (nb >= 0) S->sv_nbr[id].push_back(nb);
+                        }
+                }
+    // full-sweep launch lists, one per phase rotation
+    S->sv_rot.assign(nphase, {});
+    for (int r = 0; r < nphase; r++) {
+        std::vector<int> ids(S->sv_all.size());
+        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
+        sv_sort(S, ids, r);
+        sv_build_list(S, ids, buf, S->sv_rot[r]);
+    }
+}
+
+static void sv_schedule(MbirStage *S, const SvParams &sp, int gz, std::vector<int> &buf)
+{
+    std::string key(reinterpret_cast<const char *>(S->mask.data()), S->mask.size());
+    const int dims[7] = {S->st.N_x, S->st.N_y, S->st.N_z, S->sg.N_time, sp.S, gz, S->nzg};
+    key.append(reinterpret_cast<const char *>(dims), sizeof(dims));
+    std::shared_ptr<const SvScheduleCache> hit;
+    {
+        std::lock_guard<std::mutex> lock(g_sched_mu);
+        for (auto &e : g_sched_cache)
+            if (e.first == key) hit = e.second;
+    }
+    if (!hit) {
+        sv_schedule_build(S, sp, gz, buf);
+        auto c = std::make_shared<SvScheduleCache>();
+        c->all = S->sv_all;
+        c->phase = S->sv_all_phase;
+        c->rank = S->sv_rank;
+        c->nbr = S->sv_nbr;
+        c->rot = S->sv_rot;
+        c->buf = buf;
+        c->nphase = S->sv_nphase;
+        std::lock_guard<std::mutex> lock(g_sched_mu);
+        g_sched_cache.emplace_back(std::move(key), std::move(c));
+        if (g_sched_cache.size() > 8) g_sched_cache.erase(g_sched_cache.begin());
+        return;
+    }
+    S->sv_all = hit->all;
+    S->sv_all_phase = hit->phase;
+    S->sv_rank = hit->rank;
+    S->sv_nbr = hit->nbr;
+    S->sv_rot = hit->rot;
+    S->sv_nphase = hit->nphase;
+    buf = hit->buf;
+    for (SvTask &t : S->sv_all) t.mag = S->d_mag + (size_t)t.plane * S->nxy();
 }
 
 // dynamic shared memory per CTA: the 227 KB opt-in limit less the kernels' static
@@ -757,94 +1105,12 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
         S->nr.assign((size_t)S->sg.N_time * S->nblk, 0);
         S->nn.assign((size_t)S->sg.N_time * S->nblk, 0);
     }
-    // super-voxels, coloured by SV x / y parity, z-group parity, frame parity
     if (S->mask.empty()) object_mask(S->sg, S->st, S->mask);
-    const int side_ = sp.S, N_x = S->st.N_x, N_y = S->st.N_y, N_time = S->sg.N_time;
-    const int ntx = (N_x + side_ - 1) / side_, nty = (N_y + side_ - 1) / side_;
-    std::vector<int> phase_of(16, -1), cell((size_t)N_time * S->nzg * nty * ntx, -1);
-    auto cell_of = [&](int i, int zg, int ty, int tx) { return (((size_t)i * S->nzg + zg) * nty + ty) * ntx + tx; };
-    int nphase = 0;
-    S->sv_all.clear();
-    S->sv_all_phase.clear();
-    for (int i = 0; i < N_time; i++)
-        for (int zg = 0; zg < S->nzg; zg++)
-            for (int ty = 0; ty < nty; ty++)
-                for (int tx = 0; tx < ntx; tx++) {
-                    const int k0 = tx * side_, j0 = ty * side_;
-                    int lines = 0;
-                    for (int y = j0; y < std::min(N_y, j0 + side_); y++)
-                        for (int x = k0; x < std::min(N_x, k0 + side_); x++)
-                            if (S->mask[(size_t)y * N_x + x]) lines++;
-                    if (!lines) continue;
-                    const int colour = (tx & 1) | ((ty & 1) << 1) | ((S->nzg > 1 ? (zg & 1) : 0) << 2) |
-                                       ((N_time > 1 ? (i & 1) : 0) << 3);
-                    if (phase_of[colour] < 0) phase_of[colour] = nphase++;
-                    SvTask t{};
-                    t.frame = i;
-                    t.k0 = k0;
-                    t.j0 = j0;
-                    t.z0 = zg * gz;
-                    t.nz = std::min(gz, Nz - t.z0);
-                    t.nlines = lines;
-                    t.mag = S->d_mag + ((size_t)i * S->nzg + zg) * S->nxy();
-                    t.plane = i * S->nzg + zg;
-                    cell[cell_of(i, zg, ty, tx)] = (int)S->sv_all.size();
-                    S->sv_all.push_back(t);
-                    S->sv_all_phase.push_back(phase_of[colour]);
-                }
-    S->sv_nphase = nphase;
-    // size rank within (phase, frame, z-group)
-    {
-        std::vector<int> ids(S->sv_all.size());
-        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
-        auto key = [&](int a) {
-            return ((long long)S->sv_all_phase[a] * N_time + S->sv_all[a].frame) * S->nzg + S->sv_all[a].z0 / gz;
-        };
-        std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
-            if (key(a) != key(b)) return key(a) < key(b);
-            return S->sv_all[a].nlines > S->sv_all[b].nlines;
-        });
-        S->sv_rank.assign(ids.size(), 0);
-        for (size_t q = 1; q < ids.size(); q++)
-            S->sv_rank[ids[q]] = key(ids[q]) == key(ids[q - 1]) ? S->sv_rank[ids[q - 1]] + 1 : 0;
-    }
-    // conflicts: super-voxels sharing a prior neighbourhood -- x-y-z neighbours
-    // in the same frame, the same block in adjacent frames
-    S->sv_nbr.assign(S->sv_all.size(), {});
-    for (int i = 0; i < N_time; i++)
-        for (int zg = 0; zg < S->nzg; zg++)
-            for (int ty = 0; ty < nty; ty++)
-                for (int tx = 0; tx < ntx; tx++) {
-                    const int id = cell[cell_of(i, zg, ty, tx)];
-                    if (id < 0) continue;
-                    for (int dz = -1; dz <= 1; dz++)
-                        for (int dy = -1; dy <= 1; dy++)
-                            for (int dx = -1; dx <= 1; dx++) {
-                                const int z2 = zg + dz, y2 = ty + dy, x2 = tx + dx;
-                                if ((dz | dy | dx) == 0 || z2 < 0 || z2 >= S->nzg || y2 < 0 || y2 >= nty || x2 < 0 ||
-                                    x2 >= ntx)
-                                    continue;
-                                const int nb = cell[cell_of(i, z2, y2, x2)];
-                                if (nb >= 0) S->sv_nbr[id].push_back(nb);
-                            }
-                    for (int di = -1; di <= 1; di += 2)
-                        if (i + di >= 0 && i + di < N_time) {
-                            const int nb = cell[cell_of(i + di, zg, ty, tx)];
-                            if (nb >= 0) S->sv_nbr[id].push_back(nb);
-                        }
-                }
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&S->sm_count, cudaDevAttrMultiProcessorCount, dev));
-    // full-sweep launch lists, one per phase rotation
     std::vector<int> buf;
-    S->sv_rot.assign(nphase, {});
-    for (int r = 0; r < nphase; r++) {
-        std::vector<int> ids(S->sv_all.size());
-        for (size_t q = 0; q < ids.size(); q++) ids[q] = (int)q;
-        sv_sort(S, ids, r);
-        sv_build_list(S, ids, buf, S->sv_rot[r]);
-    }
+    sv_schedule(S, sp, gz, buf);
     dfree(S->d_sv_all);
     dfree(S->d_sv_done);
     dfree(S->d_sv_lists);
@@ -867,7 +1133,7 @@ extern "C" int mbir_set_schedule(MbirStage *S, int32_t schedule, int32_t sv_side
     // NHICD selection buffers; n_sel per plane = nh_fraction of the in-mask
     // lines (XT_NHICD.c:171: the lines updated / NHICD iterations)
     {
-        const int planes = N_time * S->nzg;
+        const int planes = S->sg.N_time * S->nzg;
         dfree(S->d_nh_sel);
         dfree(S->d_nh_nsel);
         dfree(S->d_nh_count);
@@ -1003,6 +1269,22 @@ extern "C" int mbir_nhicd_select(const float *mag, int32_t planes, int32_t N_y, 
     return 0;
 }
 
+extern "C" int mbir_upsample(const float *in, float *out, int32_t n_z, int32_t n_y, int32_t n_x, int32_t z_too)
+{
+    if (n_z < 1 || n_y < 2 || n_x < 2 || (z_too && n_z < 2)) return fail("up-sampling needs n_y, n_x >= 2 (and n_z >= 2 with z)");
+    const size_t ni = (size_t)n_z * n_y * n_x, no = (z_too ? 8 : 4) * ni;
+    float *d_in = nullptr, *d_out = nullptr;
+    cudaError_t e = dalloc(&d_in, ni);
+    if (e == cudaSuccess) e = dalloc(&d_out, no);
+    if (e == cudaSuccess) e = cudaMemcpy(d_in, in, ni * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = mbir_launch_upsample(d_in, d_out, n_z, n_y, n_x, z_too != 0, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_out, no * sizeof(float), cudaMemcpyDeviceToHost);
+    dfree(d_in);
+    dfree(d_out);
+    if (e != cudaSuccess) return fail("up-sampling: %s", cudaGetErrorString(e));
+    return 0;
+}
+
 extern "C" int mbir_set_sv_guard(MbirStage *S, int32_t on)
 {
     S->guard = on != 0;
@@ -1076,13 +1358,14 @@ extern "C" int mbir_get_schedule(MbirStage *S, int32_t *schedule, int32_t *sv_si
 // the positions in d_nh_pos, their count in d_nh_nt, and only the lines
 // selected in d_nh_sel are visited.
 static int sv_launch(MbirStage *S, const int *list, const std::array<size_t, 4> &meta, int iter, uint32_t seed,
-                     int qslot, SvTaskOut *acc, bool subset = false)
+                     int qslot, SvTaskOut *acc, bool subset = false, int first = 0, int count = -1, int epoch = 0)
 {
-    const int n = (int)meta[0];
+    const int n = count >= 0 ? count : (int)meta[0];
     if (n <= 0) return 0;
     const int ctas = std::min(n, S->sv_ctas > 0 ? std::min(S->sv_ctas, S->sv_fit) : S->sv_grid);
     SvACache ac{S->d_acol};
-    SvLaunch L{S->d_sv_all, list + meta[1], list + meta[2], list + meta[3], n, S->d_sv_done, ++S->sv_epoch};
+    SvLaunch L{S->d_sv_all, list + meta[1] + first, list + meta[2] + first, list + meta[3], n, S->d_sv_done,
+               epoch > 0 ? epoch : ++S->sv_epoch};
     if (subset) {
         L.pos = S->d_nh_pos;
         L.ntasks_dev = S->d_nh_nt;
@@ -1155,15 +1438,16 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
         S->acol_built = true;
         S->launches++;
     }
+    // queue counters: slot 0 the sweep, slot 1 the NHICD pass
     CK(cudaMemsetAsync(S->d_queue, 0, 2 * sizeof(int), S->stream));
     CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
     const int rot = iter % P;
+    // the sweep: one launch over every super-voxel, then the ring offsets
+    const uint32_t sweep_seed = (uint32_t)(S->rng.next() * 4294967295.0);
     CK(cudaEventRecord(S->sv_ev[0], S->stream));
-    if (sv_launch(S, S->d_sv_lists, S->sv_rot[rot], iter, (uint32_t)(S->rng.next() * 4294967295.0), 0,
-                  S->d_sv_out))
-        return -1;
+    if (sv_launch(S, S->d_sv_lists, S->sv_rot[rot], iter, sweep_seed, 0, S->d_sv_out)) return -1;
     CK(cudaEventRecord(S->sv_ev[1], S->stream));
-    if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+    if (S->upd_offset > 1 && offset_update_async(S)) return -1;
     bool nh = false;
     if (iter > 1 && S->nh_fraction > 0) {
         // non-homogeneous pass over the lines the sweep changed most
@@ -1175,7 +1459,7 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
                       S->d_sv_out + 1, true))
             return -1;
         CK(cudaEventRecord(S->sv_ev[3], S->stream));
-        if (S->upd_offset > 1 && mbir_update_sinogram_offset(S)) return -1;
+        if (S->upd_offset > 1 && offset_update_async(S)) return -1;
     }
     if (S->upd_var == 1 && mbir_update_variance_parameter(S)) return -1;
     SvTaskOut acc[2];
@@ -1193,6 +1477,7 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
     if (err & 2) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
     if (err & 4) return fail("super-voxel dependency wait timed out");
+    if (err & 16) return fail("ring-offset constraint system is not positive definite");
     // Stability guard.  Super-voxels in flight together over-correct the
     // rays they share; the in-flight cap bounds that for the geometries it
     // was measured on.  Every step of an iteration (the voxel updates with
@@ -1678,6 +1963,7 @@ extern "C" int mbir_batch_iterate(MbirBatch *B, int32_t max_iters, int32_t check
     if (err & 1) return fail("super-voxel band overflow (A-matrix column outside the staged band)");
     if (err & 2) return fail("A-matrix column wider than 2 mult_xy + 1 detector columns");
     if (err & 4) return fail("super-voxel dependency wait timed out");
+    if (err & 16) return fail("ring-offset constraint system is not positive definite");
     if (err & 8) return fail("super-voxel in-flight wait timed out");
     // the stages' own counters
     std::vector<SvBatchState> st(B->n);

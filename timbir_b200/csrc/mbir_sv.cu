@@ -157,18 +157,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-// waits until at most n (0..6) of this thread's commit groups are pending
-__device__ __forceinline__ void cp_async_wait_upto(int n)
+// waits until at most N of this thread's commit groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_upto()
 {
-    switch (n) {
-    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
-    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
-    default: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
-    }
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Exact A-matrix column of the voxel line centred at (x, y) for one view
@@ -554,7 +547,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         const int NpS = sp.max_views;  // smem stride (views)
         const int S2 = S + 2;
         const size_t rowstride = (size_t)W * NpS;  // band entries per detector row
-        const int R = sp.ring, D = R - 2;  // ring slots; column prefetch distance (lines)
+        // ring slots (the host always plans 4) and column prefetch distance (lines)
+        constexpr int R = kSvRing, D = kSvRing - 2;
         const double inv_dr = 1.0 / g.delta_r, inv_off = 1.0 / g.OffsetR;
         const float inv_off_f = (float)inv_off;
         const float alpha = (float)pr.alpha, hT = (float)pr.hT, hTd = (float)(pr.hT * pr.hdelta);
@@ -887,12 +881,18 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
 
         if (AC) {
             for (int q = 0; q < D; q++) fetch(q, q);
-            cp_async_wait_upto(D - 1);
+            cp_async_wait_upto<D - 1>();
         } else if (nl > 0) {
             acol(0, 0, 0, av_all);
         }
         __syncthreads();
 
+        // the neighbour of this lane exists in z (spatial) or time (temporal)
+        // for every voxel of the super-voxel; in x and y too when the block
+        // keeps one voxel away from the image edges
+        const bool nfix = spatial ? (zg + ndz >= 0 && zg + ndz < g.N_z)
+                                  : temporal && i + (lane == 26 ? -1 : 1) >= 0 && i + (lane == 26 ? -1 : 1) < g.N_time;
+        const bool interior = k0 >= 1 && j0 >= 1 && k0 + kx < g.N_x && j0 + ky < g.N_y;
         // full resolution: this lane's views (vh * 32 + lane + 32 vsplit u, u
         // < VU) as a mask of those the frame has, and their band origins
         constexpr int VRL = VU > 0 ? VU : 1;
@@ -916,15 +916,15 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 const float V = *xc;
                 // ---- prior neighbourhood ----
                 float nbv = 0.0f;
-                bool valid = false;
+                bool valid = nfix;
                 if (spatial) {
-                    const int zz = zg + ndz, yy = row + ndy, xx = col + ndx;
-                    valid = zz >= 0 && zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x;
+                    if (!interior) {
+                        const int yy = row + ndy, xx = col + ndx;
+                        valid = valid && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x;
+                    }
                     if (valid) nbv = xc[nboff];
-                } else if (temporal) {
-                    const int ti = i + (lane == 26 ? -1 : 1);
-                    valid = ti >= 0 && ti < g.N_time;
-                    if (valid) nbv = tb[((lane - 26) * nz + zl) * S * S + ly * S + lx];
+                } else if (valid) {
+                    nbv = tb[((lane - 26) * nz + zl) * S * S + ly * S + lx];
                 }
                 const unsigned pos = __ballot_sync(0xffffffffu, valid && nbv > 0.0f);
                 if (V == 0.0f && iter > 1 && pos == 0u) {
@@ -1090,7 +1090,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             }
             if (AC) {
                 fetch(step + D, sl + D >= R ? sl + D - R : sl + D);
-                cp_async_wait_upto(D - 1);
+                cp_async_wait_upto<D - 1>();
             } else if (step + 1 < nl) {
                 const int sn1 = sl + 1 == R ? 0 : sl + 1;
                 if (nprod > 0) {

@@ -6,6 +6,9 @@
 
 #include "mbir_internal.h"
 
+// A-column ring slots of the super-voxel kernel
+constexpr int kSvRing = 4;
+
 struct SvParams {
     int S;          // super-voxel side (voxel lines)
     int W;          // band width (detector columns per view)
@@ -16,7 +19,7 @@ struct SvParams {
     int max_rows;   // detector rows per CTA: max_nz * m_z
     int vsplit;     // warps per slice (1, 2 or 4; > 1 needs max_nz <= 15)
     int prod_warps; // warps computing the next line's A-matrix column (0 with a column cache)
-    int ring;       // A-column ring slots, 4..8 (the cache is read ring - 2 lines ahead)
+    int ring;       // A-column ring slots: kSvRing (the cache is read ring - 2 lines ahead)
     int ahalf;      // the column cache holds FP16 values (8-byte entries; full resolution)
     size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
 };
