@@ -355,14 +355,37 @@ C3_PRIOR = dict(sig_s=0.002, sig_t=1.0, c_s=1.0, c_t=1.0, convg_thresh=1.0, remo
 C3_DATA = "synthetic (seeded random-ellipsoid phantoms, exact line integrals, Poisson counts)"
 
 
-def c3_sample_workload(specs):
-    """The CPU baseline's bounded sample: the smallest problem of the batch."""
-    k = min(range(len(specs)), key=lambda q: specs[q]["side"] ** 2 * specs[q]["slices"] * specs[q]["views"])
+def c3_problem_workload(specs, k):
     sp = specs[k]
     prior = dict(C3_PRIOR, convg_thresh=0.0)
-    w = Workload("c3-sample", f"problem {k} of the batch: {sp['side']}x{sp['side']}x{sp['slices']}, "
-                 f"{sp['views']} views, I0={sp['I0']:.0f}", sp["side"], sp["slices"], sp["views"], 1, prior, C3_DATA)
-    return k, w
+    return Workload("c3-sample", f"problem {k} of the batch: {sp['side']}x{sp['side']}x{sp['slices']}, "
+                    f"{sp['views']} views, I0={sp['I0']:.0f}", sp["side"], sp["slices"], sp["views"], 1, prior, C3_DATA)
+
+
+def c3_cpu_baseline(specs, weights, threads):
+    """The reference's CPU rate on the batch: for each problem size, one ICD
+    iteration (after one warm-up) of that size's problem with the fewest
+    slices, run from zero; the per-size rates are combined as one sequential
+    pass over every problem of the batch, each weighted by `weights` (its
+    voxel updates per iteration), i.e. total updates / sum(updates / rate of
+    its size).  Returns (rate, per-size dict, kind, cores, seconds)."""
+    by_side = {}
+    for k, sp in enumerate(specs):
+        if sp["side"] not in by_side or sp["slices"] < specs[by_side[sp["side"]]]["slices"]:
+            by_side[sp["side"]] = k
+    per, kind, cores, secs_all = {}, None, None, 0.0
+    for side, k in sorted(by_side.items()):
+        sp = specs[k]
+        w = c3_problem_workload(specs, k)
+        scan = synth.ellipsoid_scan(sp["side"], sp["slices"], sp["views"], I0=sp["I0"], seed=sp["seed"])
+        z = np.zeros((1, w.rows // 2, w.n_xy // 2, w.n_xy // 2), np.float32)
+        zf = np.zeros((1, w.rows, w.n_xy, w.n_xy), np.float32)
+        v, kind, cores, n, secs = cpu_measure(w, scan, z, zf, 1, 1, threads)
+        per[str(side)] = {"value": v, "problem": k, "slices": sp["slices"], "views": sp["views"], "seconds": round(secs, 2)}
+        secs_all += secs
+    total = float(sum(weights))
+    t = sum(float(weights[k]) / per[str(sp["side"])]["value"] for k, sp in enumerate(specs))
+    return total / t, per, kind, cores, secs_all
 
 
 def c3_build(specs, scans, tuned=None, autotune=True):
@@ -526,12 +549,12 @@ def c3_arm(args, rank, world, local_rank):
     if ttc:
         line["time_to_converge"] = ttc
     if not args.no_cpu:
-        k, w = c3_sample_workload(specs)
-        z = np.zeros((1, w.rows // 2, w.n_xy // 2, w.n_xy // 2), np.float32)
-        zf = np.zeros((1, w.rows, w.n_xy, w.n_xy), np.float32)
-        v, kind, cores, n, secs = cpu_measure(w, scans[k], z, zf, 1, 1, os.cpu_count() or 1)
+        v, per, kind, cores, secs = c3_cpu_baseline(specs, [int(d) for d in du], os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
-                                "sample": f"{w.desc}: {n} ICD iteration(s) after 1 warm-up, {secs:.1f} s"}
+                                "sample": "per problem size, one ICD iteration after one warm-up of its problem with "
+                                          "the fewest slices (from zero), %.1f s in all; combined as one sequential pass "
+                                          "over the batch weighted by each problem's updates" % secs,
+                                "per_size": per}
     print(json.dumps(line), flush=True)
 
 
@@ -1052,13 +1075,23 @@ def reference_arm(args, rank):
               flush=True)
         return
     if args.config == "c3":
-        # the batch's smallest problem, one problem at a time as the reference runs
+        # per-size samples combined over the batch (the reference runs one
+        # problem per process; weights: the problems' voxel counts)
         specs = synth.batch_problem_specs(64, 0)
-        k, w = c3_sample_workload(specs)
-        sp = specs[k]
-        scan = synth.ellipsoid_scan(sp["side"], sp["slices"], sp["views"], I0=sp["I0"], seed=sp["seed"])
-        coarse = np.zeros((1, w.rows // 2, w.n_xy // 2, w.n_xy // 2), np.float32)
-        fine = np.zeros((1, w.rows, w.n_xy, w.n_xy), np.float32)
+        threads = os.cpu_count() or 1
+        v, per, kind, cores, secs = c3_cpu_baseline(specs, [sp["side"] ** 2 * sp["slices"] for sp in specs], threads)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "voxel-updates/s", "n_gpus": 0, "steps": 1,
+            "warmup": 1, "ms_per_step": 1e3 * secs / max(len(per), 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 scalars)", "data": C3_DATA,
+            "config": {"workload": C3_DESC, "threads": threads,
+                       "sample": "one ICD iteration after one warm-up per problem size (its problem with the fewest "
+                                 "slices), combined over the 64 problems weighted by voxels (bounded: one step)"},
+            "cpu_baseline": {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind, "per_size": per,
+                             "sample": "per-size samples, %.1f s" % secs},
+            "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
     else:
         w = WORKLOADS[args.config]
         scan = w.scan(0)

@@ -87,9 +87,16 @@ struct OffsetWindows {
 };
 // Ring-offset update of the given type; with type 3 and windows (M > 0) the
 // constrained solve (err |= 16 if its system is not positive definite).
+// With `chunks` (2 mbir_offset_chunks(g) N_t N_r doubles of scratch) the view
+// sums are spread over view chunks of kOffsetViewChunk and the sinogram is
+// updated by one thread per entry; without, one thread per detector element
+// sums all views (the scratch is num, den and the partials only).
+constexpr int kOffsetViewChunk = 16;
+int mbir_offset_chunks(const MbirGeom &g);
 cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
                                double *num, double *den, double *partials, int nparts,
-                               cudaStream_t s, const OffsetWindows *win = nullptr, int *err = nullptr);
+                               cudaStream_t s, const OffsetWindows *win = nullptr, int *err = nullptr,
+                               double *chunks = nullptr);
 cudaError_t mbir_launch_variance(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
                                  double var_est, double *partials, int nparts, double *result,
                                  cudaStream_t s);

@@ -89,7 +89,10 @@ __device__ __forceinline__ double qggmrf_deriv(double d, double sQ, double sQP, 
 __device__ __forceinline__ double qggmrf_value(double d, double sQ, double sQP, double c)
 {
     const double ad = fabs(d);
-    return (__dmul_rn(ad, ad) / sQ) / (c + pow(ad, kQ - kP) / sQP);
+    // |d|^(q - p) as exp((q - p) log |d|) in FP64 (within a few ulp of pow;
+    // 0 for d = 0)
+    const double pw = ad > 0.0 ? exp((kQ - kP) * log(ad)) : 0.0;
+    return (__dmul_rn(ad, ad) / sQ) / (c + pw / sQP);
 }
 
 template <typename T>
@@ -437,6 +440,108 @@ __global__ void k_offset_apply(MbirGeom g, MbirDev dv, int type, const double *n
             const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
             dv.e[o] = (float)__dsub_rn((double)dv.e[o], sh);
         }
+    }
+}
+
+// The same update spread over the views: k_offset_chunks sums views
+// [c VC, (c + 1) VC) of each detector element into partial num / den
+// [c][element]; k_offset_combine adds the chunks in chunk order (a fixed
+// order: deterministic) and forms the block partials of the zero-mean gamma;
+// k_offset_shift turns num / den (and gamma, or the constrained solution)
+// into each element's shift and new offset; k_offset_apply_e applies the
+// shift to every sinogram entry.
+__global__ void k_offset_chunks(MbirGeom g, MbirPrior pr, MbirDev dv, int type, int vc, double *__restrict__ pnum,
+                                double *__restrict__ pden)
+{
+    const int nel = g.N_t * g.N_r;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    if (q >= nel) return;
+    const int t = q / g.N_r, r = q - t * g.N_r;
+    const float dq = dv.d[q];
+    double nm = 0.0, dn = 0.0;
+    const int p1 = min(g.N_p, (c + 1) * vc);
+    for (int p = c * vc; p < p1; p++) {
+        const size_t o = ((size_t)t * g.N_p + p) * g.N_r + r;
+        const float ef = dv.e[o], wf = dv.w[o];
+        const double sw = sqrt((double)wf);
+        const double tmp = __dmul_rn(__dmul_rn(pr.hT, pr.hdelta), sw);
+        const bool sel = fabs(__dmul_rn((double)ef, sw)) < pr.hT;
+        if (type == 3) {
+            if (sel) {
+                dn += (double)wf;
+                nm += (double)__fmul_rn(__fadd_rn(ef, dq), wf);
+            } else {
+                const double om = __ddiv_rn(tmp, fabs((double)ef));
+                dn += om;
+                nm += __ddiv_rn(__dmul_rn((double)__fadd_rn(ef, dq), tmp), fabs((double)ef));
+            }
+        } else {
+            if (sel) {
+                nm += (double)__fmul_rn(ef, wf);
+                dn += (double)wf;
+            } else {
+                const double sg = (double)((ef > 0) - (ef < 0));
+                nm += __dmul_rn(tmp, sg);
+                dn += __ddiv_rn(tmp, fabs((double)ef));
+            }
+        }
+    }
+    pnum[(size_t)c * nel + q] = nm;
+    pden[(size_t)c * nel + q] = dn;
+}
+
+__global__ void k_offset_combine(MbirGeom g, MbirDev dv, int nchunks, const double *__restrict__ pnum,
+                                 const double *__restrict__ pden, double *__restrict__ num, double *__restrict__ den,
+                                 double *partials, int nparts)
+{
+    double v[2] = {0.0, 0.0};
+    const size_t nel = (size_t)g.N_t * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nel; q += stride) {
+        double nm = 0.0, dn = 0.0;
+        for (int c = 0; c < nchunks; c++) {
+            nm += pnum[(size_t)c * nel + q];
+            dn += pden[(size_t)c * nel + q];
+        }
+        num[q] = nm;
+        den[q] = dn;
+        v[0] += (double)dv.d[q] + nm / dn;
+        v[1] += 1.0 / dn;
+    }
+    block_partials<2>(v, partials, nparts);
+}
+
+// per element: the shift of e (types 1, 2: (num - gamma) / den, e -= shift;
+// type 3: d_old - x, e += it), into num[q]; the new offset into d
+__global__ void k_offset_shift(MbirGeom g, MbirDev dv, int type, double *num, const double *den, const double *sums,
+                               const double *xw)
+{
+    const size_t nel = (size_t)g.N_t * g.N_r;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nel) return;
+    if (type == 3) {
+        const float xn = xw ? (float)xw[q] : (float)((num[q] - 0.0) / den[q]);
+        num[q] = (double)__fsub_rn(dv.d[q], xn);
+        dv.d[q] = xn;
+    } else {
+        const double gamma = type == 2 ? sums[0] / sums[1] : 0.0;
+        const double sh = __ddiv_rn(num[q] - gamma, den[q]);
+        dv.d[q] = (float)__dadd_rn((double)dv.d[q], sh);
+        num[q] = sh;
+    }
+}
+
+__global__ void k_offset_apply_e(MbirGeom g, MbirDev dv, int type, const double *__restrict__ shift)
+{
+    const size_t ns = (size_t)g.N_t * g.N_p * g.N_r;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < ns; o += stride) {
+        const size_t r = o % g.N_r, t = o / ((size_t)g.N_p * g.N_r);
+        const double sh = shift[t * g.N_r + r];
+        if (type == 3)
+            dv.e[o] = __fadd_rn(dv.e[o], (float)sh);
+        else
+            dv.e[o] = (float)__dsub_rn((double)dv.e[o], sh);
     }
 }
 
@@ -797,15 +902,33 @@ cudaError_t mbir_launch_icd_ref(const MbirGeom &g, const MbirPrior &pr, const Mb
 cudaError_t mbir_launch_cost(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv,
                              double *partials, int nparts, double *result, cudaStream_t s)
 {
-    k_cost<<<nparts, 256, 0, s>>>(g, pr, dv, partials, nparts);
+    k_cost<<<nparts, 1024, 0, s>>>(g, pr, dv, partials, nparts);
     k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, result);
     return cudaGetLastError();
 }
 
+int mbir_offset_chunks(const MbirGeom &g) { return (g.N_p + kOffsetViewChunk - 1) / kOffsetViewChunk; }
+
 cudaError_t mbir_launch_offset(const MbirGeom &g, const MbirPrior &pr, const MbirDev &dv, int type,
                                double *num, double *den, double *partials, int nparts,
-                               cudaStream_t s, const OffsetWindows *win, int *err)
+                               cudaStream_t s, const OffsetWindows *win, int *err, double *chunks)
 {
+    if (chunks) {
+        const int nel = g.N_t * g.N_r, nc = mbir_offset_chunks(g);
+        double *pnum = chunks, *pden = chunks + (size_t)nc * nel;
+        k_offset_chunks<<<dim3((nel + 127) / 128, nc), 128, 0, s>>>(g, pr, dv, type, kOffsetViewChunk, pnum, pden);
+        k_offset_combine<<<nparts, 128, 0, s>>>(g, dv, nc, pnum, pden, num, den, partials, nparts);
+        double *sums = partials + 2 * (size_t)nparts;
+        k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, sums);
+        const double *xw = nullptr;
+        if (type == 3 && win && win->M > 0) {
+            k_offset_windows<<<1, 1024, 0, s>>>(*win, num, den, win->x, err);
+            xw = win->x;
+        }
+        k_offset_shift<<<(nel + 127) / 128, 128, 0, s>>>(g, dv, type, num, den, sums, xw);
+        k_offset_apply_e<<<1184, 256, 0, s>>>(g, dv, type, num);
+        return cudaGetLastError();
+    }
     k_offset_terms<<<nparts, 128, 0, s>>>(g, pr, dv, type, num, den, partials, nparts);
     double *sums = partials + 2 * (size_t)nparts;
     k_sum_partials<<<1, 1024, 0, s>>>(partials, nparts, 2, sums);

@@ -92,7 +92,7 @@ struct MbirStage {
     float *d_e = nullptr, *d_w = nullptr, *d_y = nullptr, *d_d = nullptr, *d_x = nullptr,
           *d_mag = nullptr, *d_filt = nullptr, *d_H = nullptr;
     double *d_cos = nullptr, *d_sin = nullptr, *d_num = nullptr, *d_den = nullptr,
-           *d_partials = nullptr, *d_result = nullptr;
+           *d_partials = nullptr, *d_result = nullptr, *d_ochunk = nullptr;
     int *d_vidx = nullptr, *d_vnum = nullptr, *d_fov = nullptr, *d_xr = nullptr, *d_yr = nullptr,
         *d_xn = nullptr, *d_yn = nullptr;
     uint8_t *d_mask = nullptr;
@@ -178,7 +178,7 @@ struct MbirStage {
     ~MbirStage()
     {
         void *bufs[] = {d_e,   d_w,   d_y,    d_d,   d_x,   d_mag, d_filt,     d_H,      d_cos,
-                        d_sin, d_num, d_den,  d_partials, d_result, d_vidx, d_vnum, d_fov,
+                        d_sin, d_num, d_den,  d_partials, d_result, d_ochunk, d_vidx, d_vnum, d_fov,
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
                         d_sv_all, d_sv_done, d_sv_lists, d_sv_out, d_scratch, d_err, d_queue, d_acol,
                         d_snap_x, d_snap_e, d_snap_w, d_snap_d, d_nh_sel, d_nh_nsel, d_nh_count, d_nh_pos,
@@ -267,6 +267,11 @@ extern "C" int mbir_init_stage(MbirStage **out, const float *projections, const 
     CKS(dalloc(&S->d_num, (size_t)sg.N_t * sg.N_r));
     CKS(dalloc(&S->d_den, (size_t)sg.N_t * sg.N_r));
     CKS(dalloc(&S->d_partials, (size_t)4 * S->nparts));
+    {
+        MbirGeom gg{};
+        gg.N_p = sg.N_p;
+        CKS(dalloc(&S->d_ochunk, (size_t)2 * mbir_offset_chunks(gg) * sg.N_t * sg.N_r));
+    }
     CKS(dalloc(&S->d_result, 8));
     const int mv = S->max_views();
     CKS(dalloc(&S->d_vidx, (size_t)recon_num * mv));
@@ -553,8 +558,8 @@ static int run_half(MbirStage *S, int j, int second, int nhicd, int iter, double
 static int offset_update_async(MbirStage *S)
 {
     CK(mbir_launch_offset(S->g, S->pr, S->dv, S->offset_type, S->d_num, S->d_den, S->d_partials,
-                          S->nparts, S->stream, &S->win, S->d_err));
-    S->launches += S->offset_type == 3 && S->win.M > 0 ? 4 : 3;
+                          S->nparts, S->stream, &S->win, S->d_err, S->d_ochunk));
+    S->launches += S->offset_type == 3 && S->win.M > 0 ? 6 : 5;
     return 0;
 }
 
