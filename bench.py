@@ -215,16 +215,54 @@ def mean_amatrix_count(stage, scan):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clocks and clock-event (throttle) reasons while the timed region
+    runs: NVML polled every 2 ms from a thread (the timed region of a small
+    workload lasts a few milliseconds, shorter than nvidia-smi's sampling
+    period), nvidia-smi at 200 ms where NVML cannot be loaded.  Read-only
+    queries; no setting of the GPU is touched."""
 
     Q = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    # NVML clock-event reason bits (nvml.h): HW slowdown 0x8, HW thermal 0x40,
+    # SW thermal 0x20, SW power cap 0x4
+    BITS = [0x8, 0x40, 0x20, 0x4]
 
     def __init__(self, index):
-        self.index, self.rows, self.proc = index, [], None
+        self.index, self.rows, self.proc, self.nvml, self.stop = index, [], None, None, None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:  # the CUDA device's own PCI address (CUDA_VISIBLE_DEVICES renumbers devices)
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            self.nvml, h = self._nvml_handle()
+            nv = self.nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+
+            def poll():
+                while True:
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    self.rows.append((sm, r))
+                    if self.stop.wait(0.002):
+                        return
+
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         if shutil.which("nvidia-smi"):
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -238,6 +276,9 @@ class ClockSampler:
             self.rows.append([v.strip() for v in line.split(",")])
 
     def __exit__(self, *a):
+        if self.stop is not None:
+            self.stop.set()
+            self.t.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             self.proc.wait(timeout=5)
@@ -245,12 +286,16 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        if self.nvml is not None:
+            sm = [r[0] for r in self.rows]
+            reasons = sorted({n for _, r in self.rows for n, b in zip(self.NAMES, self.BITS) if r & b})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML, 2 ms polling"}
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        reasons = sorted({self.NAMES[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": float(self.rows[0][2]) if self.rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": reasons}
+                "reasons": reasons, "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # --------------------------------------------------------------------- CPU --
@@ -474,8 +519,12 @@ def c3_arm(args, rank, world, local_rank):
         batch = timbir_b200.Batch(stages)
         left = batch.iterate(200, check_every=1)
         bst = batch.stats()
+        un = [k for k in range(len(specs)) if not bst["converged"][k]]
         ttc = {"value": batch.info()["ms"] / 1e3, "unit": "s", "iterations_max": int(bst["iterations"].max()),
                "iterations_mean": float(bst["iterations"].mean()), "unconverged": int(left),
+               "unconverged_problems": [{"problem": k, "side": specs[k]["side"], "slices": specs[k]["slices"],
+                                         "views": specs[k]["views"], "I0": round(specs[k]["I0"]),
+                                         "last_pct": float(bst["percent"][k])} for k in un],
                "target": "every problem's convergence ratio below convg_thresh = 1 % (XT_ICD_update.c:1066-1103)",
                "start": "zero", "timed": "graph replays of the batched iterations (device events)"}
         batch.close()
@@ -613,7 +662,7 @@ def icd_from(scan, start, cstar=None, max_iters=600, flat=1e-10, prior=None, blo
     return it, ms, c, x
 
 
-def c4_arm(args, rank, world, local_rank, four_d=False, n_train=24, train_iters=100, steps=1500):
+def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
     """Learned warm start: training pairs from the plain method, the network
     trained on them, then ICD from its output against ICD from FBP on held-out
     scans.  four_d: the 4-D workload (16 frames, 64 interlaced views per
@@ -635,16 +684,17 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=24, train_iters=
     kw = dict(prior=prior, blocks=blocks)
     t0 = time.perf_counter()
     fbps, tgts = [], []
+    target_iters = []
     for k in range(n_train):
         sc = scan_of(k)
         st = c4_stage(sc, prior, blocks)
         f = st.fbp()
-        st.prepare(f)
-        for it in range(1, train_iters + 1):
-            st.iterate(it)
-        fbps.extend(list(f))
-        tgts.extend(list(st.object()))
         st.close()
+        # target: the converged MAP image (ICD from the FBP until the cost is flat)
+        n_it, _, _, x_map = icd_from(sc, f, max_iters=400, **kw)
+        target_iters.append(n_it)
+        fbps.extend(list(f))
+        tgts.extend(list(x_map))
     data_s = time.perf_counter() - t0
     X = torch.from_numpy(np.stack(fbps)).cuda()
     T = torch.from_numpy(np.stack(tgts)).cuda()
@@ -699,7 +749,9 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=24, train_iters=
         "unit": "x (plain time / warm time, start images included)", "n_gpus": world, "higher_is_better": True,
         "config": {"workload": (W4D.desc + "; learned warm start (network trained on 4-D scans of other seeds)")
                    if four_d else C4_DESC,
-                   "training_volumes": pairs, "pair_target": f"{train_iters} plain ICD iterations from FBP",
+                   "training_volumes": pairs,
+                   "pair_target": "converged MAP image (plain ICD from FBP until two successive costs agree to 1e-10; "
+                                  "mean %.0f iterations)" % float(np.mean(target_iters)),
                    "train_steps": steps, "train_batch": "4 patches 16x64x64", "params": int(net.n)},
         "training": {"ms": round(train_ms, 1), "ms_per_step": round(train_ms / steps, 3),
                      "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
