@@ -515,10 +515,11 @@ def c3_arm(args, rank, world, local_rank):
     if not args.no_ttm:
         for st in stages:
             st.set_convergence_threshold(C3_PRIOR["convg_thresh"])
-            st.prepare()
+            st.prepare(st.fbp() if args.c3_start == "fbp" else None)
         batch = timbir_b200.Batch(stages)
         left = batch.iterate(200, check_every=1)
         bst = batch.stats()
+        adj = [st.schedule_info()["stability_adjustments"] for st in stages]
         un = [k for k in range(len(specs)) if not bst["converged"][k]]
         ttc = {"value": batch.info()["ms"] / 1e3, "unit": "s", "iterations_max": int(bst["iterations"].max()),
                "iterations_mean": float(bst["iterations"].mean()), "unconverged": int(left),
@@ -526,7 +527,9 @@ def c3_arm(args, rank, world, local_rank):
                                          "views": specs[k]["views"], "I0": round(specs[k]["I0"]),
                                          "last_pct": float(bst["percent"][k])} for k in un],
                "target": "every problem's convergence ratio below convg_thresh = 1 % (XT_ICD_update.c:1066-1103)",
-               "start": "zero", "timed": "graph replays of the batched iterations (device events)"}
+               "start": "filtered backprojection (this library's FBP kernels)" if args.c3_start == "fbp" else "zero",
+               "stability_adjustments": {"total": int(sum(adj)), "problems": int(sum(1 for a in adj if a))},
+               "timed": "graph replays of the batched iterations and the per-problem cost guard (device events)"}
         batch.close()
     for st in stages:
         st.close()
@@ -731,7 +734,19 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
         n_warm, ms_warm, c_warm, x_warm = icd_from(sc, ws, cstar, acache=acache_warm, **kw)
         rng_ = float(x_star.max() - x_star.min())
         rm = lambda a: float(np.sqrt(np.mean((a - x_star) ** 2))) / rng_  # noqa: E731
+        # how far ICD's iteration count moves with the start: the FBP's error
+        # halved everywhere, and the FBP's low frequencies under the MAP
+        # image's high frequencies (Gaussian low-pass, sigma 2 slices x 8 x 8)
+        from scipy import ndimage
+        lp = lambda a: ndimage.gaussian_filter(a.astype(np.float64), sigma=(0, 2, 8, 8)).astype(np.float32)  # noqa
+        sens = {}
+        for key, s0 in (("fbp_error_halved", 0.5 * (fbp + x_star)),
+                        ("map_high_frequencies_fbp_low", lp(fbp) + (x_star - lp(x_star)))):
+            s0 = (s0 * mask).astype(np.float32)
+            n_s, _, _, _ = icd_from(sc, s0, cstar, **kw)
+            sens[key] = {"iterations": n_s, "start_rmse_over_range": rm(s0)}
         results.append({
+            "start_sensitivity": sens,
             "phantom": name, "cstar": cstar, "cstar_iterations": n_star,
             "plain": {"iterations": n_plain, "icd_ms": round(ms_plain, 2), "start_ms": round(fbp_ms, 2),
                       "total_ms": round(ms_plain + fbp_ms, 2), "a_matrix": "fp32"},
@@ -794,7 +809,19 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    # the forward pass alone (its convolutions are forward ones only)
+    fwd_flops = sum(2.0 * B * (D >> lv) * (H >> lv) * (Wd >> lv) * 27 * ci * co for ci, co, lv in warm.LAYERS)
+    for _ in range(args.warmup):
+        net.forward(x)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        net.forward(x)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / args.steps
     net.close()
+    umma = os.environ.get("TIMBIR_NET_CONV", "") != "mma"
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -804,7 +831,12 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     print(json.dumps({
         "metric": "warm-start network training steps/s", "value": 1e3 / ms, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "dtype": "bf16 operands, fp32 accumulation (mma.sync m16n8k16)", "data": "synthetic (random patches)",
+        "dtype": ("bf16 operands, fp32 accumulation (convolutions and input gradients: tcgen05.mma kind::f16, "
+                  "accumulators in tensor memory; weight gradients: mma.sync m16n8k16)") if umma else
+                 "bf16 operands, fp32 accumulation (mma.sync m16n8k16)", "data": "synthetic (random patches)",
+        "forward": {"ms": fwd_ms, "tflops": fwd_flops / (fwd_ms / 1e3) / 1e12,
+                    "note": "inference pass alone (15 convolutions, pooling, up-sampling; includes the "
+                            "host-synchronised output copy of mbir_net_forward)"},
         "config": {"workload": f"one training step on {B} patches {D}x{H}x{Wd} (forward, loss, backward, Adam)",
                    "params": sum(27 * ci * co + co for ci, co, _ in warm.LAYERS)},
         "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
@@ -1174,6 +1206,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
+    ap.add_argument("--c3-start", default="fbp", choices=["fbp", "zero"],
+                    help="start of the batched problems' convergence run (c3)")
     ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net", "kernels"],
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
                          "c3: 64 independent 3-D problems batched; c4: learned warm start (3-D); 4d-warm: learned warm "

@@ -193,6 +193,34 @@ int mbir_get_offset_windows(MbirStage *stage);
 /* update_variance_parameter (XT_ICD_update.c:720-751). */
 int mbir_update_variance_parameter(MbirStage *stage);
 
+/* ---- z-slab sharding (the reference's MPI decomposition, XT_MPI.c:47-122)
+ * A volume split into `ranks` z-slabs, one per process (or GPU): the stage
+ * holds slab `rank`, built from that slab's detector rows, as each MPI rank
+ * of the reference holds its slab.  The slab's first and last slices take
+ * the neighbouring slabs' boundary slices as prior neighbours (halo slices
+ * 0 and N_z + 1 of the reference's object, XT_VoxUpdate.c:126-131), and the
+ * cost counts the pairs with the slab above (XT_ICD_update.c:207-210).
+ * `allreduce(values, count, ctx)` sums `count` doubles over the ranks in
+ * place and returns 0 (nonzero: failure); the stage calls it where the
+ * reference reduces over MPI_COMM_WORLD: the cost's data and prior sums
+ * (XT_ICD_update.c:301-317), the variance's sum (:738-739), and the
+ * convergence sums (:1079-1081).  Every rank must make the same calls in the
+ * same order, so every rank runs the same stage settings.  Ring-offset mode 3
+ * with constraint windows (which reduces its window system over ranks) is
+ * refused for a sharded stage; modes 1 and 2 are per slab, as in the
+ * reference.  ranks = 1 restores the whole-volume behaviour. */
+typedef int (*MbirAllreduceFn)(double *values, int32_t count, void *ctx);
+int mbir_set_z_slab(MbirStage *stage, int32_t rank, int32_t ranks, MbirAllreduceFn allreduce, void *ctx);
+/* This slab's boundary slices: slice 0 (to the slab below) into lo and
+ * slice N_z - 1 (to the slab above) into hi, each [N_time][N_y][N_x] in
+ * DEVICE memory; returns when they are written.  Either may be NULL. */
+int mbir_get_slab_faces(MbirStage *stage, float *lo, float *hi);
+/* The halo slices from DEVICE memory [N_time][N_y][N_x]: lo = the slab
+ * below's slice N_z - 1, hi = the slab above's slice 0 (NULL: unchanged).
+ * MPI_Send_Recv_Z_Slices' exchange (XT_MPI.c:47-82) is the caller's: the
+ * faces of each slab go to its neighbours' halos between iterations. */
+int mbir_set_slab_halo(MbirStage *stage, const float *lo, const float *hi);
+
 /* State read-back.  dims: N_p, N_r, N_t, N_x, N_y, N_z, N_time,
  * num_z_blocks, z_overlap_num. */
 int mbir_stage_dims(MbirStage *stage, int32_t *dims);

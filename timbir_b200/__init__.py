@@ -29,6 +29,8 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _VP = C.c_void_p
 
 _lib = None
+# int (*)(double *values, int32_t count, void *ctx): the sum over z-slab ranks
+_ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int32, C.c_void_p)
 
 
 def load_library() -> C.CDLL:
@@ -56,6 +58,9 @@ def load_library() -> C.CDLL:
     lib.mbir_set_offset_windows.argtypes = [_VP, i32]
     lib.mbir_get_offset_windows.argtypes = [_VP]
     lib.mbir_update_variance_parameter.argtypes = [_VP]
+    lib.mbir_set_z_slab.argtypes = [_VP, i32, i32, _ALLREDUCE_FN, _VP]
+    lib.mbir_get_slab_faces.argtypes = [_VP, _VP, _VP]
+    lib.mbir_set_slab_halo.argtypes = [_VP, _VP, _VP]
     lib.mbir_stage_dims.argtypes = [_VP, _i32p]
     for n in ("mbir_get_object", "mbir_set_object", "mbir_get_errorsino", "mbir_get_weight", "mbir_get_offset",
               "mbir_get_magmap", "mbir_get_hr"):
@@ -166,6 +171,45 @@ class Stage:
 
     SCHEDULE_REFERENCE = 0
     SCHEDULE_SUPERVOXEL = 1
+
+    # --- z-slab sharding (XT_MPI.c:47-122) -------------------------------
+    def set_z_slab(self, rank: int, ranks: int, allreduce=None):
+        """Make this stage z-slab `rank` of `ranks` (its scan holds that slab's
+        detector rows).  allreduce(values) sums a float64 numpy array over the
+        ranks in place; the stage calls it where the reference reduces over
+        its MPI ranks (cost, variance, convergence)."""
+        if allreduce is None:
+            cb = _ALLREDUCE_FN()
+        else:
+            def cb_py(ptr, n, _ctx):
+                try:
+                    v = np.ctypeslib.as_array(ptr, shape=(n,))
+                    allreduce(v)
+                    return 0
+                except Exception:  # reported to the stage as a failed reduction
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+            cb = _ALLREDUCE_FN(cb_py)
+        self._allreduce_cb = cb  # kept alive while the stage may call it
+        _check(self.lib.mbir_set_z_slab(self.h, rank, ranks, cb, None))
+
+    def slab_faces(self):
+        """This slab's slice 0 and slice N_z - 1 of every frame, as CUDA
+        tensors [N_time][N_y][N_x] (the faces its neighbours take as halos)."""
+        import torch
+        lo = torch.empty((self.N_time, self.N_y, self.N_x), dtype=torch.float32, device="cuda")
+        hi = torch.empty_like(lo)
+        _check(self.lib.mbir_get_slab_faces(self.h, lo.data_ptr(), hi.data_ptr()))
+        return lo, hi
+
+    def set_slab_halo(self, lo=None, hi=None):
+        """Halo slices from CUDA tensors [N_time][N_y][N_x]: lo = the slab
+        below's top slice, hi = the slab above's bottom slice (None: kept)."""
+        lo = None if lo is None else lo.contiguous()
+        hi = None if hi is None else hi.contiguous()
+        _check(self.lib.mbir_set_slab_halo(self.h, None if lo is None else lo.data_ptr(),
+                                           None if hi is None else hi.data_ptr()))
 
     def set_schedule(self, schedule: int, sv_side: int = 0, warps_per_slice: int = 0, acache: int = -1):
         """0: the reference's checkerboard z-block schedule; 1: super-voxel

@@ -46,7 +46,31 @@ struct MbirPrior {
 struct MbirDev {
     float *e, *w, *d, *x, *mag;
     const uint8_t *mask;   // [N_y][N_x]
+    // z-slab of a volume sharded over ranks (XT_MPI.c:47-82): the slab
+    // below's top slice (halo_lo) and the slab above's bottom slice
+    // (halo_hi) of every frame, [2][N_time][N_y][N_x]; they are neighbours
+    // of this slab's first and last slices, read but never updated
+    const float *halo;
+    int halo_lo, halo_hi;
 };
+
+#ifdef __CUDACC__
+// Does slice zz (-1 .. N_z) exist as a neighbour: the slab's own slices, and
+// the halo slices when the neighbouring slab exists (XT_VoxUpdate.c:126-131).
+__device__ __forceinline__ bool slab_has_z(const MbirGeom &g, const MbirDev &dv, int zz)
+{
+    return zz >= (dv.halo_lo ? -1 : 0) && zz < g.N_z + (dv.halo_hi ? 1 : 0);
+}
+
+// Plane [N_y][N_x] of slice zz of frame i (zz = -1 and N_z: the halo slices).
+__device__ __forceinline__ const float *slab_plane(const MbirGeom &g, const MbirDev &dv, int i, int zz)
+{
+    const size_t plane = (size_t)g.N_y * g.N_x;
+    if (zz < 0) return dv.halo + (size_t)i * plane;
+    if (zz >= g.N_z) return dv.halo + ((size_t)g.N_time + i) * plane;
+    return dv.x + ((size_t)i * g.N_z + zz) * plane;
+}
+#endif
 
 // One task of a reference-schedule half-sweep: a (frame, z-block) pair and a
 // range of one of its line lists.

@@ -190,9 +190,9 @@ __global__ void __launch_bounds__(NT) k_icd_ref(MbirGeom g, MbirPrior pr, MbirDe
                 if (lane < 27 && lane != 13) {
                     const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
                     const int zz = s + dz, yy = j + dy, xx = k + dx;
-                    if (zz >= 0 && zz < N_z && yy >= 0 && yy < N_y && xx >= 0 && xx < N_x) {
+                    if (slab_has_z(g, dv, zz) && yy >= 0 && yy < N_y && xx >= 0 && xx < N_x) {
                         valid = true;
-                        nb = xf[(size_t)zz * plane + (size_t)yy * N_x + xx];
+                        nb = slab_plane(g, dv, i, zz)[(size_t)yy * N_x + xx];
                     }
                     if (valid) {
                         const double d0 = V - nb;
@@ -349,8 +349,10 @@ __global__ void k_cost(MbirGeom g, MbirPrior pr, MbirDev dv, double *partials, i
         const float xv = dv.x[o];
         for (int n = 0; n < 13; n++) {
             const int zz = s + off[n][0], yy = j + off[n][1], xx = k + off[n][2];
-            if (zz < g.N_z && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x) {
-                const float nbv = dv.x[((size_t)i * g.N_z + zz) * plane + (size_t)yy * g.N_x + xx];
+            if (zz < g.N_z + (dv.halo_hi ? 1 : 0) && yy >= 0 && yy < g.N_y && xx >= 0 && xx < g.N_x) {
+                // the pair with the slab above's bottom slice is this slab's
+                // (computeCost, XT_ICD_update.c:207-210)
+                const float nbv = slab_plane(g, dv, i, zz)[(size_t)yy * g.N_x + xx];
                 const double dl = (double)__fsub_rn(xv, nbv);
                 const int fi = 9 * (off[n][0] + 1) + 3 * (off[n][1] + 1) + (off[n][2] + 1);
                 v[1] += pr.SF[fi] * qggmrf_value(dl, pr.sSQ, pr.sSQP, pr.c_s);

@@ -69,6 +69,9 @@ static cudaError_t dalloc(T **p, size_t n)
     return cudaStreamSynchronize(0);
 }
 
+struct MbirStage;
+static int slab_sum(MbirStage *S, double *v, int n);
+
 static void dfree(void *p)
 {
     if (p) cudaFreeAsync(p, 0);
@@ -162,6 +165,13 @@ struct MbirStage {
     // rectangular-patch constraint windows of offset mode 3 (win.M = 0: none)
     OffsetWindows win{};
     std::vector<void *> win_bufs;
+    // z-slab `slab_rank` of `slab_count` (one slab per rank; 1: the whole
+    // volume): the halo slices [2][N_time][N_y][N_x] and the sum over ranks
+    // that takes the place of the reference's MPI reductions
+    float *d_halo = nullptr;
+    int slab_rank = 0, slab_count = 1;
+    MbirAllreduceFn allreduce = nullptr;
+    void *allreduce_ctx = nullptr;
 
     size_t nsino() const { return (size_t)sg.N_t * sg.N_p * sg.N_r; }
     size_t nvox() const { return (size_t)sg.N_time * st.N_z * st.N_y * st.N_x; }
@@ -182,7 +192,7 @@ struct MbirStage {
                         d_xr,  d_yr,  d_xn,   d_yn,  d_mask, d_tasks, d_tout, d_acache,
                         d_sv_all, d_sv_done, d_sv_lists, d_sv_out, d_scratch, d_err, d_queue, d_acol,
                         d_snap_x, d_snap_e, d_snap_w, d_snap_d, d_nh_sel, d_nh_nsel, d_nh_count, d_nh_pos,
-                        d_nh_nt, d_nh_thresh};
+                        d_nh_nt, d_nh_thresh, d_halo};
         if (stream) cudaStreamSynchronize(stream);
         for (void *b : bufs) dfree(b);
         for (void *b : win_bufs) dfree(b);
@@ -581,6 +591,8 @@ extern "C" int mbir_update_sinogram_offset(MbirStage *S)
 // in the reference's element order (detector column major, row inner).
 extern "C" int mbir_set_offset_windows(MbirStage *S, int32_t on)
 {
+    if (on && S->slab_count > 1)
+        return fail("ring-offset constraint windows reduce over the ranks; not supported on a sharded stage");
     CK(cudaStreamSynchronize(S->stream));
     for (void *b : S->win_bufs) dfree(b);
     S->win_bufs.clear();
@@ -702,6 +714,63 @@ extern "C" int mbir_set_offset_windows(MbirStage *S, int32_t on)
 
 extern "C" int mbir_get_offset_windows(MbirStage *S) { return S->win.M; }
 
+// ---------------------------------------------------------------------------
+// z-slab sharding (XT_MPI.c:47-122)
+// ---------------------------------------------------------------------------
+// Sum of n doubles over the slabs, in place; the identity for a whole volume.
+static int slab_sum(MbirStage *S, double *v, int n)
+{
+    if (S->slab_count <= 1) return 0;
+    if (!S->allreduce || S->allreduce(v, n, S->allreduce_ctx) != 0)
+        return fail("z-slab reduction over the ranks failed");
+    return 0;
+}
+
+extern "C" int mbir_set_z_slab(MbirStage *S, int32_t rank, int32_t ranks, MbirAllreduceFn allreduce, void *ctx)
+{
+    if (ranks < 1 || rank < 0 || rank >= ranks) return fail("z-slab %d of %d", rank, ranks);
+    if (ranks > 1 && !allreduce) return fail("a sharded stage needs a reduction over its ranks");
+    if (ranks > 1 && S->win.M > 0)
+        return fail("ring-offset constraint windows reduce over the ranks; not supported on a sharded stage");
+    const size_t n = 2 * (size_t)S->sg.N_time * S->nxy();
+    if (ranks > 1 && !S->d_halo) {
+        CK(dalloc(&S->d_halo, n));
+        CK(cudaMemsetAsync(S->d_halo, 0, n * sizeof(float), S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+    }
+    S->slab_rank = rank;
+    S->slab_count = ranks;
+    S->allreduce = ranks > 1 ? allreduce : nullptr;
+    S->allreduce_ctx = ranks > 1 ? ctx : nullptr;
+    S->dv.halo = ranks > 1 ? S->d_halo : nullptr;
+    S->dv.halo_lo = ranks > 1 && rank > 0;
+    S->dv.halo_hi = ranks > 1 && rank < ranks - 1;
+    S->have_cost = false;  // the guard's cost is the whole volume's from here
+    return 0;
+}
+
+extern "C" int mbir_get_slab_faces(MbirStage *S, float *lo, float *hi)
+{
+    const size_t plane = S->nxy() * sizeof(float), frame = (size_t)S->st.N_z * plane;
+    if (lo)
+        CK(cudaMemcpy2DAsync(lo, plane, S->d_x, frame, plane, S->sg.N_time, cudaMemcpyDeviceToDevice, S->stream));
+    if (hi)
+        CK(cudaMemcpy2DAsync(hi, plane, S->d_x + (size_t)(S->st.N_z - 1) * S->nxy(), frame, plane, S->sg.N_time,
+                             cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
+extern "C" int mbir_set_slab_halo(MbirStage *S, const float *lo, const float *hi)
+{
+    if (!S->d_halo) return fail("not a sharded stage (mbir_set_z_slab with ranks > 1)");
+    const size_t n = (size_t)S->sg.N_time * S->nxy();
+    if (lo) CK(cudaMemcpyAsync(S->d_halo, lo, n * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    if (hi) CK(cudaMemcpyAsync(S->d_halo + n, hi, n * sizeof(float), cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return 0;
+}
+
 extern "C" int mbir_update_variance_parameter(MbirStage *S)
 {
     CK(mbir_launch_variance(S->g, S->pr, S->dv, S->var_est, S->d_partials, S->nparts, S->d_result,
@@ -710,7 +779,9 @@ extern "C" int mbir_update_variance_parameter(MbirStage *S)
     double sum = 0;
     CK(cudaMemcpyAsync(&sum, S->d_result, sizeof(double), cudaMemcpyDeviceToHost, S->stream));
     CK(cudaStreamSynchronize(S->stream));
-    S->var_est = sum / ((double)1 * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t);
+    // summed over the slabs (XT_ICD_update.c:738-739)
+    if (slab_sum(S, &sum, 1)) return -1;
+    S->var_est = sum / ((double)S->slab_count * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t);
     CK(mbir_launch_variance_apply(S->g, S->dv, S->var_est, S->stream));
     CK(cudaStreamSynchronize(S->stream));
     return 0;
@@ -1494,8 +1565,11 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     // (divergence from a poor start shows at once), later ones eight (one
     // FP64 cost evaluation per eight iterations).  mbir_set_sv_guard turns
     // it off.
-    const double ax = acc[0].sum_abs_x;
-    const double pct = ax > 0 ? 100.0 * S->K * acc[0].sum_abs_dx / ax : 0.0;
+    // summed over the slabs (XT_ICD_update.c:1079-1081)
+    double sums[2] = {acc[0].sum_abs_dx, acc[0].sum_abs_x};
+    if (slab_sum(S, sums, 2)) return -1;
+    const double ax = sums[1];
+    const double pct = ax > 0 ? 100.0 * S->K * sums[0] / ax : 0.0;
     if (adjustable && S->win_open && ++S->win_iters >= (S->guard_checks < 4 ? 1 : 8)) {
         double c = 0;
         if (mbir_compute_cost(S, &c, nullptr, nullptr)) return -1;
@@ -1561,7 +1635,9 @@ extern "C" int mbir_update_voxels_time_slices(MbirStage *S, int32_t iter, int32_
     for (int pl = 0; pl < S->sg.N_time * S->nblk; pl++)
         for (int q = 0; q < S->nr[pl]; q++)
             avg += mag[(size_t)pl * nxy + (size_t)ys[(size_t)pl * nxy + q] * S->st.N_x + xs[(size_t)pl * nxy + q]];
-    S->last_pct = 100 * avg / vox;
+    double sums[2] = {avg, vox};
+    if (slab_sum(S, sums, 2)) return -1;
+    S->last_pct = 100 * sums[0] / sums[1];
     *converged = S->last_pct < S->stop_thresh ? 1 : 0;
     return 0;
 }
@@ -1574,8 +1650,10 @@ extern "C" int mbir_compute_cost(MbirStage *S, double *total, double *forward, d
     double r[2];
     CK(cudaMemcpyAsync(r, S->d_result, sizeof(r), cudaMemcpyDeviceToHost, S->stream));
     CK(cudaStreamSynchronize(S->stream));
+    // data and prior terms summed over the slabs (XT_ICD_update.c:301-317)
+    if (slab_sum(S, r, 2)) return -1;
     const double data = r[0] / 2.0;
-    const double fw = data + (double)1 * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t *
+    const double fw = data + (double)S->slab_count * (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t *
                                  log(S->var_est) / 2;
     if (forward) *forward = fw;
     if (prior) *prior = r[1];
@@ -1759,12 +1837,28 @@ struct MbirBatch {
     double ms = 0;
     long long replays = 0;
     std::vector<long long> seen;  // updates already added to each stage's count
+    // stability guard per problem, as the single stage's (sv_iterate): the
+    // problem's state at the start of its current window of iterations and
+    // the MAP cost there; a cost that rose restores that state and halves
+    // the problem's super-voxels in flight
+    struct Guard {
+        float *x = nullptr, *e = nullptr;
+        double cost = 0;
+        int win = 0, checks = 0, last_iters = 0, cap = 1;
+        long long upd = 0, zs = 0;
+    };
+    bool guard = false;
+    std::vector<Guard> gd;
     ~MbirBatch()
     {
         if (stream) cudaStreamSynchronize(stream);
         for (auto g : graphs) cudaGraphExecDestroy(g);
         void *bufs[] = {d_probs, d_state, d_tasks, d_lists, d_done, d_queue, d_err, d_ctl, d_scratch};
         for (void *b : bufs) dfree(b);
+        for (auto &g : gd) {
+            dfree(g.x);
+            dfree(g.e);
+        }
         if (h_ctl) cudaFreeHost(h_ctl);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -1821,6 +1915,40 @@ static void batch_build_list(const std::vector<MbirStage *> &st, const std::vect
     buf.insert(buf.end(), deps.begin(), deps.end());
     meta[4] = buf.size();
     for (const Ent &e : all) buf.push_back(e.k);
+}
+
+// MAP cost of a batch problem (as mbir_compute_cost), on the batch's stream.
+static int batch_cost(MbirBatch *B, int p, double *total)
+{
+    MbirStage *S = B->stages[p];
+    CK(mbir_launch_cost(S->g, S->pr, S->dv, S->d_partials, S->nparts, S->d_result, B->stream));
+    double r[2];
+    CK(cudaMemcpyAsync(r, S->d_result, sizeof(r), cudaMemcpyDeviceToHost, B->stream));
+    CK(cudaStreamSynchronize(B->stream));
+    *total = r[0] / 2.0 + (double)S->sg.N_p * (double)S->sg.N_r * (double)S->sg.N_t * log(S->var_est) / 2 + r[1];
+    return 0;
+}
+
+// The guard's snapshot of problem p: object and error sinogram, cost (given,
+// or evaluated when cost is null), counts.
+static int batch_snapshot(MbirBatch *B, int p, const SvBatchState &st, const double *cost = nullptr)
+{
+    MbirStage *S = B->stages[p];
+    MbirBatch::Guard &g = B->gd[p];
+    if (!g.x) {
+        CK(dalloc(&g.x, S->nvox()));
+        CK(dalloc(&g.e, S->nsino()));
+    }
+    CK(cudaMemcpyAsync(g.x, S->d_x, S->nvox() * sizeof(float), cudaMemcpyDeviceToDevice, B->stream));
+    CK(cudaMemcpyAsync(g.e, S->d_e, S->nsino() * sizeof(float), cudaMemcpyDeviceToDevice, B->stream));
+    if (cost)
+        g.cost = *cost;
+    else if (batch_cost(B, p, &g.cost))
+        return -1;
+    g.upd = st.updates;
+    g.zs = st.zero_skips;
+    g.win = 0;
+    return 0;
 }
 
 extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int32_t n, int32_t uncapped)
@@ -1917,6 +2045,14 @@ extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int3
     CK(cudaMemsetAsync(B->d_err, 0, sizeof(int), B->stream));
     CK(cudaStreamSynchronize(B->stream));
     B->seen.assign(n, 0);
+    // the stability guard (not for the autotuner's uncapped timing runs)
+    B->guard = !uncapped;
+    B->gd.assign(n, MbirBatch::Guard{});
+    if (B->guard)
+        for (int p = 0; p < n; p++) {
+            B->gd[p].cap = probs[p].cap;
+            if (batch_snapshot(B.get(), p, state[p])) return -1;
+        }
     // one graph per phase rotation: the sweep, then the end of the iteration
     CK(mbir_sv_batch_prepare(B->smem, B->half));
     for (int r = 0; r < B->nrot; r++) {
@@ -1943,6 +2079,59 @@ extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int3
 
 extern "C" void mbir_batch_free(MbirBatch *B) { delete B; }
 
+// After a batched iteration: for every problem that iterated and whose
+// window is due (one iteration for its first four checks, then eight, or
+// when it has just passed the convergence test), the MAP cost against the
+// window's start.  Every step of a problem's iteration lowers its cost, so a
+// rise of more than 1e-6 of it means its super-voxels in flight diverged: its
+// state and counts at the window's start are restored, it is set iterating
+// again, and its in-flight cap halves.
+static int batch_guard(MbirBatch *B)
+{
+    std::vector<SvBatchState> st(B->n);
+    CK(cudaMemcpyAsync(st.data(), B->d_state, B->n * sizeof(SvBatchState), cudaMemcpyDeviceToHost, B->stream));
+    CK(cudaStreamSynchronize(B->stream));
+    bool reactivated = false;
+    for (int p = 0; p < B->n; p++) {
+        MbirBatch::Guard &g = B->gd[p];
+        if (st[p].iters == g.last_iters) continue;  // not iterating
+        g.last_iters = st[p].iters;
+        if (++g.win < (g.checks < 4 ? 1 : 8) && !st[p].converged) continue;
+        double c = 0;
+        if (batch_cost(B, p, &c)) return -1;
+        MbirStage *S = B->stages[p];
+        if (!(c - g.cost <= 1e-6 * std::fabs(g.cost))) {
+            CK(cudaMemcpyAsync(S->d_x, g.x, S->nvox() * sizeof(float), cudaMemcpyDeviceToDevice, B->stream));
+            CK(cudaMemcpyAsync(S->d_e, g.e, S->nsino() * sizeof(float), cudaMemcpyDeviceToDevice, B->stream));
+            g.cap = std::max(1, g.cap / 2);
+            CK(cudaMemcpyAsync(reinterpret_cast<char *>(B->d_probs + p) + offsetof(SvProblem, cap), &g.cap,
+                               sizeof(int), cudaMemcpyHostToDevice, B->stream));
+            reactivated |= !st[p].active;
+            st[p].updates = g.upd;
+            st[p].zero_skips = g.zs;
+            st[p].active = 1;
+            st[p].converged = 0;
+            st[p].prev_ax = 0;
+            st[p].adjustments++;
+            CK(cudaMemcpyAsync(B->d_state + p, &st[p], sizeof(SvBatchState), cudaMemcpyHostToDevice, B->stream));
+            CK(cudaStreamSynchronize(B->stream));
+            S->stab_events++;
+            g.win = 0;
+            g.checks = 0;
+        } else {
+            if (batch_snapshot(B, p, st[p], &c)) return -1;
+            g.checks++;
+        }
+    }
+    if (reactivated) {  // the control word counts the problems iterating
+        int act = 0;
+        for (auto &x : st) act += x.active;
+        CK(cudaMemcpyAsync(B->d_ctl + 1, &act, sizeof(int), cudaMemcpyHostToDevice, B->stream));
+        CK(cudaStreamSynchronize(B->stream));
+    }
+    return 0;
+}
+
 extern "C" int mbir_batch_iterate(MbirBatch *B, int32_t max_iters, int32_t check_every, int32_t *active_left)
 {
     if (check_every <= 0) check_every = 1;
@@ -1951,6 +2140,7 @@ extern "C" int mbir_batch_iterate(MbirBatch *B, int32_t max_iters, int32_t check
     for (int k = 0; k < max_iters; k++) {
         CK(cudaGraphLaunch(B->graphs[B->replays % B->nrot], B->stream));
         B->replays++;
+        if (B->guard && batch_guard(B)) return -1;
         if ((k + 1) % check_every == 0 || k + 1 == max_iters) {
             CK(cudaMemcpyAsync(B->h_ctl, B->d_ctl, 4 * sizeof(int), cudaMemcpyDeviceToHost, B->stream));
             CK(cudaStreamSynchronize(B->stream));

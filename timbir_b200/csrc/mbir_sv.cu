@@ -825,8 +825,12 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 const int lx = q % S2, ly = q / S2;
                 const int xx = k0 + lx - 1, yy = j0 + ly - 1, zz = z0 + lz - 1;
                 float v = 0.0f;
-                if (xx >= 0 && xx < g.N_x && yy >= 0 && yy < g.N_y && zz >= 0 && zz < g.N_z)
-                    v = __ldcg(xf + (size_t)zz * plane + (size_t)yy * g.N_x + xx);
+                if (xx >= 0 && xx < g.N_x && yy >= 0 && yy < g.N_y) {
+                    if (zz >= 0 && zz < g.N_z)
+                        v = __ldcg(xf + (size_t)zz * plane + (size_t)yy * g.N_x + xx);
+                    else if (slab_has_z(g, dv, zz))
+                        v = __ldcg(slab_plane(g, dv, i, zz) + (size_t)yy * g.N_x + xx);
+                }
                 xb[lz * S2 * S2 + q] = v;
             }
         for (int sz = warp; sz < 2 * nz; sz += nwarps) {
@@ -890,7 +894,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         // the neighbour of this lane exists in z (spatial) or time (temporal)
         // for every voxel of the super-voxel; in x and y too when the block
         // keeps one voxel away from the image edges
-        const bool nfix = spatial ? (zg + ndz >= 0 && zg + ndz < g.N_z)
+        const bool nfix = spatial ? slab_has_z(g, dv, zg + ndz)
                                   : temporal && i + (lane == 26 ? -1 : 1) >= 0 && i + (lane == 26 ? -1 : 1) < g.N_time;
         const bool interior = k0 >= 1 && j0 >= 1 && k0 + kx < g.N_x && j0 + ky < g.N_y;
         // full resolution: this lane's views (vh * 32 + lane + 32 vsplit u, u
@@ -1208,12 +1212,8 @@ __global__ void __launch_bounds__(256) k_sv_batch_end(SvProblem *__restrict__ pr
             // the reference's convergence ratio (XT_ICD_update.c:1066-1103)
             const double ax = b.out.sum_abs_x;
             const double pct = ax > 0 ? 100.0 * probs[q].K * b.out.sum_abs_dx / ax : 0.0;
-            // stability guard: halve the problem's super-voxels in flight
-            // when a sweep's summed |x'| jumps (values blowing up)
-            if (b.iters >= 2 && b.prev_ax > 0 && ax > 2.0 * b.prev_ax && probs[q].cap > 1) {
-                probs[q].cap = max(1, probs[q].cap / 2);
-                b.adjustments++;
-            }
+            // (the stability guard is the host's: mbir_batch_iterate
+            // compares each problem's MAP cost over a window of iterations)
             b.prev_ax = ax;
             b.pct = pct;
             if (b.pct < probs[q].stop) {

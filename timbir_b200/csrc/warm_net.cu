@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -187,6 +188,277 @@ __global__ void __launch_bounds__(128) k_conv3t(const float *__restrict__ X, int
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Convolution on the 5th-generation tensor cores (tcgen05, accumulators in
+// tensor memory).  Implicit GEMM: M = 128 output voxels (8 along x by 16
+// along y, one z-plane; ZT planes per CTA, one accumulator each), N = Cout,
+// K = 27 taps x Cin, one tcgen05.mma of K = 16 per (tap, 16-channel input
+// chunk, plane).
+//
+// Operands in shared memory, canonical K-major layouts without swizzle
+// (8-row core matrices of 16 bytes per row; SBO = byte stride between 8-row
+// groups along M or N, LBO = byte stride between the two 8-element halves
+// of K = 16):
+//   A: the CTA's input block with a one-voxel halo for one 16-channel chunk,
+//      [half h][z][y][x][8 channels] BF16 (AZ x 18 x 10 voxels per half):
+//      8 consecutive x of one (z, y) row are one core matrix, the next y row
+//      is SBO = 160 B on, the other channel half LBO = one half-plane on.  A
+//      tap (dz, dy, dx) is the same layout started (dz, dy, dx) voxels away,
+//      so all 27 taps read the one staged block (no im2col copy);
+//   B: the chunk's weights for all 27 taps, [tap][h][n][8] BF16, packed in
+//      global memory in that order by k_pack_umma and brought in by one bulk
+//      copy (cp.async.bulk, completion counted on an mbarrier).
+// The block is staged by the CTA's threads (FP32 activations rounded to
+// BF16, zero outside the volume) into one of two buffers while the tensor
+// cores work on the other; one thread issues the MMAs and commits them to a
+// per-buffer mbarrier.  The epilogue reads the accumulators with
+// tcgen05.ld (warp w: rows 32w..32w+31), adds bias / skip input, applies
+// ReLU or accumulates, and writes FP32 channels-last.  Every wait is bounded
+// (1 s of global time); a wait that runs out sets *err and the kernel skips
+// its remaining MMAs, waits (bounded) for those in flight and frees its
+// tensor memory.
+constexpr int UX = 8, UY = 16, UZT = 2, UHX = UX + 2, UHY = UY + 2, UAZ = UZT + 2;
+constexpr int kUmmaHalf = UAZ * UHY * UHX * 16;  // bytes of one channel half of the staged block
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t gtime()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait until the mbarrier's phase of parity `par` has completed; false after 1 s
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t par)
+{
+    const uint64_t t0 = gtime();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(par)
+            : "memory");
+        if (done) return true;
+        if (gtime() - t0 > 1000000000ull) return false;
+    }
+}
+
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+template <int N, int NB>
+__global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, int Cin,
+                                                   const __nv_bfloat16 *__restrict__ Wu,
+                                                   const float *__restrict__ bias, const float *__restrict__ add,
+                                                   int relu, int accumulate, float *__restrict__ Y, Shape s,
+                                                   int *__restrict__ err)
+{
+    constexpr int kBBytes = 27 * N * 32;  // one chunk's weights
+    constexpr uint32_t kCols = UZT * N < 32 ? 32 : UZT * N;
+    extern __shared__ __align__(128) uint8_t usm[];
+    uint8_t *As = usm;                          // [2][2 halves][kUmmaHalf]
+    uint8_t *Bs = usm + 2 * 2 * kUmmaHalf;      // [NB][kBBytes]
+    __shared__ __align__(8) uint64_t bar_w[2], bar_mma[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_bad;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntx = (s.W + UX - 1) / UX, nty = (s.H + UY - 1) / UY, ntz = (s.D + UZT - 1) / UZT;
+    int t = blockIdx.x;
+    const int bx = t % ntx;
+    t /= ntx;
+    const int by = t % nty;
+    t /= nty;
+    const int bz = t % ntz;
+    const int b = t / ntz;
+    const int x0 = bx * UX, y0 = by * UY, z0 = bz * UZT;
+    const int KC = Cin / 16;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int q = 0; q < 2; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar_w[q])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar_mma[q])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_bad = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t idesc = umma_idesc(N);
+    int committed = 0;  // chunks whose MMAs thread 0 committed
+
+    for (int kc = 0; kc < KC; kc++) {
+        const int sa = kc & 1, sb = NB == 2 ? (kc & 1) : 0;
+        // the A buffer is free once chunk kc - 2's MMAs are done (after a
+        // failed wait nothing more is issued, and nothing more is waited for)
+        if (kc >= 2 && !*(volatile int *)&s_bad && !mbar_wait(&bar_mma[sa], ((kc - 2) >> 1) & 1))
+            atomicOr(&s_bad, 1);
+        if (tid == 0 && !*(volatile int *)&s_bad) {
+            // the B buffer: free after chunk kc - NB's MMAs
+            bool ok = true;
+            if (NB == 1 && kc >= 1) ok = mbar_wait(&bar_mma[(kc - 1) & 1], ((kc - 1) >> 1) & 1);
+            if (!ok) {
+                s_bad = 1;
+            } else {
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar_w[sb])),
+                             "r"((uint32_t)kBBytes)
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_addr(Bs + (size_t)sb * kBBytes)),
+                    "l"(Wu + (size_t)kc * 27 * N * 16), "r"((uint32_t)kBBytes), "r"(smem_addr(&bar_w[sb]))
+                    : "memory");
+            }
+        }
+        // stage the input block of chunk kc: per voxel 16 channels = 4 float4
+        uint8_t *Ab = As + (size_t)sa * 2 * kUmmaHalf;
+        for (int q = tid; q < UAZ * UHY * UHX * 4; q += 128) {
+            const int v = q >> 2, part = q & 3;
+            const int lx = v % UHX, ly = (v / UHX) % UHY, lz = v / (UHX * UHY);
+            const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
+                f = __ldg(reinterpret_cast<const float4 *>(
+                    X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
+            // channels 4 part .. 4 part + 3: half part / 2, offset 4 (part & 1)
+            uint2 *dst = reinterpret_cast<uint2 *>(Ab + (size_t)(part >> 1) * kUmmaHalf + (size_t)v * 16 +
+                                                   (part & 1) * 8);
+            *dst = make_uint2(pack_bf16(f.x, f.y), pack_bf16(f.z, f.w));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0 && !*(volatile int *)&s_bad) {
+            if (!mbar_wait(&bar_w[sb], (uint32_t)((kc / NB) & 1))) {
+                s_bad = 1;
+            } else {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a0 = smem_addr(Ab), b0 = smem_addr(Bs + (size_t)sb * kBBytes);
+                for (int tap = 0; tap < 27; tap++) {
+                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                    const uint64_t bd = umma_sdesc(b0 + (uint32_t)tap * N * 32, N * 16, 128);
+#pragma unroll
+                    for (int m = 0; m < UZT; m++) {
+                        const uint32_t aoff = (uint32_t)((((m + dz) * UHY + dy) * UHX + dx) * 16);
+                        const uint64_t ad = umma_sdesc(a0 + aoff, kUmmaHalf, UHX * 16);
+                        const uint32_t acc = (kc > 0 || tap > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + m * N),
+                            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_addr(&bar_mma[sa]))
+                             : "memory");
+                committed = kc + 1;
+            }
+        }
+    }
+    // all MMAs done: the last committed chunk's barrier (they complete in order)
+    __shared__ int s_last;
+    if (tid == 0) s_last = committed;
+    __syncthreads();
+    bool ok = !s_bad && s_last == KC;
+    if (s_last > 0) {
+        const int c = s_last - 1;
+        if (!mbar_wait(&bar_mma[c & 1], (c >> 1) & 1)) ok = false;
+    }
+    ok = __syncthreads_and(ok) != 0;  // the same for every thread (tcgen05.ld is warp-collective)
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 32);
+    } else {
+        // epilogue: thread = accumulator row 32 warp + lane = voxel (x0 + r % 8, y0 + r / 8)
+        const int r = warp * 32 + lane;
+        const int x = x0 + (r & 7), y = y0 + (r >> 3);
+#pragma unroll 1
+        for (int m = 0; m < UZT; m++) {
+            const int z = z0 + m;
+            const bool live = x < s.W && y < s.H && z < s.D;
+            const size_t mo = live ? ((((size_t)b * s.D + z) * s.H + y) * s.W + x) : 0;
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 8) {
+                uint32_t v[8];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7])
+                    : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * N + c0)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (!live) continue;
+                float o[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) o[j] = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
+                float4 *yp = reinterpret_cast<float4 *>(Y + mo * N + c0);
+                if (add) {
+                    const float4 a0 = *reinterpret_cast<const float4 *>(add + mo * N + c0);
+                    const float4 a1 = *reinterpret_cast<const float4 *>(add + mo * N + c0 + 4);
+                    o[0] += a0.x, o[1] += a0.y, o[2] += a0.z, o[3] += a0.w;
+                    o[4] += a1.x, o[5] += a1.y, o[6] += a1.z, o[7] += a1.w;
+                }
+                if (relu)
+#pragma unroll
+                    for (int j = 0; j < 8; j++) o[j] = fmaxf(o[j], 0.0f);
+                if (accumulate) {
+                    const float4 p0 = yp[0], p1 = yp[1];
+                    o[0] += p0.x, o[1] += p0.y, o[2] += p0.z, o[3] += p0.w;
+                    o[4] += p1.x, o[5] += p1.y, o[6] += p1.z, o[7] += p1.w;
+                }
+                yp[0] = make_float4(o[0], o[1], o[2], o[3]);
+                yp[1] = make_float4(o[4], o[5], o[6], o[7]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
+// Weights of a layer in the tensor-core layout of k_conv_umma: per input
+// chunk kc, tap, channel half h, output channel n, the 8 input channels
+// kc 16 + 8 h + j (j = 0..7), BF16.  Forward: K = cin, N = cout, element
+// W[tap][k][n]; input gradient: K = cout, N = cin, element W[26 - tap][n][k]
+// (the flipped, transposed kernel).
+__global__ void k_pack_umma(const float *__restrict__ W, int cin, int cout, int flip, __nv_bfloat16 *__restrict__ out)
+{
+    const int K = flip ? cout : cin, N = flip ? cin : cout;
+    const long long total = 27LL * K * N;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int j = (int)(i % 8);
+    long long r = i / 8;
+    const int n = (int)(r % N);
+    r /= N;
+    const int h = (int)(r % 2);
+    r /= 2;
+    const int tap = (int)(r % 27);
+    const int kc = (int)(r / 27);
+    const int k = kc * 16 + h * 8 + j;
+    const float v = flip ? W[((size_t)(26 - tap) * cin + n) * cout + k] : W[((size_t)tap * cin + k) * cout + n];
+    out[i] = __float2bfloat16_rn(v);
 }
 
 // Weight gradient, tiled: a CTA owns one 16-channel input chunk and NT
@@ -509,7 +781,11 @@ struct NetTensor {
 struct MbirNet {
     size_t w_off[kLayers], b_off[kLayers], nparams = 0, pack_off[kLayers], dpack_off[kLayers], npack = 0;
     float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
-    uint2 *pack = nullptr;  // forward and input-gradient fragments of every layer
+    uint2 *pack = nullptr;  // forward and input-gradient fragments of every layer (mma.sync)
+    // the same weights in the tensor-core layout of k_conv_umma (BF16)
+    __nv_bfloat16 *upack = nullptr;
+    size_t upack_off[kLayers], udpack_off[kLayers], nupack = 0;
+    int *d_err = nullptr;  // wait time-outs of the tensor-core convolution (bit 32)
     long long step = 0;
     Shape shape{0, 0, 0, 0};
     // activations: X0 (input), A[k] (layer outputs), P1..P3 (pooled), U0..U2 (up-sampled)
@@ -518,7 +794,8 @@ struct MbirNet {
     size_t npart = 0;
     ~MbirNet()
     {
-        for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)pack, (void *)part})
+        for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)pack, (void *)part,
+                        (void *)upack, (void *)d_err})
             if (q) cudaFree(q);
         for (auto &t : act)
             if (t.p) cudaFree(t.p);
@@ -587,9 +864,54 @@ static int net_shape(MbirNet *N, const Shape &s, bool train)
     return 0;
 }
 
-static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, const float *bias, const float *add,
-                        int relu, int accumulate, float *Y, const Shape &s, cudaStream_t st)
+// The convolutions run on tcgen05 (k_conv_umma) unless TIMBIR_NET_CONV=mma
+// selects the mma.sync kernel (k_conv3t), kept for comparison.
+static bool use_umma()
 {
+    static const bool on = [] {
+        const char *e = getenv("TIMBIR_NET_CONV");
+        return !(e && std::string(e) == "mma");
+    }();
+    return on;
+}
+
+template <int N, int NB>
+static cudaError_t conv_umma_launch(const float *X, int cin, const __nv_bfloat16 *Wu, const float *bias,
+                                    const float *add, int relu, int accumulate, float *Y, const Shape &s, int *err,
+                                    cudaStream_t st)
+{
+    const size_t smem = (size_t)2 * 2 * kUmmaHalf + (size_t)NB * 27 * N * 32;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv_umma<N, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const long long tiles =
+        (long long)s.B * ((s.D + UZT - 1) / UZT) * ((s.H + UY - 1) / UY) * ((s.W + UX - 1) / UX);
+    k_conv_umma<N, NB><<<(unsigned)tiles, 128, smem, st>>>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err);
+    return cudaGetLastError();
+}
+
+static cudaError_t conv_umma(const float *X, int cin, const __nv_bfloat16 *Wu, int cout, const float *bias,
+                             const float *add, int relu, int accumulate, float *Y, const Shape &s, int *err,
+                             cudaStream_t st)
+{
+    switch (cout) {
+    case 16: return conv_umma_launch<16, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 32: return conv_umma_launch<32, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 64: return conv_umma_launch<64, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 128: return conv_umma_launch<128, 1>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, const float *bias, const float *add,
+                        int relu, int accumulate, float *Y, const Shape &s, cudaStream_t st,
+                        const __nv_bfloat16 *Wu = nullptr, int *err = nullptr)
+{
+    if (Wu && use_umma()) return conv_umma(X, cin, Wu, cout, bias, add, relu, accumulate, Y, s, err, st);
     const int NT = std::min(cout / 8, 8);
     const long long tiles = (long long)s.B * ((s.D + TZ - 1) / TZ) * ((s.H + TY - 1) / TY) * ((s.W + TX - 1) / TX);
     const dim3 grid((unsigned)tiles, (unsigned)(cout / 8 / NT));
@@ -634,6 +956,14 @@ static int pack_all(MbirNet *N, cudaStream_t st)
             k_pack<<<blocks(nb), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1, N->pack + N->dpack_off[k]);
             NK(cudaGetLastError());
         }
+        const long long nu = 27LL * ci * co;
+        k_pack_umma<<<blocks(nu), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->upack + N->upack_off[k]);
+        NK(cudaGetLastError());
+        if (k > 0) {
+            k_pack_umma<<<blocks(nu), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1,
+                                                    N->upack + N->udpack_off[k]);
+            NK(cudaGetLastError());
+        }
     }
     return 0;
 }
@@ -647,7 +977,7 @@ static int forward(MbirNet *N, const float *in, float scale, cudaStream_t st)
     NK(cudaGetLastError());
     auto L = [&](int k, const float *x, const float *add, int relu, const Shape &sh) {
         return conv(x, kCh[k][0], N->pack + N->pack_off[k], kCh[k][1], N->params + N->b_off[k], add, relu, 0,
-                    A[T_A0 + k].p, sh, st);
+                    A[T_A0 + k].p, sh, st, N->upack + N->upack_off[k], N->d_err);
     };
     const Shape s1 = level_shape(s, 1), s2 = level_shape(s, 2), s3 = level_shape(s, 3);
     NK(L(0, A[T_X0].p, nullptr, 1, s));
@@ -688,7 +1018,8 @@ static int backward(MbirNet *N, cudaStream_t st)
         const float *dz = G[T_A0 + k].p;
         NK(wgrad(x, kCh[k][0], dz, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, st));
         if (dx)
-            NK(conv(dz, kCh[k][1], N->pack + N->dpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, st));
+            NK(conv(dz, kCh[k][1], N->pack + N->dpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, st,
+                    N->upack + N->udpack_off[k], N->d_err));
         return 0;
     };
     auto mask = [&](int t) -> int {  // dA -> dZ of a ReLU output
@@ -736,6 +1067,19 @@ static int backward(MbirNet *N, cudaStream_t st)
     return 0;
 }
 
+// time-outs recorded by the tensor-core convolutions since the last check
+static int net_err_check(MbirNet *N, cudaStream_t st)
+{
+    int e = 0;
+    NK(cudaMemcpyAsync(&e, N->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    NK(cudaStreamSynchronize(st));
+    if (e) {
+        cudaMemsetAsync(N->d_err, 0, sizeof(int), st);
+        return net_fail("tensor-core convolution: a wait for its operands or MMAs timed out");
+    }
+    return 0;
+}
+
 extern "C" {
 
 const char *mbir_net_last_error(void) { return g_net_err; }
@@ -762,6 +1106,10 @@ int mbir_net_create(MbirNet **out, uint32_t seed)
         poff += 27 * (size_t)(ci / 16) * (co / 8) * 32;
         N->dpack_off[k] = poff;
         if (k > 0) poff += 27 * (size_t)(co / 16) * (ci / 8) * 32;
+        N->upack_off[k] = N->nupack;
+        N->nupack += 27 * (size_t)ci * co;
+        N->udpack_off[k] = N->nupack;
+        if (k > 0) N->nupack += 27 * (size_t)ci * co;
     }
     N->nparams = off;
     N->npack = poff;
@@ -770,6 +1118,9 @@ int mbir_net_create(MbirNet **out, uint32_t seed)
     NK(cudaMalloc(&N->m, off * sizeof(float)));
     NK(cudaMalloc(&N->v, off * sizeof(float)));
     NK(cudaMalloc(&N->pack, poff * sizeof(uint2)));
+    NK(cudaMalloc(&N->upack, N->nupack * sizeof(__nv_bfloat16)));
+    NK(cudaMalloc(&N->d_err, sizeof(int)));
+    NK(cudaMemset(N->d_err, 0, sizeof(int)));
     NK(cudaMemset(N->params, 0, off * sizeof(float)));
     NK(cudaMemset(N->grads, 0, off * sizeof(float)));
     NK(cudaMemset(N->m, 0, off * sizeof(float)));
@@ -833,6 +1184,7 @@ int mbir_net_forward(MbirNet *N, const float *in, float *out, int32_t B, int32_t
     k_output<<<blocks(M), 256, 0, st>>>(in, N->act[T_A0 + 14].p, scale, out, M);
     NK(cudaGetLastError());
     NK(cudaStreamSynchronize(st));
+    if (net_err_check(N, st)) return -1;
     return 0;
 }
 
@@ -849,6 +1201,7 @@ int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t
     std::vector<double> part(nb);
     NK(cudaMemcpyAsync(part.data(), N->part, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
     NK(cudaStreamSynchronize(st));
+    if (net_err_check(N, st)) return -1;
     double l = 0;
     for (double v : part) l += v;
     if (loss) *loss = l / (double)M;
