@@ -845,6 +845,138 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     }), flush=True)
 
 
+# ------------------------------------------------------------ ingestion --
+INGEST = dict(views=1536, rows=128, cols=4100, whites=22, darks=12, proj_rows=64, proj_cols=2048)
+INGEST_DESC = ("APS raw-count normalisation (read_data): 1536 views of 128 x 4100 uint16 counts (4 edge columns "
+               "trimmed, 2 x 2 down-sampling to 64 x 2048), 22 bright and 12 dark frames, beam-hardening 0.5")
+
+
+def ingest_data(seed=0):
+    c = INGEST
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(200, 30000, size=(c["views"], c["rows"], c["cols"]), dtype=np.uint16)
+    whites = rng.integers(30000, 40000, size=(c["whites"], c["rows"], c["cols"]), dtype=np.uint16)
+    darks = rng.integers(0, 120, size=(c["darks"], c["rows"], c["cols"]), dtype=np.uint16)
+    return counts, whites, darks
+
+
+def ingest_reference_rate(counts, whites, darks, views):
+    """The reference's read_data (oracle/_ref/libref_io.so: its sources
+    compiled against an in-memory HDF5 stand-in) on the first `views` views:
+    output samples / s (its normalisation loop is single-threaded)."""
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_io.so"))
+    VP, I = C.c_void_p, C.c_int
+    lib.ref_read_aps.argtypes = [VP, I, VP, I, VP, I, I, I, I, I, I, I, I, VP, VP]
+    c = INGEST
+    sub = np.ascontiguousarray(counts[:views])
+    P = np.zeros((views, c["proj_rows"], c["proj_cols"]), np.float32)
+    W = np.zeros_like(P)
+    t0 = time.perf_counter()
+    rc = lib.ref_read_aps(sub.ctypes.data, views, whites.ctypes.data, c["whites"], darks.ctypes.data, c["darks"],
+                          c["rows"], c["cols"], 0, c["proj_rows"], c["proj_cols"], 0, views, P.ctypes.data,
+                          W.ctypes.data)
+    secs = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("reference read_data failed")
+    return P.size / secs, secs
+
+
+def ingest_arm(args, rank, world, local_rank):
+    """Normalisation of raw counts (mbir_frame_mean_device +
+    mbir_normalize_counts_device on device-resident stacks; e2e through
+    mbir_normalize_counts from pinned host stacks); each rank its own scan."""
+    import torch
+    from timbir_b200 import ingest
+    torch.cuda.set_device(local_rank)
+    c = INGEST
+    counts, whites, darks = ingest_data(rank)
+    lib = ingest._lib()
+    extras = c["cols"] % c["proj_cols"]
+    ncols, ratio = c["cols"] - extras, (c["cols"] - extras) // c["proj_cols"]
+    nrows = c["proj_rows"] * ratio
+    win = lambda a, f0, nf: np.ascontiguousarray(a[f0:f0 + nf, :nrows, extras // 2:extras // 2 + ncols])  # noqa
+    dc = torch.from_numpy(win(counts, 0, c["views"]).view(np.int16)).cuda()
+    dw = torch.from_numpy(win(whites, 1, c["whites"] - 2).view(np.int16)).cuda()
+    dd = torch.from_numpy(win(darks, 1, c["darks"] - 2).view(np.int16)).cuda()
+    mw = torch.empty((nrows, ncols), dtype=torch.float32, device="cuda")
+    md = torch.empty_like(mw)
+    P = torch.empty((c["views"], c["proj_rows"], c["proj_cols"]), dtype=torch.float32, device="cuda")
+    W = torch.empty_like(P)
+    st = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        rc = (lib.mbir_frame_mean_device(dw.data_ptr(), c["whites"] - 2, nrows, ncols, mw.data_ptr(), st) or
+              lib.mbir_frame_mean_device(dd.data_ptr(), c["darks"] - 2, nrows, ncols, md.data_ptr(), st) or
+              lib.mbir_normalize_counts_device(dc.data_ptr(), mw.data_ptr(), md.data_ptr(), c["views"], nrows, ncols,
+                                               ratio, 0.5, P.data_ptr(), W.data_ptr(), st))
+        if rc:
+            raise RuntimeError(lib.mbir_ingest_last_error().decode())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            ev[2 * k].record()
+            step()
+            ev[2 * k + 1].record()
+        torch.cuda.synchronize()
+    ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+    samples = P.numel()
+    value = samples * args.steps / (sum(ms) / 1e3)
+    # algorithmic bytes of a step: the counts window once, the bright / dark
+    # stacks once, the two means written and read once, both outputs written
+    byts = dc.numel() * 2 + (dw.numel() + dd.numel()) * 2 + 2 * 2 * mw.numel() * 4 + 2 * P.numel() * 4
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = byts / (sum(ms) / args.steps / 1e3) / 1e9
+    # end to end: pinned host stacks -> the public call -> host outputs
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    pc, pw, pd = pin(counts), pin(whites), pin(darks)
+    hp = pin(np.zeros((c["views"], c["proj_rows"], c["proj_cols"]), np.float32))
+    hw = pin(np.zeros_like(hp))
+    e2e_ms = []
+    for k in range(max(1, min(args.steps, 3)) + 1):
+        t0 = time.perf_counter()
+        _check = lib.mbir_normalize_counts(pc.ctypes.data, c["views"], pw.ctypes.data, c["whites"], pd.ctypes.data,
+                                           c["darks"], c["rows"], c["cols"], 0, c["proj_rows"], c["proj_cols"], 0,
+                                           c["views"], 0, 1, 0.5, hp.ctypes.data, hw.ctypes.data)
+        if _check:
+            raise RuntimeError(lib.mbir_ingest_last_error().decode())
+        if k:  # the first call pays one-time set-up (context, module)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    same = bool(np.array_equal(hw, W.cpu().numpy()))
+    line = {
+        "metric": "projection samples normalised/s", "value": value, "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(ms) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16 counts, f32 sums (f64 fabs / log as the reference)",
+        "data": "synthetic (seeded uniform counts, bright and dark fields)",
+        "config": {"workload": INGEST_DESC, "l2": "inputs (1.6 GB of counts) larger than L2"},
+        "e2e": {"value": samples / (statistics.median(e2e_ms) / 1e3), "unit": "samples/s",
+                "h2d_bytes_per_step": int(c["views"] * nrows * ncols * 2 + (c["whites"] + c["darks"] - 4) * nrows *
+                                          ncols * 2),
+                "d2h_bytes_per_step": int(2 * P.numel() * 4), "step_ms": [round(v, 2) for v in e2e_ms],
+                "step": "mbir_normalize_counts from pinned host stacks (hyperslab copies in, outputs back)",
+                "weights_equal_device_path": same},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "bytes_per_step": byts, "kernel": "k_normalize + k_frame_mean", "traffic": None,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "gpu_launches": 3 * args.steps, "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu:
+        rate, secs = ingest_reference_rate(counts, whites, darks, 48)
+        line["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": 1, "kind": "reference",
+                                "sample": f"the reference's read_data on the first 48 views, {secs:.1f} s "
+                                          "(its normalisation loop is single-threaded)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------ auxiliary kernels --
 def kernels_arm(args, rank, world, local_rank):
     """Each kernel of the path besides the super-voxel sweep, run on the 4-D
@@ -987,6 +1119,8 @@ def gpu_arm(args, rank, world, local_rank):
         return net_arm(args, rank, world, local_rank)
     if args.config == "kernels":
         return kernels_arm(args, rank, world, local_rank)
+    if args.config == "ingest":
+        return ingest_arm(args, rank, world, local_rank)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -1000,9 +1134,15 @@ def gpu_arm(args, rank, world, local_rank):
     sched = 1 if args.schedule == "sv" else 0
     st = workload_stage(w, scan, sched, args)
     sched_info = st.schedule_info()
+    big = w.name == "c5"  # hundreds of iterations of about a second, ~100 s per reference iteration
+    if big and args.c5_start == "fbp":  # this library's filtered backprojection as the start
+        fine = st.fbp()
     st.prepare(fine, zero_offsets(scan) if w.prior["remove_rings"] else None)
+    cost_trace = [st.cost()[0]] if big else None
     for it in range(1, args.warmup + 1):
         st.iterate(it)
+        if big:
+            cost_trace.append(st.cost()[0])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
     ms0, n_icd0, n_all0 = st.kernel_stats()
     upd0 = st.update_count()
@@ -1017,6 +1157,8 @@ def gpu_arm(args, rank, world, local_rank):
             st.time_begin()
             st.iterate(args.warmup + 1 + k)
             step_ms.append(st.time_end())
+            if big:  # the MAP cost after each iteration (outside the timed region)
+                cost_trace.append(st.cost()[0])
     torch.cuda.synchronize()
     ms1, n_icd1, n_all1 = st.kernel_stats()
     updates = st.update_count() - upd0
@@ -1034,7 +1176,6 @@ def gpu_arm(args, rank, world, local_rank):
     st.close()
 
     # time to the MAP target (every rank: its iteration count sizes the e2e solve)
-    big = w.name == "c5"  # hundreds of iterations of about a second, ~100 s per reference iteration
     ttm = time_to_map(w, scan, fine, sched, args) if not args.no_ttm and not big else None
     n_solve = ttm["iterations"] if ttm and ttm["iterations"] else args.steps
 
@@ -1135,6 +1276,11 @@ def gpu_arm(args, rank, world, local_rank):
     if ttm:
         line["time_to_map"] = ttm
     if big:
+        line["cost_trace"] = {"start": "filtered backprojection" if args.c5_start == "fbp" else "zero",
+                              "costs": [float(c) for c in cost_trace],
+                              "note": "FP64 MAP cost after the prologue and after each warm-up and timed iteration",
+                              "falling": bool(all(b <= a for a, b in zip(cost_trace, cost_trace[1:])))}
+    if big:
         line["cpu_baseline"] = {"unavailable": "the reference's CPU code needs minutes per iteration at this size"}
     elif not args.no_cpu:
         v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, 1, 1, os.cpu_count() or 1)
@@ -1152,6 +1298,24 @@ def reference_arm(args, rank):
     if args.config == "kernels":
         print(json.dumps({"impl": "reference", "unavailable": "a profiling helper of this library's kernels; no "
                           "reference counterpart"}), flush=True)
+        return
+    if args.config == "ingest":
+        counts, whites, darks = ingest_data(0)
+        rates = []
+        for k in range(args.warmup + args.steps):
+            r, secs = ingest_reference_rate(counts, whites, darks, 48)
+            if k >= args.warmup:
+                rates.append(r)
+        v = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": "projection samples normalised/s", "value": v, "unit": "samples/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "config": {"workload": INGEST_DESC},
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": 1, "kind": "reference",
+                             "sample": "the reference's read_data (its sources compiled against an in-memory HDF5 "
+                                       "stand-in) on the first 48 views per step; single-threaded loop"},
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
         return
     if args.config in ("c4", "4d-warm", "net"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start (its coarsest "
@@ -1194,6 +1358,11 @@ def reference_arm(args, rank):
             "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if ttm:
         line["time_to_map"] = ttm
+    if big:
+        line["cost_trace"] = {"start": "filtered backprojection" if args.c5_start == "fbp" else "zero",
+                              "costs": [float(c) for c in cost_trace],
+                              "note": "FP64 MAP cost after the prologue and after each warm-up and timed iteration",
+                              "falling": bool(all(b <= a for a, b in zip(cost_trace, cost_trace[1:])))}
     print(json.dumps(line), flush=True)
 
 
@@ -1206,9 +1375,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-ttm", action="store_true", help="skip the time-to-MAP measurement")
     ap.add_argument("--schedule", default="sv", choices=["sv", "reference"])
+    ap.add_argument("--c5-start", default="fbp", choices=["fbp", "zero"],
+                    help="start of the large 4-D z-subset (c5)")
     ap.add_argument("--c3-start", default="fbp", choices=["fbp", "zero"],
                     help="start of the batched problems' convergence run (c3)")
-    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net", "kernels"],
+    ap.add_argument("--config", default="3d", choices=sorted(WORKLOADS) + ["c3", "c4", "4d-warm", "net", "kernels", "ingest"],
                     help="3d: the single-GPU 3-D workload (default); 4d: 16-frame interlaced 4-D workload; "
                          "c3: 64 independent 3-D problems batched; c4: learned warm start (3-D); 4d-warm: learned warm "
                          "start on the 4-D workload; net: the network's training step; c5: large 4-D z-subset; "

@@ -193,6 +193,53 @@ int mbir_get_offset_windows(MbirStage *stage);
 /* update_variance_parameter (XT_ICD_update.c:720-751). */
 int mbir_update_variance_parameter(MbirStage *stage);
 
+/* ---- data ingestion (the drivers' readers, before reconstruct()) --------
+ * The HDF5 file access is the caller's; these take the datasets' arrays as
+ * the file holds them, [frames][rows][cols] in HOST memory, and select the
+ * readers' hyperslabs: columns trimmed symmetrically to a multiple of
+ * proj_cols (ratio = kept columns / proj_cols, the same along rows), rows
+ * datafile_row0 + rank (proj_rows / ranks) ratio onwards (rank / ranks in
+ * place of MPI_Comm_rank / MPI_Comm_size), views proj_start ..
+ * proj_start + proj_num - 1.  Outputs projections and weights [proj_num]
+ * [proj_rows / ranks][proj_cols] (host).  Return 0, or -1 with
+ * mbir_ingest_last_error().
+ *
+ * APS counts (read_data, aps_data/XT_HDFIO.c:46-236): bright and dark
+ * stacks averaged over their frames 1 .. n - 2, per output sample over its
+ * ratio x ratio raw samples weights = sum |count - dark|, bright =
+ * sum |white - dark|, t = log(bright / weights), projection = bh t^2 + t
+ * (bh: BH_QUAD_COEF, 0.5 in the APS driver). */
+const char *mbir_ingest_last_error(void);
+int mbir_normalize_counts(const uint16_t *counts, int32_t n_counts, const uint16_t *whites, int32_t n_whites,
+                          const uint16_t *darks, int32_t n_darks, int32_t rows, int32_t cols, int32_t datafile_row0,
+                          int32_t proj_rows, int32_t proj_cols, int32_t proj_start, int32_t proj_num, int32_t rank,
+                          int32_t ranks, double bh_quad_coef, float *projections, float *weights);
+/* Standard-format projections and weights (read_ProjWeightData,
+ * std_data/XT_HDFIO.c:41-158): per output sample the mean of the ratio x
+ * ratio projections through bh t^2 + t (bh 0 in that driver) and the sum of
+ * the weights. */
+int mbir_downsample_projections(const float *projs, const float *wts, int32_t n_views, int32_t rows, int32_t cols,
+                                int32_t datafile_row0, int32_t proj_rows, int32_t proj_cols, int32_t proj_start,
+                                int32_t proj_num, int32_t rank, int32_t ranks, double bh_quad_coef,
+                                float *projections, float *weights);
+/* The same normalisation on DEVICE arrays (stream: a cudaStream_t, NULL for
+ * the default stream; enqueued, not waited for): frame means of a
+ * [n_frames][rows][cols] uint16 stack, and projections / weights of
+ * counts [views][win_rows][win_cols] against the bright and dark means of
+ * the same window. */
+int mbir_frame_mean_device(const uint16_t *frames, int32_t n_frames, int32_t rows, int32_t cols, float *out,
+                           void *stream);
+int mbir_normalize_counts_device(const uint16_t *counts, const float *white_mean, const float *dark_mean,
+                                 int32_t views, int32_t win_rows, int32_t win_cols, int32_t ratio, double bh_quad_coef,
+                                 float *projections, float *weights, void *stream);
+/* gen_interlaced_views_0_to_Inf (aps_data/XT_Views.c:41-80): angles
+ * (radians) and times of views proj_start .. proj_start + N_p - 1 of an
+ * interlaced scan of K interlaced sub-scans of N_theta / K views per half
+ * turn (bit-reversed offsets), views closer than rot_speed x min_acq_time to
+ * the last kept one skipped.  Returns the kept views generated, or -1. */
+int32_t mbir_gen_interlaced_views(float *views, float *times, int32_t K, int32_t N_theta, int32_t proj_start,
+                                  int32_t N_p, float min_acq_time, float rot_speed);
+
 /* ---- z-slab sharding (the reference's MPI decomposition, XT_MPI.c:47-122)
  * A volume split into `ranks` z-slabs, one per process (or GPU): the stage
  * holds slab `rank`, built from that slab's detector rows, as each MPI rank

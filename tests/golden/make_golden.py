@@ -19,6 +19,10 @@ Outputs (committed):
                            remove_rings 2 (object, offsets, cost trace)
   upsample.npz             the reference's x2 up-sampling between stages
                            (upsample_object_bilinear_2D / _3D) of seeded slices
+  ingest.npz               the reference's data readers and view generator
+                           (aps_data read_data, std_data read_ProjWeightData,
+                           gen_interlaced_views_0_to_Inf) on seeded arrays,
+                           through oracle/_ref/libref_io.so
 """
 from __future__ import annotations
 
@@ -137,7 +141,60 @@ def upsample_fixture():
     print("upsample", sorted(out))
 
 
+INGEST_CASES = {
+    # name: (views, rows, cols, n_whites, n_darks, datafile_row0, proj_rows, proj_cols, proj_start, proj_num)
+    "ratio1": (5, 8, 12, 4, 3, 0, 8, 12, 1, 3),
+    "ratio2_trim": (6, 12, 27, 5, 4, 2, 4, 12, 0, 6),   # 27 columns: 3 trimmed, ratio 2
+    "ratio3": (4, 9, 30, 6, 5, 0, 3, 10, 2, 2),
+}
+VIEW_CASES = [  # K, N_theta, proj_start, N_p, min_acq_time, rot_speed
+    (16, 1024, 0, 1024, 0.0, 0.0), (32, 1024, 17, 200, 0.0, 0.0), (4, 256, 3, 150, 0.01, 1.5),
+    (8, 24, 0, 40, 0.0, 0.0), (1, 64, 0, 70, 0.0, 0.0),
+]
+
+
+def ingest_fixture():
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_io.so"))
+    VP, I = C.c_void_p, C.c_int
+    lib.ref_read_aps.argtypes = [VP, I, VP, I, VP, I, I, I, I, I, I, I, I, VP, VP]
+    lib.ref_read_std.argtypes = [VP, VP, I, I, I, I, I, I, I, I, VP, VP]
+    lib.ref_gen_views.argtypes = [VP, VP, I, I, I, I, C.c_float, C.c_float]
+    out = {}
+    for k, (name, (n, rows, cols, nw, nd, r0, pr, pc, ps, pn)) in enumerate(sorted(INGEST_CASES.items())):
+        rng = np.random.default_rng(70 + k)
+        counts = rng.integers(50, 4000, size=(n, rows, cols)).astype(np.uint16)
+        whites = rng.integers(4000, 6000, size=(nw, rows, cols)).astype(np.uint16)
+        darks = rng.integers(0, 60, size=(nd, rows, cols)).astype(np.uint16)
+        P = np.zeros((pn, pr, pc), np.float32)
+        W = np.zeros_like(P)
+        assert lib.ref_read_aps(counts.ctypes.data, n, whites.ctypes.data, nw, darks.ctypes.data, nd, rows, cols, r0,
+                                pr, pc, ps, pn, P.ctypes.data, W.ctypes.data) == 0
+        projs = rng.normal(1.0, 0.5, size=(n, rows, cols)).astype(np.float32)
+        wts = rng.uniform(10, 1000, size=(n, rows, cols)).astype(np.float32)
+        Ps = np.zeros_like(P)
+        Ws = np.zeros_like(P)
+        assert lib.ref_read_std(projs.ctypes.data, wts.ctypes.data, n, rows, cols, r0, pr, pc, ps, pn, Ps.ctypes.data,
+                                Ws.ctypes.data) == 0
+        for key, v in dict(counts=counts, whites=whites, darks=darks, aps_proj=P, aps_weight=W, std_in_proj=projs,
+                           std_in_weight=wts, std_proj=Ps, std_weight=Ws,
+                           params=np.array([n, rows, cols, nw, nd, r0, pr, pc, ps, pn], np.int32)).items():
+            out[f"{name}/{key}"] = v
+    for k, (K, Nt, ps, npv, mat, rs) in enumerate(VIEW_CASES):
+        v = np.zeros(npv, np.float32)
+        t = np.zeros(npv, np.float32)
+        kept = lib.ref_gen_views(v.ctypes.data, t.ctypes.data, K, Nt, ps, npv, mat, rs)
+        out[f"views{k}/angles"] = v
+        out[f"views{k}/times"] = t
+        out[f"views{k}/kept"] = np.int32(kept)
+        out[f"views{k}/params"] = np.array([K, Nt, ps, npv, mat, rs], np.float64)
+    np.savez_compressed(os.path.join(HERE, "ingest.npz"), **out)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "ingest":
+        ingest_fixture()
+        sys.exit(0)
     if len(sys.argv) > 1 and sys.argv[1] == "upsample":
         upsample_fixture()
         sys.exit(0)

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtimbir_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["mbir_kernels.cu", "mbir_sv.cu", "mbir_fbp.cu", "warm_net.cu", "mbir_stage.cu", "mbir_noalloc.cu", "mbir_nhicd.cu", "mbir_setup.cpp", "mbir_reconstruct.cpp"]
+SOURCES = ["mbir_kernels.cu", "mbir_sv.cu", "mbir_fbp.cu", "warm_net.cu", "mbir_stage.cu", "mbir_noalloc.cu", "mbir_nhicd.cu", "mbir_ingest.cu", "mbir_setup.cpp", "mbir_reconstruct.cpp"]
 
 
 def nvcc() -> str:

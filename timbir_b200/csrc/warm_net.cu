@@ -572,16 +572,24 @@ __global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restri
 }
 
 // db[c] += sum over voxels of dY[m][c]
-__global__ void k_bias_grad(const float *__restrict__ dY, int C, long long M, long long chunk, float *__restrict__ db)
+// (blockDim 256, C <= 256 and dividing 256: the block's lanes of a channel
+// are summed in shared memory first, one atomic per channel per block)
+__global__ void __launch_bounds__(256) k_bias_grad(const float *__restrict__ dY, int C, long long M, long long chunk,
+                                                   float *__restrict__ db)
 {
+    __shared__ float red[256];
     const int c = threadIdx.x % C;
     const int lanes = blockDim.x / C;
     const int l = threadIdx.x / C;
-    if (l >= lanes) return;
     const long long start = (long long)blockIdx.x * chunk, end = min(M, start + chunk);
     float acc = 0.0f;
     for (long long m = start + l; m < end; m += lanes) acc += dY[(size_t)m * C + c];
-    atomicAdd(db + c, acc);
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    if (l == 0) {
+        for (int q = 1; q < lanes; q++) acc += red[q * C + c];
+        atomicAdd(db + c, acc);
+    }
 }
 
 // Packed B fragments of a layer: forward (K = cin, N = cout, element
@@ -948,13 +956,15 @@ static int pack_all(MbirNet *N, cudaStream_t st)
 {
     for (int k = 0; k < kLayers; k++) {
         const int ci = kCh[k][0], co = kCh[k][1];
-        const long long nf = 27LL * (ci / 16) * (co / 8) * 32;
-        k_pack<<<blocks(nf), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->pack + N->pack_off[k]);
-        NK(cudaGetLastError());
-        if (k > 0) {
-            const long long nb = 27LL * (co / 16) * (ci / 8) * 32;
-            k_pack<<<blocks(nb), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1, N->pack + N->dpack_off[k]);
+        if (!use_umma()) {  // fragments of the mma.sync convolution
+            const long long nf = 27LL * (ci / 16) * (co / 8) * 32;
+            k_pack<<<blocks(nf), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->pack + N->pack_off[k]);
             NK(cudaGetLastError());
+            if (k > 0) {
+                const long long nb = 27LL * (co / 16) * (ci / 8) * 32;
+                k_pack<<<blocks(nb), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1, N->pack + N->dpack_off[k]);
+                NK(cudaGetLastError());
+            }
         }
         const long long nu = 27LL * ci * co;
         k_pack_umma<<<blocks(nu), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->upack + N->upack_off[k]);
