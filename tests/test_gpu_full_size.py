@@ -11,9 +11,10 @@ reference library iterated to a flat cost, then the FP64 oracle from there):
     oracle, and image RMSE against the FP64 oracle's converged image below
     1e-3 of its range -- with FP32 and with FP16 A-matrix values;
   * convex 4-D workload (16 frames of 256x256x16, 1024 interlaced views,
-    zingers and rings in the data, quadratic data term, zero-mean ring
-    offsets): the GPU's fresh cost (error sinogram recomputed from the
-    object and offsets, FP64 sums) within 1e-5 relative of C*, and RMSE at
+    zingers and rings in the data, quadratic data term, no ring correction:
+    the reference's zero-mean ring-offset iteration creeps too slowly to fix
+    a C* at this size): the GPU's fresh cost (error sinogram recomputed from
+    the object, FP64 sums) within 1e-5 relative of C*, and RMSE at
     262,144 seeded voxel positions against the FP64 oracle below 1e-3 of
     the range -- with FP32 and with FP16 A-matrix values.
 

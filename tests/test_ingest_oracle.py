@@ -37,3 +37,23 @@ def test_view_generators_match_the_reference(name):
         assert np.array_equal(a, G[f"{name}/angles"])
         assert np.array_equal(t, G[f"{name}/times"])
         assert kept == int(G[f"{name}/kept"])
+
+
+def test_refused_ingestion_inputs_fail_before_any_device_work():
+    # the readers' checks run on the host, before any CUDA call, so they hold
+    # on a machine without a GPU too
+    from timbir_b200 import ingest
+    counts = np.zeros((4, 8, 16), np.uint16)
+    stack = np.zeros((5, 8, 16), np.uint16)
+    with pytest.raises(RuntimeError, match="rows"):  # 16 rows x ratio 1 > 8 in the file
+        ingest.normalize_counts(counts, stack, stack, 16, 16)
+    with pytest.raises(RuntimeError, match="ranks"):  # 8 rows over 3 ranks
+        ingest.normalize_counts(counts, stack, stack, 8, 16, ranks=3)
+    with pytest.raises(RuntimeError, match="columns"):  # more output columns than the file has
+        ingest.normalize_counts(counts, stack, stack, 8, 32)
+    with pytest.raises(RuntimeError, match="3 frames"):
+        ingest.normalize_counts(counts, stack[:2], stack, 8, 16)
+    with pytest.raises(RuntimeError, match="proj_start"):
+        ingest.normalize_counts(counts, stack, stack, 8, 16, proj_start=2, proj_num=3)
+    with pytest.raises(ValueError):
+        ingest.interlaced_views(0, 16, 4)

@@ -271,8 +271,11 @@ __global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, 
     constexpr int kBBytes = 27 * N * 32;  // one chunk's weights
     constexpr uint32_t kCols = UZT * N < 32 ? 32 : UZT * N;
     extern __shared__ __align__(128) uint8_t usm[];
-    uint8_t *As = usm;                          // [2][2 halves][kUmmaHalf]
-    uint8_t *Bs = usm + 2 * 2 * kUmmaHalf;      // [NB][kBBytes]
+    // A buffers: min(chunks, 2) x [2 halves][kUmmaHalf]; then the B buffers
+    // (the host sizes the dynamic shared memory the same way)
+    const int nA = Cin / 16 < 2 ? 1 : 2;
+    uint8_t *As = usm;
+    uint8_t *Bs = usm + (size_t)nA * 2 * kUmmaHalf;  // [min(chunks, NB)][kBBytes]
     __shared__ __align__(8) uint64_t bar_w[2], bar_mma[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_bad;
@@ -333,18 +336,31 @@ __global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, 
         }
         // stage the input block of chunk kc: per voxel 16 channels = 4 float4
         uint8_t *Ab = As + (size_t)sa * 2 * kUmmaHalf;
-        for (int q = tid; q < UAZ * UHY * UHX * 4; q += 128) {
-            const int v = q >> 2, part = q & 3;
-            const int lx = v % UHX, ly = (v / UHX) % UHY, lz = v / (UHX * UHY);
-            const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
-                f = __ldg(reinterpret_cast<const float4 *>(
-                    X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
-            // channels 4 part .. 4 part + 3: half part / 2, offset 4 (part & 1)
-            uint2 *dst = reinterpret_cast<uint2 *>(Ab + (size_t)(part >> 1) * kUmmaHalf + (size_t)v * 16 +
-                                                   (part & 1) * 8);
-            *dst = make_uint2(pack_bf16(f.x, f.y), pack_bf16(f.z, f.w));
+        // four loads in flight per thread before their conversions and stores
+        constexpr int kStage = UAZ * UHY * UHX * 4, kU = 4;
+        for (int q0 = tid; q0 < kStage; q0 += 128 * kU) {
+            float4 f[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int q = q0 + u * 128;
+                const int v = q >> 2, part = q & 3;
+                const int lx = v % UHX, ly = (v / UHX) % UHY, lz = v / (UHX * UHY);
+                const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
+                f[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (q < kStage && x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
+                    f[u] = __ldg(reinterpret_cast<const float4 *>(
+                        X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int q = q0 + u * 128;
+                if (q >= kStage) break;
+                const int v = q >> 2, part = q & 3;
+                // channels 4 part .. 4 part + 3: half part / 2, offset 4 (part & 1)
+                uint2 *dst = reinterpret_cast<uint2 *>(Ab + (size_t)(part >> 1) * kUmmaHalf + (size_t)v * 16 +
+                                                       (part & 1) * 8);
+                *dst = make_uint2(pack_bf16(f[u].x, f[u].y), pack_bf16(f[u].z, f[u].w));
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -582,8 +598,17 @@ __global__ void __launch_bounds__(256) k_bias_grad(const float *__restrict__ dY,
     const int lanes = blockDim.x / C;
     const int l = threadIdx.x / C;
     const long long start = (long long)blockIdx.x * chunk, end = min(M, start + chunk);
-    float acc = 0.0f;
-    for (long long m = start + l; m < end; m += lanes) acc += dY[(size_t)m * C + c];
+    // four independent sums in flight per thread
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+    long long m = start + l;
+    for (; m + 3 * lanes < end; m += 4 * lanes) {
+        a0 += dY[(size_t)m * C + c];
+        a1 += dY[(size_t)(m + lanes) * C + c];
+        a2 += dY[(size_t)(m + 2 * lanes) * C + c];
+        a3 += dY[(size_t)(m + 3 * lanes) * C + c];
+    }
+    for (; m < end; m += lanes) a0 += dY[(size_t)m * C + c];
+    float acc = (a0 + a1) + (a2 + a3);
     red[threadIdx.x] = acc;
     __syncthreads();
     if (l == 0) {
@@ -888,11 +913,13 @@ static cudaError_t conv_umma_launch(const float *X, int cin, const __nv_bfloat16
                                     const float *add, int relu, int accumulate, float *Y, const Shape &s, int *err,
                                     cudaStream_t st)
 {
-    const size_t smem = (size_t)2 * 2 * kUmmaHalf + (size_t)NB * 27 * N * 32;
+    // as the kernel carves it: min(chunks, 2) A buffers, min(chunks, NB) B buffers
+    const int kc = cin / 16;
+    const size_t smem = (size_t)std::min(kc, 2) * 2 * kUmmaHalf + (size_t)std::min(kc, NB) * 27 * N * 32;
     static bool attr = false;
-    if (!attr) {
+    if (!attr) {  // the largest size this instantiation launches with
         cudaError_t e = cudaFuncSetAttribute(k_conv_umma<N, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+                                             (int)(2 * 2 * kUmmaHalf + (size_t)NB * 27 * N * 32));
         if (e != cudaSuccess) return e;
         attr = true;
     }
@@ -946,7 +973,7 @@ static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, flo
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const long long M = s.voxels();
-    const long long bch = std::max(1LL, std::min(M / 1024, 1024LL));
+    const long long bch = std::max(1LL, std::min(M / 256, 4096LL));
     const long long bchunk = (M + bch - 1) / bch;
     k_bias_grad<<<(unsigned)bch, 256, 0, st>>>(dY, cout, M, bchunk, db);
     return cudaGetLastError();
