@@ -126,6 +126,10 @@ def workload_stage(w, scan, sched, args, prior=None):
     st.set_switches(**finest_stage_switches(prior))
     if args.zgroup:
         st.set_sv_zgroup(args.zgroup)
+    if getattr(args, "sv_alpha", 0.0):
+        st.set_sv_relaxation(args.sv_alpha)
+    if getattr(args, "sv_ctas", 0):
+        st.set_sv_ctas(args.sv_ctas)
     st.set_schedule(sched, args.sv_side, args.warps_per_slice, args.acache)
     if sched and getattr(args, "nhicd", -1.0) >= 0:
         st.set_sv_nhicd(args.nhicd)
@@ -1400,6 +1404,9 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="c3: default schedules instead of the autotuner's")
     ap.add_argument("--warps-per-slice", type=int, default=0, help="1, 2 or 4 (0: automatic)")
     ap.add_argument("--zgroup", type=int, default=0, help="slices per super-voxel z-group (0: automatic)")
+    ap.add_argument("--sv-alpha", type=float, default=0.0,
+                    help="over-relaxation of the super-voxel schedule (0: automatic from the in-flight cap)")
+    ap.add_argument("--sv-ctas", type=int, default=0, help="persistent CTAs per sweep (0: automatic)")
     ap.add_argument("--nhicd", type=float, default=-1.0,
                     help="share of each plane's lines the NHICD pass selects (default: the library's 0.1)")
     ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,
