@@ -489,7 +489,7 @@ constexpr int kWgWarps = 9;
 template <int NT>
 __global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restrict__ X, int Cin,
                                                           const float *__restrict__ dY, int Cout,
-                                                          float *__restrict__ dW, Shape s)
+                                                          float *__restrict__ dW, float *__restrict__ part, Shape s)
 {
     __shared__ __align__(16) __nv_bfloat16 xs[2][16][HV];
     __shared__ __align__(16) __nv_bfloat16 ys[NT * 8][TZ * TY * TX];
@@ -571,20 +571,43 @@ __global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restri
             }
         }
     }
+    // this CTA's sums: into its own slice of `part` (summed over the CTAs
+    // by k_wgrad_reduce), or added to dW with atomics when part is null
+    float *dst = part ? part + (size_t)blockIdx.x * 27 * Cin * Cout : dW;
 #pragma unroll
     for (int u = 0; u < 3; u++) {
         const int tap = warp + kWgWarps * u;
 #pragma unroll
         for (int j = 0; j < NT; j++) {
             const int co = co0 + j * 8 + 2 * tq;
-            float *w0 = dW + ((size_t)tap * Cin + ci0 + g) * Cout + co;
+            float *w0 = dst + ((size_t)tap * Cin + ci0 + g) * Cout + co;
             float *w1 = w0 + (size_t)8 * Cout;
-            atomicAdd(w0, acc[u][j][0]);
-            atomicAdd(w0 + 1, acc[u][j][1]);
-            atomicAdd(w1, acc[u][j][2]);
-            atomicAdd(w1 + 1, acc[u][j][3]);
+            if (part) {
+                *reinterpret_cast<float2 *>(w0) = make_float2(acc[u][j][0], acc[u][j][1]);
+                *reinterpret_cast<float2 *>(w1) = make_float2(acc[u][j][2], acc[u][j][3]);
+            } else {
+                atomicAdd(w0, acc[u][j][0]);
+                atomicAdd(w0 + 1, acc[u][j][1]);
+                atomicAdd(w1, acc[u][j][2]);
+                atomicAdd(w1 + 1, acc[u][j][3]);
+            }
         }
     }
+}
+
+// dW[i] += sum over the nx CTA slices of part (each n values), in slice order
+__global__ void k_wgrad_reduce(const float *__restrict__ part, int nx, int n, float *__restrict__ dW)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a0 = 0.0f, a1 = 0.0f;
+    int x = 0;
+    for (; x + 1 < nx; x += 2) {
+        a0 += part[(size_t)x * n + i];
+        a1 += part[(size_t)(x + 1) * n + i];
+    }
+    if (x < nx) a0 += part[(size_t)x * n + i];
+    dW[i] += a0 + a1;
 }
 
 // db[c] += sum over voxels of dY[m][c]
@@ -819,6 +842,7 @@ struct MbirNet {
     __nv_bfloat16 *upack = nullptr;
     size_t upack_off[kLayers], udpack_off[kLayers], nupack = 0;
     int *d_err = nullptr;  // wait time-outs of the tensor-core convolution (bit 32)
+    float *wg_part = nullptr;  // per-CTA weight-gradient sums (kWgPartFloats)
     long long step = 0;
     Shape shape{0, 0, 0, 0};
     // activations: X0 (input), A[k] (layer outputs), P1..P3 (pooled), U0..U2 (up-sampled)
@@ -828,7 +852,7 @@ struct MbirNet {
     ~MbirNet()
     {
         for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)pack, (void *)part,
-                        (void *)upack, (void *)d_err})
+                        (void *)upack, (void *)d_err, (void *)wg_part})
             if (q) cudaFree(q);
         for (auto &t : act)
             if (t.p) cudaFree(t.p);
@@ -959,19 +983,31 @@ static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, cons
     return cudaGetLastError();
 }
 
+// Weight gradient: CTAs along x split the voxel blocks; each writes its sums
+// to its own slice of `part` (kWgPartFloats floats: as many x-CTAs as fit,
+// up to four per SM) and k_wgrad_reduce adds them to dW.
+constexpr size_t kWgPartFloats = 4u << 20;
+
 static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, float *dW, float *db, const Shape &s,
-                         cudaStream_t st)
+                         float *part, cudaStream_t st)
 {
     const int NT = std::min(cout / 8, 4);
     const long long blocks_ = (long long)s.B * ((s.D + TZ - 1) / TZ) * ((s.H + TY - 1) / TY) * ((s.W + TX - 1) / TX);
-    const dim3 grid((unsigned)std::min<long long>(blocks_, 128), (unsigned)(cin / 16), (unsigned)(cout / 8 / NT));
+    const long long n = 27LL * cin * cout;
+    const long long nx = std::max(1LL, std::min({blocks_, (long long)(kWgPartFloats / n), 4LL * 148}));
+    const dim3 grid((unsigned)nx, (unsigned)(cin / 16), (unsigned)(cout / 8 / NT));
     switch (NT) {
-    case 1: k_wgrad3t<1><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
-    case 2: k_wgrad3t<2><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
-    default: k_wgrad3t<4><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, s); break;
+    case 1: k_wgrad3t<1><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, part, s); break;
+    case 2: k_wgrad3t<2><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, part, s); break;
+    default: k_wgrad3t<4><<<grid, 32 * kWgWarps, 0, st>>>(X, cin, dY, cout, dW, part, s); break;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (part) {
+        k_wgrad_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, (int)nx, (int)n, dW);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const long long M = s.voxels();
     const long long bch = std::max(1LL, std::min(M / 256, 4096LL));
     const long long bchunk = (M + bch - 1) / bch;
@@ -1053,7 +1089,7 @@ static int backward(MbirNet *N, cudaStream_t st)
     // gradient dz; the input gradient (into dx, optionally accumulated)
     auto layer = [&](int k, const float *x, const Shape &sh, float *dx, int acc) -> int {
         const float *dz = G[T_A0 + k].p;
-        NK(wgrad(x, kCh[k][0], dz, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, st));
+        NK(wgrad(x, kCh[k][0], dz, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, N->wg_part, st));
         if (dx)
             NK(conv(dz, kCh[k][1], N->pack + N->dpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, st,
                     N->upack + N->udpack_off[k], N->d_err));
@@ -1157,6 +1193,7 @@ int mbir_net_create(MbirNet **out, uint32_t seed)
     NK(cudaMalloc(&N->pack, poff * sizeof(uint2)));
     NK(cudaMalloc(&N->upack, N->nupack * sizeof(__nv_bfloat16)));
     NK(cudaMalloc(&N->d_err, sizeof(int)));
+    NK(cudaMalloc(&N->wg_part, kWgPartFloats * sizeof(float)));
     NK(cudaMemset(N->d_err, 0, sizeof(int)));
     NK(cudaMemset(N->params, 0, off * sizeof(float)));
     NK(cudaMemset(N->grads, 0, off * sizeof(float)));
