@@ -129,3 +129,14 @@ def test_sharded_stage_refuses_constraint_windows():
     with pytest.raises(timbir_b200.MbirError):
         st.set_offset_windows(True)
     st.close()
+
+
+def test_sharded_stage_is_refused_by_the_batch():
+    scan = scan_3d()
+    st = timbir_b200.Stage(slab.split_scan(scan, 1, 2), **PRIOR, blocks=2)
+    st.set_batch_schedule(0, 1, 1)
+    st.prepare()
+    st.set_z_slab(1, 2, lambda v: None)
+    with pytest.raises(timbir_b200.MbirError):
+        timbir_b200.Batch([st])
+    st.close()

@@ -1965,6 +1965,8 @@ extern "C" int mbir_batch_create(MbirBatch **out, MbirStage *const *stages, int3
             return fail("batch problem %d: the super-voxel schedule with a column cache is required", p);
         if (S->upd_offset > 1 || S->upd_var == 1)
             return fail("batch problem %d: batched iterations run plain ICD (no ring-offset or variance update)", p);
+        if (S->slab_count > 1)
+            return fail("batch problem %d: a z-slab of a sharded volume (its sums reduce over ranks)", p);
         const SvParams &sp = S->sp;
         const int vpl = (sp.max_views + 32 * sp.vsplit - 1) / (32 * sp.vsplit);
         if (sp.amax != 3 || S->st.m_z != 1 || vpl > kSvBatchViewsPerLane ||
