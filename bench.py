@@ -836,7 +836,7 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1) / args.steps
     net.close()
-    umma = os.environ.get("TIMBIR_NET_CONV", "") != "mma"
+
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -846,9 +846,10 @@ def net_arm(args, rank, world, local_rank, shape=(4, 16, 64, 64)):
     print(json.dumps({
         "metric": "warm-start network training steps/s", "value": 1e3 / ms, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "dtype": ("bf16 operands, fp32 accumulation (convolutions and input gradients: tcgen05.mma kind::f16, "
-                  "accumulators in tensor memory; weight gradients: mma.sync m16n8k16)") if umma else
-                 "bf16 operands, fp32 accumulation (mma.sync m16n8k16)", "data": "synthetic (random patches)",
+        "dtype": ("bf16 activations and operands, fp32 accumulation (convolutions and input gradients: "
+                  "tcgen05.mma kind::f16 with TMA-loaded inputs and accumulators in tensor memory; weight "
+                  "gradients: mma.sync m16n8k16); fp32 master weights and Adam state"),
+        "data": "synthetic (random patches)",
         "forward": {"ms": fwd_ms, "tflops": fwd_flops / (fwd_ms / 1e3) / 1e12,
                     "note": "inference pass alone (15 convolutions, pooling, up-sampling; includes the "
                             "host-synchronised output copy of mbir_net_forward)"},

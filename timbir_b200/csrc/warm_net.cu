@@ -27,8 +27,10 @@
 // weights; the weight gradient is a GEMM over voxels (M = input channels,
 // N = output channels, K = voxels) over staged blocks, reduced over CTAs
 // with FP32 atomics.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -85,110 +87,12 @@ __device__ __forceinline__ bool decode(const Shape &s, long long m, int &b, int 
     return true;
 }
 
-// Y[m][n] = act(sum over taps and input channels + bias[n] + add[m][n]), or
-// (accumulate) Y[m][n] += the sum.  Wp: packed B fragments, per (tap,
-// 16-channel input chunk, 8-channel output tile) one uint2 per lane.  A CTA
-// computes a 2 x 4 x 16 block of output voxels (eight m-tiles of 16
-// consecutive x, two per warp) for NT output tiles; per 16-channel input
-// chunk it stages the block's input with a one-voxel halo (4 x 6 x 18
-// voxels, BF16, 13.8 KB) in shared memory once, and every tap takes its A
-// fragments from there.
+// Voxel blocks of the weight gradient: 2 x 4 x 16 voxels, with a one-voxel halo.
 constexpr int TZ = 2, TY = 4, TX = 16, HZ = TZ + 2, HY = TY + 2, HX = TX + 2, HV = HZ * HY * HX;
 
-template <int NT>
-__global__ void __launch_bounds__(128) k_conv3t(const float *__restrict__ X, int Cin, const uint2 *__restrict__ Wp,
-                                                int Cout, const float *__restrict__ bias,
-                                                const float *__restrict__ add, int relu, int accumulate,
-                                                float *__restrict__ Y, Shape s)
-{
-    __shared__ __align__(16) uint2 tile[HV * 4];  // per voxel 16 BF16 channels = 4 x uint2
-    const uint32_t *tw = reinterpret_cast<const uint32_t *>(tile);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, tq = lane & 3;
-    const int ntx = (s.W + TX - 1) / TX, nty = (s.H + TY - 1) / TY, ntz = (s.D + TZ - 1) / TZ;
-    int t = blockIdx.x;
-    const int bx = t % ntx;
-    t /= ntx;
-    const int by = t % nty;
-    t /= nty;
-    const int bz = t % ntz;
-    const int b = t / ntz;
-    const int x0 = bx * TX, y0 = by * TY, z0 = bz * TZ;
-    const int nt0 = blockIdx.y * NT, ntiles = Cout / 8, KC = Cin / 16;
-    float acc[2][NT][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int j = 0; j < NT; j++) acc[mt][j][0] = acc[mt][j][1] = acc[mt][j][2] = acc[mt][j][3] = 0.0f;
-    for (int kc = 0; kc < KC; kc++) {
-        __syncthreads();  // the previous chunk's tile is consumed
-        for (int q = threadIdx.x; q < HV * 4; q += blockDim.x) {
-            const int v = q >> 2, part = q & 3;
-            const int lx = v % HX, ly = (v / HX) % HY, lz = v / (HX * HY);
-            const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
-                f = __ldg(reinterpret_cast<const float4 *>(
-                    X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
-            tile[q] = make_uint2(pack_bf16(f.x, f.y), pack_bf16(f.z, f.w));
-        }
-        __syncthreads();
-        for (int tap = 0; tap < 27; tap++) {
-            const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-            const uint2 *wp = Wp + ((size_t)(tap * KC + kc) * ntiles + nt0) * 32 + lane;
-            uint2 bb[NT];
-#pragma unroll
-            for (int j = 0; j < NT; j++) bb[j] = __ldg(wp + j * 32);
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++) {
-                const int m = warp * 2 + mt;  // m-tile: output row (oz, oy), x = 0..15
-                const int oz = m / TY, oy = m % TY;
-                const int vb = ((oz + 1 + dz) * HY + (oy + 1 + dy)) * HX + 1 + dx;
-                const uint32_t *r0 = tw + (size_t)(vb + g) * 8, *r1 = tw + (size_t)(vb + g + 8) * 8;
-                const uint32_t a0 = r0[tq], a1 = r1[tq], a2 = r0[4 + tq], a3 = r1[4 + tq];
-#pragma unroll
-                for (int j = 0; j < NT; j++) mma_bf16(acc[mt][j], a0, a1, a2, a3, bb[j].x, bb[j].y);
-            }
-        }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-        const int m = warp * 2 + mt;
-        const int oz = m / TY, oy = m % TY;
-        const int z = z0 + oz, y = y0 + oy;
-        if (z >= s.D || y >= s.H) continue;
-        for (int r = 0; r < 2; r++) {
-            const int x = x0 + g + 8 * r;
-            if (x >= s.W) continue;
-            const size_t mo = (((size_t)b * s.D + z) * s.H + y) * s.W + x;
-#pragma unroll
-            for (int j = 0; j < NT; j++) {
-                const int n = (nt0 + j) * 8 + 2 * tq;
-                float v0 = acc[mt][j][2 * r], v1 = acc[mt][j][2 * r + 1];
-                if (bias) {
-                    v0 += bias[n];
-                    v1 += bias[n + 1];
-                }
-                float2 *yp = reinterpret_cast<float2 *>(Y + mo * Cout + n);
-                if (add) {
-                    const float2 a = *reinterpret_cast<const float2 *>(add + mo * Cout + n);
-                    v0 += a.x;
-                    v1 += a.y;
-                }
-                if (relu) {
-                    v0 = fmaxf(v0, 0.0f);
-                    v1 = fmaxf(v1, 0.0f);
-                }
-                if (accumulate) {
-                    const float2 o = *yp;
-                    v0 += o.x;
-                    v1 += o.y;
-                }
-                *yp = make_float2(v0, v1);
-            }
-        }
-    }
-}
+using bf16 = __nv_bfloat16;
+__device__ __forceinline__ float b2f(bf16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ bf16 f2b(float v) { return __float2bfloat16_rn(v); }
 
 // ---------------------------------------------------------------------------
 // Convolution on the 5th-generation tensor cores (tcgen05, accumulators in
@@ -202,23 +106,28 @@ __global__ void __launch_bounds__(128) k_conv3t(const float *__restrict__ X, int
 // groups along M or N, LBO = byte stride between the two 8-element halves
 // of K = 16):
 //   A: the CTA's input block with a one-voxel halo for one 16-channel chunk,
-//      [half h][z][y][x][8 channels] BF16 (AZ x 18 x 10 voxels per half):
-//      8 consecutive x of one (z, y) row are one core matrix, the next y row
-//      is SBO = 160 B on, the other channel half LBO = one half-plane on.  A
-//      tap (dz, dy, dx) is the same layout started (dz, dy, dx) voxels away,
-//      so all 27 taps read the one staged block (no im2col copy);
+//      [half h][z][y][x][8 channels] BF16 (AZ x 18 x 10 voxels per half),
+//      brought in by two TMA tensor copies per chunk (one per channel half;
+//      the activations are BF16 channels-last, and a box {8 channels, 10 x,
+//      18 y, AZ z, 1 batch} lands exactly in that layout, zeros outside the
+//      volume): 8 consecutive x of one (z, y) row are one core matrix, the
+//      next y row is SBO = 160 B on, the other channel half LBO = one
+//      half-block on.  A tap (dz, dy, dx) is the same layout started
+//      (dz, dy, dx) voxels away, so all 27 taps read the one block (no im2col);
 //   B: the chunk's weights for all 27 taps, [tap][h][n][8] BF16, packed in
 //      global memory in that order by k_pack_umma and brought in by one bulk
-//      copy (cp.async.bulk, completion counted on an mbarrier).
-// The block is staged by the CTA's threads (FP32 activations rounded to
-// BF16, zero outside the volume) into one of two buffers while the tensor
-// cores work on the other; one thread issues the MMAs and commits them to a
-// per-buffer mbarrier.  The epilogue reads the accumulators with
-// tcgen05.ld (warp w: rows 32w..32w+31), adds bias / skip input, applies
-// ReLU or accumulates, and writes FP32 channels-last.  Every wait is bounded
-// (1 s of global time); a wait that runs out sets *err and the kernel skips
-// its remaining MMAs, waits (bounded) for those in flight and frees its
-// tensor memory.
+//      copy.
+// One thread drives the pipeline: per chunk it waits until the MMAs that
+// last used the stage's buffers are done, starts the chunk's three copies
+// on the stage's mbarrier (byte count), waits for them and issues the
+// chunk's MMAs, committed to the stage's MMA mbarrier; the copies of chunk
+// k + 1 thus run while the tensor cores work on chunk k (NS = 2 stages; one
+// for 128 output channels, whose weights fill most of shared memory).  The
+// epilogue reads the accumulators with tcgen05.ld (warp w: rows
+// 32w..32w+31), adds bias and skip input, applies ReLU or accumulates, and
+// writes BF16 channels-last.  Every wait is bounded (1 s of global time);
+// one that runs out sets *err, nothing more is issued, the copies and MMAs
+// in flight are waited for (bounded again) and the tensor memory is freed.
 constexpr int UX = 8, UY = 16, UZT = 2, UHX = UX + 2, UHY = UY + 2, UAZ = UZT + 2;
 constexpr int kUmmaHalf = UAZ * UHY * UHX * 16;  // bytes of one channel half of the staged block
 
@@ -261,24 +170,33 @@ __host__ __device__ constexpr uint32_t umma_idesc(int n)
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
-template <int N, int NB>
-__global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, int Cin,
-                                                   const __nv_bfloat16 *__restrict__ Wu,
-                                                   const float *__restrict__ bias, const float *__restrict__ add,
-                                                   int relu, int accumulate, float *__restrict__ Y, Shape s,
-                                                   int *__restrict__ err)
+// tile copy of a 5-D box of tensor map tm at (c0..c4) into shared memory,
+// completion counted in bytes on bar
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+        : "memory");
+}
+
+template <int N, int NS>
+__global__ void __launch_bounds__(128) k_conv_umma(const __grid_constant__ CUtensorMap tmX, int Cin,
+                                                   const bf16 *__restrict__ Wu, const float *__restrict__ bias,
+                                                   const bf16 *__restrict__ add, int relu, int accumulate,
+                                                   bf16 *__restrict__ Y, Shape s, int *__restrict__ err)
 {
     constexpr int kBBytes = 27 * N * 32;  // one chunk's weights
+    constexpr int kStage = 2 * kUmmaHalf + kBBytes;
     constexpr uint32_t kCols = UZT * N < 32 ? 32 : UZT * N;
-    extern __shared__ __align__(128) uint8_t usm[];
-    // A buffers: min(chunks, 2) x [2 halves][kUmmaHalf]; then the B buffers
-    // (the host sizes the dynamic shared memory the same way)
-    const int nA = Cin / 16 < 2 ? 1 : 2;
-    uint8_t *As = usm;
-    uint8_t *Bs = usm + (size_t)nA * 2 * kUmmaHalf;  // [min(chunks, NB)][kBBytes]
-    __shared__ __align__(8) uint64_t bar_w[2], bar_mma[2];
+    extern __shared__ __align__(128) uint8_t usm_raw[];
+    // stages [NS][A halves | B], from a 128-byte aligned base (tensor copies)
+    uint8_t *usm = usm_raw + ((128u - (smem_addr(usm_raw) & 127u)) & 127u);
+    __shared__ __align__(8) uint64_t bar_full[NS], bar_mma[NS];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_bad;
+    __shared__ int s_ok;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntx = (s.W + UX - 1) / UX, nty = (s.H + UY - 1) / UY, ntz = (s.D + UZT - 1) / UZT;
     int t = blockIdx.x;
@@ -297,114 +215,86 @@ __global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, 
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int q = 0; q < 2; q++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar_w[q])));
+        for (int q = 0; q < NS; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar_full[q])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar_mma[q])));
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_bad = 0;
+        s_ok = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    constexpr uint32_t idesc = umma_idesc(N);
-    int committed = 0;  // chunks whose MMAs thread 0 committed
 
-    for (int kc = 0; kc < KC; kc++) {
-        const int sa = kc & 1, sb = NB == 2 ? (kc & 1) : 0;
-        // the A buffer is free once chunk kc - 2's MMAs are done (after a
-        // failed wait nothing more is issued, and nothing more is waited for)
-        if (kc >= 2 && !*(volatile int *)&s_bad && !mbar_wait(&bar_mma[sa], ((kc - 2) >> 1) & 1))
-            atomicOr(&s_bad, 1);
-        if (tid == 0 && !*(volatile int *)&s_bad) {
-            // the B buffer: free after chunk kc - NB's MMAs
-            bool ok = true;
-            if (NB == 1 && kc >= 1) ok = mbar_wait(&bar_mma[(kc - 1) & 1], ((kc - 1) >> 1) & 1);
-            if (!ok) {
-                s_bad = 1;
-            } else {
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar_w[sb])),
-                             "r"((uint32_t)kBBytes)
-                             : "memory");
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        smem_addr(Bs + (size_t)sb * kBBytes)),
-                    "l"(Wu + (size_t)kc * 27 * N * 16), "r"((uint32_t)kBBytes), "r"(smem_addr(&bar_w[sb]))
-                    : "memory");
+    if (tid == 0) {
+        constexpr uint32_t idesc = umma_idesc(N);
+        bool ok = true;
+        int committed = 0, started = 0;  // chunks whose MMAs were committed / copies started
+        for (int kc = 0; kc < KC && ok; kc++) {
+            const int st = kc % NS;
+            const uint32_t use = (uint32_t)(kc / NS);  // earlier chunks on this stage
+            // the stage's buffers are free once the MMAs of its last chunk are done
+            if (use > 0 && !mbar_wait(&bar_mma[st], (use - 1) & 1)) {
+                ok = false;
+                break;
             }
-        }
-        // stage the input block of chunk kc: per voxel 16 channels = 4 float4
-        uint8_t *Ab = As + (size_t)sa * 2 * kUmmaHalf;
-        // four loads in flight per thread before their conversions and stores
-        constexpr int kStage = UAZ * UHY * UHX * 4, kU = 4;
-        for (int q0 = tid; q0 < kStage; q0 += 128 * kU) {
-            float4 f[kU];
-#pragma unroll
-            for (int u = 0; u < kU; u++) {
-                const int q = q0 + u * 128;
-                const int v = q >> 2, part = q & 3;
-                const int lx = v % UHX, ly = (v / UHX) % UHY, lz = v / (UHX * UHY);
-                const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-                f[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (q < kStage && x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
-                    f[u] = __ldg(reinterpret_cast<const float4 *>(
-                        X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + kc * 16 + part * 4));
+            uint8_t *Ab = usm + (size_t)st * kStage, *Bb = Ab + 2 * kUmmaHalf;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar_full[st])),
+                         "r"((uint32_t)kStage)
+                         : "memory");
+            tma_load_5d(Ab, &tmX, kc * 16, x0 - 1, y0 - 1, z0 - 1, b, &bar_full[st]);
+            tma_load_5d(Ab + kUmmaHalf, &tmX, kc * 16 + 8, x0 - 1, y0 - 1, z0 - 1, b, &bar_full[st]);
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(Bb)),
+                "l"(Wu + (size_t)kc * 27 * N * 16), "r"((uint32_t)kBBytes), "r"(smem_addr(&bar_full[st]))
+                : "memory");
+            started = kc + 1;
+            if (!mbar_wait(&bar_full[st], use & 1)) {
+                ok = false;
+                break;
             }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(Ab), b0 = smem_addr(Bb);
+            for (int tap = 0; tap < 27; tap++) {
+                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                const uint64_t bd = umma_sdesc(b0 + (uint32_t)tap * N * 32, N * 16, 128);
 #pragma unroll
-            for (int u = 0; u < kU; u++) {
-                const int q = q0 + u * 128;
-                if (q >= kStage) break;
-                const int v = q >> 2, part = q & 3;
-                // channels 4 part .. 4 part + 3: half part / 2, offset 4 (part & 1)
-                uint2 *dst = reinterpret_cast<uint2 *>(Ab + (size_t)(part >> 1) * kUmmaHalf + (size_t)v * 16 +
-                                                       (part & 1) * 8);
-                *dst = make_uint2(pack_bf16(f[u].x, f[u].y), pack_bf16(f[u].z, f[u].w));
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0 && !*(volatile int *)&s_bad) {
-            if (!mbar_wait(&bar_w[sb], (uint32_t)((kc / NB) & 1))) {
-                s_bad = 1;
-            } else {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t a0 = smem_addr(Ab), b0 = smem_addr(Bs + (size_t)sb * kBBytes);
-                for (int tap = 0; tap < 27; tap++) {
-                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                    const uint64_t bd = umma_sdesc(b0 + (uint32_t)tap * N * 32, N * 16, 128);
-#pragma unroll
-                    for (int m = 0; m < UZT; m++) {
-                        const uint32_t aoff = (uint32_t)((((m + dz) * UHY + dy) * UHX + dx) * 16);
-                        const uint64_t ad = umma_sdesc(a0 + aoff, kUmmaHalf, UHX * 16);
-                        const uint32_t acc = (kc > 0 || tap > 0) ? 1u : 0u;
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + m * N),
-                            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                            : "memory");
-                    }
+                for (int m = 0; m < UZT; m++) {
+                    const uint32_t aoff = (uint32_t)((((m + dz) * UHY + dy) * UHX + dx) * 16);
+                    const uint64_t ad = umma_sdesc(a0 + aoff, kUmmaHalf, UHX * 16);
+                    const uint32_t acc = (kc > 0 || tap > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + m * N),
+                        "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                        : "memory");
                 }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_addr(&bar_mma[sa]))
-                             : "memory");
-                committed = kc + 1;
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&bar_mma[st]))
+                         : "memory");
+            committed = kc + 1;
         }
+        // the last committed MMAs (they complete in order); on a failure also
+        // the copies of a chunk started but not multiplied, so that nothing
+        // writes this CTA's shared memory after it exits
+        if (committed > 0) {
+            const int c = committed - 1;
+            if (!mbar_wait(&bar_mma[c % NS], (uint32_t)(c / NS) & 1)) ok = false;
+        }
+        if (started > committed) {
+            const int c = started - 1;
+            mbar_wait(&bar_full[c % NS], (uint32_t)(c / NS) & 1);
+        }
+        s_ok = ok && committed == KC;
     }
-    // all MMAs done: the last committed chunk's barrier (they complete in order)
-    __shared__ int s_last;
-    if (tid == 0) s_last = committed;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    bool ok = !s_bad && s_last == KC;
-    if (s_last > 0) {
-        const int c = s_last - 1;
-        if (!mbar_wait(&bar_mma[c & 1], (c >> 1) & 1)) ok = false;
-    }
-    ok = __syncthreads_and(ok) != 0;  // the same for every thread (tcgen05.ld is warp-collective)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!ok) {
+    if (!s_ok) {
         if (tid == 0) atomicOr(err, 32);
     } else {
         // epilogue: thread = accumulator row 32 warp + lane = voxel (x0 + r % 8, y0 + r / 8)
@@ -428,23 +318,27 @@ __global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, 
                 float o[8];
 #pragma unroll
                 for (int j = 0; j < 8; j++) o[j] = __uint_as_float(v[j]) + (bias ? bias[c0 + j] : 0.0f);
-                float4 *yp = reinterpret_cast<float4 *>(Y + mo * N + c0);
+                uint4 *yp = reinterpret_cast<uint4 *>(Y + mo * N + c0);  // 8 BF16 channels
                 if (add) {
-                    const float4 a0 = *reinterpret_cast<const float4 *>(add + mo * N + c0);
-                    const float4 a1 = *reinterpret_cast<const float4 *>(add + mo * N + c0 + 4);
-                    o[0] += a0.x, o[1] += a0.y, o[2] += a0.z, o[3] += a0.w;
-                    o[4] += a1.x, o[5] += a1.y, o[6] += a1.z, o[7] += a1.w;
+                    const uint4 a = *reinterpret_cast<const uint4 *>(add + mo * N + c0);
+                    const bf16 *ab = reinterpret_cast<const bf16 *>(&a);
+#pragma unroll
+                    for (int j = 0; j < 8; j++) o[j] += b2f(ab[j]);
                 }
                 if (relu)
 #pragma unroll
                     for (int j = 0; j < 8; j++) o[j] = fmaxf(o[j], 0.0f);
                 if (accumulate) {
-                    const float4 p0 = yp[0], p1 = yp[1];
-                    o[0] += p0.x, o[1] += p0.y, o[2] += p0.z, o[3] += p0.w;
-                    o[4] += p1.x, o[5] += p1.y, o[6] += p1.z, o[7] += p1.w;
+                    const uint4 pv = *yp;
+                    const bf16 *pb = reinterpret_cast<const bf16 *>(&pv);
+#pragma unroll
+                    for (int j = 0; j < 8; j++) o[j] += b2f(pb[j]);
                 }
-                yp[0] = make_float4(o[0], o[1], o[2], o[3]);
-                yp[1] = make_float4(o[4], o[5], o[6], o[7]);
+                uint4 w;
+                uint32_t *wv = reinterpret_cast<uint32_t *>(&w);
+#pragma unroll
+                for (int j = 0; j < 4; j++) wv[j] = pack_bf16(o[2 * j], o[2 * j + 1]);
+                *yp = w;
             }
         }
     }
@@ -458,12 +352,26 @@ __global__ void __launch_bounds__(128) k_conv_umma(const float *__restrict__ X, 
 // kc 16 + 8 h + j (j = 0..7), BF16.  Forward: K = cin, N = cout, element
 // W[tap][k][n]; input gradient: K = cout, N = cin, element W[26 - tap][n][k]
 // (the flipped, transposed kernel).
-__global__ void k_pack_umma(const float *__restrict__ W, int cin, int cout, int flip, __nv_bfloat16 *__restrict__ out)
+// All layers in one launch: segment q packs layer layer[q] (flip[q]: the
+// input-gradient weights) into out + dst[q]; a thread finds its segment by
+// the segments' first element indices (at most 2 kLayers of them).
+struct PackPlan {
+    int nseg;
+    long long first[2 * kLayers + 1];  // segment q: elements [first[q], first[q + 1])
+    long long src[2 * kLayers], dst[2 * kLayers];
+    int cin[2 * kLayers], cout[2 * kLayers], flip[2 * kLayers];
+};
+
+__global__ void k_pack_umma(const float *__restrict__ params, bf16 *__restrict__ out, const PackPlan plan)
 {
-    const int K = flip ? cout : cin, N = flip ? cin : cout;
-    const long long total = 27LL * K * N;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= plan.first[plan.nseg]) return;
+    int q = 0;
+    while (g >= plan.first[q + 1]) q++;
+    const long long i = g - plan.first[q];
+    const int cin = plan.cin[q], cout = plan.cout[q], flip = plan.flip[q];
+    const int N = flip ? cin : cout;
+    const float *W = params + plan.src[q];
     const int j = (int)(i % 8);
     long long r = i / 8;
     const int n = (int)(r % N);
@@ -474,7 +382,7 @@ __global__ void k_pack_umma(const float *__restrict__ W, int cin, int cout, int 
     const int kc = (int)(r / 27);
     const int k = kc * 16 + h * 8 + j;
     const float v = flip ? W[((size_t)(26 - tap) * cin + n) * cout + k] : W[((size_t)tap * cin + k) * cout + n];
-    out[i] = __float2bfloat16_rn(v);
+    out[plan.dst[q] + i] = f2b(v);
 }
 
 // Weight gradient, tiled: a CTA owns one 16-channel input chunk and NT
@@ -487,8 +395,8 @@ __global__ void k_pack_umma(const float *__restrict__ W, int cin, int cout, int 
 constexpr int kWgWarps = 9;
 
 template <int NT>
-__global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restrict__ X, int Cin,
-                                                          const float *__restrict__ dY, int Cout,
+__global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const bf16 *__restrict__ X, int Cin,
+                                                          const bf16 *__restrict__ dY, int Cout,
                                                           float *__restrict__ dW, float *__restrict__ part, Shape s)
 {
     __shared__ __align__(16) __nv_bfloat16 xs[2][16][HV];
@@ -517,16 +425,15 @@ __global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restri
             const int v = q >> 2, part = q & 3;
             const int lx = v % HX, ly = (v / HX) % HY, lz = v / (HX * HY);
             const int x = x0 + lx - 1, y = y0 + ly - 1, z = z0 + lz - 1;
-            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            uint2 f = make_uint2(0u, 0u);  // four BF16 channels
             if (x >= 0 && x < s.W && y >= 0 && y < s.H && z >= 0 && z < s.D)
-                f = __ldg(reinterpret_cast<const float4 *>(
+                f = __ldg(reinterpret_cast<const uint2 *>(
                     X + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cin + ci0 + part * 4));
-            const float fv[4] = {f.x, f.y, f.z, f.w};
+            const bf16 *fv = reinterpret_cast<const bf16 *>(&f);
 #pragma unroll
             for (int c = 0; c < 4; c++) {
-                const __nv_bfloat16 h = __float2bfloat16_rn(fv[c]);
-                xs[0][part * 4 + c][v] = h;
-                if (v > 0) xs[1][part * 4 + c][v - 1] = h;
+                xs[0][part * 4 + c][v] = fv[c];
+                if (v > 0) xs[1][part * 4 + c][v - 1] = fv[c];
             }
             if (v == HV - 1)
 #pragma unroll
@@ -536,14 +443,15 @@ __global__ void __launch_bounds__(32 * kWgWarps) k_wgrad3t(const float *__restri
             const int i = q / (NT * 2), part = q % (NT * 2);  // block voxel, 4 output channels
             const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
             const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-            float4 f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            uint2 f = make_uint2(0u, 0u);
             if (x < s.W && y < s.H && z < s.D)
-                f = __ldg(reinterpret_cast<const float4 *>(
+                f = __ldg(reinterpret_cast<const uint2 *>(
                     dY + ((((size_t)b * s.D + z) * s.H + y) * s.W + x) * Cout + co0 + part * 4));
-            ys[part * 4 + 0][i] = __float2bfloat16_rn(f.x);
-            ys[part * 4 + 1][i] = __float2bfloat16_rn(f.y);
-            ys[part * 4 + 2][i] = __float2bfloat16_rn(f.z);
-            ys[part * 4 + 3][i] = __float2bfloat16_rn(f.w);
+            const bf16 *fv = reinterpret_cast<const bf16 *>(&f);
+            ys[part * 4 + 0][i] = fv[0];
+            ys[part * 4 + 1][i] = fv[1];
+            ys[part * 4 + 2][i] = fv[2];
+            ys[part * 4 + 3][i] = fv[3];
         }
         __syncthreads();
         const uint32_t *yw = reinterpret_cast<const uint32_t *>(&ys[0][0]);
@@ -613,7 +521,7 @@ __global__ void k_wgrad_reduce(const float *__restrict__ part, int nx, int n, fl
 // db[c] += sum over voxels of dY[m][c]
 // (blockDim 256, C <= 256 and dividing 256: the block's lanes of a channel
 // are summed in shared memory first, one atomic per channel per block)
-__global__ void __launch_bounds__(256) k_bias_grad(const float *__restrict__ dY, int C, long long M, long long chunk,
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16 *__restrict__ dY, int C, long long M, long long chunk,
                                                    float *__restrict__ db)
 {
     __shared__ float red[256];
@@ -625,12 +533,12 @@ __global__ void __launch_bounds__(256) k_bias_grad(const float *__restrict__ dY,
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
     long long m = start + l;
     for (; m + 3 * lanes < end; m += 4 * lanes) {
-        a0 += dY[(size_t)m * C + c];
-        a1 += dY[(size_t)(m + lanes) * C + c];
-        a2 += dY[(size_t)(m + 2 * lanes) * C + c];
-        a3 += dY[(size_t)(m + 3 * lanes) * C + c];
+        a0 += b2f(dY[(size_t)m * C + c]);
+        a1 += b2f(dY[(size_t)(m + lanes) * C + c]);
+        a2 += b2f(dY[(size_t)(m + 2 * lanes) * C + c]);
+        a3 += b2f(dY[(size_t)(m + 3 * lanes) * C + c]);
     }
-    for (; m < end; m += lanes) a0 += dY[(size_t)m * C + c];
+    for (; m < end; m += lanes) a0 += b2f(dY[(size_t)m * C + c]);
     float acc = (a0 + a1) + (a2 + a3);
     red[threadIdx.x] = acc;
     __syncthreads();
@@ -640,126 +548,146 @@ __global__ void __launch_bounds__(256) k_bias_grad(const float *__restrict__ dY,
     }
 }
 
-// Packed B fragments of a layer: forward (K = cin, N = cout, element
-// W[tap][k][n]) or input gradient (K = cout, N = cin, element
-// W[26 - tap][n][k]: the flipped, transposed kernel).
-__global__ void k_pack(const float *__restrict__ W, int cin, int cout, int flip, uint2 *__restrict__ out)
+// Elementwise kernels over groups of 8 BF16 channels (16 bytes; every
+// tensor has a multiple of 16 channels): thread q handles channels
+// 8 (q mod C/8) .. + 7 of voxel q / (C/8).
+struct V8 {
+    float v[8];
+};
+__device__ __forceinline__ V8 ld8(const bf16 *p)
 {
-    const int K = flip ? cout : cin, N = flip ? cin : cout;
-    const int KC = K / 16, NTL = N / 8;
-    const long long total = 27LL * KC * NTL * 32;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    const int lane = (int)(i % 32);
-    long long r = i / 32;
-    const int nt = (int)(r % NTL);
-    r /= NTL;
-    const int kc = (int)(r % KC);
-    const int tap = (int)(r / KC);
-    const int g = lane >> 2, tq = lane & 3;
-    const int n = nt * 8 + g, k = kc * 16 + 2 * tq;
-    auto val = [&](int kk) {
-        return flip ? W[((size_t)(26 - tap) * cin + n) * cout + kk] : W[((size_t)tap * cin + kk) * cout + n];
-    };
-    out[i] = make_uint2(pack_bf16(val(k), val(k + 1)), pack_bf16(val(k + 8), val(k + 9)));
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const bf16 *b = reinterpret_cast<const bf16 *>(&u);
+    V8 r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) r.v[j] = b2f(b[j]);
+    return r;
+}
+__device__ __forceinline__ void st8(bf16 *p, const V8 &r)
+{
+    uint4 u;
+    uint32_t *w = reinterpret_cast<uint32_t *>(&u);
+#pragma unroll
+    for (int j = 0; j < 4; j++) w[j] = pack_bf16(r.v[2 * j], r.v[2 * j + 1]);
+    *reinterpret_cast<uint4 *>(p) = u;
 }
 
-// dA *= (A > 0): the ReLU's gradient mask
-__global__ void k_relu_mask(float *__restrict__ dA, const float *__restrict__ A, long long n)
+// dA *= (A > 0): the ReLU's gradient mask (n: elements, a multiple of 8)
+__global__ void k_relu_mask(bf16 *__restrict__ dA, const bf16 *__restrict__ A, long long n)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && !(A[i] > 0.0f)) dA[i] = 0.0f;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q * 8 >= n) return;
+    const V8 a = ld8(A + q * 8);
+    V8 d = ld8(dA + q * 8);
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        if (!(a.v[j] > 0.0f)) d.v[j] = 0.0f;
+    st8(dA + q * 8, d);
 }
 
 // 2 x 2 x 2 average pooling; forward fine -> coarse, backward coarse -> fine
-// (accumulate adds to the fine gradient)
-__global__ void k_pool(const float *__restrict__ X, float *__restrict__ Y, Shape c, int C)
+// (accumulate adds to the fine gradient); FP32 sums of BF16 values
+__global__ void k_pool(const bf16 *__restrict__ X, bf16 *__restrict__ Y, Shape c, int C)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.voxels() * C) return;
-    const int ch = (int)(i % C);
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = C / 8;
+    if (q >= c.voxels() * G) return;
+    const int ch = (int)(q % G) * 8;
     int b, z, y, x;
-    decode(c, i / C, b, z, y, x);
+    decode(c, q / G, b, z, y, x);
     const Shape f{c.B, 2 * c.D, 2 * c.H, 2 * c.W};
-    float s = 0.0f;
-    for (int q = 0; q < 8; q++) {
-        const int zz = 2 * z + (q >> 2), yy = 2 * y + ((q >> 1) & 1), xx = 2 * x + (q & 1);
-        s += X[((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch];
+    V8 s{};
+    for (int k = 0; k < 8; k++) {
+        const int zz = 2 * z + (k >> 2), yy = 2 * y + ((k >> 1) & 1), xx = 2 * x + (k & 1);
+        const V8 a = ld8(X + ((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch);
+#pragma unroll
+        for (int j = 0; j < 8; j++) s.v[j] += a.v[j];
     }
-    Y[i] = 0.125f * s;
+#pragma unroll
+    for (int j = 0; j < 8; j++) s.v[j] *= 0.125f;
+    st8(Y + q * 8, s);
 }
 
-__global__ void k_pool_bwd(const float *__restrict__ dY, float *__restrict__ dX, Shape f, int C, int accumulate)
+__global__ void k_pool_bwd(const bf16 *__restrict__ dY, bf16 *__restrict__ dX, Shape f, int C, int accumulate)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= f.voxels() * C) return;
-    const int ch = (int)(i % C);
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = C / 8;
+    if (q >= f.voxels() * G) return;
+    const int ch = (int)(q % G) * 8;
     int b, z, y, x;
-    decode(f, i / C, b, z, y, x);
+    decode(f, q / G, b, z, y, x);
     const Shape c{f.B, f.D / 2, f.H / 2, f.W / 2};
-    const float v = 0.125f * dY[((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch];
-    dX[i] = accumulate ? dX[i] + v : v;
+    V8 v = ld8(dY + ((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch);
+    const V8 o = accumulate ? ld8(dX + q * 8) : V8{};
+#pragma unroll
+    for (int j = 0; j < 8; j++) v.v[j] = 0.125f * v.v[j] + o.v[j];
+    st8(dX + q * 8, v);
 }
 
 // nearest-neighbour x2 up-sampling; backward sums the 8 fine gradients
-__global__ void k_up(const float *__restrict__ X, float *__restrict__ Y, Shape f, int C)
+__global__ void k_up(const bf16 *__restrict__ X, bf16 *__restrict__ Y, Shape f, int C)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= f.voxels() * C) return;
-    const int ch = (int)(i % C);
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = C / 8;
+    if (q >= f.voxels() * G) return;
+    const int ch = (int)(q % G) * 8;
     int b, z, y, x;
-    decode(f, i / C, b, z, y, x);
+    decode(f, q / G, b, z, y, x);
     const Shape c{f.B, f.D / 2, f.H / 2, f.W / 2};
-    Y[i] = X[((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch];
+    *reinterpret_cast<uint4 *>(Y + q * 8) =
+        *reinterpret_cast<const uint4 *>(X + ((((size_t)b * c.D + z / 2) * c.H + y / 2) * c.W + x / 2) * C + ch);
 }
 
-__global__ void k_up_bwd(const float *__restrict__ dY, float *__restrict__ dX, Shape c, int C)
+__global__ void k_up_bwd(const bf16 *__restrict__ dY, bf16 *__restrict__ dX, Shape c, int C)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.voxels() * C) return;
-    const int ch = (int)(i % C);
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = C / 8;
+    if (q >= c.voxels() * G) return;
+    const int ch = (int)(q % G) * 8;
     int b, z, y, x;
-    decode(c, i / C, b, z, y, x);
+    decode(c, q / G, b, z, y, x);
     const Shape f{c.B, 2 * c.D, 2 * c.H, 2 * c.W};
-    float s = 0.0f;
-    for (int q = 0; q < 8; q++) {
-        const int zz = 2 * z + (q >> 2), yy = 2 * y + ((q >> 1) & 1), xx = 2 * x + (q & 1);
-        s += dY[((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch];
+    V8 s{};
+    for (int k = 0; k < 8; k++) {
+        const int zz = 2 * z + (k >> 2), yy = 2 * y + ((k >> 1) & 1), xx = 2 * x + (k & 1);
+        const V8 a = ld8(dY + ((((size_t)b * f.D + zz) * f.H + yy) * f.W + xx) * C + ch);
+#pragma unroll
+        for (int j = 0; j < 8; j++) s.v[j] += a.v[j];
     }
-    dX[i] = s;
+    st8(dX + q * 8, s);
 }
 
 // network input: channel 0 = s * in, channels 1..15 = 0
-__global__ void k_input(const float *__restrict__ in, float s, float *__restrict__ X0, long long M)
+__global__ void k_input(const float *__restrict__ in, float s, bf16 *__restrict__ X0, long long M)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M * 16) return;
-    X0[i] = (i % 16) == 0 ? s * in[i / 16] : 0.0f;
+    X0[i] = f2b((i % 16) == 0 ? s * in[i / 16] : 0.0f);
 }
 
 // out = in + r / s (r = channel 0 of the last layer)
-__global__ void k_output(const float *__restrict__ in, const float *__restrict__ Z, float s, float *__restrict__ out,
+__global__ void k_output(const float *__restrict__ in, const bf16 *__restrict__ Z, float s, float *__restrict__ out,
                          long long M)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M) out[i] = in[i] + Z[(size_t)i * 16] / s;
+    if (i < M) out[i] = in[i] + b2f(Z[(size_t)i * 16]) / s;
 }
 
 // loss = mean (s in + r - s t)^2; dZ channel 0 = its gradient, others 0;
 // per-block partial sums (FP64) into part
 __global__ void __launch_bounds__(256) k_loss(const float *__restrict__ in, const float *__restrict__ t,
-                                              const float *__restrict__ Z, float s, float *__restrict__ dZ,
+                                              const bf16 *__restrict__ Z, float s, bf16 *__restrict__ dZ,
                                               long long M, double *__restrict__ part)
 {
     __shared__ double red[256];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double l = 0.0;
     if (i < M) {
-        const float d = s * in[i] + Z[(size_t)i * 16] - s * t[i];
+        const float d = s * in[i] + b2f(Z[(size_t)i * 16]) - s * t[i];
         l = (double)d * d;
-        float *g = dZ + (size_t)i * 16;
-        g[0] = 2.0f * d / (float)M;
-        for (int c = 1; c < 16; c++) g[c] = 0.0f;
+        bf16 *g = dZ + (size_t)i * 16;
+        g[0] = f2b(2.0f * d / (float)M);
+        for (int c = 1; c < 16; c++) g[c] = f2b(0.0f);
     }
     red[threadIdx.x] = l;
     __syncthreads();
@@ -829,17 +757,21 @@ static int net_fail(const char *msg, cudaError_t e = cudaSuccess)
         if (_e != cudaSuccess) return net_fail(#call, _e);                   \
     } while (0)
 
+// A BF16 channels-last activation or gradient tensor and the tensor map the
+// convolutions read it through (box {8 channels, 10 x, 18 y, 4 z, 1 batch})
 struct NetTensor {
-    float *p = nullptr;
+    bf16 *p = nullptr;
     size_t n = 0;
+    int C = 0;
+    CUtensorMap tm;
 };
 
 struct MbirNet {
-    size_t w_off[kLayers], b_off[kLayers], nparams = 0, pack_off[kLayers], dpack_off[kLayers], npack = 0;
+    size_t w_off[kLayers], b_off[kLayers], nparams = 0;
     float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
-    uint2 *pack = nullptr;  // forward and input-gradient fragments of every layer (mma.sync)
-    // the same weights in the tensor-core layout of k_conv_umma (BF16)
-    __nv_bfloat16 *upack = nullptr;
+    // the weights in the tensor-core layout of k_conv_umma (BF16), forward and
+    // input-gradient (flipped, transposed) per layer
+    bf16 *upack = nullptr;
     size_t upack_off[kLayers], udpack_off[kLayers], nupack = 0;
     int *d_err = nullptr;  // wait time-outs of the tensor-core convolution (bit 32)
     float *wg_part = nullptr;  // per-CTA weight-gradient sums (kWgPartFloats)
@@ -851,8 +783,8 @@ struct MbirNet {
     size_t npart = 0;
     ~MbirNet()
     {
-        for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)pack, (void *)part,
-                        (void *)upack, (void *)d_err, (void *)wg_part})
+        for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)part, (void *)upack,
+                        (void *)d_err, (void *)wg_part})
             if (q) cudaFree(q);
         for (auto &t : act)
             if (t.p) cudaFree(t.p);
@@ -885,6 +817,42 @@ static void slot_info(int t, int &lv, int &C)
     }
 }
 
+// cuTensorMapEncodeTiled from the driver (no link against libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of a BF16 channels-last tensor [B][D][H][W][C] for the
+// convolution's input boxes {8 channels, UHX, UHY, UAZ, 1}; zeros outside.
+static int make_tmap(CUtensorMap *m, const bf16 *p, const Shape &s, int C)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    if (!enc) return net_fail("cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[5] = {(cuuint64_t)C, (cuuint64_t)s.W, (cuuint64_t)s.H, (cuuint64_t)s.D, (cuuint64_t)s.B};
+    const cuuint64_t e = sizeof(bf16);
+    const cuuint64_t strides[4] = {C * e, (cuuint64_t)s.W * C * e, (cuuint64_t)s.H * s.W * C * e,
+                                   (cuuint64_t)s.D * s.H * s.W * C * e};
+    const cuuint32_t box[5] = {8, UHX, UHY, UAZ, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(p), dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(g_net_err, sizeof g_net_err, "cuTensorMapEncodeTiled failed (%d) for a %d-channel tensor", (int)r, C);
+        return -1;
+    }
+    return 0;
+}
+
 static int net_shape(MbirNet *N, const Shape &s, bool train)
 {
     if (s.B == N->shape.B && s.D == N->shape.D && s.H == N->shape.H && s.W == N->shape.W &&
@@ -903,12 +871,14 @@ static int net_shape(MbirNet *N, const Shape &s, bool train)
     for (int t = 0; t < T_COUNT; t++) {
         int lv, C;
         slot_info(t, lv, C);
-        const size_t n = (size_t)level_shape(s, lv).voxels() * C;
-        NK(cudaMalloc(&N->act[t].p, n * sizeof(float)));
-        N->act[t].n = n;
-        if (train) {
-            NK(cudaMalloc(&N->grad[t].p, n * sizeof(float)));
-            N->grad[t].n = n;
+        const Shape ls = level_shape(s, lv);
+        const size_t n = (size_t)ls.voxels() * C;
+        for (int g = 0; g < (train ? 2 : 1); g++) {
+            NetTensor &x = g ? N->grad[t] : N->act[t];
+            NK(cudaMalloc(&x.p, n * sizeof(bf16)));
+            x.n = n;
+            x.C = C;
+            if (make_tmap(&x.tm, x.p, ls, C)) return -1;
         }
     }
     const size_t np = (size_t)blocks(s.voxels());
@@ -921,66 +891,39 @@ static int net_shape(MbirNet *N, const Shape &s, bool train)
     return 0;
 }
 
-// The convolutions run on tcgen05 (k_conv_umma) unless TIMBIR_NET_CONV=mma
-// selects the mma.sync kernel (k_conv3t), kept for comparison.
-static bool use_umma()
+template <int N, int NS>
+static cudaError_t conv_umma_launch(const NetTensor &X, const bf16 *Wu, const float *bias, const bf16 *add, int relu,
+                                    int accumulate, bf16 *Y, const Shape &s, int *err, cudaStream_t st)
 {
-    static const bool on = [] {
-        const char *e = getenv("TIMBIR_NET_CONV");
-        return !(e && std::string(e) == "mma");
-    }();
-    return on;
-}
-
-template <int N, int NB>
-static cudaError_t conv_umma_launch(const float *X, int cin, const __nv_bfloat16 *Wu, const float *bias,
-                                    const float *add, int relu, int accumulate, float *Y, const Shape &s, int *err,
-                                    cudaStream_t st)
-{
-    // as the kernel carves it: min(chunks, 2) A buffers, min(chunks, NB) B buffers
-    const int kc = cin / 16;
-    const size_t smem = (size_t)std::min(kc, 2) * 2 * kUmmaHalf + (size_t)std::min(kc, NB) * 27 * N * 32;
+    // as the kernel carves it: min(chunks, NS) stages of (two A halves, B), a
+    // 128-byte alignment margin
+    const int kc = X.C / 16;
+    const size_t stage = (size_t)2 * kUmmaHalf + (size_t)27 * N * 32;
+    const size_t smem = (size_t)std::min(kc, NS) * stage + 128;
     static bool attr = false;
     if (!attr) {  // the largest size this instantiation launches with
-        cudaError_t e = cudaFuncSetAttribute(k_conv_umma<N, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(2 * 2 * kUmmaHalf + (size_t)NB * 27 * N * 32));
+        cudaError_t e = cudaFuncSetAttribute(k_conv_umma<N, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(NS * stage + 128));
         if (e != cudaSuccess) return e;
         attr = true;
     }
     const long long tiles =
         (long long)s.B * ((s.D + UZT - 1) / UZT) * ((s.H + UY - 1) / UY) * ((s.W + UX - 1) / UX);
-    k_conv_umma<N, NB><<<(unsigned)tiles, 128, smem, st>>>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err);
+    k_conv_umma<N, NS><<<(unsigned)tiles, 128, smem, st>>>(X.tm, X.C, Wu, bias, add, relu, accumulate, Y, s, err);
     return cudaGetLastError();
 }
 
-static cudaError_t conv_umma(const float *X, int cin, const __nv_bfloat16 *Wu, int cout, const float *bias,
-                             const float *add, int relu, int accumulate, float *Y, const Shape &s, int *err,
-                             cudaStream_t st)
+// Y = conv(X) (+ bias, + add, ReLU), or Y += conv(X); X at shape s
+static cudaError_t conv(const NetTensor &X, const bf16 *Wu, int cout, const float *bias, const bf16 *add, int relu,
+                        int accumulate, bf16 *Y, const Shape &s, int *err, cudaStream_t st)
 {
     switch (cout) {
-    case 16: return conv_umma_launch<16, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
-    case 32: return conv_umma_launch<32, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
-    case 64: return conv_umma_launch<64, 2>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
-    case 128: return conv_umma_launch<128, 1>(X, cin, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 16: return conv_umma_launch<16, 2>(X, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 32: return conv_umma_launch<32, 2>(X, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 64: return conv_umma_launch<64, 2>(X, Wu, bias, add, relu, accumulate, Y, s, err, st);
+    case 128: return conv_umma_launch<128, 1>(X, Wu, bias, add, relu, accumulate, Y, s, err, st);
     default: return cudaErrorInvalidValue;
     }
-}
-
-static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, const float *bias, const float *add,
-                        int relu, int accumulate, float *Y, const Shape &s, cudaStream_t st,
-                        const __nv_bfloat16 *Wu = nullptr, int *err = nullptr)
-{
-    if (Wu && use_umma()) return conv_umma(X, cin, Wu, cout, bias, add, relu, accumulate, Y, s, err, st);
-    const int NT = std::min(cout / 8, 8);
-    const long long tiles = (long long)s.B * ((s.D + TZ - 1) / TZ) * ((s.H + TY - 1) / TY) * ((s.W + TX - 1) / TX);
-    const dim3 grid((unsigned)tiles, (unsigned)(cout / 8 / NT));
-    switch (NT) {
-    case 1: k_conv3t<1><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    case 2: k_conv3t<2><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    case 4: k_conv3t<4><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    default: k_conv3t<8><<<grid, 128, 0, st>>>(X, cin, Wp, cout, bias, add, relu, accumulate, Y, s); break;
-    }
-    return cudaGetLastError();
 }
 
 // Weight gradient: CTAs along x split the voxel blocks; each writes its sums
@@ -988,7 +931,7 @@ static cudaError_t conv(const float *X, int cin, const uint2 *Wp, int cout, cons
 // up to four per SM) and k_wgrad_reduce adds them to dW.
 constexpr size_t kWgPartFloats = 4u << 20;
 
-static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, float *dW, float *db, const Shape &s,
+static cudaError_t wgrad(const bf16 *X, int cin, const bf16 *dY, int cout, float *dW, float *db, const Shape &s,
                          float *part, cudaStream_t st)
 {
     const int NT = std::min(cout / 8, 4);
@@ -1017,27 +960,23 @@ static cudaError_t wgrad(const float *X, int cin, const float *dY, int cout, flo
 
 static int pack_all(MbirNet *N, cudaStream_t st)
 {
-    for (int k = 0; k < kLayers; k++) {
-        const int ci = kCh[k][0], co = kCh[k][1];
-        if (!use_umma()) {  // fragments of the mma.sync convolution
-            const long long nf = 27LL * (ci / 16) * (co / 8) * 32;
-            k_pack<<<blocks(nf), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->pack + N->pack_off[k]);
-            NK(cudaGetLastError());
-            if (k > 0) {
-                const long long nb = 27LL * (co / 16) * (ci / 8) * 32;
-                k_pack<<<blocks(nb), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1, N->pack + N->dpack_off[k]);
-                NK(cudaGetLastError());
-            }
+    PackPlan plan{};
+    long long first = 0;
+    int q = 0;
+    for (int k = 0; k < kLayers; k++)
+        for (int flip = 0; flip < (k > 0 ? 2 : 1); flip++, q++) {
+            plan.first[q] = first;
+            plan.src[q] = (long long)N->w_off[k];
+            plan.dst[q] = (long long)(flip ? N->udpack_off[k] : N->upack_off[k]);
+            plan.cin[q] = kCh[k][0];
+            plan.cout[q] = kCh[k][1];
+            plan.flip[q] = flip;
+            first += 27LL * kCh[k][0] * kCh[k][1];
         }
-        const long long nu = 27LL * ci * co;
-        k_pack_umma<<<blocks(nu), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 0, N->upack + N->upack_off[k]);
-        NK(cudaGetLastError());
-        if (k > 0) {
-            k_pack_umma<<<blocks(nu), 256, 0, st>>>(N->params + N->w_off[k], ci, co, 1,
-                                                    N->upack + N->udpack_off[k]);
-            NK(cudaGetLastError());
-        }
-    }
+    plan.nseg = q;
+    plan.first[q] = first;
+    k_pack_umma<<<blocks(first), 256, 0, st>>>(N->params, N->upack, plan);
+    NK(cudaGetLastError());
     return 0;
 }
 
@@ -1048,32 +987,33 @@ static int forward(MbirNet *N, const float *in, float scale, cudaStream_t st)
     const long long M = s.voxels();
     k_input<<<blocks(M * 16), 256, 0, st>>>(in, scale, A[T_X0].p, M);
     NK(cudaGetLastError());
-    auto L = [&](int k, const float *x, const float *add, int relu, const Shape &sh) {
-        return conv(x, kCh[k][0], N->pack + N->pack_off[k], kCh[k][1], N->params + N->b_off[k], add, relu, 0,
-                    A[T_A0 + k].p, sh, st, N->upack + N->upack_off[k], N->d_err);
+    // layer k from input slot x (with skip input add, ReLU or not) into A[k]
+    auto L = [&](int k, int x, const bf16 *add, int relu, const Shape &sh) {
+        return conv(A[x], N->upack + N->upack_off[k], kCh[k][1], N->params + N->b_off[k], add, relu, 0,
+                    A[T_A0 + k].p, sh, N->d_err, st);
     };
     const Shape s1 = level_shape(s, 1), s2 = level_shape(s, 2), s3 = level_shape(s, 3);
-    NK(L(0, A[T_X0].p, nullptr, 1, s));
-    NK(L(1, A[T_A0 + 0].p, nullptr, 1, s));
-    k_pool<<<blocks(s1.voxels() * 16), 256, 0, st>>>(A[T_A0 + 1].p, A[T_P1].p, s1, 16);
-    NK(L(2, A[T_P1].p, nullptr, 1, s1));
-    NK(L(3, A[T_A0 + 2].p, nullptr, 1, s1));
-    k_pool<<<blocks(s2.voxels() * 32), 256, 0, st>>>(A[T_A0 + 3].p, A[T_P2].p, s2, 32);
-    NK(L(4, A[T_P2].p, nullptr, 1, s2));
-    NK(L(5, A[T_A0 + 4].p, nullptr, 1, s2));
-    k_pool<<<blocks(s3.voxels() * 64), 256, 0, st>>>(A[T_A0 + 5].p, A[T_P3].p, s3, 64);
-    NK(L(6, A[T_P3].p, nullptr, 1, s3));
-    NK(L(7, A[T_A0 + 6].p, nullptr, 1, s3));
-    k_up<<<blocks(s2.voxels() * 128), 256, 0, st>>>(A[T_A0 + 7].p, A[T_U2].p, s2, 128);
-    NK(L(8, A[T_U2].p, A[T_A0 + 5].p, 1, s2));
-    NK(L(9, A[T_A0 + 8].p, nullptr, 1, s2));
-    k_up<<<blocks(s1.voxels() * 64), 256, 0, st>>>(A[T_A0 + 9].p, A[T_U1].p, s1, 64);
-    NK(L(10, A[T_U1].p, A[T_A0 + 3].p, 1, s1));
-    NK(L(11, A[T_A0 + 10].p, nullptr, 1, s1));
-    k_up<<<blocks(s.voxels() * 32), 256, 0, st>>>(A[T_A0 + 11].p, A[T_U0].p, s, 32);
-    NK(L(12, A[T_U0].p, A[T_A0 + 1].p, 1, s));
-    NK(L(13, A[T_A0 + 12].p, nullptr, 1, s));
-    NK(L(14, A[T_A0 + 13].p, nullptr, 0, s));
+    NK(L(0, T_X0, nullptr, 1, s));
+    NK(L(1, T_A0 + 0, nullptr, 1, s));
+    k_pool<<<blocks(s1.voxels() * 2), 256, 0, st>>>(A[T_A0 + 1].p, A[T_P1].p, s1, 16);
+    NK(L(2, T_P1, nullptr, 1, s1));
+    NK(L(3, T_A0 + 2, nullptr, 1, s1));
+    k_pool<<<blocks(s2.voxels() * 4), 256, 0, st>>>(A[T_A0 + 3].p, A[T_P2].p, s2, 32);
+    NK(L(4, T_P2, nullptr, 1, s2));
+    NK(L(5, T_A0 + 4, nullptr, 1, s2));
+    k_pool<<<blocks(s3.voxels() * 8), 256, 0, st>>>(A[T_A0 + 5].p, A[T_P3].p, s3, 64);
+    NK(L(6, T_P3, nullptr, 1, s3));
+    NK(L(7, T_A0 + 6, nullptr, 1, s3));
+    k_up<<<blocks(s2.voxels() * 16), 256, 0, st>>>(A[T_A0 + 7].p, A[T_U2].p, s2, 128);
+    NK(L(8, T_U2, A[T_A0 + 5].p, 1, s2));
+    NK(L(9, T_A0 + 8, nullptr, 1, s2));
+    k_up<<<blocks(s1.voxels() * 8), 256, 0, st>>>(A[T_A0 + 9].p, A[T_U1].p, s1, 64);
+    NK(L(10, T_U1, A[T_A0 + 3].p, 1, s1));
+    NK(L(11, T_A0 + 10, nullptr, 1, s1));
+    k_up<<<blocks(s.voxels() * 4), 256, 0, st>>>(A[T_A0 + 11].p, A[T_U0].p, s, 32);
+    NK(L(12, T_U0, A[T_A0 + 1].p, 1, s));
+    NK(L(13, T_A0 + 12, nullptr, 1, s));
+    NK(L(14, T_A0 + 13, nullptr, 0, s));
     return 0;
 }
 
@@ -1087,16 +1027,16 @@ static int backward(MbirNet *N, cudaStream_t st)
     NK(cudaMemsetAsync(N->grads, 0, N->nparams * sizeof(float), st));
     // layer k: weight and bias gradients from its input x and output
     // gradient dz; the input gradient (into dx, optionally accumulated)
-    auto layer = [&](int k, const float *x, const Shape &sh, float *dx, int acc) -> int {
-        const float *dz = G[T_A0 + k].p;
-        NK(wgrad(x, kCh[k][0], dz, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, N->wg_part, st));
+    auto layer = [&](int k, const bf16 *x, const Shape &sh, bf16 *dx, int acc) -> int {
+        const NetTensor &dz = G[T_A0 + k];
+        NK(wgrad(x, kCh[k][0], dz.p, kCh[k][1], N->grads + N->w_off[k], N->grads + N->b_off[k], sh, N->wg_part,
+                 st));
         if (dx)
-            NK(conv(dz, kCh[k][1], N->pack + N->dpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, st,
-                    N->upack + N->udpack_off[k], N->d_err));
+            NK(conv(dz, N->upack + N->udpack_off[k], kCh[k][0], nullptr, nullptr, 0, acc, dx, sh, N->d_err, st));
         return 0;
     };
     auto mask = [&](int t) -> int {  // dA -> dZ of a ReLU output
-        k_relu_mask<<<blocks((long long)A[t].n), 256, 0, st>>>(G[t].p, A[t].p, (long long)A[t].n);
+        k_relu_mask<<<blocks((long long)A[t].n / 8), 256, 0, st>>>(G[t].p, A[t].p, (long long)A[t].n);
         NK(cudaGetLastError());
         return 0;
     };
@@ -1104,35 +1044,35 @@ static int backward(MbirNet *N, cudaStream_t st)
     if (layer(13, A[T_A0 + 12].p, s, G[T_A0 + 12].p, 0) || mask(T_A0 + 12)) return -1;
     // layer 12: input U0, skip from A1 (its gradient seeds dA1)
     if (layer(12, A[T_U0].p, s, G[T_U0].p, 0)) return -1;
-    NK(cudaMemcpyAsync(G[T_A0 + 1].p, G[T_A0 + 12].p, A[T_A0 + 1].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    k_up_bwd<<<blocks(s1.voxels() * 32), 256, 0, st>>>(G[T_U0].p, G[T_A0 + 11].p, s1, 32);
+    NK(cudaMemcpyAsync(G[T_A0 + 1].p, G[T_A0 + 12].p, A[T_A0 + 1].n * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s1.voxels() * 4), 256, 0, st>>>(G[T_U0].p, G[T_A0 + 11].p, s1, 32);
     NK(cudaGetLastError());
     if (mask(T_A0 + 11)) return -1;
     if (layer(11, A[T_A0 + 10].p, s1, G[T_A0 + 10].p, 0) || mask(T_A0 + 10)) return -1;
     if (layer(10, A[T_U1].p, s1, G[T_U1].p, 0)) return -1;
-    NK(cudaMemcpyAsync(G[T_A0 + 3].p, G[T_A0 + 10].p, A[T_A0 + 3].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    k_up_bwd<<<blocks(s2.voxels() * 64), 256, 0, st>>>(G[T_U1].p, G[T_A0 + 9].p, s2, 64);
+    NK(cudaMemcpyAsync(G[T_A0 + 3].p, G[T_A0 + 10].p, A[T_A0 + 3].n * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s2.voxels() * 8), 256, 0, st>>>(G[T_U1].p, G[T_A0 + 9].p, s2, 64);
     NK(cudaGetLastError());
     if (mask(T_A0 + 9)) return -1;
     if (layer(9, A[T_A0 + 8].p, s2, G[T_A0 + 8].p, 0) || mask(T_A0 + 8)) return -1;
     if (layer(8, A[T_U2].p, s2, G[T_U2].p, 0)) return -1;
-    NK(cudaMemcpyAsync(G[T_A0 + 5].p, G[T_A0 + 8].p, A[T_A0 + 5].n * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    k_up_bwd<<<blocks(s3.voxels() * 128), 256, 0, st>>>(G[T_U2].p, G[T_A0 + 7].p, s3, 128);
+    NK(cudaMemcpyAsync(G[T_A0 + 5].p, G[T_A0 + 8].p, A[T_A0 + 5].n * sizeof(bf16), cudaMemcpyDeviceToDevice, st));
+    k_up_bwd<<<blocks(s3.voxels() * 16), 256, 0, st>>>(G[T_U2].p, G[T_A0 + 7].p, s3, 128);
     NK(cudaGetLastError());
     if (mask(T_A0 + 7)) return -1;
     if (layer(7, A[T_A0 + 6].p, s3, G[T_A0 + 6].p, 0) || mask(T_A0 + 6)) return -1;
     if (layer(6, A[T_P3].p, s3, G[T_P3].p, 0)) return -1;
-    k_pool_bwd<<<blocks(s2.voxels() * 64), 256, 0, st>>>(G[T_P3].p, G[T_A0 + 5].p, s2, 64, 1);
+    k_pool_bwd<<<blocks(s2.voxels() * 8), 256, 0, st>>>(G[T_P3].p, G[T_A0 + 5].p, s2, 64, 1);
     NK(cudaGetLastError());
     if (mask(T_A0 + 5)) return -1;
     if (layer(5, A[T_A0 + 4].p, s2, G[T_A0 + 4].p, 0) || mask(T_A0 + 4)) return -1;
     if (layer(4, A[T_P2].p, s2, G[T_P2].p, 0)) return -1;
-    k_pool_bwd<<<blocks(s1.voxels() * 32), 256, 0, st>>>(G[T_P2].p, G[T_A0 + 3].p, s1, 32, 1);
+    k_pool_bwd<<<blocks(s1.voxels() * 4), 256, 0, st>>>(G[T_P2].p, G[T_A0 + 3].p, s1, 32, 1);
     NK(cudaGetLastError());
     if (mask(T_A0 + 3)) return -1;
     if (layer(3, A[T_A0 + 2].p, s1, G[T_A0 + 2].p, 0) || mask(T_A0 + 2)) return -1;
     if (layer(2, A[T_P1].p, s1, G[T_P1].p, 0)) return -1;
-    k_pool_bwd<<<blocks(s.voxels() * 16), 256, 0, st>>>(G[T_P1].p, G[T_A0 + 1].p, s, 16, 1);
+    k_pool_bwd<<<blocks(s.voxels() * 2), 256, 0, st>>>(G[T_P1].p, G[T_A0 + 1].p, s, 16, 1);
     NK(cudaGetLastError());
     if (mask(T_A0 + 1)) return -1;
     if (layer(1, A[T_A0 + 0].p, s, G[T_A0 + 0].p, 0) || mask(T_A0 + 0)) return -1;
@@ -1168,30 +1108,24 @@ int mbir_net_create(MbirNet **out, uint32_t seed)
 {
     *out = nullptr;
     auto N = std::make_unique<MbirNet>();
-    size_t off = 0, poff = 0;
+    size_t off = 0;
     for (int k = 0; k < kLayers; k++) {
         const int ci = kCh[k][0], co = kCh[k][1];
         N->w_off[k] = off;
         off += 27 * (size_t)ci * co;
         N->b_off[k] = off;
         off += co;
-        N->pack_off[k] = poff;
-        poff += 27 * (size_t)(ci / 16) * (co / 8) * 32;
-        N->dpack_off[k] = poff;
-        if (k > 0) poff += 27 * (size_t)(co / 16) * (ci / 8) * 32;
         N->upack_off[k] = N->nupack;
         N->nupack += 27 * (size_t)ci * co;
         N->udpack_off[k] = N->nupack;
         if (k > 0) N->nupack += 27 * (size_t)ci * co;
     }
     N->nparams = off;
-    N->npack = poff;
     NK(cudaMalloc(&N->params, off * sizeof(float)));
     NK(cudaMalloc(&N->grads, off * sizeof(float)));
     NK(cudaMalloc(&N->m, off * sizeof(float)));
     NK(cudaMalloc(&N->v, off * sizeof(float)));
-    NK(cudaMalloc(&N->pack, poff * sizeof(uint2)));
-    NK(cudaMalloc(&N->upack, N->nupack * sizeof(__nv_bfloat16)));
+    NK(cudaMalloc(&N->upack, N->nupack * sizeof(bf16)));
     NK(cudaMalloc(&N->d_err, sizeof(int)));
     NK(cudaMalloc(&N->wg_part, kWgPartFloats * sizeof(float)));
     NK(cudaMemset(N->d_err, 0, sizeof(int)));
@@ -1245,7 +1179,14 @@ int mbir_net_get_activation(MbirNet *N, int32_t layer, int32_t which, float *out
     if (which == 1 && N->grad.empty()) return net_fail("no gradients computed");
     const NetTensor &x = which == 1 ? N->grad[t] : N->act[t];
     if (count) *count = (int64_t)x.n;
-    if (out) NK(cudaMemcpy(out, x.p, x.n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (out) {  // BF16 on the device; widened to float here
+        std::vector<uint16_t> h(x.n);
+        NK(cudaMemcpy(h.data(), x.p, x.n * sizeof(bf16), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < x.n; i++) {
+            const uint32_t u = (uint32_t)h[i] << 16;
+            memcpy(out + i, &u, sizeof u);
+        }
+    }
     return 0;
 }
 
