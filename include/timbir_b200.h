@@ -379,8 +379,10 @@ int mbir_autotune_stage(MbirStage *stage, int32_t *sv_side, int32_t *warps_per_s
  * A 3-D encoder-decoder convolutional network (4 levels, 16-128 channels,
  * 3x3x3 convolutions, average-pool down, nearest up, additive skips; 1.33 M
  * parameters) mapping a frame's filtered backprojection to an ICD start
- * image: out = in + r(s in) / s.  BF16 weights and operands on the tensor
- * cores with FP32 accumulation; FP32 master parameters and Adam state.
+ * image: out = in + r(s in) / s.  BF16 activations, weights and operands on
+ * the tensor cores (tcgen05, FP32 accumulation in tensor memory); FP32 master
+ * parameters, Adam state and loss.  Activations read back by
+ * mbir_net_get_activation are the BF16 values widened to float.
  * Tensors are device float arrays [B][D][H][W] with D, H, W multiples of 8;
  * stream is a cudaStream_t (NULL: the default stream); calls return after
  * the stream has run them.  No counterpart in the reference. */
