@@ -193,6 +193,20 @@ int mbir_get_offset_windows(MbirStage *stage);
 /* update_variance_parameter (XT_ICD_update.c:720-751). */
 int mbir_update_variance_parameter(MbirStage *stage);
 
+/* ---- fault injection, for testing the error paths (no counterpart) ------
+ * mbir_set_device_bytes_cap: the library's device allocator refuses an
+ * allocation that would take the memory its stages hold above `bytes`, as an
+ * exhausted device would (0: no cap); mbir_get_device_bytes: the bytes held.
+ * mbir_debug_sv_skip_tasks: the next super-voxel sweep of the stage starts
+ * its work queue n entries in, so those super-voxels never run and the ones
+ * ordered after them that conflict with them wait for them until the
+ * kernel's bounded wait gives up (about half a second); the iteration then
+ * returns an error ("dependency wait timed out") and the context stays
+ * usable.  The stage's state afterwards is that of an interrupted sweep. */
+int mbir_set_device_bytes_cap(int64_t bytes);
+int64_t mbir_get_device_bytes(void);
+int mbir_debug_sv_skip_tasks(MbirStage *stage, int32_t n);
+
 /* ---- data ingestion (the drivers' readers, before reconstruct()) --------
  * The HDF5 file access is the caller's; these take the datasets' arrays as
  * the file holds them, [frames][rows][cols] in HOST memory, and select the

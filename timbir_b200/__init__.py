@@ -58,6 +58,9 @@ def load_library() -> C.CDLL:
     lib.mbir_set_offset_windows.argtypes = [_VP, i32]
     lib.mbir_get_offset_windows.argtypes = [_VP]
     lib.mbir_update_variance_parameter.argtypes = [_VP]
+    lib.mbir_set_device_bytes_cap.argtypes = [C.c_int64]
+    lib.mbir_get_device_bytes.restype = C.c_int64
+    lib.mbir_debug_sv_skip_tasks.argtypes = [_VP, i32]
     lib.mbir_set_z_slab.argtypes = [_VP, i32, i32, _ALLREDUCE_FN, _VP]
     lib.mbir_get_slab_faces.argtypes = [_VP, _VP, _VP]
     lib.mbir_set_slab_halo.argtypes = [_VP, _VP, _VP]

@@ -49,9 +49,24 @@ static int fail(const char *fmt, ...)
 // freed memory cached (release threshold raised once per device), so stages
 // set up one after another reuse it instead of paying for fresh allocations.
 // Allocation is stream-ordered on the legacy stream and completed before use.
+// Device memory the stages hold, and an optional cap on it
+// (mbir_set_device_bytes_cap: the allocator refuses what would exceed it,
+// as an exhausted device would; for testing the error paths).
+static std::mutex g_alloc_mu;
+static std::map<void *, size_t> g_alloc_live;
+static size_t g_alloc_bytes = 0, g_alloc_cap = 0;
+
 template <typename T>
 static cudaError_t dalloc(T **p, size_t n)
 {
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    {
+        std::lock_guard<std::mutex> lock(g_alloc_mu);
+        if (g_alloc_cap && g_alloc_bytes + bytes > g_alloc_cap) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
     static bool pool_ready[64] = {false};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -64,8 +79,13 @@ static cudaError_t dalloc(T **p, size_t n)
         }
         pool_ready[dev] = true;
     }
-    e = cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), 0);
+    e = cudaMallocAsync((void **)p, bytes, 0);
     if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(g_alloc_mu);
+        g_alloc_live[(void *)*p] = bytes;
+        g_alloc_bytes += bytes;
+    }
     return cudaStreamSynchronize(0);
 }
 
@@ -74,7 +94,29 @@ static int slab_sum(MbirStage *S, double *v, int n);
 
 static void dfree(void *p)
 {
-    if (p) cudaFreeAsync(p, 0);
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lock(g_alloc_mu);
+        auto it = g_alloc_live.find(p);
+        if (it != g_alloc_live.end()) {
+            g_alloc_bytes -= it->second;
+            g_alloc_live.erase(it);
+        }
+    }
+    cudaFreeAsync(p, 0);
+}
+
+extern "C" int mbir_set_device_bytes_cap(int64_t bytes)
+{
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    g_alloc_cap = bytes > 0 ? (size_t)bytes : 0;
+    return 0;
+}
+
+extern "C" int64_t mbir_get_device_bytes(void)
+{
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    return (int64_t)g_alloc_bytes;
 }
 
 struct MbirStage {
@@ -170,6 +212,10 @@ struct MbirStage {
     // that takes the place of the reference's MPI reductions
     float *d_halo = nullptr;
     int slab_rank = 0, slab_count = 1;
+    // fault injection (mbir_debug_sv_skip_tasks): the next sweep's work queue
+    // starts this many entries in, so those super-voxels never run and the
+    // ones that depend on them wait until the wait gives up
+    int debug_skip = 0;
     MbirAllreduceFn allreduce = nullptr;
     void *allreduce_ctx = nullptr;
 
@@ -225,6 +271,14 @@ extern "C" int mbir_init_stage(MbirStage **out, const float *projections, const 
                     proj_cols, proj_rows);
     if (remove_rings < 0 || remove_rings > 3) return fail("remove_rings must be 0..3");
     if (quad_convex < 0 || quad_convex > 1) return fail("quad_convex must be 0 or 1");
+    // a NaN or infinite projection or weight would turn every cost and
+    // update it touches into NaN (the reference does not check); refused here
+    {
+        const size_t n = (size_t)proj_num * proj_rows * proj_cols;
+        for (size_t q = 0; q < n; q++)
+            if (!std::isfinite(projections[q]) || !std::isfinite(weights[q]) || weights[q] < 0.0f)
+                return fail("projection / weight %zu is not finite (or the weight is negative)", q);
+    }
     MbirStage *S = new MbirStage();
     char err[256];
     if (scan_geom(S->sg, proj_angles, proj_times, recon_times, proj_rows, proj_cols, proj_num,
@@ -723,6 +777,13 @@ static int slab_sum(MbirStage *S, double *v, int n)
     if (S->slab_count <= 1) return 0;
     if (!S->allreduce || S->allreduce(v, n, S->allreduce_ctx) != 0)
         return fail("z-slab reduction over the ranks failed");
+    return 0;
+}
+
+extern "C" int mbir_debug_sv_skip_tasks(MbirStage *S, int32_t n)
+{
+    if (S->schedule != 1) return fail("the super-voxel schedule is not set");
+    S->debug_skip = std::max(0, n);
     return 0;
 }
 
@@ -1516,6 +1577,11 @@ static int sv_iterate(MbirStage *S, int iter, int32_t *converged)
     }
     // queue counters: slot 0 the sweep, slot 1 the NHICD pass
     CK(cudaMemsetAsync(S->d_queue, 0, 2 * sizeof(int), S->stream));
+    if (S->debug_skip > 0) {
+        CK(cudaMemcpyAsync(S->d_queue, &S->debug_skip, sizeof(int), cudaMemcpyHostToDevice, S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+        S->debug_skip = 0;
+    }
     CK(cudaMemsetAsync(S->d_sv_out, 0, 2 * sizeof(SvTaskOut), S->stream));
     const int rot = iter % P;
     // the sweep: one launch over every super-voxel, then the ring offsets
