@@ -34,8 +34,48 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def sources_digest() -> str:
+    """SHA-256 over the library's sources and public headers, in a fixed order."""
+    import hashlib
+    h = hashlib.sha256()
+    names = sorted(os.listdir(CSRC))
+    for n in names:
+        with open(os.path.join(CSRC, n), "rb") as f:
+            h.update(n.encode() + b"\0" + f.read())
+    for n in ("mbir4d.h", "timbir_b200.h"):
+        with open(os.path.join(HERE, "..", "include", n), "rb") as f:
+            h.update(n.encode() + b"\0" + f.read())
+    return h.hexdigest()
+
+
+INFO = os.path.join(HERE, "_build", "build_info.json")
+
+
+def build_info() -> dict:
+    """What the last build() did: the sources' digest the library was built
+    from, and whether that call compiled or found the library current."""
+    import json
+    try:
+        with open(INFO) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _record(compiled: bool) -> None:
+    import json
+    import time
+    os.makedirs(os.path.dirname(INFO), exist_ok=True)
+    info = build_info() if not compiled else {}
+    info.update({"sources_sha256": sources_digest() if compiled else info.get("sources_sha256", sources_digest()),
+                 "compiled_by_last_call": compiled, "time": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())})
+    with open(INFO, "w") as f:
+        json.dump(info, f)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
+        _record(False)
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -54,6 +94,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
     cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
     subprocess.run(cmd, check=True, env=env)
+    _record(True)
     return LIB
 
 
