@@ -14,7 +14,9 @@ when reconstructed alone:
   * a problem whose convergence test passes is retired (its object no longer
     changes) while the others go on;
   * the autotuner leaves the stage's state as prepared and picks a
-    configuration the batch runs.
+    configuration the batch runs;
+  * problems whose detector rows are not a multiple of four columns wide
+    reach the FP64 oracle's MAP inside a batch.
 """
 import os
 
@@ -179,3 +181,30 @@ def test_autotune_restores_the_stage_and_runs_in_a_batch():
     b.close()
     assert s.cost()[0] < c0
     s.close()
+
+
+def test_batch_of_ragged_detectors_reaches_the_fp64_map():
+    # detector rows of 30 and 33 columns: the band is staged and committed
+    # element by element instead of by 16-byte words
+    stages = [make_stage(cols, 4, 48, seed=11) for cols in (30, 33)]
+    b = timbir_b200.Batch(stages)
+    run_until_flat(lambda n: b.iterate(n, check_every=50), lambda: [s.cost()[0] for s in stages], tol=1e-10)
+    for s in stages:
+        x = s.object()
+        o = Oracle(s.scan, blocks=2, f64=True, **dict(scenarios.BASE, convg_thresh=0.0))
+        o.prepare()
+        hist = []
+        for it in range(1, 3000):
+            o.iterate(it)
+            hist.append(o.cost()[0])
+            if it > 10 and abs(hist[-6] - hist[-1]) <= 1e-12 * abs(hist[-1]):
+                break
+        ref, cref = o.object(), hist[-1]
+        o.close()
+        c = fresh_cost_fp64(s.scan, x)
+        rmse = float(np.sqrt(np.mean((x.astype(np.float64) - ref) ** 2)))
+        print(f"{s.scan.projections.shape[2]} columns in a batch: fresh FP64 cost - oracle MAP cost = "
+              f"{(c - cref) / cref:.3g} relative, RMSE / range = {rmse / SCALE:.3g}")
+        assert abs(c - cref) / cref < 1e-5
+        assert rmse < 1e-3 * SCALE
+    b.close()

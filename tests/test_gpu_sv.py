@@ -14,7 +14,10 @@ judged on the result:
     the iteration call fails);
   * the A-matrix column cache holds the reference's columns (bin indices
     bit-exact, values to float rounding) and gives the same iterates as
-    columns computed in the kernel.
+    columns computed in the kernel;
+  * detectors whose width is not a multiple of four columns (staged and
+    committed element by element instead of by 16-byte words) reach the
+    FP64 oracle's MAP as well.
 """
 import os
 
@@ -24,6 +27,7 @@ import pytest
 import scenarios
 import timbir_b200
 from oracle.bind import Oracle
+from timbir_b200 import synth
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
@@ -289,3 +293,41 @@ def test_stability_guard_recovers_a_diverging_sweep():
     assert unguarded[2] > unguarded[1]  # the unguarded sweep diverges
     assert adjustments >= 1
     assert all(np.isfinite(guarded)) and all(b <= a * (1 + 1e-6) for a, b in zip(guarded, guarded[1:]))
+
+
+RAGGED_KW = dict(blocks=2, mult_xy=1, mult_z=1, **scenarios.BASE)
+_ragged_map = {}
+
+
+def ragged_map(cols):
+    """(scan, converged FP64 oracle object, its cost) of a 4-slice, 48-view
+    scan whose detector rows have `cols` columns."""
+    if cols not in _ragged_map:
+        scan = synth.ellipsoid_scan(cols, 4, 48, seed=11)
+        o = Oracle(scan, f64=True, **RAGGED_KW)
+        o.prepare()
+        run_to_flat(o, flat=1e-12)
+        _ragged_map[cols] = (scan, o.object(), o.cost()[0])
+        o.close()
+    return _ragged_map[cols]
+
+
+@pytest.mark.parametrize("acache", [1, 0], ids=["cached", "computed"])
+@pytest.mark.parametrize("cols", [30, 33])
+def test_sv_ragged_detector_reaches_the_fp64_map(cols, acache):
+    scan, ref, cref = ragged_map(cols)
+    s = timbir_b200.Stage(scan, **RAGGED_KW)
+    s.set_schedule(timbir_b200.Stage.SCHEDULE_SUPERVOXEL, 0, 0, acache)
+    s.prepare()
+    run_to_flat(s)
+    x = s.object()
+    s.close()
+    o = Oracle(scan, f64=True, **RAGGED_KW)
+    o.prepare(x)
+    c = o.cost()[0]
+    o.close()
+    rmse = float(np.sqrt(np.mean((x.astype(np.float64) - ref) ** 2)))
+    print(f"{cols} columns: fresh FP64 cost - oracle MAP cost = {(c - cref) / cref:.3g} relative, "
+          f"RMSE / range = {rmse / SCALE:.3g}")
+    assert abs(c - cref) / cref < 1e-5
+    assert rmse < 1e-3 * SCALE
