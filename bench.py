@@ -680,6 +680,23 @@ def icd_from(scan, start, cstar=None, max_iters=600, flat=1e-10, prior=None, blo
     return it, ms, c, x
 
 
+def edge_weights(T, beta):
+    """Per-voxel loss weights 1 + beta |grad T| / mean |grad T| of target
+    volumes T (CUDA [N][D][H][W]; central differences, zero on the border):
+    the loss leans on the MAP images' edges, where an ICD start's error
+    decays slowest."""
+    import torch
+    g2 = torch.zeros_like(T)
+    for ax in (1, 2, 3):
+        n = T.shape[ax]
+        if n < 3:
+            continue
+        d = (T.narrow(ax, 2, n - 2) - T.narrow(ax, 0, n - 2)) * 0.5
+        g2.narrow(ax, 1, n - 2).add_(d * d)
+    g = g2.sqrt()
+    return (1.0 + beta * g / g.mean().clamp_min(1e-30)).contiguous()
+
+
 def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
     """Learned warm start: training pairs from the plain method, the network
     trained on them, then ICD from its output against ICD from FBP on held-out
@@ -716,16 +733,18 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
     data_s = time.perf_counter() - t0
     X = torch.from_numpy(np.stack(fbps)).cuda()
     T = torch.from_numpy(np.stack(tgts)).cuda()
+    beta = float(getattr(args, "c4_edge_weight", 0.0))
+    WT = edge_weights(T, beta) if beta > 0 else None
     net = warm.WarmNet(seed=7)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    losses = warm.train(net, X, T, steps=steps, batch=4, patch=(16, 64, 64), lr=1e-3, seed=3)
+    losses = warm.train(net, X, T, steps=steps, batch=4, patch=(16, 64, 64), lr=1e-3, seed=3, weights=WT)
     e1.record()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
     pairs = int(X.shape[0])
-    del X, T
+    del X, T, WT
     results = []
     for sc, name in held_out:
         st = c4_stage(sc, prior, blocks)
@@ -755,8 +774,12 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
         from scipy import ndimage
         lp = lambda a: ndimage.gaussian_filter(a.astype(np.float64), sigma=(0, 2, 8, 8)).astype(np.float32)  # noqa
         sens = {}
+        lpw = lambda a, sg: ndimage.gaussian_filter(a.astype(np.float64), sigma=sg).astype(np.float32)  # noqa
         for key, s0 in (("fbp_error_halved", 0.5 * (fbp + x_star)),
-                        ("map_high_frequencies_fbp_low", lp(fbp) + (x_star - lp(x_star)))):
+                        ("map_high_frequencies_fbp_low", lp(fbp) + (x_star - lp(x_star))),
+                        ("network_high_frequencies_fbp_low_s1x4", lpw(fbp, (0, 1, 4, 4)) + ws - lpw(ws, (0, 1, 4, 4))),
+                        ("network_high_frequencies_fbp_low_s2x8", lp(fbp) + (ws - lp(ws))),
+                        ("network_high_frequencies_fbp_low_s4x16", lpw(fbp, (0, 4, 16, 16)) + ws - lpw(ws, (0, 4, 16, 16)))):
             s0 = (s0 * mask).astype(np.float32)
             n_s, _, _, _ = icd_from(sc, s0, cstar, **kw)
             sens[key] = {"iterations": n_s, "start_rmse_over_range": rm(s0)}
@@ -782,7 +805,10 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
                    "training_volumes": pairs,
                    "pair_target": "converged MAP image (plain ICD from FBP until two successive costs agree to 1e-10; "
                                   "mean %.0f iterations)" % float(np.mean(target_iters)),
-                   "train_steps": steps, "train_batch": "4 patches 16x64x64", "params": int(net.n)},
+                   "train_steps": steps, "train_batch": "4 patches 16x64x64", "params": int(net.n),
+                   "loss": ("mean squared error" if beta <= 0 else
+                            f"mean squared error weighted per voxel by 1 + {beta:g} |grad target| / "
+                            "mean |grad target|")},
         "training": {"ms": round(train_ms, 1), "ms_per_step": round(train_ms / steps, 3),
                      "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
                      "pairs_s": round(data_s, 1)},
@@ -1408,6 +1434,8 @@ def main():
     ap.add_argument("--sv-alpha", type=float, default=0.0,
                     help="over-relaxation of the super-voxel schedule (0: automatic from the in-flight cap)")
     ap.add_argument("--sv-ctas", type=int, default=0, help="persistent CTAs per sweep (0: automatic)")
+    ap.add_argument("--c4-edge-weight", type=float, default=0.0,
+                    help="c4 / 4d-warm: weight the training loss per voxel by 1 + BETA |grad target| / mean")
     ap.add_argument("--nhicd", type=float, default=-1.0,
                     help="share of each plane's lines the NHICD pass selects (default: the library's 0.1)")
     ap.add_argument("--a-fp16", dest="acache", action="store_const", const=2, default=-1,

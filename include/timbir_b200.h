@@ -413,10 +413,14 @@ int mbir_net_set_params(MbirNet *net, const float *in);
 int mbir_net_get_grads(MbirNet *net, float *out);
 int mbir_net_forward(MbirNet *net, const float *in, float *out, int32_t B, int32_t D, int32_t H, int32_t W,
                      float scale, void *stream);
-/* Parameter gradients of the loss mean((s in + r - s target)^2) into the
- * network's gradient array; *loss (may be NULL) = the loss. */
+/* Parameter gradients of the loss mean(wt (s in + r - s target)^2) into the
+ * network's gradient array (wt = 1 unless loss weights are set); *loss (may
+ * be NULL) = the loss. */
 int mbir_net_gradients(MbirNet *net, const float *in, const float *target, int32_t B, int32_t D, int32_t H,
                        int32_t W, float scale, double *loss, void *stream);
+/* Per-voxel loss weights for the following mbir_net_gradients calls: a
+ * device float array of the input's shape, read by each call (NULL: none). */
+int mbir_net_set_loss_weights(MbirNet *net, const float *w);
 /* Layer k's output (which 0; layer -1: the network input) or its gradient
  * (which 1) from the last forward / gradient call, as host float
  * [B][D][H][W][C] at the layer's level; *count (may be NULL) = elements,

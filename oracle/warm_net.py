@@ -139,8 +139,9 @@ def predict(flat, fbp, s):
     return np.asarray(fbp, np.float64) + r / s
 
 
-def loss_and_grads(flat, fbp, target, s, trace=None, acts=None):
-    """Loss mean((s fbp + r - s target)^2) and its gradient with respect to
+def loss_and_grads(flat, fbp, target, s, trace=None, acts=None, weights=None):
+    """Loss mean(w (s fbp + r - s target)^2) (w = the per-voxel weights, 1
+    when None) and its gradient with respect to
     the flat parameters; trace (a dict), when given, receives each layer's
     output gradient (after its ReLU's mask) under the layer's index.  acts,
     when given, are the layer outputs to differentiate at ({"x0": input,
@@ -156,9 +157,10 @@ def loss_and_grads(flat, fbp, target, s, trace=None, acts=None):
         r = A[14][..., 0]
     d = s * np.asarray(fbp, np.float64) + r - s * np.asarray(target, np.float64)
     M = d.size
-    loss = float(np.mean(d * d))
+    wt = np.ones_like(d) if weights is None else np.asarray(weights, np.float64)
+    loss = float(np.mean(wt * d * d))
     dz14 = np.zeros(A[14].shape)
-    dz14[..., 0] = 2.0 * d / M
+    dz14[..., 0] = 2.0 * wt * d / M
     grads = [None] * 15
     mask = lambda g, a: g * (a > 0)  # noqa: E731
 
@@ -205,7 +207,7 @@ def adam(p, g, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8):
     return p, m, v
 
 
-def loss_exact(flat, fbp, target, s):
+def loss_exact(flat, fbp, target, s, weights=None):
     """The loss without BF16 rounding (for finite differences of the
     oracle's own gradients, whose step would be lost in BF16)."""
     global bf16
@@ -216,20 +218,21 @@ def loss_exact(flat, fbp, target, s):
     finally:
         bf16 = saved
     d = s * np.asarray(fbp, np.float64) + r - s * np.asarray(target, np.float64)
-    return float(np.mean(d * d))
+    wt = 1.0 if weights is None else np.asarray(weights, np.float64)
+    return float(np.mean(wt * d * d))
 
 
-def grads_exact(flat, fbp, target, s):
+def grads_exact(flat, fbp, target, s, weights=None):
     global bf16
     saved = bf16
     bf16 = lambda a: np.asarray(a, np.float64)  # noqa: E731
     try:
-        return loss_and_grads(flat, fbp, target, s)
+        return loss_and_grads(flat, fbp, target, s, weights=weights)
     finally:
         bf16 = saved
 
 
-def finite_difference(flat, fbp, target, s, idx, h=1e-6):
+def finite_difference(flat, fbp, target, s, idx, h=1e-6, weights=None):
     """Central differences of loss_exact at parameters idx."""
     out = []
     for i in idx:
@@ -237,5 +240,5 @@ def finite_difference(flat, fbp, target, s, idx, h=1e-6):
         p2 = p1.copy()
         p1[i] += h
         p2[i] -= h
-        out.append((loss_exact(p1, fbp, target, s) - loss_exact(p2, fbp, target, s)) / (2 * h))
+        out.append((loss_exact(p1, fbp, target, s, weights) - loss_exact(p2, fbp, target, s, weights)) / (2 * h))
     return np.array(out)

@@ -91,18 +91,23 @@ def gpu_activations(net, shape):
     return acts
 
 
-def test_network_gradients_match_the_oracle():
+@pytest.mark.parametrize("weighted", [False, True], ids=["plain", "weighted"])
+def test_network_gradients_match_the_oracle(weighted):
     # the backward pass on its own: the oracle differentiates at the GPU's
     # own layer outputs (a forward difference near a ReLU's kink would
-    # otherwise flip its mask on one side only)
+    # otherwise flip its mask on one side only); weighted: per-voxel loss
+    # weights
     net = warm.WarmNet(0)
     p = random_params(3)
     net.set_params(p)
     fbp, tgt = inputs(4)
+    wts = np.random.default_rng(5).uniform(0.5, 4.0, fbp.shape).astype(np.float32) if weighted else None
+    net.set_loss_weights(torch.from_numpy(wts).cuda() if weighted else None)
     loss = net.gradients(torch.from_numpy(fbp).cuda(), torch.from_numpy(tgt).cuda())
+    net.set_loss_weights(None)
     g = net.grads()
     trace = {}
-    loss_ref, g_ref = W.loss_and_grads(p, fbp, tgt, warm.SCALE, trace, gpu_activations(net, fbp.shape))
+    loss_ref, g_ref = W.loss_and_grads(p, fbp, tgt, warm.SCALE, trace, gpu_activations(net, fbp.shape), weights=wts)
     assert abs(loss - loss_ref) < 1e-4 * loss_ref
     for k in range(15):  # each layer's output gradient (after its ReLU's mask)
         assert rel(net.activation(k, grad=True), trace[k].reshape(-1)) < 1e-2, k

@@ -2,6 +2,7 @@
 hand-written backward pass against central differences of its own loss, and
 BF16 rounding to nearest even."""
 import numpy as np
+import pytest
 
 from oracle import warm_net as W
 
@@ -17,19 +18,21 @@ def random_params(rng):
     return flat
 
 
-def test_oracle_gradients_match_finite_differences():
+@pytest.mark.parametrize("weighted", [False, True], ids=["plain", "weighted"])
+def test_oracle_gradients_match_finite_differences(weighted):
     rng = np.random.default_rng(0)
     flat = random_params(rng)
     fbp = rng.random((1, 8, 16, 16)) * 0.02
     tgt = fbp + rng.normal(0, 0.002, fbp.shape)
-    loss, g = W.grads_exact(flat, fbp, tgt, 50.0)
+    wts = rng.uniform(0.5, 4.0, fbp.shape) if weighted else None
+    loss, g = W.grads_exact(flat, fbp, tgt, 50.0, weights=wts)
     assert loss > 0
     # parameters with a gradient, from first, middle and last layers
     live = np.nonzero(np.abs(g) > 1e-6 * np.abs(g).max())[0]
     idx = np.concatenate([live[:3], live[len(live) // 2:len(live) // 2 + 3], live[-3:],
                           rng.choice(live, 6, replace=False)])
     # a small step keeps ReLU inputs near zero from changing sign
-    fd = W.finite_difference(flat, fbp, tgt, 50.0, idx, h=1e-7)
+    fd = W.finite_difference(flat, fbp, tgt, 50.0, idx, h=1e-7, weights=wts)
     assert np.allclose(g[idx], fd, rtol=1e-4, atol=1e-8 * np.abs(g).max())
 
 

@@ -673,20 +673,21 @@ __global__ void k_output(const float *__restrict__ in, const bf16 *__restrict__ 
     if (i < M) out[i] = in[i] + b2f(Z[(size_t)i * 16]) / s;
 }
 
-// loss = mean (s in + r - s t)^2; dZ channel 0 = its gradient, others 0;
-// per-block partial sums (FP64) into part
+// loss = mean wt (s in + r - s t)^2 (wt = 1 without weights); dZ channel 0
+// = its gradient, others 0; per-block partial sums (FP64) into part
 __global__ void __launch_bounds__(256) k_loss(const float *__restrict__ in, const float *__restrict__ t,
-                                              const bf16 *__restrict__ Z, float s, bf16 *__restrict__ dZ,
-                                              long long M, double *__restrict__ part)
+                                              const float *__restrict__ wt, const bf16 *__restrict__ Z, float s,
+                                              bf16 *__restrict__ dZ, long long M, double *__restrict__ part)
 {
     __shared__ double red[256];
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double l = 0.0;
     if (i < M) {
         const float d = s * in[i] + b2f(Z[(size_t)i * 16]) - s * t[i];
-        l = (double)d * d;
+        const float wi = wt ? wt[i] : 1.0f;
+        l = (double)wi * d * d;
         bf16 *g = dZ + (size_t)i * 16;
-        g[0] = f2b(2.0f * d / (float)M);
+        g[0] = f2b(2.0f * wi * d / (float)M);
         for (int c = 1; c < 16; c++) g[c] = f2b(0.0f);
     }
     red[threadIdx.x] = l;
@@ -786,7 +787,8 @@ struct MbirNet {
     // them and replayed while they repeat (one launch instead of ~130)
     cudaStream_t gstream = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    const float *g_in = nullptr, *g_t = nullptr;
+    const float *g_in = nullptr, *g_t = nullptr, *g_w = nullptr;
+    const float *loss_w = nullptr;  // per-voxel loss weights (device, the input's shape) or null
     float g_scale = 0.0f;
     Shape g_shape{0, 0, 0, 0};
     int g_seen = 0;
@@ -1225,13 +1227,14 @@ int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t
     cudaStream_t caller = (cudaStream_t)stream;
     const Shape sh{B, D, H, W};
     if (net_shape(N, sh, true)) return -1;
-    const bool same = N->g_in == in && N->g_t == target && N->g_scale == scale && N->g_shape.B == B &&
-                      N->g_shape.D == D && N->g_shape.H == H && N->g_shape.W == W;
+    const bool same = N->g_in == in && N->g_t == target && N->g_w == N->loss_w && N->g_scale == scale &&
+                      N->g_shape.B == B && N->g_shape.D == D && N->g_shape.H == H && N->g_shape.W == W;
     if (!same) {  // a new key: the graph of the old one is dropped
         if (N->gexec) cudaGraphExecDestroy(N->gexec);
         N->gexec = nullptr;
         N->g_in = in;
         N->g_t = target;
+        N->g_w = N->loss_w;
         N->g_scale = scale;
         N->g_shape = sh;
         N->g_seen = 0;
@@ -1240,7 +1243,8 @@ int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t
     const int nb = blocks(M);
     auto enqueue = [&](cudaStream_t st) -> int {
         if (forward(N, in, scale, st)) return -1;
-        k_loss<<<nb, 256, 0, st>>>(in, target, N->act[T_A0 + 14].p, scale, N->grad[T_A0 + 14].p, M, N->part);
+        k_loss<<<nb, 256, 0, st>>>(in, target, N->loss_w, N->act[T_A0 + 14].p, scale, N->grad[T_A0 + 14].p, M,
+                                   N->part);
         NK(cudaGetLastError());
         return backward(N, st);
     };
@@ -1280,6 +1284,13 @@ int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t
     double l = 0;
     for (double v : part) l += v;
     if (loss) *loss = l / (double)M;
+    return 0;
+}
+
+int mbir_net_set_loss_weights(MbirNet *N, const float *w)
+{
+    if (!N) return net_fail("null network");
+    N->loss_w = w;
     return 0;
 }
 

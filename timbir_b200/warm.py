@@ -37,6 +37,7 @@ def _lib():
         lib.mbir_net_forward.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, vp]
         lib.mbir_net_gradients.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.POINTER(C.c_double), vp]
         lib.mbir_net_adam_step.argtypes = [vp, C.c_float, vp]
+        lib.mbir_net_set_loss_weights.argtypes = [vp, vp]
         lib.mbir_net_get_activation.argtypes = [vp, i32, i32, vp, C.POINTER(C.c_int64)]
         lib._net_bound = True
     return lib
@@ -115,15 +116,24 @@ class WarmNet:
                                            scale, C.byref(loss), _stream()))
         return loss.value
 
+    def set_loss_weights(self, w) -> None:
+        """Per-voxel weights of the loss, mean(w (s x + r - s t)^2), for the
+        following gradients() calls: a CUDA float32 tensor of the inputs'
+        shape (kept referenced here), or None for unit weights."""
+        self._loss_w = None if w is None else w.contiguous()
+        _check(self.lib.mbir_net_set_loss_weights(
+            self.h, None if self._loss_w is None else C.c_void_p(self._loss_w.data_ptr())))
+
     def adam_step(self, lr: float) -> None:
         _check(self.lib.mbir_net_adam_step(self.h, lr, _stream()))
 
 
 def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 64, 64), lr: float = 1e-3,
-          seed: int = 0, scale: float = SCALE, log_every: int = 0):
+          seed: int = 0, scale: float = SCALE, log_every: int = 0, weights=None):
     """Adam on random patches of the (input, target) volumes (CUDA tensors
-    [N][D][H][W]); the learning rate decays by cosine to a tenth.  Returns the
-    per-step losses."""
+    [N][D][H][W]), the loss weighted per voxel by the same patches of
+    `weights` when given; the learning rate decays by cosine to a tenth.
+    Returns the per-step losses."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
     N, D, H, W = inputs.shape
@@ -131,6 +141,8 @@ def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 
     losses = []
     xb = torch.empty((batch, pd, ph, pw), dtype=torch.float32, device=inputs.device)
     tb = torch.empty_like(xb)
+    wb = torch.empty_like(xb) if weights is not None else None
+    net.set_loss_weights(wb)
     for step in range(steps):
         for b in range(batch):
             n = int(torch.randint(N, (1,), generator=g))
@@ -139,11 +151,15 @@ def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 
             x = int(torch.randint(W - pw + 1, (1,), generator=g))
             xb[b] = inputs[n, z:z + pd, y:y + ph, x:x + pw]
             tb[b] = targets[n, z:z + pd, y:y + ph, x:x + pw]
+            if wb is not None:
+                wb[b] = weights[n, z:z + pd, y:y + ph, x:x + pw]
         losses.append(net.gradients(xb, tb, scale))
         cur = lr * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * step / max(steps, 1))))
         net.adam_step(cur)
         if log_every and (step + 1) % log_every == 0:
             print(f"step {step + 1} loss {np.mean(losses[-log_every:]):.5f}", flush=True)
+    if wb is not None:
+        net.set_loss_weights(None)
     return losses
 
 
