@@ -428,6 +428,15 @@ int mbir_net_set_loss_weights(MbirNet *net, const float *w);
 int mbir_net_get_activation(MbirNet *net, int32_t layer, int32_t which, float *out, int64_t *count);
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the last gradients. */
 int mbir_net_adam_step(MbirNet *net, float lr, void *stream);
+/* start += G (ref - start) on device float arrays [N][D][H][W], G the
+ * separable Gaussian low-pass of widths sigma_z (slices) and sigma_xy (x and
+ * y voxels) per volume n (radius int(4 sigma + 0.5), edges mirrored about
+ * the half-sample point; a width of 0 skips the axis; widths up to 15.9):
+ * the low frequencies of `ref` under the high frequencies of `start`.
+ * scratch: device float array of 2 N D H W.  Returns after the stream has
+ * run it; errors via mbir_net_last_error().  No counterpart in the reference. */
+int mbir_lowpass_blend(const float *ref, float *start, float *scratch, int32_t N, int32_t D, int32_t H, int32_t W,
+                       float sigma_z, float sigma_xy, void *stream);
 
 #ifdef __cplusplus
 }

@@ -183,8 +183,24 @@ def test_trained_network_starts_closer_to_the_map_than_fbp():
     losses = warm.train(net, X, T, steps=400, batch=4, patch=(16, 32, 32), lr=1e-3, seed=3)
     assert np.mean(losses[-20:]) < np.mean(losses[:20])
     fbp, x_map, mask = _scan_and_map(999)
-    start = warm.warm_start(net, fbp, mask)
+    start = warm.warm_start(net, fbp, mask, blend=None)  # the network's own output
     net.close()
     rmse = lambda a: float(np.sqrt(np.mean((a.astype(np.float64) - x_map) ** 2)))  # noqa: E731
     print(f"held-out scan: RMSE to the MAP image, FBP {rmse(fbp):.3g}, network {rmse(start):.3g}")
     assert rmse(start) < 0.7 * rmse(fbp)
+
+
+@pytest.mark.parametrize("sig", [(1.0, 4.0), (0.0, 2.5), (2.0, 0.0)])
+def test_lowpass_blend_matches_scipy(sig):
+    # start + G (ref - start), G the Gaussian low-pass with scipy.ndimage's
+    # truncation (4 sigma) and mirrored edges, per volume
+    from scipy import ndimage
+    rng = np.random.default_rng(9)
+    ref = rng.random((2, 8, 40, 24)).astype(np.float32)
+    start = rng.random((2, 8, 40, 24)).astype(np.float32)
+    want = start.astype(np.float64) + ndimage.gaussian_filter((ref - start).astype(np.float64),
+                                                              sigma=(0, sig[0], sig[1], sig[1]), mode="reflect")
+    s = torch.from_numpy(start).cuda()
+    warm.lowpass_blend(torch.from_numpy(ref).cuda(), s, *sig)
+    got = s.cpu().numpy()
+    assert np.abs(got - want).max() < 1e-5 * np.abs(want).max()

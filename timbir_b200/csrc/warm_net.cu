@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -1111,9 +1112,91 @@ static int net_err_check(MbirNet *N, cudaStream_t st)
     return 0;
 }
 
+// ---- low-frequency blend of two starts ----
+// Gaussian taps of one axis: radius int(4 sigma + 0.5), exp(-x^2 / (2 sigma^2))
+// normalised to sum 1 (the truncation and normalisation of scipy.ndimage's
+// gaussian_filter); edges mirrored about the half-sample point (d c b a | a b
+// c d | d c b a).
+constexpr int kBlurMaxRadius = 64;
+struct BlurTaps {
+    int r;
+    float w[2 * kBlurMaxRadius + 1];
+};
+
+__global__ void k_blend_diff(const float *__restrict__ a, const float *__restrict__ b, float *__restrict__ d,
+                             long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = a[i] - b[i];
+}
+
+// out = in filtered along one axis (length len, element stride stride)
+__global__ void k_blur_axis(const float *__restrict__ in, float *__restrict__ out, long long n, long long stride,
+                            int len, BlurTaps t)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = (int)((i / stride) % len);
+    const float *base = in + (i - (long long)c * stride);
+    float acc = 0.0f;
+    for (int k = -t.r; k <= t.r; k++) {
+        int q = c + k;
+        while (q < 0 || q >= len) q = q < 0 ? -q - 1 : 2 * len - q - 1;
+        acc = fmaf(t.w[k + t.r], base[(long long)q * stride], acc);
+    }
+    out[i] = acc;
+}
+
+__global__ void k_blend_add(float *__restrict__ start, const float *__restrict__ d, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) start[i] += d[i];
+}
+
+static BlurTaps blur_taps(float sigma)
+{
+    BlurTaps t{};
+    t.r = (int)(4.0 * sigma + 0.5);
+    double w[2 * kBlurMaxRadius + 1], sum = 0.0;
+    for (int k = -t.r; k <= t.r; k++) sum += w[k + t.r] = std::exp(-0.5 * k * k / ((double)sigma * sigma));
+    for (int k = 0; k <= 2 * t.r; k++) t.w[k] = (float)(w[k] / sum);
+    return t;
+}
+
 extern "C" {
 
 const char *mbir_net_last_error(void) { return g_net_err; }
+
+int mbir_lowpass_blend(const float *ref, float *start, float *scratch, int32_t N, int32_t D, int32_t H, int32_t W,
+                       float sigma_z, float sigma_xy, void *stream)
+{
+    if (N < 1 || D < 1 || H < 1 || W < 1) return net_fail("blend: empty volume");
+    if (!(sigma_z >= 0.0f && sigma_xy >= 0.0f) || 4.0f * sigma_z + 0.5f > (float)kBlurMaxRadius ||
+        4.0f * sigma_xy + 0.5f > (float)kBlurMaxRadius)
+        return net_fail("blend: Gaussian widths must be in [0, 15.9]");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long n = (long long)N * D * H * W;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    float *a = scratch, *b = scratch + n;
+    k_blend_diff<<<nb, 256, 0, st>>>(ref, start, a, n);
+    NK(cudaGetLastError());
+    // x (stride 1), y (stride W), z (stride H W); a zero width skips the axis
+    const struct {
+        float sigma;
+        long long stride;
+        int len;
+    } axes[3] = {{sigma_xy, 1, W}, {sigma_xy, W, H}, {sigma_z, (long long)H * W, D}};
+    for (const auto &ax : axes) {
+        if (ax.sigma <= 0.0f) continue;
+        k_blur_axis<<<nb, 256, 0, st>>>(a, b, n, ax.stride, ax.len, blur_taps(ax.sigma));
+        NK(cudaGetLastError());
+        std::swap(a, b);
+    }
+    k_blend_add<<<nb, 256, 0, st>>>(start, a, n);
+    NK(cudaGetLastError());
+    NK(cudaStreamSynchronize(st));
+    return 0;
+}
 
 int64_t mbir_net_param_count(void)
 {

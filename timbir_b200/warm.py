@@ -38,6 +38,7 @@ def _lib():
         lib.mbir_net_gradients.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.POINTER(C.c_double), vp]
         lib.mbir_net_adam_step.argtypes = [vp, C.c_float, vp]
         lib.mbir_net_set_loss_weights.argtypes = [vp, vp]
+        lib.mbir_lowpass_blend.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.c_float, vp]
         lib.mbir_net_get_activation.argtypes = [vp, i32, i32, vp, C.POINTER(C.c_int64)]
         lib._net_bound = True
     return lib
@@ -163,11 +164,34 @@ def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 
     return losses
 
 
-def warm_start(net: WarmNet, fbp: np.ndarray, mask: np.ndarray, scale: float = SCALE) -> np.ndarray:
+def lowpass_blend(ref, start, sigma_z: float, sigma_xy: float) -> None:
+    """start += G (ref - start) in place (CUDA float32 tensors [N][D][H][W];
+    G the Gaussian low-pass of widths sigma_z slices, sigma_xy voxels): the
+    low frequencies of ref under the high frequencies of start."""
+    import torch
+    ref = ref.contiguous()
+    assert start.is_contiguous() and ref.shape == start.shape
+    N, D, H, W = start.shape
+    scratch = torch.empty((2,) + tuple(start.shape), dtype=torch.float32, device=start.device)
+    lib = _lib()
+    _check(lib.mbir_lowpass_blend(C.c_void_p(ref.data_ptr()), C.c_void_p(start.data_ptr()),
+                                  C.c_void_p(scratch.data_ptr()), N, D, H, W, sigma_z, sigma_xy, _stream()))
+
+
+# widths of the low-pass under which warm_start keeps the FBP's frequencies
+BLEND_SIGMA = (1.0, 4.0)
+
+
+def warm_start(net: WarmNet, fbp: np.ndarray, mask: np.ndarray, scale: float = SCALE,
+               blend=BLEND_SIGMA) -> np.ndarray:
     """Warm start [N_time][N_z][N_y][N_x] from the frames' filtered
-    backprojections: the network per frame, zero outside the reconstruction
-    mask (ICD never updates those voxels)."""
+    backprojections: the network per frame, its low frequencies replaced by
+    the FBP's (Gaussian low-pass of widths blend = (slices, voxels); None:
+    the network's output as it is), zero outside the reconstruction mask
+    (ICD never updates those voxels)."""
     import torch
     x = torch.from_numpy(np.ascontiguousarray(fbp, np.float32)).cuda()
-    out = net.forward(x, scale).cpu().numpy()
-    return (out * mask[None, None, :, :]).astype(np.float32)
+    out = net.forward(x, scale)
+    if blend:
+        lowpass_blend(x, out, float(blend[0]), float(blend[1]))
+    return (out.cpu().numpy() * mask[None, None, :, :]).astype(np.float32)
