@@ -740,7 +740,9 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    losses = warm.train(net, X, T, steps=steps, batch=4, patch=(16, 64, 64), lr=1e-3, seed=3, weights=WT)
+    hp = warm.BLEND_SIGMA if getattr(args, "c4_loss", "highpass") == "highpass" else None
+    losses = warm.train(net, X, T, steps=steps, batch=4, patch=(16, 64, 64), lr=1e-3, seed=3, weights=WT,
+                        highpass=hp)
     e1.record()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
@@ -810,7 +812,9 @@ def c4_arm(args, rank, world, local_rank, four_d=False, n_train=32, steps=2000):
                    "train_steps": steps, "train_batch": "4 patches 16x64x64", "params": int(net.n),
                    "loss": ("mean squared error" if beta <= 0 else
                             f"mean squared error weighted per voxel by 1 + {beta:g} |grad target| / "
-                            "mean |grad target|")},
+                            "mean |grad target|")
+                           + ("" if not hp else f" of the residual's high frequencies ((I - G) d, G a Gaussian "
+                                                f"low-pass of {hp[0]:g} slice x {hp[1]:g} x {hp[1]:g} voxels)")},
         "training": {"ms": round(train_ms, 1), "ms_per_step": round(train_ms / steps, 3),
                      "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
                      "pairs_s": round(data_s, 1)},
@@ -1436,6 +1440,8 @@ def main():
     ap.add_argument("--sv-alpha", type=float, default=0.0,
                     help="over-relaxation of the super-voxel schedule (0: automatic from the in-flight cap)")
     ap.add_argument("--sv-ctas", type=int, default=0, help="persistent CTAs per sweep (0: automatic)")
+    ap.add_argument("--c4-loss", default="highpass", choices=["highpass", "mse"],
+                    help="c4 / 4d-warm: train on the residual's high frequencies (those the start keeps) or on all")
     ap.add_argument("--c4-edge-weight", type=float, default=0.0,
                     help="c4 / 4d-warm: weight the training loss per voxel by 1 + BETA |grad target| / mean")
     ap.add_argument("--nhicd", type=float, default=-1.0,

@@ -421,6 +421,13 @@ int mbir_net_gradients(MbirNet *net, const float *in, const float *target, int32
 /* Per-voxel loss weights for the following mbir_net_gradients calls: a
  * device float array of the input's shape, read by each call (NULL: none). */
 int mbir_net_set_loss_weights(MbirNet *net, const float *w);
+/* High-pass loss for the following mbir_net_gradients calls: the loss
+ * becomes mean(wt ((I - G) d)^2), d = s in + r - s target, G the separable
+ * Gaussian low-pass of widths sigma_z (slices) and sigma_xy (voxels) per
+ * patch, zeros outside the patch, radius int(4 sigma + 0.5): the network is
+ * trained on the frequencies a start keeps under mbir_lowpass_blend.  Widths
+ * 0, 0: the plain loss; at most 15.9. */
+int mbir_net_set_loss_highpass(MbirNet *net, float sigma_z, float sigma_xy);
 /* Layer k's output (which 0; layer -1: the network input) or its gradient
  * (which 1) from the last forward / gradient call, as host float
  * [B][D][H][W][C] at the layer's level; *count (may be NULL) = elements,

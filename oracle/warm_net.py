@@ -139,9 +139,19 @@ def predict(flat, fbp, s):
     return np.asarray(fbp, np.float64) + r / s
 
 
-def loss_and_grads(flat, fbp, target, s, trace=None, acts=None, weights=None):
+def _lowpass_zero_edge(a, hp):
+    """Gaussian low-pass of widths hp = (slices, voxels) of [B][D][H][W], zeros
+    outside the volume, radius int(4 sigma + 0.5) (scipy.ndimage)."""
+    from scipy import ndimage
+    return ndimage.gaussian_filter(np.asarray(a, np.float64), sigma=(0, hp[0], hp[1], hp[1]), mode="constant",
+                                   truncate=4.0)
+
+
+def loss_and_grads(flat, fbp, target, s, trace=None, acts=None, weights=None, highpass=None):
     """Loss mean(w (s fbp + r - s target)^2) (w = the per-voxel weights, 1
-    when None) and its gradient with respect to
+    when None; with highpass = (sigma_z, sigma_xy) the residual is first
+    high-passed, (I - G) d, G the zero-edge Gaussian low-pass) and its
+    gradient with respect to
     the flat parameters; trace (a dict), when given, receives each layer's
     output gradient (after its ReLU's mask) under the layer's index.  acts,
     when given, are the layer outputs to differentiate at ({"x0": input,
@@ -158,9 +168,15 @@ def loss_and_grads(flat, fbp, target, s, trace=None, acts=None, weights=None):
     d = s * np.asarray(fbp, np.float64) + r - s * np.asarray(target, np.float64)
     M = d.size
     wt = np.ones_like(d) if weights is None else np.asarray(weights, np.float64)
-    loss = float(np.mean(wt * d * d))
     dz14 = np.zeros(A[14].shape)
-    dz14[..., 0] = 2.0 * wt * d / M
+    if highpass:
+        h = d - _lowpass_zero_edge(d, highpass)
+        u = wt * h
+        loss = float(np.mean(u * h))
+        dz14[..., 0] = 2.0 * (u - _lowpass_zero_edge(u, highpass)) / M
+    else:
+        loss = float(np.mean(wt * d * d))
+        dz14[..., 0] = 2.0 * wt * d / M
     grads = [None] * 15
     mask = lambda g, a: g * (a > 0)  # noqa: E731
 
@@ -207,7 +223,7 @@ def adam(p, g, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8):
     return p, m, v
 
 
-def loss_exact(flat, fbp, target, s, weights=None):
+def loss_exact(flat, fbp, target, s, weights=None, highpass=None):
     """The loss without BF16 rounding (for finite differences of the
     oracle's own gradients, whose step would be lost in BF16)."""
     global bf16
@@ -218,21 +234,23 @@ def loss_exact(flat, fbp, target, s, weights=None):
     finally:
         bf16 = saved
     d = s * np.asarray(fbp, np.float64) + r - s * np.asarray(target, np.float64)
+    if highpass:
+        d = d - _lowpass_zero_edge(d, highpass)
     wt = 1.0 if weights is None else np.asarray(weights, np.float64)
     return float(np.mean(wt * d * d))
 
 
-def grads_exact(flat, fbp, target, s, weights=None):
+def grads_exact(flat, fbp, target, s, weights=None, highpass=None):
     global bf16
     saved = bf16
     bf16 = lambda a: np.asarray(a, np.float64)  # noqa: E731
     try:
-        return loss_and_grads(flat, fbp, target, s, weights=weights)
+        return loss_and_grads(flat, fbp, target, s, weights=weights, highpass=highpass)
     finally:
         bf16 = saved
 
 
-def finite_difference(flat, fbp, target, s, idx, h=1e-6, weights=None):
+def finite_difference(flat, fbp, target, s, idx, h=1e-6, weights=None, highpass=None):
     """Central differences of loss_exact at parameters idx."""
     out = []
     for i in idx:
@@ -240,5 +258,6 @@ def finite_difference(flat, fbp, target, s, idx, h=1e-6, weights=None):
         p2 = p1.copy()
         p1[i] += h
         p2[i] -= h
-        out.append((loss_exact(p1, fbp, target, s, weights) - loss_exact(p2, fbp, target, s, weights)) / (2 * h))
+        out.append((loss_exact(p1, fbp, target, s, weights, highpass)
+                    - loss_exact(p2, fbp, target, s, weights, highpass)) / (2 * h))
     return np.array(out)

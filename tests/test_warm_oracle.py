@@ -18,21 +18,22 @@ def random_params(rng):
     return flat
 
 
-@pytest.mark.parametrize("weighted", [False, True], ids=["plain", "weighted"])
-def test_oracle_gradients_match_finite_differences(weighted):
+@pytest.mark.parametrize("loss", ["plain", "weighted", "highpass"])
+def test_oracle_gradients_match_finite_differences(loss):
     rng = np.random.default_rng(0)
     flat = random_params(rng)
     fbp = rng.random((1, 8, 16, 16)) * 0.02
     tgt = fbp + rng.normal(0, 0.002, fbp.shape)
-    wts = rng.uniform(0.5, 4.0, fbp.shape) if weighted else None
-    loss, g = W.grads_exact(flat, fbp, tgt, 50.0, weights=wts)
+    wts = rng.uniform(0.5, 4.0, fbp.shape) if loss != "plain" else None
+    hp = (1.0, 2.0) if loss == "highpass" else None
+    loss, g = W.grads_exact(flat, fbp, tgt, 50.0, weights=wts, highpass=hp)
     assert loss > 0
     # parameters with a gradient, from first, middle and last layers
     live = np.nonzero(np.abs(g) > 1e-6 * np.abs(g).max())[0]
     idx = np.concatenate([live[:3], live[len(live) // 2:len(live) // 2 + 3], live[-3:],
                           rng.choice(live, 6, replace=False)])
     # a small step keeps ReLU inputs near zero from changing sign
-    fd = W.finite_difference(flat, fbp, tgt, 50.0, idx, h=1e-7, weights=wts)
+    fd = W.finite_difference(flat, fbp, tgt, 50.0, idx, h=1e-7, weights=wts, highpass=hp)
     assert np.allclose(g[idx], fd, rtol=1e-4, atol=1e-8 * np.abs(g).max())
 
 

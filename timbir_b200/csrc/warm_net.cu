@@ -790,6 +790,11 @@ struct MbirNet {
     cudaGraphExec_t gexec = nullptr;
     const float *g_in = nullptr, *g_t = nullptr, *g_w = nullptr;
     const float *loss_w = nullptr;  // per-voxel loss weights (device, the input's shape) or null
+    // high-pass loss: widths of the Gaussian G in mean(wt ((I - G) d)^2)
+    // (0, 0: the plain loss) and its three float work volumes
+    float hp_sz = 0.0f, hp_sxy = 0.0f;
+    float *hp_buf = nullptr;
+    size_t hp_n = 0;
     float g_scale = 0.0f;
     Shape g_shape{0, 0, 0, 0};
     int g_seen = 0;
@@ -798,7 +803,7 @@ struct MbirNet {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (gstream) cudaStreamDestroy(gstream);
         for (void *q : {(void *)params, (void *)grads, (void *)m, (void *)v, (void *)part, (void *)upack,
-                        (void *)d_err, (void *)wg_part})
+                        (void *)d_err, (void *)wg_part, (void *)hp_buf})
             if (q) cudaFree(q);
         for (auto &t : act)
             if (t.p) cudaFree(t.p);
@@ -1112,6 +1117,47 @@ static int net_err_check(MbirNet *N, cudaStream_t st)
     return 0;
 }
 
+// ---- high-pass loss: mean(wt ((I - G) d)^2), d = s in + r - s t ----
+__global__ void k_loss_residual(const float *__restrict__ in, const float *__restrict__ t,
+                                const bf16 *__restrict__ Z, float s, float *__restrict__ d, long long M)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M) d[i] = s * in[i] + b2f(Z[(size_t)i * 16]) - s * t[i];
+}
+
+// h = d - G d; u = wt h (in place of d); per-block sums of wt h^2 into part
+__global__ void __launch_bounds__(256) k_hp_loss(float *__restrict__ du, const float *__restrict__ gd,
+                                                 const float *__restrict__ wt, long long M, double *__restrict__ part)
+{
+    __shared__ double red[256];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (i < M) {
+        const float h = du[i] - gd[i];
+        const float wi = wt ? wt[i] : 1.0f;
+        du[i] = wi * h;
+        l = (double)wi * h * h;
+    }
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// dZ channel 0 = 2 (I - G) u / M (G symmetric: zero edges), others 0
+__global__ void k_hp_grad(const float *__restrict__ u, const float *__restrict__ gu, bf16 *__restrict__ dZ,
+                          long long M)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    bf16 *g = dZ + (size_t)i * 16;
+    g[0] = f2b(2.0f * (u[i] - gu[i]) / (float)M);
+    for (int c = 1; c < 16; c++) g[c] = f2b(0.0f);
+}
+
 // ---- low-frequency blend of two starts ----
 // Gaussian taps of one axis: radius int(4 sigma + 0.5), exp(-x^2 / (2 sigma^2))
 // normalised to sum 1 (the truncation and normalisation of scipy.ndimage's
@@ -1130,9 +1176,11 @@ __global__ void k_blend_diff(const float *__restrict__ a, const float *__restric
     if (i < n) d[i] = a[i] - b[i];
 }
 
-// out = in filtered along one axis (length len, element stride stride)
+// out = in filtered along one axis (length len, element stride stride);
+// mirrored edges, or zeros outside (zero_edge: the filter is then a symmetric
+// matrix, its own transpose)
 __global__ void k_blur_axis(const float *__restrict__ in, float *__restrict__ out, long long n, long long stride,
-                            int len, BlurTaps t)
+                            int len, BlurTaps t, int zero_edge)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1141,16 +1189,14 @@ __global__ void k_blur_axis(const float *__restrict__ in, float *__restrict__ ou
     float acc = 0.0f;
     for (int k = -t.r; k <= t.r; k++) {
         int q = c + k;
-        while (q < 0 || q >= len) q = q < 0 ? -q - 1 : 2 * len - q - 1;
+        if (zero_edge) {
+            if (q < 0 || q >= len) continue;
+        } else {
+            while (q < 0 || q >= len) q = q < 0 ? -q - 1 : 2 * len - q - 1;
+        }
         acc = fmaf(t.w[k + t.r], base[(long long)q * stride], acc);
     }
     out[i] = acc;
-}
-
-__global__ void k_blend_add(float *__restrict__ start, const float *__restrict__ d, long long n)
-{
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) start[i] += d[i];
 }
 
 static BlurTaps blur_taps(float sigma)
@@ -1162,6 +1208,36 @@ static BlurTaps blur_taps(float sigma)
     for (int k = 0; k <= 2 * t.r; k++) t.w[k] = (float)(w[k] / sum);
     return t;
 }
+
+// G x of a float volume [B][D][H][W] into one of the two work buffers
+// (a, b; x may be either); returns the buffer holding the result
+static float *blur3(const float *x, float *a, float *b, const Shape &s, float sz, float sxy, int zero_edge,
+                    cudaStream_t st)
+{
+    const long long n = s.voxels();
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    const struct {
+        float sigma;
+        long long stride;
+        int len;
+    } axes[3] = {{sxy, 1, s.W}, {sxy, s.W, s.H}, {sz, (long long)s.H * s.W, s.D}};
+    const float *cur = x;
+    float *dst = (x == a) ? b : a;
+    for (const auto &ax : axes) {
+        if (ax.sigma <= 0.0f) continue;
+        k_blur_axis<<<nb, 256, 0, st>>>(cur, dst, n, ax.stride, ax.len, blur_taps(ax.sigma), zero_edge);
+        cur = dst;
+        dst = (dst == a) ? b : a;
+    }
+    return const_cast<float *>(cur);
+}
+
+__global__ void k_blend_add(float *__restrict__ start, const float *__restrict__ d, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) start[i] += d[i];
+}
+
 
 extern "C" {
 
@@ -1188,7 +1264,7 @@ int mbir_lowpass_blend(const float *ref, float *start, float *scratch, int32_t N
     } axes[3] = {{sigma_xy, 1, W}, {sigma_xy, W, H}, {sigma_z, (long long)H * W, D}};
     for (const auto &ax : axes) {
         if (ax.sigma <= 0.0f) continue;
-        k_blur_axis<<<nb, 256, 0, st>>>(a, b, n, ax.stride, ax.len, blur_taps(ax.sigma));
+        k_blur_axis<<<nb, 256, 0, st>>>(a, b, n, ax.stride, ax.len, blur_taps(ax.sigma), 0);
         NK(cudaGetLastError());
         std::swap(a, b);
     }
@@ -1324,10 +1400,30 @@ int mbir_net_gradients(MbirNet *N, const float *in, const float *target, int32_t
     }
     const long long M = N->shape.voxels();
     const int nb = blocks(M);
+    const bool hp = N->hp_sz > 0.0f || N->hp_sxy > 0.0f;
+    if (hp && N->hp_n < 3 * (size_t)M) {  // work volumes of the high-pass loss
+        if (N->gexec) cudaGraphExecDestroy(N->gexec);
+        N->gexec = nullptr;
+        N->g_seen = 0;
+        if (N->hp_buf) cudaFree(N->hp_buf);
+        N->hp_buf = nullptr;
+        N->hp_n = 0;
+        NK(cudaMalloc(&N->hp_buf, 3 * (size_t)M * sizeof(float)));
+        N->hp_n = 3 * (size_t)M;
+    }
     auto enqueue = [&](cudaStream_t st) -> int {
         if (forward(N, in, scale, st)) return -1;
-        k_loss<<<nb, 256, 0, st>>>(in, target, N->loss_w, N->act[T_A0 + 14].p, scale, N->grad[T_A0 + 14].p, M,
-                                   N->part);
+        if (hp) {
+            float *du = N->hp_buf, *a = du + M, *b = a + M;
+            k_loss_residual<<<nb, 256, 0, st>>>(in, target, N->act[T_A0 + 14].p, scale, du, M);
+            const float *gd = blur3(du, a, b, N->shape, N->hp_sz, N->hp_sxy, 1, st);
+            k_hp_loss<<<nb, 256, 0, st>>>(du, gd, N->loss_w, M, N->part);
+            const float *gu = blur3(du, a, b, N->shape, N->hp_sz, N->hp_sxy, 1, st);
+            k_hp_grad<<<nb, 256, 0, st>>>(du, gu, N->grad[T_A0 + 14].p, M);
+        } else {
+            k_loss<<<nb, 256, 0, st>>>(in, target, N->loss_w, N->act[T_A0 + 14].p, scale, N->grad[T_A0 + 14].p, M,
+                                       N->part);
+        }
         NK(cudaGetLastError());
         return backward(N, st);
     };
@@ -1374,6 +1470,23 @@ int mbir_net_set_loss_weights(MbirNet *N, const float *w)
 {
     if (!N) return net_fail("null network");
     N->loss_w = w;
+    return 0;
+}
+
+int mbir_net_set_loss_highpass(MbirNet *N, float sigma_z, float sigma_xy)
+{
+    if (!N) return net_fail("null network");
+    if (!(sigma_z >= 0.0f && sigma_xy >= 0.0f) || 4.0f * sigma_z + 0.5f > (float)kBlurMaxRadius ||
+        4.0f * sigma_xy + 0.5f > (float)kBlurMaxRadius)
+        return net_fail("high-pass loss: Gaussian widths must be in [0, 15.9]");
+    if (sigma_z != N->hp_sz || sigma_xy != N->hp_sxy) {  // another loss: the captured evaluation is dropped
+        if (N->gexec) cudaGraphExecDestroy(N->gexec);
+        N->gexec = nullptr;
+        N->g_seen = 0;
+        N->g_in = nullptr;
+    }
+    N->hp_sz = sigma_z;
+    N->hp_sxy = sigma_xy;
     return 0;
 }
 

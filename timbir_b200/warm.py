@@ -38,6 +38,7 @@ def _lib():
         lib.mbir_net_gradients.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.POINTER(C.c_double), vp]
         lib.mbir_net_adam_step.argtypes = [vp, C.c_float, vp]
         lib.mbir_net_set_loss_weights.argtypes = [vp, vp]
+        lib.mbir_net_set_loss_highpass.argtypes = [vp, C.c_float, C.c_float]
         lib.mbir_lowpass_blend.argtypes = [vp, vp, vp, i32, i32, i32, i32, C.c_float, C.c_float, vp]
         lib.mbir_net_get_activation.argtypes = [vp, i32, i32, vp, C.POINTER(C.c_int64)]
         lib._net_bound = True
@@ -125,16 +126,23 @@ class WarmNet:
         _check(self.lib.mbir_net_set_loss_weights(
             self.h, None if self._loss_w is None else C.c_void_p(self._loss_w.data_ptr())))
 
+    def set_loss_highpass(self, sigma_z: float = 0.0, sigma_xy: float = 0.0) -> None:
+        """High-pass loss mean(w ((I - G) d)^2) for the following gradients()
+        calls (G: Gaussian low-pass of widths sigma_z slices, sigma_xy voxels,
+        zeros outside the patch); 0, 0 restores the plain loss."""
+        _check(self.lib.mbir_net_set_loss_highpass(self.h, sigma_z, sigma_xy))
+
     def adam_step(self, lr: float) -> None:
         _check(self.lib.mbir_net_adam_step(self.h, lr, _stream()))
 
 
 def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 64, 64), lr: float = 1e-3,
-          seed: int = 0, scale: float = SCALE, log_every: int = 0, weights=None):
+          seed: int = 0, scale: float = SCALE, log_every: int = 0, weights=None, highpass=None):
     """Adam on random patches of the (input, target) volumes (CUDA tensors
     [N][D][H][W]), the loss weighted per voxel by the same patches of
-    `weights` when given; the learning rate decays by cosine to a tenth.
-    Returns the per-step losses."""
+    `weights` when given, and taken on the residual's high frequencies when
+    `highpass` = (sigma_z, sigma_xy) is given; the learning rate decays by
+    cosine to a tenth.  Returns the per-step losses."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
     N, D, H, W = inputs.shape
@@ -144,6 +152,7 @@ def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 
     tb = torch.empty_like(xb)
     wb = torch.empty_like(xb) if weights is not None else None
     net.set_loss_weights(wb)
+    net.set_loss_highpass(*(highpass or (0.0, 0.0)))
     for step in range(steps):
         for b in range(batch):
             n = int(torch.randint(N, (1,), generator=g))
@@ -161,6 +170,8 @@ def train(net: WarmNet, inputs, targets, steps: int, batch: int = 4, patch=(16, 
             print(f"step {step + 1} loss {np.mean(losses[-log_every:]):.5f}", flush=True)
     if wb is not None:
         net.set_loss_weights(None)
+    if highpass:
+        net.set_loss_highpass(0.0, 0.0)
     return losses
 
 
