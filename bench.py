@@ -1406,11 +1406,6 @@ def reference_arm(args, rank):
             "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if ttm:
         line["time_to_map"] = ttm
-    if big:
-        line["cost_trace"] = {"start": "filtered backprojection" if args.c5_start == "fbp" else "zero",
-                              "costs": [float(c) for c in cost_trace],
-                              "note": "FP64 MAP cost after the prologue and after each warm-up and timed iteration",
-                              "falling": bool(all(b <= a for a, b in zip(cost_trace, cost_trace[1:])))}
     print(json.dumps(line), flush=True)
 
 
