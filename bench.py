@@ -1330,6 +1330,8 @@ def gpu_arm(args, rank, world, local_rank):
                               "falling": bool(all(b <= a for a, b in zip(cost_trace, cost_trace[1:])))}
     if big:
         line["cpu_baseline"] = {"unavailable": "the reference's CPU code needs minutes per iteration at this size"}
+    elif world > 1:
+        line["cpu_baseline"] = {"unavailable": "measured on rank 0 of a one-GPU run only"}
     elif not args.no_cpu:
         v, kind, cores, n, secs = cpu_measure(w, scan, coarse, fine, 1, 1, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": "voxel-updates/s", "cores": cores, "kind": kind,
