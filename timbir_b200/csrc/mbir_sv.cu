@@ -1124,13 +1124,12 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             for (int z = 0; z < nz; z++) m += magl[(z * S + ly) * S + lx];
             task.mag[(size_t)(j0 + ly) * g.N_x + k0 + lx] = m;
         }
-        // band change back to e: vector atomics over the same words (zeros
-        // outside the band), one lane per (row, view), so that the atomics of
-        // one instruction go to different rows
+        // band change back to e: vector atomics over the same 16-byte words
+        // as the staging (zeros outside the band), four lanes per (row, view)
         if (vec) {
             // word c of pair pq: its change (zeros outside the band) and its
             // global address (-1: past the band or the row); the reads of a
-            // batch of four words are issued before any of their atomics
+            // thread's U words are issued before any of their atomics
             auto commit_word = [&](int pq, int c, float *d) -> long long {
                 const int row = pq / Np, v = pq - row * Np;
                 const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
@@ -1145,7 +1144,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 }
                 return (long long)((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r + a0 + 4 * c;
             };
-            constexpr int U = 3;
+            constexpr int U = 2;
             const int total = 4 * npairs;
             for (int b = tid; b < total; b += U * nthr) {
                 float d[U][4];
