@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     ev[u] = wv[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     if (at[u] >= 0) {
                         ev[u] = __ldcg(reinterpret_cast<const float4 *>(dv.e + at[u]));
-                        wv[u] = __ldg(reinterpret_cast<const float4 *>(dv.w + at[u]));
+                        wv[u] = __ldcg(reinterpret_cast<const float4 *>(dv.w + at[u]));
                     }
                 }
 #pragma unroll
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                         float4 ev = make_float4(0.0f, 0.0f, 0.0f, 0.0f), wv = ev;
                         if (a >= 0) {
                             ev = __ldcg(reinterpret_cast<const float4 *>(dv.e + a));
-                            wv = __ldg(reinterpret_cast<const float4 *>(dv.w + a));
+                            wv = __ldcg(reinterpret_cast<const float4 *>(dv.w + a));
                         }
                         stage_word(pqc >> 2, c, ev, wv);
                     }
