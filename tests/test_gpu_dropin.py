@@ -3,8 +3,8 @@
 oracle/_ref/XT_Main_gpu is src/reconstruct/bin_data/XT_Main.c, unmodified,
 compiled with this repository's include/mbir4d.h and linked against
 timbir_b200/libtimbir_b200.so instead of the reference's libmbir4d.a (the
-link line INTEGRATION.md gives; oracle/Makefile builds it where the
-reference sources are).  It reads the bin_data file set, calls reconstruct()
+integration notes' link line; oracle/Makefile builds it where the reference
+sources are).  It reads the bin_data file set, calls reconstruct()
 and leaves the output files in its working directory.  Its results are
 compared with full runs of the reference's driver on the same inputs
 (tests/golden/recon_small.npz, recon_rings.npz), by the MAP cost of the final

@@ -1,7 +1,7 @@
 """Parity of the default super-voxel schedule at the benchmark sizes.
 
 The super-voxel schedule's trajectory differs from the reference's, so parity
-is judged on the MAP estimate it converges to, at the full sizes the
+is checked on the MAP estimate it converges to, at the full sizes the
 benchmark runs (fixtures from tests/golden/make_converged_full.py: the
 reference library iterated to a flat cost, then the FP64 oracle from there):
 

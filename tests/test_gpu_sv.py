@@ -3,7 +3,7 @@
 The super-voxel schedule updates voxels in a different order than the
 reference (many super-voxels at once, each from a private copy of its
 error-sinogram band), so its trajectory is not the reference's; parity is
-judged on the result:
+checked on the result:
   * the MAP it converges to: final cost within 1e-5 relative of the
     reference's converged cost, and image RMSE below 1e-3 of the phantom's
     dynamic range against the FP64 oracle (both from

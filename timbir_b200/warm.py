@@ -2,10 +2,11 @@
 (mbir_net_*), its training on (filtered backprojection, converged MBIR)
 pairs that the plain method generates, and the warm start it gives.
 
-The network maps a frame's filtered backprojection to a start image; ICD then
-runs from it to its own convergence test, so the result is the MAP estimate
+The network maps a frame's filtered backprojection to a start image (whose
+low frequencies are then taken back from the backprojection); ICD then runs
+from it to its own convergence test, so the result is the MAP estimate
 whatever the start (qGGMRF with 1 <= p <= 2 is convex) and FBP-initialised
-ICD stays both the fallback and the judge.  Device memory comes from torch
+ICD stays both the fallback and the yardstick.  Device memory comes from torch
 (plumbing only); every kernel is the native library's.
 """
 from __future__ import annotations
