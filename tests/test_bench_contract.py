@@ -1,5 +1,6 @@
-"""CPU checks of bench.py's contract: every name its functions read is
-defined (a static scan of the module's scopes), and the reference arm --
+"""CPU checks of bench.py's contract: every name the functions of bench.py,
+the build entry and the Python packages read is defined (a static scan of
+the modules' scopes), and the reference arm --
 the reference's own CPU code on the default workload -- runs and prints one
 JSON line with the fields the contract asks for."""
 import builtins
@@ -35,7 +36,9 @@ def undefined_globals(path):
     return out
 
 
-@pytest.mark.parametrize("name", ["bench.py", "__graft_entry__.py"])
+@pytest.mark.parametrize("name", ["bench.py", "__graft_entry__.py"] + sorted(
+    os.path.join(d, f) for d in ("timbir_b200", "oracle") for f in os.listdir(os.path.join(ROOT, d))
+    if f.endswith(".py")))
 def test_entry_scripts_read_no_undefined_name(name):
     assert undefined_globals(os.path.join(ROOT, name)) == []
 
