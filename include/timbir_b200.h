@@ -370,7 +370,11 @@ int mbir_batch_create(MbirBatch **batch, MbirStage *const *stages, int32_t n, in
 void mbir_batch_free(MbirBatch *batch);
 /* Up to max_iters iterations; every check_every iterations the host reads
  * how many problems are still active and stops at 0.  *active_left (may be
- * NULL) = problems still iterating.  Adds the updates to each stage's count. */
+ * NULL) = problems still iterating.  Adds the updates to each stage's count.
+ * A problem whose stage has a non-zero mbir_set_sv_nhicd fraction also gets
+ * its NHICD pass after each batched sweep from its second iteration (the
+ * stage's own device selection and launch, on its stream, in flight capped
+ * as the batch caps it); its convergence test stays the sweep's. */
 int mbir_batch_iterate(MbirBatch *batch, int32_t max_iters, int32_t check_every, int32_t *active_left);
 /* Per problem (arrays of n; any may be NULL): iterations done, 1 when the
  * convergence test stopped it, voxel updates, zero-skipped voxels, the last

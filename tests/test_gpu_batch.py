@@ -16,7 +16,9 @@ when reconstructed alone:
   * the autotuner leaves the stage's state as prepared and picks a
     configuration the batch runs;
   * problems whose detector rows are not a multiple of four columns wide
-    reach the FP64 oracle's MAP inside a batch.
+    reach the FP64 oracle's MAP inside a batch;
+  * a problem whose stage asks for the NHICD pass gets it after each batched
+    sweep and still reaches the reference's MAP.
 """
 import os
 
@@ -208,3 +210,33 @@ def test_batch_of_ragged_detectors_reaches_the_fp64_map():
         assert abs(c - cref) / cref < 1e-5
         assert rmse < 1e-3 * SCALE
     b.close()
+
+
+def test_batch_with_device_nhicd_reaches_the_reference_map():
+    # a problem whose stage asks for the NHICD pass gets it after every
+    # batched sweep from its second iteration (its stage's own selection and
+    # launch); the other problem of the batch does not, and both still reach
+    # the MAP: the plain scenario the reference's converged cost and the FP64
+    # oracle's image, as without the pass
+    g = np.load(os.path.join(GOLD, "converged_plain.npz"))
+    ref = float(g["ref_fresh_cost"])
+    plain = make_stage(32, 4, 48, seed=1, prepare=False)
+    plain.set_sv_nhicd(0.1)
+    plain.prepare()
+    other = make_stage(48, 6, 72, seed=11)
+    b = timbir_b200.Batch([plain, other])
+    assert b.iterate(300, check_every=50) == 2
+    assert plain.kernel_stats()[1] == 299  # one NHICD launch per batched iteration from the second
+    assert other.kernel_stats()[1] == 0
+    st = b.stats()
+    assert list(st["iterations"]) == [300, 300]
+    assert plain.update_count() > st["updates"][0]  # the sweeps' updates and the passes'
+    assert other.update_count() == st["updates"][1]
+    b.close()
+    x = plain.object()
+    c = fresh_cost_fp64(plain.scan, x)
+    assert abs(c - ref) / ref < 1e-5
+    rmse = float(np.sqrt(np.mean((x - g["f64_object"]) ** 2)))
+    assert rmse < 1e-3 * SCALE
+    plain.close()
+    other.close()

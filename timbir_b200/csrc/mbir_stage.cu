@@ -1915,9 +1915,15 @@ struct MbirBatch {
     };
     bool guard = false;
     std::vector<Guard> gd;
+    // NHICD passes (stages with a non-zero mbir_set_sv_nhicd fraction): each
+    // problem's iteration count when its last pass ran, and the event that
+    // orders a pass after the batched sweep
+    std::vector<int> nh_iters;
+    cudaEvent_t ev_sweep = nullptr;
     ~MbirBatch()
     {
         if (stream) cudaStreamSynchronize(stream);
+        if (ev_sweep) cudaEventDestroy(ev_sweep);
         for (auto g : graphs) cudaGraphExecDestroy(g);
         void *bufs[] = {d_probs, d_state, d_tasks, d_lists, d_done, d_queue, d_err, d_ctl, d_scratch};
         for (void *b : bufs) dfree(b);
@@ -2200,14 +2206,73 @@ static int batch_guard(MbirBatch *B)
     return 0;
 }
 
+// NHICD pass of every problem that iterated in the replay just launched
+// (phase rotation r), from its second iteration, when its stage's NHICD
+// fraction is non-zero: the stage's own device selection and subset launch,
+// as its single-problem iteration runs them (VSC_based_Voxel_Line_Select,
+// XT_NHICD.c:164-216, after the homogeneous sweep, XT_ICD_update.c:1010-1040),
+// on the stage's stream after the batch's sweep; the pass's super-voxels in
+// flight are capped as the batch caps the problem's.  The convergence test
+// stays the sweep's, as in the reference (HICD lines only).
+static int batch_nhicd(MbirBatch *B, int r)
+{
+    bool any = false;
+    for (MbirStage *S : B->stages) any |= S->nh_fraction > 0;
+    if (!any) return 0;
+    if (!B->ev_sweep) CK(cudaEventCreateWithFlags(&B->ev_sweep, cudaEventDisableTiming));
+    if (B->nh_iters.empty()) B->nh_iters.assign(B->n, 0);
+    std::vector<SvBatchState> st(B->n);
+    CK(cudaMemcpyAsync(st.data(), B->d_state, B->n * sizeof(SvBatchState), cudaMemcpyDeviceToHost, B->stream));
+    CK(cudaEventRecord(B->ev_sweep, B->stream));
+    CK(cudaStreamSynchronize(B->stream));
+    std::vector<int> ran;
+    for (int p = 0; p < B->n; p++) {
+        MbirStage *S = B->stages[p];
+        if (S->nh_fraction <= 0 || st[p].iters == B->nh_iters[p]) continue;  // not iterating in this replay
+        B->nh_iters[p] = st[p].iters;
+        if (st[p].iters < 2) continue;
+        CK(cudaStreamWaitEvent(S->stream, B->ev_sweep, 0));
+        CK(cudaMemsetAsync(S->d_queue + 1, 0, sizeof(int), S->stream));
+        CK(cudaMemsetAsync(S->d_sv_out + 1, 0, sizeof(SvTaskOut), S->stream));
+        const int rot = r % std::max(1, S->sv_nphase);
+        if (sv_nh_select(S, rot)) return -1;
+        const int grid = S->sv_grid, ctas = S->sv_ctas;
+        const int cap = B->guard ? B->gd[p].cap : grid;
+        S->sv_ctas = 0;
+        S->sv_grid = std::max(1, std::min(ctas > 0 ? std::min(ctas, S->sv_fit) : grid, cap));
+        const int rc = sv_launch(S, S->d_sv_lists, S->sv_rot[rot], st[p].iters,
+                                 (uint32_t)(S->rng.next() * 4294967295.0), 1, S->d_sv_out + 1, true);
+        S->sv_grid = grid;
+        S->sv_ctas = ctas;
+        if (rc) return -1;
+        ran.push_back(p);
+    }
+    for (int p : ran) {
+        MbirStage *S = B->stages[p];
+        SvTaskOut acc;
+        int err = 0;
+        CK(cudaMemcpyAsync(&acc, S->d_sv_out + 1, sizeof(acc), cudaMemcpyDeviceToHost, S->stream));
+        CK(cudaMemcpyAsync(&err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+        if (err & 1) return fail("problem %d NHICD pass: super-voxel band overflow", p);
+        if (err & 4) return fail("problem %d NHICD pass: super-voxel dependency wait timed out", p);
+        if (err) return fail("problem %d NHICD pass: device error flags 0x%x", p, err);
+        S->updates += acc.updates;
+        S->zero_skips += acc.zero_skips;
+    }
+    return 0;
+}
+
 extern "C" int mbir_batch_iterate(MbirBatch *B, int32_t max_iters, int32_t check_every, int32_t *active_left)
 {
     if (check_every <= 0) check_every = 1;
     CK(cudaEventRecord(B->ev0, B->stream));
     int left = B->n;
     for (int k = 0; k < max_iters; k++) {
-        CK(cudaGraphLaunch(B->graphs[B->replays % B->nrot], B->stream));
+        const int r = (int)(B->replays % B->nrot);
+        CK(cudaGraphLaunch(B->graphs[r], B->stream));
         B->replays++;
+        if (batch_nhicd(B, r)) return -1;
         if (B->guard && batch_guard(B)) return -1;
         if ((k + 1) % check_every == 0 || k + 1 == max_iters) {
             CK(cudaMemcpyAsync(B->h_ctl, B->d_ctl, 4 * sizeof(int), cudaMemcpyDeviceToHost, B->stream));
