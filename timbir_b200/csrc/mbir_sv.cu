@@ -591,6 +591,12 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         const int nz = task.nz, rows = nz * mz;
         const int i = task.frame;
         const int Np = g.view_num[i];
+        // (row, view) of a band pair index pq < rows Np: pq / Np as a multiply
+        // by ceil(2^32 / Np) and the high word, exact while rows Np^2 < 2^32
+        // (then pq e < 2^32 for the rounding excess e = m Np - 2^32 < Np)
+        const bool np_fast = Np > 1 && (unsigned long long)rows * Np * Np < (1ull << 32);
+        const unsigned np_magic = np_fast ? 0xFFFFFFFFu / (unsigned)Np + 1u : 1u;
+        auto div_np = [&](int pq) -> int { return np_fast ? (int)__umulhi((unsigned)pq, np_magic) : pq / Np; };
         const int k0 = task.k0, j0 = task.j0, z0 = task.z0;
         const int kx = min(S, g.N_x - k0), ky = min(S, g.N_y - j0);
         const int *vl = g.view_idx + (size_t)i * g.max_views;
@@ -745,7 +751,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         if (vec) {
             // one 16-byte word of a (row, view): pqc = 4 (row Np + v) + c
             auto stage_word = [&](int pq, int c, float4 ev, float4 wv) {
-                const int row = pq / Np, v = pq - row * Np;
+                const int row = div_np(pq), v = pq - row * Np;
                 const int sh = rlo[v] & 3;
                 const float ee[4] = {ev.x, ev.y, ev.z, ev.w};
                 const float ww[4] = {wv.x, wv.y, wv.z, wv.w};
@@ -762,7 +768,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             };
             // global address of word c of pair pq (-1: past the band or the row)
             auto word_at = [&](int pq, int c) -> long long {
-                const int row = pq / Np, v = pq - row * Np;
+                const int row = div_np(pq), v = pq - row * Np;
                 const int lo = rlo[v], a0 = lo & ~3;
                 if (4 * c >= (lo - a0) + W || a0 + 4 * c >= g.N_r) return -1;
                 return (long long)((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r + a0 + 4 * c;
@@ -803,7 +809,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     }
         } else {
             for (int pq = tid; pq < npairs; pq += nthr) {
-                const int row = pq / Np, v = pq - row * Np;
+                const int row = div_np(pq), v = pq - row * Np;
                 const int lo = rlo[v];
                 const size_t rbase = ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
                 float2 *bd = band + (size_t)row * rowstride + v;
@@ -1131,7 +1137,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             // global address (-1: past the band or the row); the reads of a
             // thread's U words are issued before any of their atomics
             auto commit_word = [&](int pq, int c, float *d) -> long long {
-                const int row = pq / Np, v = pq - row * Np;
+                const int row = div_np(pq), v = pq - row * Np;
                 const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
                 if (4 * c >= sh + W || a0 + 4 * c >= g.N_r) return -1;
                 const float2 *bd = band + (size_t)row * rowstride + v;
@@ -1169,7 +1175,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                     }
         } else {
             for (int pq = tid; pq < npairs; pq += nthr) {
-                const int row = pq / Np, v = pq - row * Np;
+                const int row = div_np(pq), v = pq - row * Np;
                 const int lo = rlo[v];
                 const float2 *bd = band + (size_t)row * rowstride + v;
                 const float *sc = scr + (size_t)row * rowstride + v;
