@@ -1282,7 +1282,10 @@ def gpu_arm(args, rank, world, local_rank):
     e2e_ms, e2e_upd = e2e_run(n_solve, reps)
     one_ms, one_upd = e2e_run(1, reps)
     if dist:
-        t = torch.tensor([sum(e2e_ms), float(e2e_upd)], dtype=torch.float64, device="cuda")
+        # a solve's median time (the slowest rank's) against the updates of
+        # one solve on every rank
+        t = torch.tensor([statistics.median(e2e_ms), float(e2e_upd) / len(e2e_ms)], dtype=torch.float64,
+                         device="cuda")
         mx = t.clone()
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
@@ -1290,7 +1293,11 @@ def gpu_arm(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     else:
-        e2e_value = e2e_upd / (sum(e2e_ms) / 1e3)
+        # the median solve: a solve's host-side work (set-up calls, one
+        # synchronisation per iteration) is exposed to other tenants of the
+        # host, which stretched single solves 2-3x; every solve's time is in
+        # step_ms
+        e2e_value = (e2e_upd / len(e2e_ms)) / (statistics.median(e2e_ms) / 1e3)
     if rank != 0:
         return
     value = updates_all / (total_ms_max / 1e3)
@@ -1321,11 +1328,13 @@ def gpu_arm(args, rank, world, local_rank):
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": "voxel-updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "step_ms": [round(v, 3) for v in e2e_ms],
+                "statistic": f"median of {len(e2e_ms)} timed solves after one untimed",
                 "updates_per_step": e2e_upd / max(len(e2e_ms), 1),
                 "step": f"stage reconstructed from pinned host arrays: set-up, prologue, {n_solve} ICD iterations "
                         f"({'the GPU iterations to the MAP target' if ttm and ttm['iterations'] else 'steps'}), "
                         "object read back into pinned memory",
-                "single_iteration": {"value": one_upd / (sum(one_ms) / 1e3), "step_ms": [round(v, 3) for v in one_ms],
+                "single_iteration": {"value": (one_upd / len(one_ms)) / (statistics.median(one_ms) / 1e3),
+                                     "step_ms": [round(v, 3) for v in one_ms],
                                      "updates_per_step": one_upd / max(len(one_ms), 1)}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
