@@ -922,7 +922,7 @@ static SvParams sv_params(const MbirStage *S, int side, int nz, int vsplit)
     // 1024-thread limit
     const int want = (sp.max_views + 31) / 32;
     sp.prod_warps = std::max(0, std::min(std::min(want, 8), (1024 - 32 * nz * sp.vsplit) / 32));
-    sp.band_floats = (size_t)sp.max_rows * sp.W * sp.max_views;
+    sp.band_floats = sv_scratch_floats(sp.max_rows, sp.W, sp.max_views);
     return sp;
 }
 

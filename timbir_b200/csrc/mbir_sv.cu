@@ -747,23 +747,23 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         //      end stage zeros) ----
         float *__restrict__ scr = scratch + (size_t)blockIdx.x * scratch_floats;
         const bool vec = (g.N_r & 3) == 0;
+        const int nw = sv_scratch_words(W);  // 16-byte words of e kept per pair
         const int npairs = rows * Np;
         if (vec) {
             // one 16-byte word of a (row, view): pqc = 4 (row Np + v) + c
+            // the scratch keeps each staged word of e as loaded, word c of
+            // pair pq at float4 index pq nw + c, for the commit's changes
             auto stage_word = [&](int pq, int c, float4 ev, float4 wv) {
                 const int row = div_np(pq), v = pq - row * Np;
                 const int sh = rlo[v] & 3;
                 const float ee[4] = {ev.x, ev.y, ev.z, ev.w};
                 const float ww[4] = {wv.x, wv.y, wv.z, wv.w};
                 float2 *bd = band + (size_t)row * rowstride + v;
-                float *sc = scr + (size_t)row * rowstride + v;
+                reinterpret_cast<float4 *>(scr)[(size_t)pq * nw + c] = ev;
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int off = 4 * c + j - sh;
-                    if (off >= 0 && off < W) {
-                        bd[(size_t)off * NpS] = make_float2(ee[j], sqrtf(ww[j]));
-                        sc[(size_t)off * NpS] = ee[j];
-                    }
+                    if (off >= 0 && off < W) bd[(size_t)off * NpS] = make_float2(ee[j], sqrtf(ww[j]));
                 }
             };
             // global address of word c of pair pq (-1: past the band or the row)
@@ -1141,12 +1141,13 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 const int lo = rlo[v], a0 = lo & ~3, sh = lo - a0;
                 if (4 * c >= sh + W || a0 + 4 * c >= g.N_r) return -1;
                 const float2 *bd = band + (size_t)row * rowstride + v;
-                const float *sc = scr + (size_t)row * rowstride + v;
+                const float4 eo = __ldcg(reinterpret_cast<const float4 *>(scr) + (size_t)pq * nw + c);
+                const float e0[4] = {eo.x, eo.y, eo.z, eo.w};
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int off = 4 * c + j - sh;
                     d[j] = 0.0f;
-                    if (off >= 0 && off < W) d[j] = bd[(size_t)off * NpS].x - sc[(size_t)off * NpS];
+                    if (off >= 0 && off < W) d[j] = bd[(size_t)off * NpS].x - e0[j];
                 }
                 return (long long)((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r + a0 + 4 * c;
             };

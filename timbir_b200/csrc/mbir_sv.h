@@ -21,8 +21,21 @@ struct SvParams {
     int prod_warps; // warps computing the next line's A-matrix column (0 with a column cache)
     int ring;       // A-column ring slots: kSvRing (the cache is read ring - 2 lines ahead)
     int ahalf;      // the column cache holds FP16 values (8-byte entries; full resolution)
-    size_t band_floats;  // scratch floats per CTA: max_rows * W * max_views
+    size_t band_floats;  // scratch floats per CTA: sv_scratch_floats()
 };
+
+// 16-byte words of e a super-voxel CTA keeps per (detector row, view) pair for
+// its band commit: the words the staging loads, at 16-byte-aligned detector
+// columns (a band of W columns starting anywhere in a word spans at most
+// ceil((W + 3) / 4)), never fewer than the staging's four per pair.
+__host__ __device__ inline int sv_scratch_words(int W) { return (W + 6) / 4 > 4 ? (W + 6) / 4 : 4; }
+// Scratch floats per CTA: the per-element copy of e (rows x W x views, detector
+// rows not a multiple of four columns) or the staged words (rows x views x 4 nw).
+inline size_t sv_scratch_floats(int max_rows, int W, int max_views)
+{
+    const size_t per = (size_t)(4 * sv_scratch_words(W) > W ? 4 * sv_scratch_words(W) : W);
+    return (size_t)max_rows * max_views * per;
+}
 
 // A-matrix column of one (voxel line, view), as the kernels store it:
 // word 0 = j0 | n << 16 (first kept detector column j0, n kept columns, which
