@@ -630,8 +630,13 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 s_bad = 1;
             }
         }
-        // ---- in-mask lines, ordered by 2x2 parity class then a per-visit hash ----
-        if (warp == 0) {
+        // the views' band origins are read by every warp below
+        __syncthreads();
+        // Warp 0 waits for the conflicting super-voxels; warp 1 (warp 0
+        // after its waits when the CTA has one warp) orders the lines while
+        // the other warps, released by warp 0 through barrier 1 (free
+        // outside the line steps), stage the band and the voxel block.
+        auto order_lines = [&]() {
             // in-mask bit of line q = 32 k + lane in bit k (all loads in flight
             // at once); a subset pass keeps the selected lines only
             const uint8_t *lsel = L.sel ? L.sel + (size_t)task.plane * g.N_y * g.N_x : nullptr;
@@ -709,6 +714,9 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 __syncwarp();
             }
             if (lane == 0) s_nlines = n;
+        };
+        const bool orderer = warp == (nwarps > 1 ? 1 : 0);
+        if (warp == 0) {
             // wait for the conflicting super-voxels earlier in this launch
             // (bounded: a wait that gives up flags err and goes on)
             if constexpr (BATCH) {
@@ -736,9 +744,16 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 }
             }
         }
+        if (orderer) order_lines();
         for (int q = tid; q < sp.max_nz * S * S; q += nthr) magl[q] = 0.0f;
-        __syncthreads();
-        const int nl = s_bad ? 0 : s_nlines;
+        // staging warps: all but warp 1 (all of one warp)
+        const int sw_n = nwarps > 1 ? nwarps - 1 : 1, sw = warp < 2 ? 0 : warp - 1;
+        const int st_n = sw_n * 32;
+        const bool stager = nwarps == 1 || !orderer;
+        const int st_first = stager ? sw * 32 + lane : (1 << 30);  // past every loop's end: no share
+        const int sw_first = stager ? sw : (1 << 30);
+        if (nwarps > 1 && !orderer) named_barrier(1, st_n);
+        int nl = 0;  // the task's lines, read after the barrier that follows the ordering
 
         // ---- stage the band: (e, sqrt(w)) pairs, e also to this CTA's
         //      scratch slot.  Four lanes serve a (detector row, view), each
@@ -775,8 +790,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             };
             // words 0-3 of every pair, four per thread in flight at once
             constexpr int U = 4;
-            const int stride = nwarps * 32, total = 4 * npairs;
-            for (int b = tid; b < total; b += U * stride) {
+            const int stride = st_n, total = 4 * npairs;
+            for (int b = st_first; b < total; b += U * stride) {
                 float4 ev[U], wv[U];
                 long long at[U];
 #pragma unroll
@@ -797,7 +812,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             }
             // words 4 and up (bands wider than 13 columns)
             if (W + 3 > 16)
-                for (int pqc = tid; pqc < total; pqc += stride)
+                for (int pqc = st_first; pqc < total; pqc += stride)
                     for (int c = (pqc & 3) + 4; 4 * c < W + 3; c += 4) {
                         const long long a = word_at(pqc >> 2, c);
                         float4 ev = make_float4(0.0f, 0.0f, 0.0f, 0.0f), wv = ev;
@@ -808,7 +823,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                         stage_word(pqc >> 2, c, ev, wv);
                     }
         } else {
-            for (int pq = tid; pq < npairs; pq += nthr) {
+            for (int pq = st_first; pq < npairs; pq += st_n) {
                 const int row = div_np(pq), v = pq - row * Np;
                 const int lo = rlo[v];
                 const size_t rbase = ((size_t)(z0 * mz + row) * g.N_p + vidx[v]) * g.N_r;
@@ -826,7 +841,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         // ---- voxel block with halo, temporal neighbours ----
         const size_t plane = (size_t)g.N_y * g.N_x;
         const float *xf = dv.x + (size_t)i * g.N_z * plane;
-        for (int lz = warp; lz < nz + 2; lz += nwarps)
+        for (int lz = sw_first; lz < nz + 2; lz += sw_n)
             for (int q = lane; q < S2 * S2; q += 32) {
                 const int lx = q % S2, ly = q / S2;
                 const int xx = k0 + lx - 1, yy = j0 + ly - 1, zz = z0 + lz - 1;
@@ -839,7 +854,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
                 }
                 xb[lz * S2 * S2 + q] = v;
             }
-        for (int sz = warp; sz < 2 * nz; sz += nwarps) {
+        for (int sz = sw_first; sz < 2 * nz; sz += sw_n) {
             const int side = sz / nz, lz = sz - side * nz;
             const int ti = i + (side == 0 ? -1 : 1);
             for (int q = lane; q < S * S; q += 32) {
@@ -889,6 +904,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             }
         };
 
+        __syncthreads();  // the line order (and the staged band and voxel block)
+        nl = s_bad ? 0 : s_nlines;
         if (AC) {
             for (int q = 0; q < D; q++) fetch(q, q);
             cp_async_wait_upto<D - 1>();
