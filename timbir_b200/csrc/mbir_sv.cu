@@ -715,6 +715,27 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             }
             if (lane == 0) s_nlines = n;
         };
+        // ---- A-matrix column of line `li` (of nlines) into ring slot `slot`
+        //      from the cache, copied by threads t0, t0 + tn, ... (one commit
+        //      group per call and thread) ----
+        auto fetch_by = [&](int li, int slot, int nlines, int t0, int tn) {
+            if (li < nlines && order[li] >= 0) {
+                const int o = order[li];
+                const size_t line = (size_t)(j0 + (o >> 8)) * g.N_x + k0 + (o & 0xff);
+                if constexpr (kHalf) {
+                    uint2 *dst = reinterpret_cast<uint2 *>(ring) + (size_t)slot * NpS;
+                    const uint2 *src = reinterpret_cast<const uint2 *>(ac.a) + line * g.N_p;
+                    for (int q = t0; q < Np; q += tn) cp_async8(dst + q, src + vidx[q]);
+                } else {
+                    int4 *dst = ring + (size_t)slot * eq * NpS;
+                    for (int q = t0; q < Np * eq; q += tn) {
+                        const int v = q / eq, w = q - v * eq;
+                        cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
+                    }
+                }
+            }
+            cp_async_commit();
+        };
         const bool orderer = warp == (nwarps > 1 ? 1 : 0);
         if (warp == 0) {
             // wait for the conflicting super-voxels earlier in this launch
@@ -745,6 +766,15 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
             }
         }
         if (orderer) order_lines();
+        // with a column cache and more than one warp, the orderer also starts
+        // the first D lines' columns while the others stage (the other
+        // threads' later waits find none of these groups of theirs pending)
+        const bool early = AC && nwarps > 1 && orderer;
+        if (early) {
+            __syncwarp();
+            const int n0 = s_bad ? 0 : s_nlines;
+            for (int q = 0; q < D; q++) fetch_by(q, q, n0, lane, 32);
+        }
         for (int q = tid; q < sp.max_nz * S * S; q += nthr) magl[q] = 0.0f;
         // staging warps: all but warp 1 (all of one warp)
         const int sw_n = nwarps > 1 ? nwarps - 1 : 1, sw = warp < 2 ? 0 : warp - 1;
@@ -868,24 +898,7 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
 
         // ---- A-matrix column of line `li` into ring slot `slot` (li mod R) ----
         // from the cache: every thread copies a share (one commit group per call)
-        auto fetch = [&](int li, int slot) {
-            if (li < nl && order[li] >= 0) {
-                const int o = order[li];
-                const size_t line = (size_t)(j0 + (o >> 8)) * g.N_x + k0 + (o & 0xff);
-                if constexpr (kHalf) {
-                    uint2 *dst = reinterpret_cast<uint2 *>(ring) + (size_t)slot * NpS;
-                    const uint2 *src = reinterpret_cast<const uint2 *>(ac.a) + line * g.N_p;
-                    for (int q = tid; q < Np; q += nthr) cp_async8(dst + q, src + vidx[q]);
-                } else {
-                    int4 *dst = ring + (size_t)slot * eq * NpS;
-                    for (int q = tid; q < Np * eq; q += nthr) {
-                        const int v = q / eq, w = q - v * eq;
-                        cp_async16(dst + q, ac.a + (line * g.N_p + vidx[v]) * eq + w);
-                    }
-                }
-            }
-            cp_async_commit();
-        };
+        auto fetch = [&](int li, int slot) { fetch_by(li, slot, nl, tid, nthr); };
         // computed: warps [w0, nwarps), av_lanes views per warp
         auto acol = [&](int li, int slot, int w0, int av_lanes) {
             const int wr = warp - w0;
@@ -907,7 +920,8 @@ __global__ void __launch_bounds__(MAXT) k_icd_sv(const __grid_constant__ SvProbl
         __syncthreads();  // the line order (and the staged band and voxel block)
         nl = s_bad ? 0 : s_nlines;
         if (AC) {
-            for (int q = 0; q < D; q++) fetch(q, q);
+            if (nwarps == 1)
+                for (int q = 0; q < D; q++) fetch(q, q);
             cp_async_wait_upto<D - 1>();
         } else if (nl > 0) {
             acol(0, 0, 0, av_all);
