@@ -142,7 +142,7 @@ METRIC = "ICD voxel-updates/s"
 # one ncu capture of a full-sweep launch on the 3-D workload (217.6 MB read +
 # 5.8 MB written over its 411,744 in-mask voxels); the line's roofline.traffic
 # scales it to the average launch.
-DRAM_BYTES_PER_UPDATE = {"3d": (218.606e6 + 5.076e6) / 411744}
+DRAM_BYTES_PER_UPDATE = {"3d": (218.342e6 + 5.682e6) / 411744}
 
 
 def fourd_scan(w, seed_offset=0):
